@@ -1,0 +1,390 @@
+"""Python binding of libchsga (include/chsga.h) via ctypes.
+
+libchsga is a B200 (sm_100a) implementation of CHSGA's ConSGA alignment DP:
+score-only alignment (``align_combo``, src/align.hpp:470-531 of the
+reference) and traceback (``align_read_with_traceback``,
+src/traceback.hpp:588-1031). This module only marshals arguments; every
+computation runs in the shared library, and importing fails loudly when the
+library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libchsga.so")
+BIN_DIR = os.path.join(_HERE, "bin")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `make -C {_HERE}` "
+        "(or __graft_entry__.build())")
+
+_lib = C.CDLL(LIB_PATH)
+
+OK, ERR_INVALID_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, \
+    ERR_NO_PATH, ERR_TIMEOUT, ERR_INTERNAL, ERR_BUSY = range(11)
+OP_DELETE, OP_MATCHSUB, OP_INSERT = 0, 1, 2
+
+u64p = C.POINTER(C.c_uint64)
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+
+
+class ChsgaError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"chsga status {status}: {msg}")
+        self.status = status
+
+
+class CsrT(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("m", C.c_uint64), ("offset", u64p), ("target", u32p),
+                ("weight", u32p)]
+
+
+class PchT(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("m", C.c_uint64), ("rm", C.c_uint64),
+                ("num_layers", C.c_uint64), ("num_cc", C.c_uint64),
+                ("rank", u32p), ("level", u32p), ("layer_offset", u32p), ("cc_offset", u32p),
+                ("up_offset", u64p), ("up_v", u32p), ("up_w", u32p),
+                ("down_offset", u64p), ("down_v", u32p), ("down_w", u32p)]
+
+
+class GraphHostT(C.Structure):
+    _fields_ = [("num_chars", C.c_uint64), ("labels", C.c_char_p), ("char_graph", CsrT),
+                ("string_graph", CsrT), ("label_offsets", u64p), ("pch", PchT)]
+
+
+class GenGraphCfg(C.Structure):
+    _fields_ = [("backbone_len", C.c_uint64), ("seed", C.c_uint64), ("bubble_gap_mean", C.c_double),
+                ("p_snp", C.c_double), ("p_indel", C.c_double), ("p_alt", C.c_double),
+                ("indel_min", C.c_uint32), ("indel_max", C.c_uint32),
+                ("alt_min", C.c_uint32), ("alt_max", C.c_uint32),
+                ("vlen_min", C.c_uint32), ("vlen_max", C.c_uint32)]
+
+
+class PchOpts(C.Structure):
+    _fields_ = [("max_pop_count", C.c_uint32), ("sample_bound", C.c_double),
+                ("weight_bound", C.c_uint64), ("use_label_lengths", C.c_int),
+                ("seed", C.c_uint64), ("threads", C.c_int), ("print_detail", C.c_int)]
+
+
+class GenReadsCfg(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("seed", C.c_uint64), ("len_min", C.c_uint32),
+                ("len_max", C.c_uint32), ("sub_rate", C.c_double), ("indel_rate", C.c_double),
+                ("n_rate", C.c_double), ("indel_len_max", C.c_uint32)]
+
+
+class GraphStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in (
+        "num_chars", "num_char_edges", "num_strings", "num_string_edges", "pch_up_edges",
+        "pch_down_edges", "pch_levels", "pch_layers", "pch_ccs", "max_label_len",
+        "single_char_strings")]
+
+
+class OptsT(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_cap_bytes", C.c_uint64), ("flags", C.c_uint32)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("steps_per_graph", C.c_uint32), ("use_graphs", C.c_uint32)]
+
+
+class TbOpts(C.Structure):
+    _fields_ = [("k", C.c_int64), ("dir", C.c_char_p), ("keep_files", C.c_int),
+                ("cap_bytes", C.c_uint64)]
+
+
+class OpT(C.Structure):
+    _fields_ = [("row", C.c_int64), ("vertex", C.c_uint32), ("op", C.c_uint8),
+                ("pad", C.c_uint8 * 3)]
+
+
+class TbResult(C.Structure):
+    _fields_ = [("ops", C.POINTER(OpT)), ("num_ops", C.c_uint64), ("score", C.c_int32),
+                ("checkpointed", C.c_uint32), ("num_checkpoints", C.c_uint64)]
+
+
+class ProfileT(C.Structure):
+    _fields_ = [("row_ms", C.c_double), ("sweep_up_ms", C.c_double), ("top_ms", C.c_double),
+                ("sweep_down_ms", C.c_double), ("other_ms", C.c_double), ("total_ms", C.c_double),
+                ("rows", C.c_uint64), ("launches", C.c_uint64)]
+
+
+def _sig(name, res, *args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+vp = C.c_void_p
+_sig("chsga_last_error_global", C.c_char_p)
+_sig("chsga_graph_read_files", C.c_int32, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
+     C.c_char_p, C.POINTER(vp))
+_sig("chsga_graph_view", C.c_int32, vp, C.POINTER(GraphHostT))
+_sig("chsga_graph_free", None, vp)
+_sig("chsga_graph_write_files", C.c_int32, vp, C.c_char_p)
+_sig("chsga_gen_graph", C.c_int32, C.POINTER(GenGraphCfg), C.POINTER(vp))
+_sig("chsga_build_pch", C.c_int32, vp, C.POINTER(PchOpts))
+_sig("chsga_graph_get_stats", C.c_int32, vp, C.POINTER(GraphStats))
+_sig("chsga_reads_load", C.c_int32, C.c_char_p, C.c_uint64, C.POINTER(vp))
+_sig("chsga_reads_from_arrays", C.c_int32, C.c_char_p, u64p, C.c_uint64, C.POINTER(vp))
+_sig("chsga_reads_count", C.c_uint64, vp)
+_sig("chsga_reads_data", C.c_void_p, vp)
+_sig("chsga_reads_offsets", C.c_void_p, vp)
+_sig("chsga_reads_write_fasta", C.c_int32, vp, C.c_char_p)
+_sig("chsga_reads_free", None, vp)
+_sig("chsga_gen_reads", C.c_int32, vp, C.POINTER(GenReadsCfg), C.POINTER(vp))
+_sig("chsga_open", C.c_int32, C.POINTER(OptsT), C.POINTER(vp))
+_sig("chsga_close", None, vp)
+_sig("chsga_last_error", C.c_char_p, vp)
+_sig("chsga_load_graph", C.c_int32, vp, C.POINTER(GraphHostT))
+_sig("chsga_load_host_graph", C.c_int32, vp, vp)
+_sig("chsga_align_scores", C.c_int32, vp, C.POINTER(C.c_char_p), u32p, C.c_uint32, i32p)
+_sig("chsga_align_scores_batched", C.c_int32, vp, C.POINTER(C.c_char_p), u32p, C.c_uint32,
+     C.POINTER(BatchOpts), i32p)
+_sig("chsga_align_rows", C.c_int32, vp, C.c_char_p, C.c_uint32, i32p)
+_sig("chsga_align_traceback", C.c_int32, vp, C.c_char_p, C.c_uint32, C.POINTER(TbOpts),
+     C.POINTER(TbResult))
+_sig("chsga_tb_result_free", None, C.POINTER(TbResult))
+_sig("chsga_ops_to_cigar", C.c_uint64, C.POINTER(OpT), C.c_uint64, C.c_char_p, C.c_uint64)
+_sig("chsga_get_profile", C.c_int32, vp, C.POINTER(ProfileT))
+
+
+def _check(status: int, ctx=None):
+    if status != OK:
+        msg = (_lib.chsga_last_error(ctx) if ctx else _lib.chsga_last_error_global()) or b""
+        raise ChsgaError(status, msg.decode(errors="replace"))
+
+
+def exported_symbols() -> List[str]:
+    """Names declared in include/chsga.h (for the load/export check)."""
+    import re
+    hdr = os.path.join(_HERE, "..", "include", "chsga.h")
+    with open(hdr) as f:
+        txt = f.read()
+    return sorted(set(re.findall(r"\b(chsga_[a-z0-9_]+)\s*\(", txt)))
+
+
+# Configurations of the benchmark workloads (graph generator settings).
+GRAPH_CONFIGS = {
+    # 100 kbp backbone, SNP every ~100 bp and a 1-10 bp indel every ~1 kbp
+    "cfg1": dict(backbone_len=100_000, seed=1, bubble_gap_mean=1.0 / (1 / 100 + 1 / 1000),
+                 p_snp=(1 / 100) / (1 / 100 + 1 / 1000), p_indel=(1 / 1000) / (1 / 100 + 1 / 1000),
+                 p_alt=0.0, indel_min=1, indel_max=10, alt_min=50, alt_max=300,
+                 vlen_min=1, vlen_max=32),
+    # 5 Mbp backbone, a bubble every ~50 bp: 70% SNP, 20% 1-20 bp indel, 10% 50-300 bp allele
+    "cfg2": dict(backbone_len=5_000_000, seed=2, bubble_gap_mean=50.0, p_snp=0.7, p_indel=0.2,
+                 p_alt=0.1, indel_min=1, indel_max=20, alt_min=50, alt_max=300,
+                 vlen_min=1, vlen_max=32),
+    # 100 Mbp backbone, a bubble every ~30 bp, same mix as cfg2
+    "cfg4": dict(backbone_len=100_000_000, seed=4, bubble_gap_mean=30.0, p_snp=0.7, p_indel=0.2,
+                 p_alt=0.1, indel_min=1, indel_max=20, alt_min=50, alt_max=300,
+                 vlen_min=1, vlen_max=32),
+}
+
+
+class Reads:
+    """Concatenated read bases plus offsets (owned by the library)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def load(cls, path: str, max_reads: int = 5) -> "Reads":
+        h = vp()
+        _check(_lib.chsga_reads_load(path.encode(), max_reads, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_list(cls, seqs: Sequence[bytes]) -> "Reads":
+        data = b"".join(seqs)
+        offs = np.zeros(len(seqs) + 1, dtype=np.uint64)
+        offs[1:] = np.cumsum([len(s) for s in seqs])
+        h = vp()
+        _check(_lib.chsga_reads_from_arrays(data, offs.ctypes.data_as(u64p), len(seqs), C.byref(h)))
+        return cls(h)
+
+    def __len__(self):
+        return int(_lib.chsga_reads_count(self._h))
+
+    def to_list(self) -> List[bytes]:
+        n = len(self)
+        offs = np.ctypeslib.as_array(C.cast(_lib.chsga_reads_offsets(self._h), u64p), (n + 1,))
+        total = int(offs[-1])
+        data = C.string_at(_lib.chsga_reads_data(self._h), total) if total else b""
+        return [data[int(offs[i]):int(offs[i + 1])] for i in range(n)]
+
+    def write_fasta(self, path: str):
+        _check(_lib.chsga_reads_write_fasta(self._h, path.encode()))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib.chsga_reads_free(self._h)
+            self._h = None
+
+
+class HostGraph:
+    """Alignment inputs held on the host: labels, char graph, string graph,
+    label offsets and the contraction hierarchy."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def read_files(cls, char_adj, string_adj, pch, labels, offsets) -> "HostGraph":
+        h = vp()
+        _check(_lib.chsga_graph_read_files(char_adj.encode(), string_adj.encode(), pch.encode(),
+                                           labels.encode(), offsets.encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def read_prefix(cls, prefix: str) -> "HostGraph":
+        return cls.read_files(*files_for(prefix))
+
+    @classmethod
+    def generate(cls, **cfg) -> "HostGraph":
+        c = GenGraphCfg(**cfg)
+        h = vp()
+        _check(_lib.chsga_gen_graph(C.byref(c), C.byref(h)))
+        return cls(h)
+
+    def build_pch(self, max_pop_count=500, sample_bound=1.0, weight_bound=0, use_label_lengths=True,
+                  seed=0x5EED, threads=0, print_detail=False):
+        o = PchOpts(max_pop_count, sample_bound, weight_bound, int(use_label_lengths), seed, threads,
+                    int(print_detail))
+        _check(_lib.chsga_build_pch(self._h, C.byref(o)))
+        return self
+
+    def write_files(self, prefix: str):
+        _check(_lib.chsga_graph_write_files(self._h, prefix.encode()))
+        return files_for(prefix)
+
+    def stats(self) -> dict:
+        s = GraphStats()
+        _check(_lib.chsga_graph_get_stats(self._h, C.byref(s)))
+        return {k: int(getattr(s, k)) for k, _ in GraphStats._fields_}
+
+    def view(self) -> GraphHostT:
+        v = GraphHostT()
+        _check(_lib.chsga_graph_view(self._h, C.byref(v)))
+        return v
+
+    def gen_reads(self, count, seed, len_min, len_max=None, sub_rate=0.0, indel_rate=0.0,
+                  n_rate=0.0, indel_len_max=3) -> Reads:
+        c = GenReadsCfg(count, seed, len_min, len_max or len_min, sub_rate, indel_rate, n_rate,
+                        indel_len_max)
+        h = vp()
+        _check(_lib.chsga_gen_reads(self._h, C.byref(c), C.byref(h)))
+        return Reads(h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib.chsga_graph_free(self._h)
+            self._h = None
+
+
+def files_for(prefix: str) -> Tuple[str, str, str, str, str]:
+    """(-I, -i, -c, -l, -o) file names written by HostGraph.write_files."""
+    return (prefix + ".char.adj", prefix + ".string.adj", prefix + ".string.out",
+            prefix + ".char.labels", prefix + ".string.label_offsets")
+
+
+def _read_ptrs(reads: Sequence[bytes]):
+    arr = (C.c_char_p * len(reads))(*reads)
+    lens = np.array([len(r) for r in reads], dtype=np.uint32)
+    return arr, lens
+
+
+class Context:
+    """A device context with a loaded graph (chsga_open + chsga_load_graph)."""
+
+    def __init__(self, device: int = 0, hbm_cap_bytes: int = 0, flags: int = 0):
+        o = OptsT(device, hbm_cap_bytes, flags)
+        h = vp()
+        _check(_lib.chsga_open(C.byref(o), C.byref(h)))
+        self._h = h
+
+    def _ck(self, st):
+        _check(st, self._h)
+
+    def load(self, g: HostGraph) -> "Context":
+        self._ck(_lib.chsga_load_host_graph(self._h, g._h))
+        return self
+
+    def load_view(self, v: GraphHostT) -> "Context":
+        self._ck(_lib.chsga_load_graph(self._h, C.byref(v)))
+        return self
+
+    def align_scores(self, reads: Sequence[bytes]) -> np.ndarray:
+        """Plain path: one read per launch sequence (align_combo)."""
+        arr, lens = _read_ptrs(reads)
+        out = np.zeros(len(reads), dtype=np.int32)
+        self._ck(_lib.chsga_align_scores(self._h, arr, lens.ctypes.data_as(u32p), len(reads),
+                                         out.ctypes.data_as(i32p)))
+        return out
+
+    def align_scores_batched(self, reads: Sequence[bytes], slots: int = 64, steps_per_graph: int = 8,
+                             use_graphs: bool = True) -> np.ndarray:
+        arr, lens = _read_ptrs(reads)
+        out = np.zeros(len(reads), dtype=np.int32)
+        o = BatchOpts(slots, steps_per_graph, int(use_graphs))
+        self._ck(_lib.chsga_align_scores_batched(self._h, arr, lens.ctypes.data_as(u32p), len(reads),
+                                                 C.byref(o), out.ctypes.data_as(i32p)))
+        return out
+
+    def align_rows(self, read: bytes, num_chars: int) -> np.ndarray:
+        out = np.zeros((len(read), num_chars), dtype=np.int32)
+        self._ck(_lib.chsga_align_rows(self._h, read, len(read), out.ctypes.data_as(i32p)))
+        return out
+
+    def align_traceback(self, read: bytes, k: int = 500, ckpt_dir: Optional[str] = None,
+                        keep_files: bool = False, cap_bytes: int = 0):
+        """Returns (ops ndarray[row, vertex, op], score, checkpointed)."""
+        o = TbOpts(k, ckpt_dir.encode() if ckpt_dir else None, int(keep_files), cap_bytes)
+        r = TbResult()
+        self._ck(_lib.chsga_align_traceback(self._h, read, len(read), C.byref(o), C.byref(r)))
+        try:
+            n = int(r.num_ops)
+            ops = np.zeros((n, 3), dtype=np.int64)
+            for i in range(n):
+                x = r.ops[i]
+                ops[i] = (x.row, x.vertex, x.op)
+            return ops, int(r.score), bool(r.checkpointed)
+        finally:
+            _lib.chsga_tb_result_free(C.byref(r))
+
+    def profile(self) -> dict:
+        p = ProfileT()
+        self._ck(_lib.chsga_get_profile(self._h, C.byref(p)))
+        return {k: getattr(p, k) for k, _ in ProfileT._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.chsga_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def ops_to_cigar(ops: np.ndarray) -> str:
+    """ops_to_cigar (src/traceback.hpp:1081-1110)."""
+    if len(ops) == 0:
+        return ""
+    letters = {OP_DELETE: "D", OP_MATCHSUB: "M", OP_INSERT: "I"}
+    out, prev, run = [], letters[int(ops[0][2])], 1
+    for r in ops[1:]:
+        c = letters[int(r[2])]
+        if c == prev:
+            run += 1
+        else:
+            out.append(f"{run}{prev}")
+            prev, run = c, 1
+    out.append(f"{run}{prev}")
+    return "".join(out)

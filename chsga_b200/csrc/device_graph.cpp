@@ -1,0 +1,245 @@
+// Host-side construction of the device layout (see device_graph.hpp), with
+// the structural checks the GPU path relies on.
+#include <algorithm>
+#include <numeric>
+
+#include "device_graph.hpp"
+
+namespace chsga {
+
+namespace {
+int base_code(unsigned char c) {
+  switch (c) {
+    case 'A': return 0;
+    case 'C': return 1;
+    case 'G': return 2;
+    case 'T': return 3;
+    default: return -1;
+  }
+}
+}  // namespace
+
+HostLayout build_layout(const chsga_graph_host& g) {
+  HostLayout L;
+  require(g.labels && g.label_offsets && g.char_graph.offset && g.string_graph.offset,
+          CHSGA_ERR_INVALID_ARG, "graph arrays missing");
+  const uint64_t N64 = g.num_chars, S64 = g.string_graph.n;
+  require(N64 > 0 && S64 > 0, CHSGA_ERR_INVALID_ARG, "empty graph");
+  require(N64 < (1ull << 31) && S64 < (1ull << 30), CHSGA_ERR_UNSUPPORTED,
+          "graph too large: chars must be < 2^31 and string vertices < 2^30");
+  require(g.char_graph.n == N64, CHSGA_ERR_FORMAT, "char graph size differs from label count");
+  require(g.label_offsets[0] == 0 && g.label_offsets[S64] == N64, CHSGA_ERR_FORMAT,
+          "label offsets must run from 0 to the number of labels");
+  const uint32_t N = (uint32_t)N64, S = (uint32_t)S64;
+  L.N = N;
+  L.S = S;
+
+  // --- labels: 2-bit code plus one "special" byte class --------------------
+  L.lab2.assign((N + 15) / 16, 0);
+  L.lab_sp.assign((N + 31) / 32, 0);
+  for (uint32_t c = 0; c < N; ++c) {
+    unsigned char ch = (unsigned char)g.labels[c];
+    int code = base_code(ch);
+    if (code < 0) {
+      if (L.special < 0) L.special = ch;
+      require(L.special == ch, CHSGA_ERR_UNSUPPORTED,
+              std::string("labels use more than one byte outside A/C/G/T ('") +
+                  (char)L.special + "' and '" + (char)ch + "')");
+      L.lab_sp[c >> 5] |= 1u << (c & 31);
+      code = 0;
+    }
+    L.lab2[c >> 4] |= (uint32_t)code << ((c & 15) * 2);
+  }
+
+  // --- string vertices and the char graph -----------------------------------
+  L.sv_off.resize(S + 1);
+  for (uint32_t s = 0; s <= S; ++s) L.sv_off[s] = (uint32_t)g.label_offsets[s];
+  std::vector<uint32_t> vertex_of(N);
+  for (uint32_t s = 0; s < S; ++s) {
+    require(L.sv_off[s] < L.sv_off[s + 1], CHSGA_ERR_UNSUPPORTED,
+            "string vertex " + std::to_string(s) + " has an empty label");
+    for (uint32_t c = L.sv_off[s]; c < L.sv_off[s + 1]; ++c) vertex_of[c] = s;
+  }
+  const chsga_csr& cg = g.char_graph;
+  // in-CSR with sources in ascending order, as build_in_csr (align.hpp:220-242)
+  std::vector<uint64_t> ioff(N + 1, 0);
+  for (uint64_t u = 0; u < N; ++u)
+    for (uint64_t e = cg.offset[u]; e < cg.offset[u + 1]; ++e) {
+      require(cg.target[e] < N, CHSGA_ERR_FORMAT, "char edge target out of range");
+      ioff[cg.target[e] + 1]++;
+    }
+  for (uint32_t v = 0; v < N; ++v) ioff[v + 1] += ioff[v];
+  std::vector<uint32_t> isrc(ioff[N]);
+  {
+    std::vector<uint64_t> cur(ioff.begin(), ioff.end() - 1);
+    for (uint64_t u = 0; u < N; ++u)
+      for (uint64_t e = cg.offset[u]; e < cg.offset[u + 1]; ++e) isrc[cur[cg.target[e]]++] = (uint32_t)u;
+  }
+  L.char_in_edges = ioff[N];
+  L.vin_off.assign(S + 1, 0);
+  for (uint32_t s = 0; s < S; ++s) {
+    const uint32_t f = L.sv_off[s], e = L.sv_off[s + 1];
+    for (uint32_t c = f + 1; c < e; ++c)
+      require(ioff[c + 1] - ioff[c] == 1 && isrc[ioff[c]] == c - 1, CHSGA_ERR_UNSUPPORTED,
+              "char " + std::to_string(c) +
+                  " is not the chain successor of char " + std::to_string(c - 1) +
+                  ": the char graph must be the expansion of the string graph "
+                  "(every char after the first of a string has the single in-edge c-1 -> c)");
+    L.vin_off[s + 1] = L.vin_off[s] + (uint32_t)(ioff[f + 1] - ioff[f]);
+  }
+  L.vin_src.resize(L.vin_off[S]);
+  L.vin_srcv.resize(L.vin_off[S]);
+  for (uint32_t s = 0; s < S; ++s) {
+    const uint32_t f = L.sv_off[s];
+    for (uint64_t k = 0; k < ioff[f + 1] - ioff[f]; ++k) {
+      uint32_t u = isrc[ioff[f] + k];
+      L.vin_src[L.vin_off[s] + k] = u;
+      L.vin_srcv[L.vin_off[s] + k] = vertex_of[u];
+    }
+  }
+
+  // --- hierarchy order -------------------------------------------------------
+  const chsga_pch& p = g.pch;
+  require(p.n == S && p.rank && p.level && p.layer_offset && p.cc_offset && p.up_offset &&
+              p.down_offset,
+          CHSGA_ERR_FORMAT, "hierarchy missing or of the wrong size");
+  std::vector<uint32_t> og(S);
+  {
+    std::vector<uint8_t> seen(S, 0);
+    for (uint32_t s = 0; s < S; ++s) {
+      require(p.rank[s] < S && !seen[p.rank[s]], CHSGA_ERR_FORMAT, "hierarchy rank is not a permutation");
+      seen[p.rank[s]] = 1;
+      og[p.rank[s]] = s;
+    }
+  }
+  // layer and component of each rank, and the level checks
+  std::vector<uint32_t> cc_of(S), layer_of(S);
+  require(p.num_cc >= 1 && p.cc_offset[0] == 0 && p.cc_offset[p.num_cc] == p.num_layers &&
+              p.layer_offset[0] == 0 && p.layer_offset[p.num_layers] == S,
+          CHSGA_ERR_FORMAT, "hierarchy layer/component offsets do not cover the vertices");
+  for (uint64_t cc = 0; cc < p.num_cc; ++cc) {
+    uint32_t prev_level = 0;
+    for (uint32_t l = p.cc_offset[cc]; l < p.cc_offset[cc + 1]; ++l) {
+      require(p.layer_offset[l] <= p.layer_offset[l + 1], CHSGA_ERR_FORMAT, "layer offsets decrease");
+      for (uint32_t r = p.layer_offset[l]; r < p.layer_offset[l + 1]; ++r) {
+        cc_of[r] = (uint32_t)cc;
+        layer_of[r] = l;
+        require(p.level[r] == p.level[p.layer_offset[l]], CHSGA_ERR_UNSUPPORTED,
+                "a hierarchy layer mixes levels");
+      }
+      if (p.layer_offset[l] < p.layer_offset[l + 1]) {
+        uint32_t lv = p.level[p.layer_offset[l]];
+        require(l == p.cc_offset[cc] || lv > prev_level, CHSGA_ERR_UNSUPPORTED,
+                "hierarchy layers of a component must have increasing levels");
+        prev_level = lv;
+      }
+    }
+  }
+  std::vector<uint32_t> order(S);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return p.level[a] < p.level[b]; });
+  std::vector<uint32_t> dev(S);
+  for (uint32_t d = 0; d < S; ++d) dev[order[d]] = d;
+  L.dv_first.resize(S);
+  L.dv_len.resize(S);
+  for (uint32_t d = 0; d < S; ++d) {
+    uint32_t s = og[order[d]];
+    L.dv_first[d] = L.sv_off[s];
+    L.dv_len[d] = L.sv_off[s + 1] - L.sv_off[s];
+  }
+  L.sv_dev.resize(S);
+  for (uint32_t s = 0; s < S; ++s) L.sv_dev[s] = dev[p.rank[s]];
+  auto bv_last = [&](uint32_t rank) { return 2 * dev[rank] + (L.dv_len[dev[rank]] > 1 ? 1 : 0); };
+  // pull lists
+  std::vector<std::vector<EdgeW>> up(S), dn(S);
+  for (uint32_t u = 0; u < S; ++u) {
+    for (uint64_t j = p.up_offset[u]; j < p.up_offset[u + 1]; ++j) {
+      uint32_t v = p.up_v[j];
+      require(v < S, CHSGA_ERR_FORMAT, "hierarchy edge out of range");
+      require(cc_of[v] == cc_of[u] && layer_of[v] > layer_of[u], CHSGA_ERR_UNSUPPORTED,
+              "upward hierarchy edge does not climb to a later layer of its component");
+      require(p.up_w[j] <= (1u << 30), CHSGA_ERR_UNSUPPORTED, "hierarchy weight too large");
+      up[dev[v]].push_back({(int32_t)bv_last(u), (int32_t)p.up_w[j]});
+    }
+    for (uint64_t j = p.down_offset[u]; j < p.down_offset[u + 1]; ++j) {
+      uint32_t v = p.down_v[j];
+      require(v < S, CHSGA_ERR_FORMAT, "hierarchy edge out of range");
+      require(cc_of[v] == cc_of[u] && layer_of[v] > layer_of[u], CHSGA_ERR_UNSUPPORTED,
+              "downward hierarchy edge does not come from a later layer of its component");
+      require(p.down_w[j] <= (1u << 30), CHSGA_ERR_UNSUPPORTED, "hierarchy weight too large");
+      dn[dev[u]].push_back({(int32_t)bv_last(v), (int32_t)p.down_w[j]});
+    }
+  }
+  auto flatten = [&](std::vector<std::vector<EdgeW>>& lists, std::vector<uint32_t>& off,
+                     std::vector<EdgeW>& out) {
+    off.assign(S + 1, 0);
+    for (uint32_t d = 0; d < S; ++d) off[d + 1] = off[d] + (uint32_t)lists[d].size();
+    out.reserve(off[S]);
+    for (auto& l : lists) out.insert(out.end(), l.begin(), l.end());
+  };
+  flatten(up, L.up_off, L.up_in);
+  flatten(dn, L.dn_off, L.dn_in);
+  // levels in hierarchy order
+  L.lvl_off.push_back(0);
+  for (uint32_t d = 1; d < S; ++d)
+    if (p.level[order[d]] != p.level[order[d - 1]]) L.lvl_off.push_back(d);
+  L.lvl_off.push_back(S);
+  L.levels = (uint32_t)L.lvl_off.size() - 1;
+  L.lvl_up_edges.resize(L.levels);
+  for (uint32_t l = 0; l < L.levels; ++l)
+    L.lvl_up_edges[l] = L.up_off[L.lvl_off[l + 1]] - L.up_off[L.lvl_off[l]];
+
+  // --- string-graph in-CSR for the traceback walk (traceback.hpp:716) -------
+  const chsga_csr& sg = g.string_graph;
+  L.istr_off.assign(S + 1, 0);
+  for (uint64_t u = 0; u < S; ++u)
+    for (uint64_t e = sg.offset[u]; e < sg.offset[u + 1]; ++e) {
+      require(sg.target[e] < S, CHSGA_ERR_FORMAT, "string edge target out of range");
+      L.istr_off[sg.target[e] + 1]++;
+    }
+  for (uint32_t v = 0; v < S; ++v) L.istr_off[v + 1] += L.istr_off[v];
+  L.istr_src.resize(L.istr_off[S]);
+  {
+    std::vector<uint32_t> cur(L.istr_off.begin(), L.istr_off.end() - 1);
+    for (uint64_t u = 0; u < S; ++u)
+      for (uint64_t e = sg.offset[u]; e < sg.offset[u + 1]; ++e) L.istr_src[cur[sg.target[e]]++] = (uint32_t)u;
+  }
+  return L;
+}
+
+HostTop build_top(const HostLayout& L, uint32_t max_vertices) {
+  HostTop t;
+  uint32_t first = L.levels;
+  while (first > 0 && L.S - L.lvl_off[first - 1] <= max_vertices) --first;
+  t.first_level = first;
+  t.K0 = L.lvl_off[first];
+  t.K = L.S - t.K0;
+  for (uint32_t l = first; l <= L.levels; ++l) t.lvl_off.push_back(L.lvl_off[l] - t.K0);
+  t.upg_off.assign(t.K + 1, 0);
+  t.upl_off.assign(t.K + 1, 0);
+  t.dn_off.assign(t.K + 1, 0);
+  const int32_t lo = (int32_t)(2 * t.K0);
+  for (uint32_t j = 0; j < t.K; ++j) {
+    const uint32_t d = t.K0 + j;
+    for (uint32_t e = L.up_off[d]; e < L.up_off[d + 1]; ++e) {
+      const EdgeW x = L.up_in[e];
+      if (x.src < lo) {
+        t.upg.push_back(x);
+      } else {
+        t.upl.push_back({x.src - lo, x.w});
+      }
+    }
+    for (uint32_t e = L.dn_off[d]; e < L.dn_off[d + 1]; ++e) {
+      const EdgeW x = L.dn_in[e];
+      require(x.src >= lo, CHSGA_ERR_INTERNAL, "downward edge into the top region from below");
+      t.dn.push_back({x.src - lo, x.w});
+    }
+    t.upg_off[j + 1] = (uint32_t)t.upg.size();
+    t.upl_off[j + 1] = (uint32_t)t.upl.size();
+    t.dn_off[j + 1] = (uint32_t)t.dn.size();
+  }
+  return t;
+}
+
+}  // namespace chsga

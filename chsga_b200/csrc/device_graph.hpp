@@ -1,0 +1,75 @@
+// Device-side layout of one alignment graph and the host code that builds it.
+//
+// The DP of src/align.hpp touches, per read row:
+//   every char c (fused_deletion_substitution, align.hpp:245-277) through the
+//     char graph's in-CSR and the char labels;
+//   every string vertex s through first(s) = off[s], last(s) = off[s+1]-1
+//     (insertion_func_parallel, align.hpp:347-397);
+//   the contraction hierarchy, layer by layer (align.hpp:279-345).
+// The layout below serves those three access patterns:
+//
+//   chars (original order)      2-bit label codes + a 1-bit "special" map
+//   string vertices (original)  sv_off[S+1] char offsets, sv_dev[S] position
+//                               in the hierarchy order, vin_* = in-edges of
+//                               the vertex's first char (every other char of
+//                               a vertex has exactly the chain edge c-1 -> c)
+//   hierarchy vertices          ordered by (level, rank): one contiguous range
+//                               per level, all components merged (components
+//                               share no edges, so their sweeps commute)
+//   boundary array BV           per hierarchy vertex d: BV[2d] = score at
+//                               first(og d), BV[2d+1] = score at last(og d);
+//                               single-char vertices use BV[2d] for both
+//   up_in / dn_in               pull form of the two sweeps: for target d the
+//                               list of (BV index of the source's last char,
+//                               weight); an upward edge u->v of GC.E becomes an
+//                               entry of up_in[v], a downward in-edge of
+//                               GC.in_E[u] an entry of dn_in[u]
+//
+// Pull instead of push: every hierarchy edge joins two different layers of
+// one component (checked at load), so the push-with-atomic-min of the
+// reference's upward sweep and this pull compute the same minima.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "common.hpp"
+
+namespace chsga {
+
+struct EdgeW {  // matches the device int2 layout
+  int32_t src;
+  int32_t w;
+};
+
+struct HostLayout {
+  uint32_t N = 0, S = 0, levels = 0;
+  // label encoding: code 0..3 for A,C,G,T; `special` holds the one other
+  // byte that may occur in the labels (usually 'N'), flagged in lab_sp
+  int special = -1;
+  std::vector<uint32_t> lab2;   // ceil(N/16) words
+  std::vector<uint32_t> lab_sp; // ceil(N/32) words
+  std::vector<uint32_t> sv_off, sv_dev, vin_off, vin_src, vin_srcv;
+  std::vector<uint32_t> dv_first, dv_len;  // by hierarchy order
+  std::vector<uint32_t> up_off, dn_off;    // S+1, by hierarchy order
+  std::vector<EdgeW> up_in, dn_in;
+  std::vector<uint32_t> lvl_off;           // levels+1
+  std::vector<uint32_t> lvl_up_edges;      // per level: number of up_in entries
+  std::vector<uint32_t> istr_off, istr_src;  // string-graph in-CSR (ascending source)
+  uint64_t char_in_edges = 0;
+};
+
+// Top region of the hierarchy (levels >= first_level), swept inside one CTA
+// per slot with the boundary values staged in shared memory.
+struct HostTop {
+  uint32_t first_level = 0;  // level index where the top region starts
+  uint32_t K0 = 0, K = 0;    // hierarchy positions [K0, K0+K)
+  std::vector<uint32_t> lvl_off;               // local level offsets
+  std::vector<uint32_t> upg_off, upl_off, dn_off;  // K+1 each
+  std::vector<EdgeW> upg, upl, dn;             // global-source / local-source / local
+};
+
+HostLayout build_layout(const chsga_graph_host& g);
+HostTop build_top(const HostLayout& L, uint32_t max_vertices);
+
+}  // namespace chsga

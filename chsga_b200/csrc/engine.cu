@@ -1,0 +1,784 @@
+// Device context, graph upload and the orchestration of the row-step kernels
+// (kernels.cuh) behind the C-ABI of include/chsga.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <filesystem>
+#include <map>
+#include <memory>
+#include <new>
+
+#include "device_graph.hpp"
+#include "host_graph.hpp"
+#include "kernels.cuh"
+
+namespace chsga {
+
+extern thread_local std::string g_last_error;
+void validate_host_graph(const chsga_host_graph& g);
+
+#define CK(x)                                                                                \
+  do {                                                                                       \
+    cudaError_t e_ = (x);                                                                    \
+    if (e_ != cudaSuccess)                                                                   \
+      fail(e_ == cudaErrorMemoryAllocation ? CHSGA_ERR_OOM : CHSGA_ERR_CUDA,                 \
+           std::string(#x) + ": " + cudaGetErrorString(e_));                                 \
+  } while (0)
+
+template <typename T>
+struct DevArr {
+  T* p = nullptr;
+  size_t n = 0;
+  DevArr() = default;
+  DevArr(const DevArr&) = delete;
+  DevArr& operator=(const DevArr&) = delete;
+  ~DevArr() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count <= n && p) return;
+    release();
+    if (count == 0) count = 1;
+    CK(cudaMalloc((void**)&p, count * sizeof(T)));
+    n = count;
+  }
+  void upload(const std::vector<T>& v, cudaStream_t s) {
+    alloc(v.size());
+    if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+};
+
+template <typename T>
+struct PinnedArr {
+  T* p = nullptr;
+  size_t n = 0;
+  PinnedArr() = default;
+  PinnedArr(const PinnedArr&) = delete;
+  PinnedArr& operator=(const PinnedArr&) = delete;
+  ~PinnedArr() {
+    if (p) cudaFreeHost(p);
+  }
+  void alloc(size_t count) {
+    if (count <= n && p) return;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    CK(cudaHostAlloc((void**)&p, std::max<size_t>(count, 1) * sizeof(T), cudaHostAllocDefault));
+    n = count;
+  }
+};
+
+struct GraphDev {
+  DevArr<uint32_t> lab2, lab_sp, sv_off, sv_dev, vin_off, vin_src, vin_srcv, dv_first, dv_len;
+  DevArr<uint32_t> up_off, dn_off, istr_off, istr_src;
+  DevArr<int2> up_in, dn_in;
+};
+
+struct TopDev {
+  HostTop h;
+  DevArr<uint32_t> lvl_off, upg_off, upl_off, dn_off;
+  DevArr<int2> upg, upl, dn;
+  dev::TopPtrs ptrs{};
+};
+
+// Buffers of one slot configuration (R slots).
+struct SlotBufs {
+  int R = 0;
+  DevArr<int> rows[2];
+  DevArr<int> BV;
+  DevArr<dev::SlotState> slots;
+  DevArr<uint32_t> word;
+  DevArr<unsigned long long> best;
+  DevArr<dev::StepCtl> ctl;
+};
+
+constexpr uint32_t kTopMaxVertices = 25000;  // 2 x int32 per vertex in shared memory
+constexpr int kTopThreads = 1024;
+
+}  // namespace chsga
+
+struct chsga_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr, side = nullptr;
+  std::string err;
+  uint64_t cap = 0;
+  uint32_t flags = 0;
+  bool loaded = false;
+  bool nul_label = false;
+  chsga::HostLayout L;
+  chsga::GraphDev gd;
+  chsga::dev::GraphPtrs gp{};
+  std::unique_ptr<chsga::TopDev> top;
+  std::map<int, std::unique_ptr<chsga::SlotBufs>> bufs;
+  chsga::DevArr<unsigned char> reads;
+  chsga::DevArr<chsga::dev::ReadDesc> queue;
+  chsga::DevArr<int32_t> res_score;
+  chsga::DevArr<uint32_t> res_vertex;
+  chsga::PinnedArr<chsga::dev::StepCtl> h_ctl;
+  chsga::PinnedArr<int32_t> h_ckpt;  // checkpoint rows of the checkpointed traceback
+  chsga_profile prof{};
+};
+
+namespace chsga {
+
+namespace {
+
+using dev::Lanes;
+
+unsigned nblocks(uint64_t items, unsigned tpb = 256) { return (unsigned)((items + tpb - 1) / tpb); }
+
+void set_device(chsga_ctx& c) { CK(cudaSetDevice(c.device)); }
+
+void check_launch() { CK(cudaGetLastError()); }
+
+template <int R>
+SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
+  auto& b = c.bufs[R];
+  if (!b) b = std::make_unique<SlotBufs>();
+  b->R = R;
+  const size_t N = c.L.N, S = c.L.S;
+  if (need_rows) {
+    b->rows[0].alloc(N * R);
+    b->rows[1].alloc(N * R);
+  }
+  b->BV.alloc(2 * S * R);
+  b->slots.alloc(R);
+  b->word.alloc(R);
+  b->best.alloc(R);
+  b->ctl.alloc(1);
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(dev::k_top<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)(kTopMaxVertices * 8)));
+    attr_set = true;
+  }
+  return *b;
+}
+
+// Uploads reads (raw bytes) and their queue descriptors; ids are 0..n-1.
+void upload_reads(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n) {
+  std::vector<unsigned char> bytes;
+  std::vector<dev::ReadDesc> q(n);
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < n; ++i) total += lens[i];
+  bytes.resize(std::max<uint64_t>(total, 1));
+  uint64_t off = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    require(reads[i] != nullptr || lens[i] == 0, CHSGA_ERR_INVALID_ARG, "null read");
+    if (lens[i]) std::memcpy(bytes.data() + off, reads[i], lens[i]);
+    q[i] = dev::ReadDesc{off, lens[i], (int32_t)i};
+    off += lens[i];
+  }
+  std::vector<unsigned char> bv(bytes.begin(), bytes.end());
+  c.reads.upload(bv, c.st);
+  c.queue.upload(q, c.st);
+  c.res_score.alloc(n);
+  c.res_vertex.alloc(n);
+}
+
+template <int R>
+void reset_slots(chsga_ctx& c, SlotBufs& b, uint32_t q_count) {
+  std::vector<dev::SlotState> s(R);
+  for (auto& x : s) x = dev::SlotState{0, 0, 0, -1, 0};
+  CK(cudaMemcpyAsync(b.slots.p, s.data(), sizeof(dev::SlotState) * R, cudaMemcpyHostToDevice, c.st));
+  dev::StepCtl ctl{};
+  ctl.q_count = q_count;
+  CK(cudaMemcpyAsync(b.ctl.p, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, c.st));
+  CK(cudaStreamSynchronize(c.st));  // host copies above are from stack memory
+}
+
+template <int R>
+void launch_advance(chsga_ctx& c, SlotBufs& b, int prime, cudaStream_t s) {
+  dev::k_advance<R><<<1, 128, 0, s>>>(b.slots.p, c.queue.p, c.reads.p, b.best.p, c.res_score.p,
+                                      c.res_vertex.p, b.word.p, b.ctl.p, c.L.special, prime);
+  check_launch();
+}
+
+// One row-step for every slot: D = previous rows, T = rows being computed.
+template <int R>
+void row_step(chsga_ctx& c, SlotBufs& b, const int* D, int* T, cudaStream_t s) {
+  const HostLayout& L = c.L;
+  const TopDev& top = *c.top;
+  constexpr int G = Lanes<R>::G;
+  dev::k_row<R><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(c.gp, D, T, b.BV.p, b.word.p, b.best.p,
+                                                            b.ctl.p);
+  const uint32_t fl = top.h.first_level;
+  for (uint32_t l = 0; l < fl; ++l) {
+    if (L.lvl_up_edges[l] == 0) continue;
+    const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
+    dev::k_pull<R><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
+        b.BV.p, lo, hi, c.gd.up_off.p, c.gd.up_in.p, 0, b.ctl.p);
+  }
+  if (top.h.K) {
+    if (!top.h.upg.empty())
+      dev::k_pull<R><<<nblocks((uint64_t)top.h.K * G), 256, 0, s>>>(
+          b.BV.p, top.h.K0, L.S, top.upg_off.p, top.upg.p, top.h.K0, b.ctl.p);
+    dev::k_top<R><<<R, kTopThreads, top.h.K * 8, s>>>(b.BV.p, top.ptrs, b.word.p, b.ctl.p);
+  }
+  if (fl == 0) {
+    dev::k_down<R><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(c.gp, b.BV.p, T, 0, 0, L.S, b.word.p,
+                                                               b.best.p, b.ctl.p);
+  } else {
+    for (int l = (int)fl - 1; l >= 0; --l) {
+      const uint32_t lo = L.lvl_off[l], mid = L.lvl_off[l + 1];
+      const uint32_t hi = (l == (int)fl - 1) ? L.S : mid;
+      dev::k_down<R><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(c.gp, b.BV.p, T, lo, mid, hi,
+                                                                       b.word.p, b.best.p, b.ctl.p);
+    }
+  }
+  launch_advance<R>(c, b, 0, s);
+}
+
+uint32_t kernels_per_step(const chsga_ctx& c) {
+  uint32_t k = 2;  // k_row + k_advance
+  const uint32_t fl = c.top->h.first_level;
+  for (uint32_t l = 0; l < fl; ++l) k += c.L.lvl_up_edges[l] ? 1 : 0;
+  if (c.top->h.K) k += 1 + (c.top->h.upg.empty() ? 0 : 1);
+  k += fl == 0 ? 1 : fl;
+  return k;
+}
+
+// Runs every queued read to completion through R slots. Steps are captured
+// in CUDA graphs of `per_graph` row-steps (even, so the two row buffers
+// alternate identically in every launch).
+template <int R>
+void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, uint32_t per_graph) {
+  SlotBufs& b = get_bufs<R>(c, true);
+  reset_slots<R>(c, b, n);
+  launch_advance<R>(c, b, 0, c.st);  // admit the first reads
+  per_graph = std::max<uint32_t>(2, per_graph + (per_graph & 1));
+  c.h_ctl.alloc(1);
+  cudaEvent_t ev[2];
+  CK(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  auto enqueue_block = [&](cudaStream_t s) {
+    for (uint32_t i = 0; i < per_graph; ++i)
+      row_step<R>(c, b, b.rows[i & 1].p, b.rows[(i + 1) & 1].p, s);
+  };
+  if (use_graphs) {
+    cudaStream_t cap;
+    CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    enqueue_block(cap);
+    CK(cudaStreamEndCapture(cap, &graph));
+    CK(cudaGraphInstantiate(&exec, graph, 0));
+    CK(cudaStreamDestroy(cap));
+  }
+  auto launch_block = [&]() {
+    if (use_graphs) {
+      CK(cudaGraphLaunch(exec, c.st));
+    } else {
+      enqueue_block(c.st);
+    }
+  };
+  // R == 1 runs exactly one row per step, so the step count is known; the
+  // batched engine polls its done counter, one block behind the device.
+  if (R == 1) {
+    const uint64_t blocks = (total_rows + per_graph - 1) / per_graph;
+    for (uint64_t i = 0; i < blocks; ++i) launch_block();
+    CK(cudaStreamSynchronize(c.st));
+  } else {
+    uint64_t launched = 0;
+    const uint64_t max_blocks = total_rows / per_graph + 4;
+    while (true) {
+      launch_block();
+      CK(cudaMemcpyAsync(c.h_ctl.p, b.ctl.p, sizeof(dev::StepCtl), cudaMemcpyDeviceToHost, c.st));
+      CK(cudaEventRecord(ev[launched & 1], c.st));
+      ++launched;
+      if (launched >= 2) {
+        CK(cudaEventSynchronize(ev[(launched - 2) & 1]));
+        // the pinned copy may already hold a newer value; both are progress
+        if (c.h_ctl.p->done >= n) break;
+      }
+      require(launched <= max_blocks + 2, CHSGA_ERR_INTERNAL, "batched engine made no progress");
+    }
+    CK(cudaStreamSynchronize(c.st));
+    require(c.h_ctl.p->done == n, CHSGA_ERR_INTERNAL, "batched engine lost reads");
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  c.prof.rows = total_rows;
+  c.prof.launches = (uint64_t)kernels_per_step(c) * ((total_rows + per_graph - 1) / per_graph) * per_graph;
+}
+
+void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
+  HostLayout L = build_layout(g);
+  GraphDev& d = c.gd;
+  cudaStream_t s = c.st;
+  d.lab2.upload(L.lab2, s);
+  d.lab_sp.upload(L.lab_sp, s);
+  d.sv_off.upload(L.sv_off, s);
+  d.sv_dev.upload(L.sv_dev, s);
+  d.vin_off.upload(L.vin_off, s);
+  d.vin_src.upload(L.vin_src, s);
+  d.vin_srcv.upload(L.vin_srcv, s);
+  d.dv_first.upload(L.dv_first, s);
+  d.dv_len.upload(L.dv_len, s);
+  d.up_off.upload(L.up_off, s);
+  d.dn_off.upload(L.dn_off, s);
+  d.istr_off.upload(L.istr_off, s);
+  d.istr_src.upload(L.istr_src, s);
+  std::vector<int2> up(L.up_in.size()), dn(L.dn_in.size());
+  for (size_t i = 0; i < up.size(); ++i) up[i] = make_int2(L.up_in[i].src, L.up_in[i].w);
+  for (size_t i = 0; i < dn.size(); ++i) dn[i] = make_int2(L.dn_in[i].src, L.dn_in[i].w);
+  d.up_in.upload(up, s);
+  d.dn_in.upload(dn, s);
+  auto top = std::make_unique<TopDev>();
+  top->h = build_top(L, kTopMaxVertices);
+  const HostTop& h = top->h;
+  top->lvl_off.upload(h.lvl_off, s);
+  top->upg_off.upload(h.upg_off, s);
+  top->upl_off.upload(h.upl_off, s);
+  top->dn_off.upload(h.dn_off, s);
+  auto to2 = [](const std::vector<EdgeW>& v) {
+    std::vector<int2> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) o[i] = make_int2(v[i].src, v[i].w);
+    return o;
+  };
+  top->upg.upload(to2(h.upg), s);
+  top->upl.upload(to2(h.upl), s);
+  top->dn.upload(to2(h.dn), s);
+  top->ptrs = dev::TopPtrs{h.K0, h.K, (uint32_t)h.lvl_off.size() - 1, top->lvl_off.p,
+                           top->upl_off.p, top->upl.p, top->dn_off.p, top->dn.p, d.dv_len.p};
+  CK(cudaStreamSynchronize(s));
+  c.gp = dev::GraphPtrs{L.N,          L.S,          L.special,      d.lab2.p,     d.lab_sp.p,
+                        d.sv_off.p,   d.sv_dev.p,   d.vin_off.p,    d.vin_src.p,  d.vin_srcv.p,
+                        d.dv_first.p, d.dv_len.p,   d.up_off.p,     d.up_in.p,    d.dn_off.p,
+                        d.dn_in.p,    d.istr_off.p, d.istr_src.p};
+  c.nul_label = false;
+  for (uint32_t i = 0; i < g.num_chars && !c.nul_label; ++i) c.nul_label = g.labels[i] == '\0';
+  c.L = std::move(L);
+  c.top = std::move(top);
+  c.bufs.clear();
+  c.loaded = true;
+}
+
+template <int R>
+void scores_with(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n,
+                 int32_t* out, bool graphs, uint32_t per_graph) {
+  // length-0 reads never reach the device: the reference scores row 0
+  // against read[0] == '\0', i.e. 1 unless a label byte is 0
+  std::vector<const char*> rp;
+  std::vector<uint32_t> rl, idx;
+  uint64_t rows = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (lens[i] == 0) {
+      out[i] = c.nul_label ? 0 : 1;
+      continue;
+    }
+    rp.push_back(reads[i]);
+    rl.push_back(lens[i]);
+    idx.push_back(i);
+    rows += lens[i];
+  }
+  if (rp.empty()) return;
+  upload_reads(c, rp.data(), rl.data(), (uint32_t)rp.size());
+  auto t0 = std::chrono::steady_clock::now();
+  run_queue<R>(c, (uint32_t)rp.size(), rows, graphs, per_graph);
+  c.prof.total_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  std::vector<int32_t> res(rp.size());
+  CK(cudaMemcpy(res.data(), c.res_score.p, res.size() * 4, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < idx.size(); ++i) out[idx[i]] = res[i];
+}
+
+// ---- traceback --------------------------------------------------------------
+
+struct TbState {
+  std::vector<dev::WalkOp> path;  // reverse order
+};
+
+// Forward rows [a+1, b] of the single read from `row_a` (row a, on the
+// device), writing row i to out + (i - a) * N if out_rows, else rotating two
+// buffers; sub-checkpoint rows every `sub_k` rows go to sub + j * N.
+void forward_rows(chsga_ctx& c, SlotBufs& b, uint32_t len, int64_t a, int64_t b_row,
+                  int* matrix /* rows a..b, row a already present */) {
+  const size_t N = c.L.N;
+  // slot 0 at row a+1 of read 0
+  dev::SlotState s{0, len, (uint32_t)(a + 1), 0, 0};
+  CK(cudaMemcpyAsync(b.slots.p, &s, sizeof(s), cudaMemcpyHostToDevice, c.st));
+  dev::StepCtl ctl{};
+  ctl.q_count = 0;
+  CK(cudaMemcpyAsync(b.ctl.p, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, c.st));
+  unsigned long long inf = ~0ull;
+  CK(cudaMemcpyAsync(b.best.p, &inf, 8, cudaMemcpyHostToDevice, c.st));
+  CK(cudaStreamSynchronize(c.st));
+  launch_advance<1>(c, b, 1, c.st);
+  for (int64_t i = a + 1; i <= b_row; ++i)
+    row_step<1>(c, b, matrix + (size_t)(i - 1 - a) * N, matrix + (size_t)(i - a) * N, c.st);
+}
+
+void walk(chsga_ctx& c, const int* M, int64_t lo, int64_t hi, uint32_t start, uint32_t len,
+          std::vector<dev::WalkOp>& path, uint32_t* landing) {
+  const uint32_t max_ops = (uint32_t)(2 * (hi - lo) + 2 * (uint64_t)len + 16);
+  DevArr<dev::WalkOp> ops;
+  ops.alloc(max_ops);
+  DevArr<dev::WalkOut> out;
+  out.alloc(1);
+  dev::k_walk<<<1, 1, 0, c.st>>>(c.gp, M, lo, hi, start, c.reads.p, ops.p, max_ops, out.p);
+  check_launch();
+  dev::WalkOut h{};
+  CK(cudaMemcpyAsync(&h, out.p, sizeof(h), cudaMemcpyDeviceToHost, c.st));
+  CK(cudaStreamSynchronize(c.st));
+  if (h.status == 7)
+    fail(CHSGA_ERR_NO_PATH, "score-matrix traceback: no valid predecessor at row " +
+                                std::to_string(h.fail_row));
+  require(h.status == 0, CHSGA_ERR_INTERNAL, "traceback walk exceeded its op budget");
+  size_t old = path.size();
+  path.resize(old + h.nops);
+  if (h.nops)
+    CK(cudaMemcpy(path.data() + old, ops.p, h.nops * sizeof(dev::WalkOp), cudaMemcpyDeviceToHost));
+  *landing = h.vertex;
+}
+
+void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts* o,
+               chsga_tb_result* res) {
+  require(len > 0, CHSGA_ERR_INVALID_ARG, "traceback of an empty read");
+  const size_t N = c.L.N;
+  const int64_t k = (o && o->k > 0) ? o->k : 500;
+  const uint64_t cap = (o && o->cap_bytes) ? o->cap_bytes : c.cap;
+  const std::string dir = (o && o->dir) ? o->dir : "";
+  const bool keep = o && o->keep_files;
+  const char* rp[1] = {read};
+  upload_reads(c, rp, &len, 1);
+  SlotBufs& b = get_bufs<1>(c, false);
+  const uint64_t row_bytes = (uint64_t)N * 4;
+  const uint64_t store = (uint64_t)len * row_bytes;
+  std::vector<dev::WalkOp> path;
+  uint32_t best_v = 0;
+  int32_t best_s = 0;
+  auto harvest = [&]() {
+    CK(cudaStreamSynchronize(c.st));
+    CK(cudaMemcpy(&best_s, c.res_score.p, 4, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&best_v, c.res_vertex.p, 4, cudaMemcpyDeviceToHost));
+  };
+  res->checkpointed = 0;
+  res->num_checkpoints = 0;
+  if (store <= cap) {
+    // one spare row: row 0 reads no previous row, but its input pointer
+    // must not alias the row it writes
+    DevArr<int> M;
+    M.alloc((size_t)(len + 1) * N);
+    reset_slots<1>(c, b, 1);
+    launch_advance<1>(c, b, 0, c.st);
+    for (uint32_t i = 0; i < len; ++i)
+      row_step<1>(c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, c.st);
+    harvest();
+    uint32_t v = best_v;
+    if (len > 1) walk(c, M.p, 0, len - 1, best_v, len, path, &v);
+    path.push_back(dev::WalkOp{0, v, CHSGA_OP_MATCHSUB});
+  } else {
+    // forward with checkpoints every k rows (src/traceback.hpp:855-892)
+    res->checkpointed = 1;
+    const uint64_t nck = (len - 1) / (uint64_t)k + 1;
+    res->num_checkpoints = nck;
+    c.h_ckpt.alloc(nck * N);
+    DevArr<int> ring;
+    ring.alloc(3 * N);
+    cudaEvent_t done_ev[3];
+    for (auto& e : done_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    bool busy[3] = {false, false, false};
+    reset_slots<1>(c, b, 1);
+    launch_advance<1>(c, b, 0, c.st);
+    // three row buffers: the previous row, the row being computed, and a
+    // checkpoint row whose copy to pinned host memory may still be running
+    int prev = 1;
+    for (uint32_t i = 0; i < len; ++i) {
+      int cur = -1;
+      for (int j = 0; j < 3 && cur < 0; ++j)
+        if (j != prev && !busy[j]) cur = j;
+      if (cur < 0) {
+        cur = (prev + 1) % 3;
+        CK(cudaEventSynchronize(done_ev[cur]));
+        busy[cur] = false;
+      }
+      row_step<1>(c, b, ring.p + (size_t)prev * N, ring.p + (size_t)cur * N, c.st);
+      if (i % k == 0) {
+        cudaEvent_t ready;
+        CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        CK(cudaEventRecord(ready, c.st));
+        CK(cudaStreamWaitEvent(c.side, ready, 0));
+        CK(cudaMemcpyAsync(c.h_ckpt.p + (size_t)(i / k) * N, ring.p + (size_t)cur * N, row_bytes,
+                           cudaMemcpyDeviceToHost, c.side));
+        CK(cudaEventRecord(done_ev[cur], c.side));
+        busy[cur] = true;
+        cudaEventDestroy(ready);
+      }
+      prev = cur;
+    }
+    harvest();
+    CK(cudaStreamSynchronize(c.side));
+    for (auto& e : done_ev) cudaEventDestroy(e);
+    ring.release();
+    if (!dir.empty())
+      for (uint64_t j = 0; j < nck; ++j)
+        write_ckpt_row(dir, (int64_t)(j * k), c.h_ckpt.p + (size_t)j * N, N);
+    // backward, one segment at a time (src/traceback.hpp:945-1011)
+    int64_t cur_row = len - 1;
+    uint32_t cur_v = best_v;
+    const uint64_t budget = cap;
+    while (cur_row > 0) {
+      int64_t seg_start = (cur_row % k == 0) ? (cur_row - k) : (cur_row / k * k);
+      if (seg_start < 0) seg_start = 0;
+      const int64_t seg_end = cur_row;
+      const int* ck = c.h_ckpt.p + (size_t)(seg_start / k) * N;
+      const uint64_t rows = (uint64_t)(seg_end - seg_start + 1);
+      uint32_t landing = cur_v;
+      if (rows * row_bytes <= budget || rows <= 2) {
+        DevArr<int> seg;
+        seg.alloc(rows * N);
+        CK(cudaMemcpyAsync(seg.p, ck, row_bytes, cudaMemcpyHostToDevice, c.st));
+        forward_rows(c, b, len, seg_start, seg_end, seg.p);
+        walk(c, seg.p, seg_start, seg_end, cur_v, len, path, &landing);
+      } else {
+        // two levels: sub-checkpoints every k2 rows inside the segment
+        const uint64_t span = (uint64_t)(seg_end - seg_start);
+        const uint64_t k2 = std::max<uint64_t>(1, (uint64_t)std::ceil(std::sqrt((double)span)));
+        const uint64_t nsub = span / k2 + 1;
+        require((nsub + k2 + 1) * row_bytes <= budget, CHSGA_ERR_OOM,
+                "traceback segment does not fit the byte cap even with two-level checkpoints");
+        DevArr<int> sub, seg;
+        sub.alloc(nsub * N);
+        seg.alloc((k2 + 1) * N);
+        CK(cudaMemcpyAsync(sub.p, ck, row_bytes, cudaMemcpyHostToDevice, c.st));
+        // forward through the segment keeping rows seg_start + j*k2
+        CK(cudaMemcpyAsync(seg.p, ck, row_bytes, cudaMemcpyHostToDevice, c.st));
+        int64_t r0 = seg_start;
+        for (uint64_t j = 1; j < nsub; ++j) {
+          const int64_t r1 = seg_start + (int64_t)(j * k2);
+          forward_rows(c, b, len, r0, r1, seg.p);
+          CK(cudaMemcpyAsync(sub.p + j * N, seg.p + (size_t)(r1 - r0) * N, row_bytes,
+                             cudaMemcpyDeviceToDevice, c.st));
+          CK(cudaMemcpyAsync(seg.p, seg.p + (size_t)(r1 - r0) * N, row_bytes,
+                             cudaMemcpyDeviceToDevice, c.st));
+          r0 = r1;
+        }
+        int64_t row = seg_end;
+        uint32_t v = cur_v;
+        while (row > seg_start) {
+          int64_t s0 = seg_start + (int64_t)(((row - seg_start - 1) / (int64_t)k2) * (int64_t)k2);
+          CK(cudaMemcpyAsync(seg.p, sub.p + (size_t)((s0 - seg_start) / (int64_t)k2) * N, row_bytes,
+                             cudaMemcpyDeviceToDevice, c.st));
+          forward_rows(c, b, len, s0, row, seg.p);
+          uint32_t l2 = v;
+          walk(c, seg.p, s0, row, v, len, path, &l2);
+          v = l2;
+          row = s0;
+        }
+        landing = v;
+      }
+      if (!dir.empty() && !keep && seg_start > 0)
+        std::filesystem::remove(ckpt_row_path(dir, seg_start));
+      cur_row = seg_start;
+      cur_v = landing;
+    }
+    path.push_back(dev::WalkOp{0, cur_v, CHSGA_OP_MATCHSUB});
+    if (!dir.empty() && !keep) std::filesystem::remove(ckpt_row_path(dir, 0));
+  }
+  std::reverse(path.begin(), path.end());
+  res->num_ops = path.size();
+  res->ops = (chsga_op*)std::malloc(std::max<size_t>(1, path.size()) * sizeof(chsga_op));
+  require(res->ops != nullptr, CHSGA_ERR_OOM, "host out of memory");
+  for (size_t i = 0; i < path.size(); ++i) {
+    res->ops[i].row = path[i].row;
+    res->ops[i].vertex = path[i].vertex;
+    res->ops[i].op = (uint8_t)path[i].op;
+    std::memset(res->ops[i].pad, 0, 3);
+  }
+  res->score = best_s;
+}
+
+template <typename F>
+chsga_status guarded_ctx(chsga_ctx* c, F&& f) {
+  try {
+    if (c) set_device(*c);
+    f();
+    return CHSGA_OK;
+  } catch (const ChsgaError& e) {
+    if (c) c->err = e.what();
+    g_last_error = e.what();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    if (c) c->err = "host out of memory";
+    return CHSGA_ERR_OOM;
+  } catch (const std::exception& e) {
+    if (c) c->err = e.what();
+    g_last_error = e.what();
+    return CHSGA_ERR_INTERNAL;
+  }
+}
+
+}  // namespace
+}  // namespace chsga
+
+using namespace chsga;
+
+extern "C" {
+
+chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out) {
+  return guarded_ctx(nullptr, [&] {
+    require(out != nullptr, CHSGA_ERR_INVALID_ARG, "null output");
+    auto c = std::make_unique<chsga_ctx>();
+    c->device = opts ? opts->device : 0;
+    c->flags = opts ? opts->flags : 0;
+    int count = 0;
+    CK(cudaGetDeviceCount(&count));
+    require(c->device >= 0 && c->device < count, CHSGA_ERR_INVALID_ARG, "no such CUDA device");
+    CK(cudaSetDevice(c->device));
+    cudaDeviceProp prop{};
+    CK(cudaGetDeviceProperties(&prop, c->device));
+    require(prop.major >= 10, CHSGA_ERR_UNSUPPORTED,
+            std::string("libchsga is built for sm_100a; device is ") + prop.name);
+    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    c->cap = (opts && opts->hbm_cap_bytes) ? opts->hbm_cap_bytes : (uint64_t)(free_b * 0.85);
+    *out = c.release();
+  });
+}
+
+void chsga_close(chsga_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->st);
+  c->bufs.clear();
+  c->top.reset();
+  if (c->st) cudaStreamDestroy(c->st);
+  if (c->side) cudaStreamDestroy(c->side);
+  delete c;
+}
+
+const char* chsga_last_error(chsga_ctx* c) { return c ? c->err.c_str() : g_last_error.c_str(); }
+
+chsga_status chsga_load_graph(chsga_ctx* c, const chsga_graph_host* g) {
+  return guarded_ctx(c, [&] {
+    require(c && g, CHSGA_ERR_INVALID_ARG, "null argument");
+    upload_graph(*c, *g);
+  });
+}
+
+chsga_status chsga_load_host_graph(chsga_ctx* c, const chsga_host_graph* g) {
+  return guarded_ctx(c, [&] {
+    require(c && g, CHSGA_ERR_INVALID_ARG, "null argument");
+    validate_host_graph(*g);
+    chsga_graph_host v{};
+    require(chsga_graph_view(g, &v) == CHSGA_OK, CHSGA_ERR_INTERNAL, "graph view");
+    upload_graph(*c, v);
+  });
+}
+
+chsga_status chsga_align_scores(chsga_ctx* c, const char* const* reads, const uint32_t* lens,
+                                uint32_t n, int32_t* scores_out) {
+  return guarded_ctx(c, [&] {
+    require(c && (n == 0 || (reads && lens && scores_out)), CHSGA_ERR_INVALID_ARG, "null argument");
+    require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
+    scores_with<1>(*c, reads, lens, n, scores_out, true, 16);
+  });
+}
+
+chsga_status chsga_align_scores_batched(chsga_ctx* c, const char* const* reads,
+                                        const uint32_t* lens, uint32_t n,
+                                        const chsga_batch_opts* o, int32_t* scores_out) {
+  return guarded_ctx(c, [&] {
+    require(c && (n == 0 || (reads && lens && scores_out)), CHSGA_ERR_INVALID_ARG, "null argument");
+    require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
+    uint32_t slots = o && o->slots ? o->slots : 64;
+    const bool graphs = o ? o->use_graphs != 0 : true;
+    const uint32_t per = o && o->steps_per_graph ? o->steps_per_graph : 8;
+    switch (slots) {
+      case 1: scores_with<1>(*c, reads, lens, n, scores_out, graphs, per); break;
+      case 2: scores_with<2>(*c, reads, lens, n, scores_out, graphs, per); break;
+      case 4: scores_with<4>(*c, reads, lens, n, scores_out, graphs, per); break;
+      case 8: scores_with<8>(*c, reads, lens, n, scores_out, graphs, per); break;
+      case 16: scores_with<16>(*c, reads, lens, n, scores_out, graphs, per); break;
+      case 32: scores_with<32>(*c, reads, lens, n, scores_out, graphs, per); break;
+      case 64: scores_with<64>(*c, reads, lens, n, scores_out, graphs, per); break;
+      case 128: scores_with<128>(*c, reads, lens, n, scores_out, graphs, per); break;
+      default: fail(CHSGA_ERR_INVALID_ARG, "slots must be 1, 2, 4, 8, 16, 32, 64 or 128");
+    }
+  });
+}
+
+chsga_status chsga_align_rows(chsga_ctx* c, const char* read, uint32_t len, int32_t* rows_out) {
+  return guarded_ctx(c, [&] {
+    require(c && read && rows_out && len > 0, CHSGA_ERR_INVALID_ARG, "bad argument");
+    require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
+    const size_t N = c->L.N;
+    const char* rp[1] = {read};
+    upload_reads(*c, rp, &len, 1);
+    SlotBufs& b = get_bufs<1>(*c, false);
+    DevArr<int> M;
+    M.alloc((size_t)(len + 1) * N);
+    reset_slots<1>(*c, b, 1);
+    launch_advance<1>(*c, b, 0, c->st);
+    for (uint32_t i = 0; i < len; ++i)
+      row_step<1>(*c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, c->st);
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaMemcpy(rows_out, M.p, (size_t)len * N * 4, cudaMemcpyDeviceToHost));
+  });
+}
+
+chsga_status chsga_align_traceback(chsga_ctx* c, const char* read, uint32_t len,
+                                   const chsga_tb_opts* opts, chsga_tb_result* out) {
+  return guarded_ctx(c, [&] {
+    require(c && read && out, CHSGA_ERR_INVALID_ARG, "null argument");
+    require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
+    std::memset(out, 0, sizeof(*out));
+    traceback(*c, read, len, opts, out);
+  });
+}
+
+void chsga_tb_result_free(chsga_tb_result* r) {
+  if (!r) return;
+  std::free(r->ops);
+  r->ops = nullptr;
+  r->num_ops = 0;
+}
+
+uint64_t chsga_ops_to_cigar(const chsga_op* ops, uint64_t n, char* buf, uint64_t cap) {
+  std::string cig;
+  auto ch = [](uint8_t op) { return op == CHSGA_OP_DELETE ? 'D' : op == CHSGA_OP_MATCHSUB ? 'M' : 'I'; };
+  if (n > 0) {
+    char prev = ch(ops[0].op);
+    uint64_t run = 1;
+    for (uint64_t i = 1; i < n; ++i) {
+      char x = ch(ops[i].op);
+      if (x == prev) {
+        ++run;
+      } else {
+        cig += std::to_string(run);
+        cig += prev;
+        prev = x;
+        run = 1;
+      }
+    }
+    cig += std::to_string(run);
+    cig += prev;
+  }
+  if (buf && cap) {
+    size_t m = std::min<size_t>(cap - 1, cig.size());
+    std::memcpy(buf, cig.data(), m);
+    buf[m] = '\0';
+  }
+  return cig.size();
+}
+
+chsga_status chsga_get_profile(chsga_ctx* c, chsga_profile* out) {
+  return guarded_ctx(c, [&] {
+    require(c && out, CHSGA_ERR_INVALID_ARG, "null argument");
+    *out = c->prof;
+  });
+}
+
+}  // extern "C"

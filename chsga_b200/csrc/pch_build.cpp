@@ -1,0 +1,417 @@
+// Contraction hierarchy over the string graph, restating the build_pch tool
+// (src/CHoverrides/build_pch.cpp:6-131, src/CHoverrides/build_pch.hpp):
+//   preprocess       drop self loops and parallel edges      build_pch.hpp:181-228
+//   witness search   bounded Dijkstra; passing through a
+//                    vertex x costs len(x)-1 more (-v)       build_pch.hpp:230-394
+//   score            edge difference formula                 build_pch.hpp:396-478
+//   selection        vertices whose (score, degree, random
+//                    priority) beats every neighbour         build_pch.hpp:536-571
+//   contraction      shortcut a->b via u unless a strictly
+//                    shorter path exists, weight
+//                    w(a,u)+w(u,b)+len(u)-1; relevant arcs
+//                    become hierarchy edges; neighbours get
+//                    level max(level, level[u]+1)            build_pch.hpp:1012-1067
+//   order            rank by (component, level, id)          build_pch.hpp:1132-1220
+// The upstream builder runs on parlaylib with concurrent hash tables; this
+// one computes the same quantities with per-round snapshots (OpenMP), so
+// selection and contraction within a round see one consistent graph.
+#include <omp.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <limits>
+#include <numeric>
+#include <queue>
+
+#include "host_graph.hpp"
+
+namespace chsga {
+
+namespace {
+
+struct Arc {
+  uint32_t v;
+  uint32_t w;
+  uint32_t hop;
+};
+
+struct Shortcut {
+  uint32_t a, b, w, hop;
+};
+
+constexpr uint64_t kInf = std::numeric_limits<uint64_t>::max();
+
+class PchBuilder {
+ public:
+  PchBuilder(const HostCsr& g, const std::vector<uint64_t>& offs, const chsga_pch_opts& o)
+      : opt_(o), n_(g.n) {
+    use_len_ = o.use_label_lengths != 0;
+    if (use_len_) {
+      require(offs.size() == n_ + 1, CHSGA_ERR_INVALID_ARG, "label offsets size");
+      len_.resize(n_);
+      for (uint64_t i = 0; i < n_; ++i) len_[i] = offs[i + 1] - offs[i];
+    }
+    k_ = o.weight_bound ? o.weight_bound : kInf;
+    pop_limit_ = o.max_pop_count ? o.max_pop_count : 500;
+    // preprocess: sort (u, v, w), drop self loops and repeated (u, v)
+    std::vector<std::tuple<uint32_t, uint32_t, uint32_t>> el;
+    el.reserve(g.m);
+    for (uint64_t u = 0; u < n_; ++u)
+      for (uint64_t e = g.offset[u]; e < g.offset[u + 1]; ++e)
+        el.emplace_back((uint32_t)u, g.target[e], g.w(e));
+    std::sort(el.begin(), el.end());
+    out_.resize(n_);
+    in_.resize(n_);
+    for (size_t i = 0; i < el.size(); ++i) {
+      auto [u, v, w] = el[i];
+      if (u == v) continue;
+      if (i > 0 && std::get<0>(el[i - 1]) == u && std::get<1>(el[i - 1]) == v) continue;
+      out_[u].push_back({v, w, 1});
+      in_[v].push_back({u, w, 1});
+    }
+    base_edges_ = el;
+  }
+
+  HostPch build() {
+    auto t0 = std::chrono::steady_clock::now();
+    level_.assign(n_, 1);
+    removed_nbr_.assign(n_, 0);
+    contracted_.assign(n_, 0);
+    ed_.assign(n_, 0.f);
+    prio_.resize(n_);
+    std::iota(prio_.begin(), prio_.end(), 1);
+    {
+      Rng rng(opt_.seed ? opt_.seed : 0x5eed);
+      for (uint64_t i = n_; i > 1; --i) std::swap(prio_[i - 1], prio_[rng.below(i)]);
+    }
+    up_.resize(n_);
+    down_.resize(n_);
+    std::vector<uint32_t> remaining(n_);
+    std::iota(remaining.begin(), remaining.end(), 0);
+    const int nthreads = opt_.threads > 0 ? opt_.threads : omp_get_max_threads();
+    scratch_.resize(nthreads);
+    for (auto& s : scratch_) s.init(n_);
+    uint32_t round = 0;
+    while (!remaining.empty()) {
+      ++round;
+      const size_t R = remaining.size();
+      std::vector<std::vector<Shortcut>> cuts(R);
+      std::vector<std::vector<uint8_t>> in_rel(R);
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+      for (size_t i = 0; i < R; ++i)
+        score(remaining[i], cuts[i], in_rel[i], scratch_[omp_get_thread_num()]);
+      double bound = upper_bound(remaining, round);
+      std::vector<uint8_t> sel(R, 0);
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+      for (size_t i = 0; i < R; ++i) sel[i] = eligible(remaining[i], bound) ? 1 : 0;
+      std::vector<std::vector<uint8_t>> out_rel(R);
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+      for (size_t i = 0; i < R; ++i)
+        if (sel[i]) out_relevance(remaining[i], out_rel[i], scratch_[omp_get_thread_num()]);
+      size_t ncontracted = 0;
+      for (size_t i = 0; i < R; ++i)
+        if (sel[i]) {
+          contract(remaining[i], cuts[i], in_rel[i], out_rel[i]);
+          ++ncontracted;
+        }
+      require(ncontracted > 0, CHSGA_ERR_INTERNAL, "hierarchy build made no progress");
+      std::vector<uint32_t> next;
+      next.reserve(R - ncontracted);
+      for (uint32_t u : remaining)
+        if (!contracted_[u]) next.push_back(u);
+      if (opt_.print_detail)
+        std::printf("Round %u\nContract %zu vertices\nOverlay vertices number: %zu\n", round,
+                    ncontracted, R);
+      remaining.swap(next);
+    }
+    HostPch p = order();
+    double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (opt_.print_detail)
+      std::printf("G.n: %llu, G.m: %llu, G.rm: %llu, G.layer: %u, total_time: %f\n",
+                  (unsigned long long)p.n, (unsigned long long)p.m, (unsigned long long)p.rm,
+                  max_level_, sec);
+    return p;
+  }
+
+ private:
+  struct Scratch {
+    std::vector<uint64_t> dist;
+    std::vector<uint32_t> stamp;
+    uint32_t cur = 0;
+    std::vector<uint32_t> touched;
+    void init(uint64_t n) {
+      dist.assign(n, kInf);
+      stamp.assign(n, 0);
+    }
+    void reset() {
+      if (++cur == 0) {
+        std::fill(stamp.begin(), stamp.end(), 0);
+        cur = 1;
+      }
+    }
+    uint64_t get(uint32_t v) const { return stamp[v] == cur ? dist[v] : kInf; }
+    void set(uint32_t v, uint64_t d) {
+      stamp[v] = cur;
+      dist[v] = d;
+    }
+  };
+
+  uint64_t through(uint32_t x) const { return use_len_ ? len_[x] - 1 : 0; }
+
+  // Bounded Dijkstra from s over the current overlay (build_pch.hpp:230-394):
+  // the first hop costs the arc weight, every later hop also pays len-1 of
+  // the vertex it leaves; never re-enters s; at most pop_limit_ pops.
+  void search(uint32_t s, uint64_t bound, Scratch& sc) const {
+    sc.reset();
+    using T = std::pair<uint64_t, uint32_t>;
+    std::priority_queue<T, std::vector<T>, std::greater<T>> pq;
+    for (const Arc& a : out_[s]) {
+      if (a.w < sc.get(a.v)) {
+        sc.set(a.v, a.w);
+        pq.push({a.w, a.v});
+      }
+    }
+    uint32_t pops = 0;
+    while (!pq.empty() && pops < pop_limit_) {
+      auto [d, x] = pq.top();
+      if (d > bound) break;
+      pq.pop();
+      if (sc.get(x) < d) continue;
+      ++pops;
+      const uint64_t base = d + through(x);
+      for (const Arc& a : out_[x]) {
+        if (a.v == s) continue;
+        uint64_t nd = base + a.w;
+        if (nd < sc.get(a.v)) {
+          sc.set(a.v, nd);
+          pq.push({nd, a.v});
+        }
+      }
+    }
+  }
+
+  // Shortcuts contracting u would need, relevance of u's in-arcs, and the
+  // edge-difference score (build_pch.hpp:396-478, 1012-1045).
+  void score(uint32_t u, std::vector<Shortcut>& cuts, std::vector<uint8_t>& in_rel, Scratch& sc) {
+    const auto& in = in_[u];
+    const auto& out = out_[u];
+    in_rel.assign(in.size(), 1);
+    uint64_t max_out = 0;
+    for (const Arc& b : out) max_out = std::max<uint64_t>(max_out, b.w);
+    uint64_t added = 0, added_hop = 0;
+    for (size_t i = 0; i < in.size(); ++i) {
+      const Arc& a = in[i];
+      search(a.v, (uint64_t)a.w + through(u) + max_out, sc);
+      in_rel[i] = sc.get(u) >= a.w ? 1 : 0;
+      for (const Arc& b : out) {
+        if (b.v == a.v) continue;
+        uint64_t total = (uint64_t)a.w + b.w + through(u);
+        if (total <= k_ && sc.get(b.v) >= total) {
+          require(total < (1ull << 32), CHSGA_ERR_UNSUPPORTED, "shortcut weight overflow");
+          cuts.push_back({a.v, b.v, (uint32_t)total, a.hop + b.hop});
+          ++added;
+          added_hop += a.hop + b.hop;
+        }
+      }
+    }
+    if (in.empty() || out.empty()) {
+      ed_[u] = 0.f;
+      return;
+    }
+    const double removed_arc = 1.0 + (double)in.size() + (double)out.size();
+    double removed_hop = 1.0;
+    for (const Arc& a : in) removed_hop += a.hop;
+    for (const Arc& b : out) removed_hop += b.hop;
+    ed_[u] = (float)(1.0 + 500.0 * level_[u] +
+                     1000.0 * ((double)added + 0.2 * removed_nbr_[u]) / removed_arc +
+                     1000.0 * (double)added_hop / removed_hop + 10.0 * removed_arc);
+  }
+
+  // Relevance of u's out-arcs: kept unless a strictly shorter u->b path exists.
+  void out_relevance(uint32_t u, std::vector<uint8_t>& rel, Scratch& sc) {
+    const auto& out = out_[u];
+    rel.assign(out.size(), 1);
+    uint64_t max_out = 0;
+    for (const Arc& b : out) max_out = std::max<uint64_t>(max_out, b.w);
+    search(u, max_out, sc);
+    for (size_t i = 0; i < out.size(); ++i) rel[i] = sc.get(out[i].v) >= out[i].w ? 1 : 0;
+  }
+
+  double upper_bound(const std::vector<uint32_t>& rem, uint32_t round) const {
+    if (opt_.sample_bound >= 1.0 || opt_.sample_bound <= 0.0)
+      return std::numeric_limits<double>::max();
+    constexpr int kSamples = 150;  // EDGEDIFF_SAMPLES, build_pch.hpp:19
+    Rng rng((opt_.seed ? opt_.seed : 0x5eed) + round);
+    if (rem.size() < kSamples) return ed_[rem[rng.below(rem.size())]];
+    std::vector<double> s(kSamples + 1);
+    for (auto& x : s) x = ed_[rem[rng.below(rem.size())]];
+    std::sort(s.begin(), s.end());
+    return s[(size_t)(kSamples * opt_.sample_bound)];
+  }
+
+  bool eligible(uint32_t u, double bound) const {
+    if (ed_[u] > bound) return false;
+    const size_t du = in_[u].size() + out_[u].size();
+    auto beats = [&](uint32_t v) {
+      if (ed_[v] > bound) return false;
+      if (ed_[v] != ed_[u]) return ed_[v] < ed_[u];
+      const size_t dv = in_[v].size() + out_[v].size();
+      if (dv != du) return dv < du;
+      return prio_[v] < prio_[u];
+    };
+    for (const Arc& a : out_[u])
+      if (beats(a.v)) return false;
+    for (const Arc& a : in_[u])
+      if (beats(a.v)) return false;
+    return true;
+  }
+
+  static void erase_arc(std::vector<Arc>& v, uint32_t x) {
+    for (size_t i = 0; i < v.size(); ++i)
+      if (v[i].v == x) {
+        v[i] = v.back();
+        v.pop_back();
+        return;
+      }
+  }
+
+  void contract(uint32_t u, const std::vector<Shortcut>& cuts, const std::vector<uint8_t>& in_rel,
+                const std::vector<uint8_t>& out_rel) {
+    const uint32_t lu = level_[u] + 1;
+    for (size_t i = 0; i < out_[u].size(); ++i) {
+      const Arc& b = out_[u][i];
+      if (out_rel[i]) {
+        up_[u].push_back({b.v, b.w, b.hop});
+        level_[b.v] = std::max(level_[b.v], lu);
+        removed_nbr_[b.v]++;
+      }
+      erase_arc(in_[b.v], u);
+    }
+    for (size_t i = 0; i < in_[u].size(); ++i) {
+      const Arc& a = in_[u][i];
+      if (in_rel[i]) {
+        down_[u].push_back({a.v, a.w, a.hop});
+        level_[a.v] = std::max(level_[a.v], lu);
+        removed_nbr_[a.v]++;
+      }
+      erase_arc(out_[a.v], u);
+    }
+    for (const Shortcut& s : cuts) {
+      bool found = false;
+      for (Arc& x : out_[s.a])
+        if (x.v == s.b) {
+          found = true;
+          if (s.w < x.w) {
+            x.w = s.w;
+            x.hop = s.hop;
+            for (Arc& y : in_[s.b])
+              if (y.v == s.a) {
+                y.w = s.w;
+                y.hop = s.hop;
+              }
+          }
+          break;
+        }
+      if (!found) {
+        out_[s.a].push_back({s.b, s.w, s.hop});
+        in_[s.b].push_back({s.a, s.w, s.hop});
+      }
+    }
+    out_[u].clear();
+    out_[u].shrink_to_fit();
+    in_[u].clear();
+    in_[u].shrink_to_fit();
+    contracted_[u] = 1;
+  }
+
+  HostPch order() {
+    // connected components of the input graph, ignoring direction
+    std::vector<uint32_t> parent(n_);
+    std::iota(parent.begin(), parent.end(), 0);
+    auto find = [&](uint32_t x) {
+      while (parent[x] != x) x = parent[x] = parent[parent[x]];
+      return x;
+    };
+    for (auto& [u, v, w] : base_edges_) {
+      (void)w;
+      uint32_t a = find(u), b = find(v);
+      if (a != b) parent[std::max(a, b)] = std::min(a, b);
+    }
+    std::vector<uint32_t> cc(n_);
+    for (uint64_t i = 0; i < n_; ++i) cc[i] = find((uint32_t)i);
+    std::vector<uint32_t> ord(n_);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+      if (cc[a] != cc[b]) return cc[a] < cc[b];
+      if (level_[a] != level_[b]) return level_[a] < level_[b];
+      return a < b;
+    });
+    HostPch p;
+    p.present = true;
+    p.n = n_;
+    p.rank.resize(n_);
+    p.level.resize(n_);
+    for (uint64_t r = 0; r < n_; ++r) {
+      p.rank[ord[r]] = (uint32_t)r;
+      p.level[r] = level_[ord[r]];
+      max_level_ = std::max(max_level_, level_[ord[r]]);
+    }
+    for (uint64_t r = 0; r <= n_; ++r) {
+      bool cut = r == 0 || r == n_ || cc[ord[r]] != cc[ord[r - 1]] ||
+                 level_[ord[r]] != level_[ord[r - 1]];
+      if (cut) p.layer_offset.push_back((uint32_t)r);
+    }
+    for (size_t l = 0; l < p.layer_offset.size(); ++l) {
+      size_t L = p.layer_offset.size() - 1;
+      bool cut = l == 0 || l == L || cc[ord[p.layer_offset[l]]] != cc[ord[p.layer_offset[l - 1]]];
+      if (cut) p.cc_offset.push_back((uint32_t)l);
+    }
+    auto emit = [&](const std::vector<std::vector<Arc>>& lists, std::vector<uint64_t>& off,
+                    std::vector<uint32_t>& vv, std::vector<uint32_t>& ww) {
+      off.assign(n_ + 1, 0);
+      for (uint64_t r = 0; r < n_; ++r) off[r + 1] = off[r] + lists[ord[r]].size();
+      vv.resize(off[n_]);
+      ww.resize(off[n_]);
+      std::vector<std::pair<uint32_t, uint32_t>> tmp;
+      for (uint64_t r = 0; r < n_; ++r) {
+        tmp.clear();
+        for (const Arc& a : lists[ord[r]]) tmp.push_back({p.rank[a.v], a.w});
+        std::sort(tmp.begin(), tmp.end());
+        for (size_t i = 0; i < tmp.size(); ++i) {
+          vv[off[r] + i] = tmp[i].first;
+          ww[off[r] + i] = tmp[i].second;
+        }
+      }
+    };
+    emit(up_, p.up_offset, p.up_v, p.up_w);
+    emit(down_, p.down_offset, p.down_v, p.down_w);
+    p.m = p.up_v.size();
+    p.rm = p.down_v.size();
+    return p;
+  }
+
+  chsga_pch_opts opt_;
+  uint64_t n_;
+  bool use_len_ = false;
+  std::vector<uint64_t> len_;
+  uint64_t k_ = kInf;
+  uint32_t pop_limit_ = 500;
+  std::vector<std::tuple<uint32_t, uint32_t, uint32_t>> base_edges_;
+  std::vector<std::vector<Arc>> out_, in_, up_, down_;
+  std::vector<uint32_t> level_, removed_nbr_;
+  std::vector<uint8_t> contracted_;
+  std::vector<float> ed_;
+  std::vector<uint64_t> prio_;
+  std::vector<Scratch> scratch_;
+  uint32_t max_level_ = 0;
+};
+
+}  // namespace
+
+HostPch build_pch(const HostCsr& g, const std::vector<uint64_t>& offs, const chsga_pch_opts& o) {
+  PchBuilder b(g, offs, o);
+  return b.build();
+}
+
+}  // namespace chsga

@@ -1,0 +1,268 @@
+/*
+ * chsga.h - C-ABI of libchsga, a B200 (sm_100a) implementation of CHSGA's
+ * per-read sequence-to-graph alignment DP (ConSGA score-only and traceback).
+ *
+ * The reference is header-only C++ (src/align.hpp, src/traceback.hpp) driven
+ * by src/ConSGA.cpp and src/ConSGA_traceback.cpp. Each entry point below names
+ * the reference interface it replaces. Plain pointers and sizes only; no
+ * exception crosses this boundary: every call returns a chsga_status and the
+ * message of the last failure is kept per context (chsga_last_error) or per
+ * thread for calls without a context (chsga_last_error_global).
+ *
+ * Scoring is the reference's fixed mismatchN scheme: match 0, substitution 1,
+ * deletion 1, insertion 1 (src/ConSGA.cpp:216, src/ConSGA_traceback.cpp:128),
+ * int32 arithmetic. Naming follows the reference: DELETE consumes a read base
+ * and stays on the graph vertex, INSERT moves along graph edges in one row.
+ */
+#ifndef CHSGA_H
+#define CHSGA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t chsga_status;
+enum {
+  CHSGA_OK = 0,
+  CHSGA_ERR_INVALID_ARG = 1, /* bad pointer, size or option */
+  CHSGA_ERR_IO = 2,          /* file missing, unreadable or short */
+  CHSGA_ERR_FORMAT = 3,      /* file or array contents malformed */
+  CHSGA_ERR_CUDA = 4,        /* CUDA runtime error */
+  CHSGA_ERR_OOM = 5,         /* device memory or byte cap exceeded */
+  CHSGA_ERR_UNSUPPORTED = 6, /* input outside what the GPU path handles */
+  CHSGA_ERR_NO_PATH = 7,     /* traceback found no predecessor (src/traceback.hpp:571-575) */
+  CHSGA_ERR_TIMEOUT = 8,     /* a bounded device-side wait gave up */
+  CHSGA_ERR_INTERNAL = 9,
+  CHSGA_ERR_BUSY = 10        /* server queue full: retry after chsga_server_poll */
+};
+
+/* Backpointer / path operation codes, src/traceback.hpp:168-170. */
+enum { CHSGA_OP_DELETE = 0, CHSGA_OP_MATCHSUB = 1, CHSGA_OP_INSERT = 2 };
+
+/* ------------------------------------------------------------------------- */
+/* Host-side input description. These mirror what the reference drivers hold */
+/* after loading their files (src/ConSGA.cpp:154-206).                       */
+/* ------------------------------------------------------------------------- */
+
+/* Out-CSR of a graph as read by read_graph() from an AdjacencyGraph file. */
+typedef struct {
+  uint64_t n;             /* vertices */
+  uint64_t m;             /* edges */
+  const uint64_t* offset; /* n+1 */
+  const uint32_t* target; /* m */
+  const uint32_t* weight; /* m integer weights; NULL means every weight is 1 */
+} chsga_csr;
+
+/* The contraction hierarchy, rank-ordered as build_pch's setOrderedLayer()
+ * leaves it (src/CHoverrides/build_pch.hpp:1132-1220) and as align.hpp:279-345
+ * indexes it through PchQuery::GC. */
+typedef struct {
+  uint64_t n;                   /* string vertices */
+  uint64_t m;                   /* upward edges (GC.E) */
+  uint64_t rm;                  /* downward in-edges (GC.in_E) */
+  uint64_t num_layers;
+  uint64_t num_cc;
+  const uint32_t* rank;         /* n: rank of original string vertex i */
+  const uint32_t* level;        /* n: level, indexed by rank */
+  const uint32_t* layer_offset; /* num_layers+1: first rank of each (cc, level) layer */
+  const uint32_t* cc_offset;    /* num_cc+1: first layer of each connected component */
+  const uint64_t* up_offset;    /* n+1, by rank */
+  const uint32_t* up_v;         /* m: head rank of u -> v, v in a higher layer */
+  const uint32_t* up_w;         /* m */
+  const uint64_t* down_offset;  /* n+1, by rank */
+  const uint32_t* down_v;       /* rm: tail rank of v -> u, v in a higher layer */
+  const uint32_t* down_w;       /* rm */
+} chsga_pch;
+
+typedef struct {
+  uint64_t num_chars;             /* N = number of labels */
+  const char* labels;             /* N bytes: -l file with newlines removed */
+  chsga_csr char_graph;           /* -I: out-CSR over the N chars */
+  chsga_csr string_graph;         /* -i: out-CSR over the S string vertices */
+  const uint64_t* label_offsets;  /* -o: S+1 char offsets of each string vertex */
+  chsga_pch pch;                  /* -c: hierarchy over the string graph */
+} chsga_graph_host;
+
+/* ------------------------------------------------------------------------- */
+/* Host graph objects: file loading, synthetic generation, hierarchy build.  */
+/* ------------------------------------------------------------------------- */
+
+typedef struct chsga_host_graph chsga_host_graph;
+
+/* Loads the five input files of ConSGA (-I -i -c -l -o), src/ConSGA.cpp:154-197. */
+chsga_status chsga_graph_read_files(const char* char_adj, const char* string_adj,
+                                    const char* pch_file, const char* labels_file,
+                                    const char* label_offsets_file, chsga_host_graph** out);
+/* Borrowed view of the arrays (valid until chsga_graph_free). */
+chsga_status chsga_graph_view(const chsga_host_graph* g, chsga_graph_host* view);
+void chsga_graph_free(chsga_host_graph* g);
+
+/* Writes prefix + {".char.adj", ".string.adj", ".char.labels",
+ * ".string.label_offsets", ".string.out"} in the reference's layouts
+ * (src/csr_to_adj.cpp:46-114); ".string.out" is the hierarchy file. */
+chsga_status chsga_graph_write_files(const chsga_host_graph* g, const char* prefix);
+
+/* Seeded variant-bubble DAG (backbone + SNP / indel / alternative-allele
+ * bubbles, string vertices split to [vlen_min, vlen_max] chars). The char
+ * graph is the expansion of src/handlegraph_to_csr.cpp:165-247; ids are in
+ * topological order. No hierarchy is attached: call chsga_build_pch. */
+typedef struct {
+  uint64_t backbone_len;
+  uint64_t seed;
+  double bubble_gap_mean;  /* mean backbone distance between bubbles (geometric) */
+  double p_snp, p_indel, p_alt; /* bubble-type mixture, sums to 1 */
+  uint32_t indel_min, indel_max; /* indel allele length */
+  uint32_t alt_min, alt_max;     /* alternative-allele length (both branches) */
+  uint32_t vlen_min, vlen_max;   /* string vertex label length */
+} chsga_gen_graph_cfg;
+chsga_status chsga_gen_graph(const chsga_gen_graph_cfg* cfg, chsga_host_graph** out);
+
+/* Contraction hierarchy over the string graph, restating build_pch
+ * (src/CHoverrides/build_pch.cpp:6-131, build_pch.hpp:912-1341): witness
+ * search bounded by max_pop_count, shortcut weights w1+w2+len(mid)-1 when
+ * use_label_lengths (build_pch -v), levels max(level[nbr], level[u]+1),
+ * rank by (cc, level, id). Replaces any hierarchy already attached. */
+typedef struct {
+  uint32_t max_pop_count;   /* -p, default 500 */
+  double sample_bound;      /* -s, default 1 */
+  uint64_t weight_bound;    /* -k, 0 = unbounded */
+  int use_label_lengths;    /* -v given */
+  uint64_t seed;            /* contraction priority permutation */
+  int threads;              /* 0 = all */
+  int print_detail;         /* -d */
+} chsga_pch_opts;
+chsga_status chsga_build_pch(chsga_host_graph* g, const chsga_pch_opts* opts);
+
+/* Reads: the concatenated bases plus offsets. */
+typedef struct chsga_reads chsga_reads;
+/* FASTA/FASTQ (gzip or plain), bases upper-cased, at most max_reads records
+ * (0 = all). The reference caps at 5 (src/load_reads.hpp:5-40). */
+chsga_status chsga_reads_load(const char* path, uint64_t max_reads, chsga_reads** out);
+chsga_status chsga_reads_from_arrays(const char* data, const uint64_t* offsets, uint64_t n,
+                                     chsga_reads** out);
+uint64_t chsga_reads_count(const chsga_reads* r);
+const char* chsga_reads_data(const chsga_reads* r);
+const uint64_t* chsga_reads_offsets(const chsga_reads* r); /* count+1 */
+chsga_status chsga_reads_write_fasta(const chsga_reads* r, const char* path);
+void chsga_reads_free(chsga_reads* r);
+
+/* Seeded reads from random source-to-sink paths at uniform offsets, with
+ * substitutions, 1..indel_len_max indels and N bases. Lengths are fixed
+ * (len_min == len_max) or log-uniform in [len_min, len_max]. */
+typedef struct {
+  uint64_t count;
+  uint64_t seed;
+  uint32_t len_min, len_max;
+  double sub_rate, indel_rate, n_rate;
+  uint32_t indel_len_max;
+} chsga_gen_reads_cfg;
+chsga_status chsga_gen_reads(const chsga_host_graph* g, const chsga_gen_reads_cfg* cfg,
+                             chsga_reads** out);
+
+/* Graph statistics (for logs, the cost model and the benchmark). */
+typedef struct {
+  uint64_t num_chars, num_char_edges, num_strings, num_string_edges;
+  uint64_t pch_up_edges, pch_down_edges, pch_levels, pch_layers, pch_ccs;
+  uint64_t max_label_len, single_char_strings;
+} chsga_graph_stats;
+chsga_status chsga_graph_get_stats(const chsga_host_graph* g, chsga_graph_stats* out);
+
+const char* chsga_last_error_global(void);
+
+/* ------------------------------------------------------------------------- */
+/* Device context and alignment                                              */
+/* ------------------------------------------------------------------------- */
+
+typedef struct chsga_ctx chsga_ctx;
+
+typedef struct {
+  int device;              /* CUDA device ordinal */
+  uint64_t hbm_cap_bytes;  /* byte cap for the full score matrix; 0 = 85% of free HBM */
+  uint32_t flags;          /* CHSGA_FLAG_* */
+} chsga_opts;
+enum { CHSGA_FLAG_PROFILE = 1u /* per-phase CUDA-event timing into chsga_profile */ };
+
+/* Context with its own streams. One context per host thread. */
+chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out);
+void chsga_close(chsga_ctx* ctx);
+const char* chsga_last_error(chsga_ctx* ctx);
+
+/* Copies the graph and hierarchy to the device (the context owns the copies).
+ * Replaces the inputs of InCSR/build_in_csr (src/align.hpp:214-242), the
+ * rank->original map (src/ConSGA.cpp:203-206) and VertexLabelMapper. */
+chsga_status chsga_load_graph(chsga_ctx* ctx, const chsga_graph_host* g);
+chsga_status chsga_load_host_graph(chsga_ctx* ctx, const chsga_host_graph* g);
+
+/* Score-only, one read per launch sequence: align_combo<int> (src/align.hpp:470-531).
+ * scores_out[i] = min over the last row of read i. Reads of length 0 are rejected. */
+chsga_status chsga_align_scores(chsga_ctx* ctx, const char* const* reads, const uint32_t* lens,
+                                uint32_t n, int32_t* scores_out);
+
+/* Every final DP row of one read (after the graph-skip closure), row-major
+ * len x N int32: what align_read_combo leaves in edits_src after each row
+ * (src/align.hpp:430-463). For parity checks on small graphs. */
+chsga_status chsga_align_rows(chsga_ctx* ctx, const char* read, uint32_t len, int32_t* rows_out);
+
+/* Batched score-only: all reads through one slot-interleaved engine that
+ * advances up to `slots` reads together, row by row; finished slots are
+ * refilled on the device. No reference counterpart (the reference aligns
+ * reads serially, src/align.hpp:488); results equal chsga_align_scores. */
+typedef struct {
+  uint32_t slots;         /* reads advanced together: 1,2,4,8,16,32,64,128; 0 = autotune */
+  uint32_t steps_per_graph; /* row-steps captured per CUDA graph launch; 0 = default */
+  uint32_t use_graphs;    /* 1 = CUDA-graph capture of the row-step sequence */
+} chsga_batch_opts;
+chsga_status chsga_align_scores_batched(chsga_ctx* ctx, const char* const* reads,
+                                        const uint32_t* lens, uint32_t n,
+                                        const chsga_batch_opts* opts, int32_t* scores_out);
+
+/* Traceback of one read: align_read_with_traceback<int> (src/traceback.hpp:588-1031).
+ * If len x N x 4 bytes fit under the byte cap the full score matrix stays in
+ * HBM and the path is walked by score equality (src/traceback.hpp:483-586);
+ * otherwise rows 0, k, 2k, ... are copied to pinned host memory and segments
+ * are recomputed on the device before the walk. */
+typedef struct {
+  int64_t k;              /* checkpoint interval, default 500 (-k) */
+  const char* dir;        /* if non-NULL, checkpoint rows are also written as
+                             dir/row_<i>.bin (src/traceback.hpp:215-227) */
+  int keep_files;         /* 0: erase row files after use, like cleanup=true */
+  uint64_t cap_bytes;     /* 0: context cap; forces the checkpointed path when small */
+} chsga_tb_opts;
+
+typedef struct {
+  int64_t row;      /* read position; INSERT keeps the row */
+  uint32_t vertex;  /* char index */
+  uint8_t op;       /* CHSGA_OP_* */
+  uint8_t pad[3];
+} chsga_op;         /* AlignOp, src/traceback.hpp:185-189 */
+
+typedef struct {
+  chsga_op* ops;      /* forward order, owned by the library */
+  uint64_t num_ops;
+  int32_t score;      /* min over the last row */
+  uint32_t checkpointed; /* 1 if the checkpointed path ran */
+  uint64_t num_checkpoints;
+} chsga_tb_result;
+chsga_status chsga_align_traceback(chsga_ctx* ctx, const char* read, uint32_t len,
+                                   const chsga_tb_opts* opts, chsga_tb_result* out);
+void chsga_tb_result_free(chsga_tb_result* r);
+
+/* ops_to_cigar (src/traceback.hpp:1081-1110): run-length string with D
+ * (DELETE), M (MATCHSUB), I (INSERT). Writes at most cap bytes including the
+ * terminator; returns the full length needed (excluding the terminator). */
+uint64_t chsga_ops_to_cigar(const chsga_op* ops, uint64_t n, char* buf, uint64_t cap);
+
+/* Per-phase device time of the last call (CHSGA_FLAG_PROFILE), in ms. */
+typedef struct {
+  double row_ms, sweep_up_ms, top_ms, sweep_down_ms, other_ms, total_ms;
+  uint64_t rows, launches;
+} chsga_profile;
+chsga_status chsga_get_profile(chsga_ctx* ctx, chsga_profile* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHSGA_H */

@@ -1,0 +1,64 @@
+"""Shared fixtures. GPU tests are marked ``gpu``; everything else runs on CPU.
+
+Small graphs are generated with the library's seeded generator and written
+to a temporary directory in the reference's file formats, so the CPU oracle
+(oracle/), the reference's own code compiled against its stand-in interfaces
+(oracle/_ref) and the GPU path all read the same five input files.
+"""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+def _ensure_built():
+    lib = os.path.join(ROOT, "chsga_b200", "lib", "libchsga.so")
+    orc = os.path.join(ROOT, "oracle", "bin", "libconsga_oracle.so")
+    if not (os.path.exists(lib) and os.path.exists(orc)):
+        import __graft_entry__
+        __graft_entry__.build()
+
+
+_ensure_built()
+
+import chsga_b200 as cb  # noqa: E402
+import oracle as orc  # noqa: E402
+
+
+def gen_graph(tmpdir, name, **over):
+    cfg = dict(cb.GRAPH_CONFIGS["cfg1"])
+    cfg.update(over)
+    g = cb.HostGraph.generate(**cfg)
+    g.build_pch()
+    files = g.write_files(os.path.join(str(tmpdir), name))
+    return g, files
+
+
+@pytest.fixture(scope="session")
+def small_graph(tmp_path_factory):
+    """cfg1 mix on a 20 kbp backbone: ~20k chars, ~1.7k string vertices."""
+    d = tmp_path_factory.mktemp("small")
+    g, files = gen_graph(d, "g", backbone_len=20_000, seed=11)
+    reads = g.gen_reads(24, 5, 150, sub_rate=0.01, indel_rate=0.003, n_rate=0.001).to_list()
+    return g, files, reads
+
+
+@pytest.fixture(scope="session")
+def oracle_small(small_graph):
+    return orc.Oracle(small_graph[1])
+
+
+def gpu_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False

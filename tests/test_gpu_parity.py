@@ -1,0 +1,111 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the CPU oracle.
+
+Integer DP, so every comparison is exact (bit-for-bit int32)."""
+import os
+
+import numpy as np
+import pytest
+
+import chsga_b200 as cb
+import oracle as orc
+from conftest import gen_graph
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx_small(small_graph):
+    g, files, reads = small_graph
+    ctx = cb.Context(0)
+    ctx.load(g)
+    yield ctx
+    ctx.close()
+
+
+def test_scores_plain_match_oracle(small_graph, ctx_small, oracle_small):
+    g, files, reads = small_graph
+    want = oracle_small.scores(reads)
+    got = ctx_small.align_scores(reads)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_every_row_matches_oracle(small_graph, ctx_small, oracle_small):
+    g, files, reads = small_graph
+    for rd in reads[:3]:
+        want = oracle_small.rows(rd)
+        got = ctx_small.align_rows(rd, oracle_small.num_chars)
+        np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("slots", [2, 8, 32, 64, 128])
+def test_batched_matches_plain(small_graph, ctx_small, oracle_small, slots):
+    g, files, reads = small_graph
+    want = oracle_small.scores(reads)
+    got = ctx_small.align_scores_batched(reads, slots=slots)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_batched_uneven_lengths(small_graph, ctx_small, oracle_small):
+    g, files, _ = small_graph
+    reads = g.gen_reads(40, 9, 1, 400, sub_rate=0.03, indel_rate=0.02).to_list()
+    want = oracle_small.scores(reads)
+    for slots, graphs in ((16, True), (64, False)):
+        got = ctx_small.align_scores_batched(reads, slots=slots, use_graphs=graphs)
+        np.testing.assert_array_equal(got, want)
+
+
+def test_traceback_full_matrix(small_graph, ctx_small, oracle_small):
+    g, files, reads = small_graph
+    labels = open(files[3], "rb").read().replace(b"\n", b"")
+    want = oracle_small.scores(reads[:6])
+    for rd, w in zip(reads[:6], want):
+        ops, score, ck = ctx_small.align_traceback(rd)
+        assert not ck
+        assert score == w
+        ps, last = orc.rescore(ops, rd, labels)
+        assert ps == w and last == len(rd) - 1
+
+
+def test_traceback_checkpointed(small_graph, ctx_small, oracle_small, tmp_path):
+    g, files, reads = small_graph
+    labels = open(files[3], "rb").read().replace(b"\n", b"")
+    rd = reads[0]
+    want = int(oracle_small.scores([rd])[0])
+    n = oracle_small.num_chars
+    # cap below the full matrix forces checkpoints; k=40 gives 4 segments
+    ops, score, ck = ctx_small.align_traceback(rd, k=40, ckpt_dir=str(tmp_path / "ck"),
+                                               keep_files=True, cap_bytes=60 * n * 4)
+    assert ck and score == want
+    ps, last = orc.rescore(ops, rd, labels)
+    assert ps == want and last == len(rd) - 1
+    rows = oracle_small.rows(rd)
+    for i in range(0, len(rd), 40):
+        got = np.fromfile(str(tmp_path / "ck" / f"row_{i}.bin"), dtype=np.int32)
+        np.testing.assert_array_equal(got, rows[i])
+
+
+def test_traceback_two_level(small_graph, ctx_small, oracle_small):
+    g, files, reads = small_graph
+    labels = open(files[3], "rb").read().replace(b"\n", b"")
+    rd = reads[1]
+    want = int(oracle_small.scores([rd])[0])
+    n = oracle_small.num_chars
+    # a segment of 100 rows does not fit 40 rows: sub-checkpoints inside it
+    ops, score, ck = ctx_small.align_traceback(rd, k=100, cap_bytes=40 * n * 4)
+    assert ck and score == want
+    ps, last = orc.rescore(ops, rd, labels)
+    assert ps == want and last == len(rd) - 1
+
+
+@pytest.mark.parametrize("seed,vmax", [(21, 1), (22, 3), (23, 32)])
+def test_random_graphs(tmp_path, seed, vmax):
+    g, files = gen_graph(tmp_path, f"r{seed}", backbone_len=3000, seed=seed, vlen_max=vmax,
+                         bubble_gap_mean=8.0, p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=2,
+                         alt_max=40)
+    reads = g.gen_reads(12, seed, 20, 120, sub_rate=0.05, indel_rate=0.05, n_rate=0.01).to_list()
+    o = orc.Oracle(files)
+    want = o.scores(reads)
+    ctx = cb.Context(0).load(g)
+    np.testing.assert_array_equal(ctx.align_scores(reads), want)
+    np.testing.assert_array_equal(ctx.align_scores_batched(reads, slots=4), want)
+    ctx.close()
