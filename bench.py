@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the batched ConSGA alignment engine (libchsga) on one B200.
+
+Workload (the batched-engine configuration): the config-2 variant-bubble DAG
+(5 Mbp random ACGT backbone, a bubble every ~50 bp: 70% SNP, 20% 1-20 bp
+indel, 10% 50-300 bp alternative allele; string vertices of 1-32 chars) and
+reads with lengths log-uniform in [150, 10000] at 5% error (60% indels, 40%
+substitutions), all generated with fixed seeds (synthetic stand-ins; the
+reference ships no datasets). A step aligns one batch of --batch reads to
+completion through the slot-interleaved engine (score-only, int32).
+
+  value   GCUPS over the K timed steps: sum(read_len * num_chars) / device
+          time (CUDA events around the device sequence, reads resident)
+  e2e     the same cells / wall time of chsga_align_scores_batched with host
+          buffers (read upload and score download inside), barrier + sync
+          on both sides, max over ranks
+The score rows of one step (slots x 25.5 MB per row buffer) exceed the 126 MB
+L2, so no flush is needed between steps.
+
+--impl reference times the reference's own CPU code (src/align.hpp's
+align_combo compiled in oracle/_ref) on the host cores for the same workload,
+one bounded sample of reads per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GCUPS on 1 B200 (batched+served vs plain per-read GPU), p50/p99 read latency"
+WORKLOAD = ("config-2 graph (5 Mbp backbone, bubble every ~50 bp) with reads log-uniform "
+            "150-10000 bp at 5% ONT-like error (the batched-engine configuration)")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="chsga", choices=["chsga", "reference"])
+    p.add_argument("--batch", type=int, default=512, help="reads per step")
+    p.add_argument("--slots", type=int, default=128)
+    p.add_argument("--warmup-batch", type=int, default=128,
+                   help="reads per warm-up step (lengths capped at 1 kbp)")
+    p.add_argument("--no-profile", action="store_true")
+    p.add_argument("--cpu-sample-s", type=float, default=15.0)
+    return p.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9
+                          for i in range(4) if r[5 + i].strip().lower() == "active"})
+        load = [s for s in sm if mx and s > 0.3 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def make_graph():
+    import chsga_b200 as cb
+    g = cb.HostGraph.generate(**cb.GRAPH_CONFIGS["cfg2"])
+    g.build_pch()
+    return g
+
+
+def make_reads(g, n, seed, len_max=10000):
+    # 5% error, 60% indels / 40% substitutions
+    return g.gen_reads(n, seed, 150, len_max, sub_rate=0.02, indel_rate=0.03, n_rate=0.0,
+                       indel_len_max=3).to_list()
+
+
+def algorithmic_row_bytes(st, slots, multi):
+    """Bytes one k_row launch must move: the previous and the new score of
+    every char for every slot (8 N R), the first/last boundary scores of
+    every vertex (4 R (S + S_multi)), 2-bit labels plus the special-char map
+    (3N/8), three words per vertex (offset, hierarchy position, in-edge
+    offset: 12 S) and the in-edges of first chars (4 E_first)."""
+    N, S = st["num_chars"], st["num_strings"]
+    e_first = st["num_char_edges"] - (N - S)
+    return 8 * N * slots + 4 * slots * (S + multi) + 3 * N / 8 + 12 * S + 4 * e_first
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    p = os.path.join(ROOT, "profiles", "k_row_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline(g, reads, budget_s):
+    """The reference's own align_combo (oracle/_ref) on the host cores, on a
+    bounded sample of the workload's reads (shortest first, until about
+    budget_s seconds of CPU work)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    st = g.stats()
+    N = st["num_chars"]
+    with tempfile.TemporaryDirectory() as d:
+        files = g.write_files(os.path.join(d, "g"))
+        if oracle.ref_available():
+            h, kind = oracle.RefHarness(files), "reference"
+        else:
+            h, kind = oracle.Oracle(files), "port"
+        cores = os.cpu_count()
+        sample = sorted(reads, key=len)
+        # calibrate on one short read, then size the sample to the budget
+        t = time.time()
+        h.scores([sample[0]])
+        per_cell = (time.time() - t) / (len(sample[0]) * N)
+        picked, est = [], 0.0
+        for r in sample:
+            c = per_cell * len(r) * N
+            if picked and est + c > budget_s:
+                break
+            picked.append(r)
+            est += c
+        t = time.time()
+        h.scores(picked)
+        dt = time.time() - t
+    cells = sum(len(r) for r in picked) * N
+    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": cores, "kind": kind,
+            "sample": f"{len(picked)} reads ({sum(len(r) for r in picked)} bases) of the workload, "
+                      f"shortest first, {dt:.1f} s on {cores} host threads"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    g = make_graph()
+    st = g.stats()
+    N = st["num_chars"]
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    with tempfile.TemporaryDirectory() as d:
+        files = g.write_files(os.path.join(d, "g"))
+        kind = "reference" if oracle.ref_available() else "port"
+        h = oracle.RefHarness(files) if kind == "reference" else oracle.Oracle(files)
+        cores = os.cpu_count()
+        # each step: the shortest reads of that step's batch until ~budget seconds
+        budget = max(2.0, min(20.0, args.cpu_sample_s))
+        t = time.time()
+        probe = sorted(make_reads(g, 8, 999), key=len)[0]
+        h.scores([probe])
+        per_cell = (time.time() - t) / (len(probe) * N)
+        samples = []
+        for s in range(args.warmup + args.steps):
+            reads = sorted(make_reads(g, 64, 1000 + s), key=len)
+            pick, est = [], 0.0
+            for r in reads:
+                c = per_cell * len(r) * N
+                if pick and est + c > budget:
+                    break
+                pick.append(r)
+                est += c
+            samples.append(pick)
+        for s in range(args.warmup):
+            h.scores(samples[s])
+        cells, tt = 0, 0.0
+        for s in range(args.warmup, args.warmup + args.steps):
+            t = time.time()
+            h.scores(samples[s])
+            tt += time.time() - t
+            cells += sum(len(r) for r in samples[s]) * N
+    v = cells / tt / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "num_chars": N, "batch": "bounded CPU sample per step"},
+        "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": cores, "kind": kind,
+                         "sample": f"per step the shortest reads of a 64-read batch up to "
+                                   f"~{budget:.0f} s of CPU work, {cores} host threads"},
+        "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    import numpy as np
+
+    import chsga_b200 as cb
+    g = make_graph()
+    st = g.stats()
+    N = st["num_chars"]
+    multi = st["num_strings"] - st["single_char_strings"]
+    ctx = cb.Context(local)
+    ctx.load(g)
+    wb = args.warmup_batch or args.batch
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    from chsga_b200 import replicas
+
+    def max_over_ranks(x):
+        return replicas.max_over_ranks(x, ws, device=f"cuda:{local}")
+
+    # warm-up: full passes of the engine (CUDA-graph instantiation, caches) on
+    # batches of the same distribution capped at 1 kbp, so a warm-up step is
+    # not held up by one 10 kbp read
+    for w in range(args.warmup):
+        reads = make_reads(g, wb, 50_000 + 1000 * rank + w, len_max=1000)
+        ctx.align_scores_batched(reads, slots=args.slots)
+    batches = [make_reads(g, args.batch, 1000 * rank + s) for s in range(args.steps)]
+    cells = sum(len(r) for b in batches for r in b) * N
+    h2d = sum(len(r) for b in batches for r in b) // args.steps + 16 * args.batch
+    d2h = 4 * args.batch
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    dev_ms, lat, launches, steps_work = 0.0, [], 0, 0
+    t0 = time.perf_counter()
+    for b in batches:
+        ctx.align_scores_batched(b, slots=args.slots)
+        p = ctx.profile()
+        dev_ms += p["total_ms"]
+        launches += int(p["launches"])
+        steps_work += int(p["steps"])
+        a, d = ctx.read_times(len(b))
+        lat.extend(((d - a).astype(np.float64) / 1e6).tolist())
+    wall = time.perf_counter() - t0
+    barrier()
+    ck = clocks.stop()
+    dev_s = max_over_ranks(dev_ms / 1e3)
+    wall_s = max_over_ranks(wall)
+    total_cells = cells * ws
+    value = total_cells / dev_s / 1e9
+    e2e = total_cells / wall_s / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "num_chars": N, "num_strings": st["num_strings"],
+                   "hierarchy_levels": st["pch_levels"], "batch_reads": args.batch,
+                   "slots": args.slots, "parallelism": f"replicas x{ws}",
+                   "l2": "score rows exceed L2 (no flush needed)"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "what": "device admission-to-completion per read"},
+        "e2e": {"value": e2e, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": ck,
+    }
+    if rank == 0:
+        # plain one-read-per-launch path on a sample of the first batch
+        sample = sorted(batches[0], key=len)[: max(2, min(6, len(batches[0])))]
+        ctx.align_scores(sample)
+        pp = ctx.profile()
+        pc = sum(len(r) for r in sample) * N
+        line["plain"] = {"value": pc / (pp["total_ms"] / 1e3) / 1e9, "unit": "GCUPS",
+                         "sample": f"{len(sample)} shortest reads of the first batch"}
+        line["batched_over_plain"] = value / line["plain"]["value"]
+    if rank == 0 and not args.no_profile:
+        # profiled pass: CUDA events around every kernel group of every row-step
+        pctx = cb.Context(local, flags=cb.FLAG_PROFILE)
+        pctx.load(g)
+        sample = make_reads(g, args.slots, 77_777, len_max=1000)
+        pctx.align_scores_batched(sample, slots=args.slots)
+        pr = pctx.profile()
+        pctx.close()
+        row_avg_s = pr["row_ms"] / max(1, pr["row_launches"]) / 1e3
+        peak, src = measured_peak()
+        ab = algorithmic_row_bytes(st, args.slots, multi)
+        tr = ncu_traffic()
+        total = pr["row_ms"] + pr["sweep_up_ms"] + pr["top_ms"] + pr["sweep_down_ms"] + pr["other_ms"]
+        line["roofline"] = {
+            "bound": "hbm", "kernel": f"k_row<{args.slots}>",
+            "achieved": ab / row_avg_s / 1e9, "peak": peak, "unit": "GB/s",
+            "frac": ab / row_avg_s / 1e9 / peak, "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)"
+            if src == "measured" else "fallback 6.65 TB/s",
+            "algorithmic_bytes_per_launch": ab, "avg_launch_ms": row_avg_s * 1e3,
+            "traffic": tr.get("bytes_per_launch_scaled") if tr else None,
+            "traffic_source": tr.get("source") if tr else None,
+            "kernel_share": {k: pr[k] / total for k in
+                             ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")},
+        }
+        line["cpu_baseline"] = cpu_baseline(g, batches[0], args.cpu_sample_s)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

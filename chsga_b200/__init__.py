@@ -29,6 +29,7 @@ _lib = C.CDLL(LIB_PATH)
 OK, ERR_INVALID_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, \
     ERR_NO_PATH, ERR_TIMEOUT, ERR_INTERNAL, ERR_BUSY = range(11)
 OP_DELETE, OP_MATCHSUB, OP_INSERT = 0, 1, 2
+FLAG_PROFILE = 1
 
 u64p = C.POINTER(C.c_uint64)
 u32p = C.POINTER(C.c_uint32)
@@ -112,7 +113,8 @@ class TbResult(C.Structure):
 class ProfileT(C.Structure):
     _fields_ = [("row_ms", C.c_double), ("sweep_up_ms", C.c_double), ("top_ms", C.c_double),
                 ("sweep_down_ms", C.c_double), ("other_ms", C.c_double), ("total_ms", C.c_double),
-                ("rows", C.c_uint64), ("launches", C.c_uint64)]
+                ("rows", C.c_uint64), ("steps", C.c_uint64), ("launches", C.c_uint64),
+                ("row_launches", C.c_uint64)]
 
 
 def _sig(name, res, *args):
@@ -154,6 +156,7 @@ _sig("chsga_align_traceback", C.c_int32, vp, C.c_char_p, C.c_uint32, C.POINTER(T
 _sig("chsga_tb_result_free", None, C.POINTER(TbResult))
 _sig("chsga_ops_to_cigar", C.c_uint64, C.POINTER(OpT), C.c_uint64, C.c_char_p, C.c_uint64)
 _sig("chsga_get_profile", C.c_int32, vp, C.POINTER(ProfileT))
+_sig("chsga_get_read_times", C.c_int32, vp, u64p, u64p, C.c_uint32)
 
 
 def _check(status: int, ctx=None):
@@ -358,6 +361,13 @@ class Context:
             return ops, int(r.score), bool(r.checkpointed)
         finally:
             _lib.chsga_tb_result_free(C.byref(r))
+
+    def read_times(self, n: int):
+        """(admit_ns, done_ns) per non-empty read of the last score call."""
+        a = np.zeros(n, dtype=np.uint64)
+        d = np.zeros(n, dtype=np.uint64)
+        self._ck(_lib.chsga_get_read_times(self._h, a.ctypes.data_as(u64p), d.ctypes.data_as(u64p), n))
+        return a, d
 
     def profile(self) -> dict:
         p = ProfileT()

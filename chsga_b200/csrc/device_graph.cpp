@@ -58,6 +58,8 @@ HostLayout build_layout(const chsga_graph_host& g) {
   for (uint32_t s = 0; s < S; ++s) {
     require(L.sv_off[s] < L.sv_off[s + 1], CHSGA_ERR_UNSUPPORTED,
             "string vertex " + std::to_string(s) + " has an empty label");
+    require(L.sv_off[s + 1] - L.sv_off[s] < (1u << 29), CHSGA_ERR_UNSUPPORTED,
+            "string vertex labels must be shorter than 2^29 chars");
     for (uint32_t c = L.sv_off[s]; c < L.sv_off[s + 1]; ++c) vertex_of[c] = s;
   }
   const chsga_csr& cg = g.char_graph;
@@ -150,6 +152,11 @@ HostLayout build_layout(const chsga_graph_host& g) {
   }
   L.sv_dev.resize(S);
   for (uint32_t s = 0; s < S; ++s) L.sv_dev[s] = dev[p.rank[s]];
+  L.vin_fix.resize(L.vin_src.size());
+  for (size_t k = 0; k < L.vin_src.size(); ++k) {
+    const uint32_t sv = L.vin_srcv[k];
+    L.vin_fix[k] = {(int32_t)L.sv_dev[sv], (int32_t)(L.vin_src[k] - L.sv_off[sv])};
+  }
   auto bv_last = [&](uint32_t rank) { return 2 * dev[rank] + (L.dv_len[dev[rank]] > 1 ? 1 : 0); };
   // pull lists
   std::vector<std::vector<EdgeW>> up(S), dn(S);
@@ -208,37 +215,47 @@ HostLayout build_layout(const chsga_graph_host& g) {
   return L;
 }
 
-HostTop build_top(const HostLayout& L, uint32_t max_vertices) {
+HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edges) {
+  require(max_vertices < 32768 && chunk_edges >= 2 && chunk_edges % 2 == 0, CHSGA_ERR_INTERNAL,
+          "top region limits");
   HostTop t;
   uint32_t first = L.levels;
   while (first > 0 && L.S - L.lvl_off[first - 1] <= max_vertices) --first;
   t.first_level = first;
   t.K0 = L.lvl_off[first];
   t.K = L.S - t.K0;
-  for (uint32_t l = first; l <= L.levels; ++l) t.lvl_off.push_back(L.lvl_off[l] - t.K0);
   t.upg_off.assign(t.K + 1, 0);
-  t.upl_off.assign(t.K + 1, 0);
-  t.dn_off.assign(t.K + 1, 0);
   const int32_t lo = (int32_t)(2 * t.K0);
   for (uint32_t j = 0; j < t.K; ++j) {
     const uint32_t d = t.K0 + j;
-    for (uint32_t e = L.up_off[d]; e < L.up_off[d + 1]; ++e) {
-      const EdgeW x = L.up_in[e];
-      if (x.src < lo) {
-        t.upg.push_back(x);
-      } else {
-        t.upl.push_back({x.src - lo, x.w});
+    for (uint32_t e = L.up_off[d]; e < L.up_off[d + 1]; ++e)
+      if (L.up_in[e].src < lo) t.upg.push_back(L.up_in[e]);
+    t.upg_off[j + 1] = (uint32_t)t.upg.size();
+  }
+  const EdgeW pad{(int32_t)(t.K << 16), 0};  // scratch target K, source 0
+  auto emit_level = [&](uint32_t l, bool up) {
+    std::vector<EdgeW> es;
+    for (uint32_t d = L.lvl_off[l]; d < L.lvl_off[l + 1]; ++d) {
+      const uint32_t j = d - t.K0;
+      const auto& off = up ? L.up_off : L.dn_off;
+      const auto& in = up ? L.up_in : L.dn_in;
+      for (uint32_t e = off[d]; e < off[d + 1]; ++e) {
+        if (in[e].src < lo) {
+          require(up, CHSGA_ERR_INTERNAL, "downward edge into the top region from below");
+          continue;  // applied by the grid-wide pull
+        }
+        es.push_back({(int32_t)((j << 16) | (uint32_t)(in[e].src - lo)), in[e].w});
       }
     }
-    for (uint32_t e = L.dn_off[d]; e < L.dn_off[d + 1]; ++e) {
-      const EdgeW x = L.dn_in[e];
-      require(x.src >= lo, CHSGA_ERR_INTERNAL, "downward edge into the top region from below");
-      t.dn.push_back({x.src - lo, x.w});
+    for (size_t i = 0; i < es.size(); i += chunk_edges) {
+      const size_t n = std::min<size_t>(chunk_edges, es.size() - i);
+      t.chunks.push_back({(int32_t)t.sched.size(), (int32_t)(n + (n & 1))});
+      t.sched.insert(t.sched.end(), es.begin() + i, es.begin() + i + n);
+      if (n & 1) t.sched.push_back(pad);
     }
-    t.upg_off[j + 1] = (uint32_t)t.upg.size();
-    t.upl_off[j + 1] = (uint32_t)t.upl.size();
-    t.dn_off[j + 1] = (uint32_t)t.dn.size();
-  }
+  };
+  for (uint32_t l = first; l < L.levels; ++l) emit_level(l, true);
+  for (uint32_t l = L.levels; l-- > first;) emit_level(l, false);
   return t;
 }
 

@@ -50,6 +50,7 @@ struct HostLayout {
   std::vector<uint32_t> lab2;   // ceil(N/16) words
   std::vector<uint32_t> lab_sp; // ceil(N/32) words
   std::vector<uint32_t> sv_off, sv_dev, vin_off, vin_src, vin_srcv;
+  std::vector<EdgeW> vin_fix;  // {hierarchy position of vertex(src), src - first(vertex(src))}
   std::vector<uint32_t> dv_first, dv_len;  // by hierarchy order
   std::vector<uint32_t> up_off, dn_off;    // S+1, by hierarchy order
   std::vector<EdgeW> up_in, dn_in;
@@ -60,16 +61,21 @@ struct HostLayout {
 };
 
 // Top region of the hierarchy (levels >= first_level), swept inside one CTA
-// per slot with the boundary values staged in shared memory.
+// per slot with the boundary values staged in shared memory. Edges from
+// below the region (upg) are applied by a grid-wide pull first; the region's
+// own edges run as a chunk schedule: upward levels low -> high, then
+// downward levels high -> low, each chunk at most kTopChunk edges of one
+// level, padded to an even count with a no-op edge into the scratch slot K.
 struct HostTop {
   uint32_t first_level = 0;  // level index where the top region starts
   uint32_t K0 = 0, K = 0;    // hierarchy positions [K0, K0+K)
-  std::vector<uint32_t> lvl_off;               // local level offsets
-  std::vector<uint32_t> upg_off, upl_off, dn_off;  // K+1 each
-  std::vector<EdgeW> upg, upl, dn;             // global-source / local-source / local
+  std::vector<uint32_t> upg_off;  // K+1
+  std::vector<EdgeW> upg;         // global source index
+  std::vector<EdgeW> sched;       // src = target << 16 | local source, w
+  std::vector<std::pair<int32_t, int32_t>> chunks;  // {first edge, count}
 };
 
 HostLayout build_layout(const chsga_graph_host& g);
-HostTop build_top(const HostLayout& L, uint32_t max_vertices);
+HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edges);
 
 }  // namespace chsga

@@ -77,13 +77,13 @@ struct PinnedArr {
 struct GraphDev {
   DevArr<uint32_t> lab2, lab_sp, sv_off, sv_dev, vin_off, vin_src, vin_srcv, dv_first, dv_len;
   DevArr<uint32_t> up_off, dn_off, istr_off, istr_src;
-  DevArr<int2> up_in, dn_in;
+  DevArr<int2> up_in, dn_in, vin_fix;
 };
 
 struct TopDev {
   HostTop h;
-  DevArr<uint32_t> lvl_off, upg_off, upl_off, dn_off;
-  DevArr<int2> upg, upl, dn;
+  DevArr<uint32_t> upg_off;
+  DevArr<int2> upg, sched, chunks;
   dev::TopPtrs ptrs{};
 };
 
@@ -91,14 +91,14 @@ struct TopDev {
 struct SlotBufs {
   int R = 0;
   DevArr<int> rows[2];
-  DevArr<int> BV;
+  DevArr<int> BV, BV2;  // BV2: second boundary buffer of the deferred score-only mode
   DevArr<dev::SlotState> slots;
   DevArr<uint32_t> word;
   DevArr<unsigned long long> best;
   DevArr<dev::StepCtl> ctl;
 };
 
-constexpr uint32_t kTopMaxVertices = 25000;  // 2 x int32 per vertex in shared memory
+constexpr uint32_t kTopMaxVertices = 23000;  // 2 x int32 per vertex in shared memory
 constexpr int kTopThreads = 1024;
 
 }  // namespace chsga
@@ -120,6 +120,8 @@ struct chsga_ctx {
   chsga::DevArr<chsga::dev::ReadDesc> queue;
   chsga::DevArr<int32_t> res_score;
   chsga::DevArr<uint32_t> res_vertex;
+  chsga::DevArr<unsigned long long> res_t0, res_t1;  // admission / completion, device ns
+  std::vector<uint32_t> last_ids;  // caller index of each queued read of the last call
   chsga::PinnedArr<chsga::dev::StepCtl> h_ctl;
   chsga::PinnedArr<int32_t> h_ckpt;  // checkpoint rows of the checkpointed traceback
   chsga_profile prof{};
@@ -146,6 +148,7 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
   if (need_rows) {
     b->rows[0].alloc(N * R);
     b->rows[1].alloc(N * R);
+    b->BV2.alloc(2 * S * R);
   }
   b->BV.alloc(2 * S * R);
   b->slots.alloc(R);
@@ -155,14 +158,17 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
   static bool attr_set = false;
   if (!attr_set) {
     CK(cudaFuncSetAttribute(dev::k_top<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)(kTopMaxVertices * 8)));
+                            (int)dev::top_smem_bytes(kTopMaxVertices)));
     attr_set = true;
   }
   return *b;
 }
 
 // Uploads reads (raw bytes) and their queue descriptors; ids are 0..n-1.
-void upload_reads(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n) {
+// With longest_first the queue admits reads in decreasing length (stable), so
+// the slots of the batched engine drain on the short reads at the end.
+void upload_reads(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n,
+                  bool longest_first = false) {
   std::vector<unsigned char> bytes;
   std::vector<dev::ReadDesc> q(n);
   uint64_t total = 0;
@@ -175,11 +181,16 @@ void upload_reads(chsga_ctx& c, const char* const* reads, const uint32_t* lens, 
     q[i] = dev::ReadDesc{off, lens[i], (int32_t)i};
     off += lens[i];
   }
-  std::vector<unsigned char> bv(bytes.begin(), bytes.end());
-  c.reads.upload(bv, c.st);
+  if (longest_first)
+    std::stable_sort(q.begin(), q.end(),
+                     [](const dev::ReadDesc& a, const dev::ReadDesc& b) { return a.len > b.len; });
+  c.reads.upload(bytes, c.st);
   c.queue.upload(q, c.st);
   c.res_score.alloc(n);
   c.res_vertex.alloc(n);
+  c.res_t0.alloc(n);
+  c.res_t1.alloc(n);
+  CK(cudaStreamSynchronize(c.st));  // the staging vectors die with this frame
 }
 
 template <int R>
@@ -193,46 +204,89 @@ void reset_slots(chsga_ctx& c, SlotBufs& b, uint32_t q_count) {
   CK(cudaStreamSynchronize(c.st));  // host copies above are from stack memory
 }
 
+// Fails with CHSGA_ERR_TIMEOUT if a kernel's bounded wait expired.
+void check_device_error(chsga_ctx& c, SlotBufs& b) {
+  dev::StepCtl fin{};
+  CK(cudaMemcpyAsync(&fin, b.ctl.p, sizeof(fin), cudaMemcpyDeviceToHost, c.st));
+  CK(cudaStreamSynchronize(c.st));
+  require(fin.error == 0, CHSGA_ERR_TIMEOUT,
+          "a bounded device-side wait expired (code " + std::to_string(fin.error) + ")");
+}
+
 template <int R>
 void launch_advance(chsga_ctx& c, SlotBufs& b, int prime, cudaStream_t s) {
   dev::k_advance<R><<<1, 128, 0, s>>>(b.slots.p, c.queue.p, c.reads.p, b.best.p, c.res_score.p,
-                                      c.res_vertex.p, b.word.p, b.ctl.p, c.L.special, prime);
+                                      c.res_vertex.p, c.res_t0.p, c.res_t1.p, b.word.p, b.ctl.p,
+                                      c.L.special, prime);
   check_launch();
 }
 
-// One row-step for every slot: D = previous rows, T = rows being computed.
-template <int R>
-void row_step(chsga_ctx& c, SlotBufs& b, const int* D, int* T, cudaStream_t s) {
+// CUDA events between the kernel groups of one row-step (profiling mode).
+struct StepEvents {
+  cudaEvent_t e[6];
+  StepEvents() {
+    for (auto& x : e) CK(cudaEventCreate(&x));
+  }
+  ~StepEvents() {
+    for (auto& x : e) cudaEventDestroy(x);
+  }
+  // accumulates the five group durations of the step just recorded
+  void add(chsga_profile& p) {
+    CK(cudaEventSynchronize(e[5]));
+    float ms[5];
+    for (int i = 0; i < 5; ++i) CK(cudaEventElapsedTime(&ms[i], e[i], e[i + 1]));
+    p.row_ms += ms[0];
+    p.sweep_up_ms += ms[1];
+    p.top_ms += ms[2];
+    p.sweep_down_ms += ms[3];
+    p.other_ms += ms[4];
+  }
+};
+
+// One row-step for every slot: D = previous rows, T = rows being computed,
+// BVc = this step's boundary scores. DEFER (score-only): rows stay raw and
+// BVp holds the previous step's swept boundary scores; otherwise every row
+// is written final (rows that are kept for traceback).
+template <int R, bool DEFER>
+void row_step(chsga_ctx& c, SlotBufs& b, const int* D, int* T, int* BVc, const int* BVp,
+              cudaStream_t s, StepEvents* ev = nullptr) {
   const HostLayout& L = c.L;
   const TopDev& top = *c.top;
   constexpr int G = Lanes<R>::G;
-  dev::k_row<R><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(c.gp, D, T, b.BV.p, b.word.p, b.best.p,
-                                                            b.ctl.p);
+  if (ev) CK(cudaEventRecord(ev->e[0], s));
+  dev::k_row<R, DEFER><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(c.gp, D, T, BVc, BVp, b.word.p,
+                                                                   b.best.p, b.ctl.p);
+  if (ev) CK(cudaEventRecord(ev->e[1], s));
   const uint32_t fl = top.h.first_level;
   for (uint32_t l = 0; l < fl; ++l) {
     if (L.lvl_up_edges[l] == 0) continue;
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
     dev::k_pull<R><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-        b.BV.p, lo, hi, c.gd.up_off.p, c.gd.up_in.p, 0, b.ctl.p);
+        BVc, lo, hi, c.gd.up_off.p, c.gd.up_in.p, 0, b.ctl.p);
   }
+  if (ev) CK(cudaEventRecord(ev->e[2], s));
   if (top.h.K) {
     if (!top.h.upg.empty())
       dev::k_pull<R><<<nblocks((uint64_t)top.h.K * G), 256, 0, s>>>(
-          b.BV.p, top.h.K0, L.S, top.upg_off.p, top.upg.p, top.h.K0, b.ctl.p);
-    dev::k_top<R><<<R, kTopThreads, top.h.K * 8, s>>>(b.BV.p, top.ptrs, b.word.p, b.ctl.p);
+          BVc, top.h.K0, L.S, top.upg_off.p, top.upg.p, top.h.K0, b.ctl.p);
+    dev::k_top<R><<<R, kTopThreads, dev::top_smem_bytes(top.h.K), s>>>(BVc, top.ptrs, b.word.p,
+                                                                       b.ctl.p);
   }
+  if (ev) CK(cudaEventRecord(ev->e[3], s));
   if (fl == 0) {
-    dev::k_down<R><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(c.gp, b.BV.p, T, 0, 0, L.S, b.word.p,
-                                                               b.best.p, b.ctl.p);
+    dev::k_down<R, !DEFER><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(c.gp, BVc, T, 0, 0, L.S,
+                                                                       b.word.p, b.best.p, b.ctl.p);
   } else {
     for (int l = (int)fl - 1; l >= 0; --l) {
       const uint32_t lo = L.lvl_off[l], mid = L.lvl_off[l + 1];
       const uint32_t hi = (l == (int)fl - 1) ? L.S : mid;
-      dev::k_down<R><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(c.gp, b.BV.p, T, lo, mid, hi,
-                                                                       b.word.p, b.best.p, b.ctl.p);
+      dev::k_down<R, !DEFER><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
+          c.gp, BVc, T, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
     }
   }
+  if (ev) CK(cudaEventRecord(ev->e[4], s));
   launch_advance<R>(c, b, 0, s);
+  if (ev) CK(cudaEventRecord(ev->e[5], s));
 }
 
 uint32_t kernels_per_step(const chsga_ctx& c) {
@@ -251,6 +305,15 @@ template <int R>
 void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, uint32_t per_graph) {
   SlotBufs& b = get_bufs<R>(c, true);
   reset_slots<R>(c, b, n);
+  const bool profile = (c.flags & CHSGA_FLAG_PROFILE) != 0;
+  if (profile) use_graphs = false;
+  std::unique_ptr<StepEvents> sev;
+  if (profile) sev = std::make_unique<StepEvents>();
+  c.prof = chsga_profile{};
+  cudaEvent_t t_start, t_stop;
+  CK(cudaEventCreate(&t_start));
+  CK(cudaEventCreate(&t_stop));
+  CK(cudaEventRecord(t_start, c.st));
   launch_advance<R>(c, b, 0, c.st);  // admit the first reads
   per_graph = std::max<uint32_t>(2, per_graph + (per_graph & 1));
   c.h_ctl.alloc(1);
@@ -259,9 +322,10 @@ void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, u
   CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
+  int* BVs[2] = {b.BV.p, b.BV2.p};
   auto enqueue_block = [&](cudaStream_t s) {
     for (uint32_t i = 0; i < per_graph; ++i)
-      row_step<R>(c, b, b.rows[i & 1].p, b.rows[(i + 1) & 1].p, s);
+      row_step<R, true>(c, b, b.rows[i & 1].p, b.rows[(i + 1) & 1].p, BVs[(i + 1) & 1], BVs[i & 1], s);
   };
   if (use_graphs) {
     cudaStream_t cap;
@@ -275,18 +339,25 @@ void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, u
   auto launch_block = [&]() {
     if (use_graphs) {
       CK(cudaGraphLaunch(exec, c.st));
+    } else if (profile) {
+      for (uint32_t i = 0; i < per_graph; ++i) {
+        row_step<R, true>(c, b, b.rows[i & 1].p, b.rows[(i + 1) & 1].p, BVs[(i + 1) & 1], BVs[i & 1],
+                          c.st, sev.get());
+        sev->add(c.prof);
+      }
     } else {
       enqueue_block(c.st);
     }
   };
   // R == 1 runs exactly one row per step, so the step count is known; the
   // batched engine polls its done counter, one block behind the device.
+  uint64_t launched = 0;
   if (R == 1) {
     const uint64_t blocks = (total_rows + per_graph - 1) / per_graph;
     for (uint64_t i = 0; i < blocks; ++i) launch_block();
+    launched = blocks;
     CK(cudaStreamSynchronize(c.st));
   } else {
-    uint64_t launched = 0;
     const uint64_t max_blocks = total_rows / per_graph + 4;
     while (true) {
       launch_block();
@@ -303,12 +374,26 @@ void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, u
     CK(cudaStreamSynchronize(c.st));
     require(c.h_ctl.p->done == n, CHSGA_ERR_INTERNAL, "batched engine lost reads");
   }
+  CK(cudaEventRecord(t_stop, c.st));
+  CK(cudaEventSynchronize(t_stop));
+  float dev_ms = 0;
+  CK(cudaEventElapsedTime(&dev_ms, t_start, t_stop));
+  cudaEventDestroy(t_start);
+  cudaEventDestroy(t_stop);
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
   cudaEventDestroy(ev[0]);
   cudaEventDestroy(ev[1]);
+  dev::StepCtl fin{};
+  CK(cudaMemcpy(&fin, b.ctl.p, sizeof(fin), cudaMemcpyDeviceToHost));
+  require(fin.error == 0, CHSGA_ERR_TIMEOUT,
+          "a bounded device-side wait expired (code " + std::to_string(fin.error) + ")");
+  c.prof.total_ms = dev_ms;
   c.prof.rows = total_rows;
-  c.prof.launches = (uint64_t)kernels_per_step(c) * ((total_rows + per_graph - 1) / per_graph) * per_graph;
+  c.prof.steps = fin.steps;
+  // every kernel launched, the early-exit ones of steps after the last read included
+  c.prof.launches = 1 + (uint64_t)kernels_per_step(c) * launched * per_graph;
+  c.prof.row_launches = profile ? fin.steps : launched * per_graph;
 }
 
 void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
@@ -328,31 +413,36 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   d.dn_off.upload(L.dn_off, s);
   d.istr_off.upload(L.istr_off, s);
   d.istr_src.upload(L.istr_src, s);
+  {
+    std::vector<int2> vf(L.vin_fix.size());
+    for (size_t i = 0; i < vf.size(); ++i) vf[i] = make_int2(L.vin_fix[i].src, L.vin_fix[i].w);
+    d.vin_fix.upload(vf, s);
+  }
   std::vector<int2> up(L.up_in.size()), dn(L.dn_in.size());
   for (size_t i = 0; i < up.size(); ++i) up[i] = make_int2(L.up_in[i].src, L.up_in[i].w);
   for (size_t i = 0; i < dn.size(); ++i) dn[i] = make_int2(L.dn_in[i].src, L.dn_in[i].w);
   d.up_in.upload(up, s);
   d.dn_in.upload(dn, s);
   auto top = std::make_unique<TopDev>();
-  top->h = build_top(L, kTopMaxVertices);
+  top->h = build_top(L, kTopMaxVertices, dev::kTopChunk);
   const HostTop& h = top->h;
-  top->lvl_off.upload(h.lvl_off, s);
-  top->upg_off.upload(h.upg_off, s);
-  top->upl_off.upload(h.upl_off, s);
-  top->dn_off.upload(h.dn_off, s);
   auto to2 = [](const std::vector<EdgeW>& v) {
     std::vector<int2> o(v.size());
     for (size_t i = 0; i < v.size(); ++i) o[i] = make_int2(v[i].src, v[i].w);
     return o;
   };
+  top->upg_off.upload(h.upg_off, s);
   top->upg.upload(to2(h.upg), s);
-  top->upl.upload(to2(h.upl), s);
-  top->dn.upload(to2(h.dn), s);
-  top->ptrs = dev::TopPtrs{h.K0, h.K, (uint32_t)h.lvl_off.size() - 1, top->lvl_off.p,
-                           top->upl_off.p, top->upl.p, top->dn_off.p, top->dn.p, d.dv_len.p};
+  top->sched.upload(to2(h.sched), s);
+  std::vector<int2> ch(h.chunks.size());
+  for (size_t i = 0; i < ch.size(); ++i) ch[i] = make_int2(h.chunks[i].first, h.chunks[i].second);
+  top->chunks.upload(ch, s);
+  top->ptrs = dev::TopPtrs{h.K0, h.K, (uint32_t)h.chunks.size(), top->chunks.p, top->sched.p,
+                           d.dv_len.p};
   CK(cudaStreamSynchronize(s));
   c.gp = dev::GraphPtrs{L.N,          L.S,          L.special,      d.lab2.p,     d.lab_sp.p,
                         d.sv_off.p,   d.sv_dev.p,   d.vin_off.p,    d.vin_src.p,  d.vin_srcv.p,
+                        d.vin_fix.p,
                         d.dv_first.p, d.dv_len.p,   d.up_off.p,     d.up_in.p,    d.dn_off.p,
                         d.dn_in.p,    d.istr_off.p, d.istr_src.p};
   c.nul_label = false;
@@ -381,12 +471,10 @@ void scores_with(chsga_ctx& c, const char* const* reads, const uint32_t* lens, u
     idx.push_back(i);
     rows += lens[i];
   }
+  c.last_ids = idx;
   if (rp.empty()) return;
-  upload_reads(c, rp.data(), rl.data(), (uint32_t)rp.size());
-  auto t0 = std::chrono::steady_clock::now();
+  upload_reads(c, rp.data(), rl.data(), (uint32_t)rp.size(), R > 1);
   run_queue<R>(c, (uint32_t)rp.size(), rows, graphs, per_graph);
-  c.prof.total_ms =
-      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   std::vector<int32_t> res(rp.size());
   CK(cudaMemcpy(res.data(), c.res_score.p, res.size() * 4, cudaMemcpyDeviceToHost));
   for (size_t i = 0; i < idx.size(); ++i) out[idx[i]] = res[i];
@@ -415,7 +503,8 @@ void forward_rows(chsga_ctx& c, SlotBufs& b, uint32_t len, int64_t a, int64_t b_
   CK(cudaStreamSynchronize(c.st));
   launch_advance<1>(c, b, 1, c.st);
   for (int64_t i = a + 1; i <= b_row; ++i)
-    row_step<1>(c, b, matrix + (size_t)(i - 1 - a) * N, matrix + (size_t)(i - a) * N, c.st);
+    row_step<1, false>(c, b, matrix + (size_t)(i - 1 - a) * N, matrix + (size_t)(i - a) * N, b.BV.p, nullptr, c.st);
+  check_device_error(c, b);
 }
 
 void walk(chsga_ctx& c, const int* M, int64_t lo, int64_t hi, uint32_t start, uint32_t len,
@@ -458,7 +547,7 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
   uint32_t best_v = 0;
   int32_t best_s = 0;
   auto harvest = [&]() {
-    CK(cudaStreamSynchronize(c.st));
+    check_device_error(c, b);
     CK(cudaMemcpy(&best_s, c.res_score.p, 4, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(&best_v, c.res_vertex.p, 4, cudaMemcpyDeviceToHost));
   };
@@ -472,7 +561,7 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
     reset_slots<1>(c, b, 1);
     launch_advance<1>(c, b, 0, c.st);
     for (uint32_t i = 0; i < len; ++i)
-      row_step<1>(c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, c.st);
+      row_step<1, false>(c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, b.BV.p, nullptr, c.st);
     harvest();
     uint32_t v = best_v;
     if (len > 1) walk(c, M.p, 0, len - 1, best_v, len, path, &v);
@@ -502,7 +591,7 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
         CK(cudaEventSynchronize(done_ev[cur]));
         busy[cur] = false;
       }
-      row_step<1>(c, b, ring.p + (size_t)prev * N, ring.p + (size_t)cur * N, c.st);
+      row_step<1, false>(c, b, ring.p + (size_t)prev * N, ring.p + (size_t)cur * N, b.BV.p, nullptr, c.st);
       if (i % k == 0) {
         cudaEvent_t ready;
         CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
@@ -723,8 +812,8 @@ chsga_status chsga_align_rows(chsga_ctx* c, const char* read, uint32_t len, int3
     reset_slots<1>(*c, b, 1);
     launch_advance<1>(*c, b, 0, c->st);
     for (uint32_t i = 0; i < len; ++i)
-      row_step<1>(*c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, c->st);
-    CK(cudaStreamSynchronize(c->st));
+      row_step<1, false>(*c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, b.BV.p, nullptr, c->st);
+    check_device_error(*c, b);
     CK(cudaMemcpy(rows_out, M.p, (size_t)len * N * 4, cudaMemcpyDeviceToHost));
   });
 }
@@ -772,6 +861,24 @@ uint64_t chsga_ops_to_cigar(const chsga_op* ops, uint64_t n, char* buf, uint64_t
     buf[m] = '\0';
   }
   return cig.size();
+}
+
+chsga_status chsga_get_read_times(chsga_ctx* c, uint64_t* admit_ns, uint64_t* done_ns,
+                                  uint32_t n) {
+  return guarded_ctx(c, [&] {
+    require(c && admit_ns && done_ns, CHSGA_ERR_INVALID_ARG, "null argument");
+    require(n == c->last_ids.size() || n == 0, CHSGA_ERR_INVALID_ARG,
+            "n must equal the number of non-empty reads of the last score call");
+    std::vector<unsigned long long> a(n), d(n);
+    if (n) {
+      CK(cudaMemcpy(a.data(), c->res_t0.p, n * 8, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(d.data(), c->res_t1.p, n * 8, cudaMemcpyDeviceToHost));
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+      admit_ns[i] = a[i];
+      done_ns[i] = d[i];
+    }
+  });
 }
 
 chsga_status chsga_get_profile(chsga_ctx* c, chsga_profile* out) {

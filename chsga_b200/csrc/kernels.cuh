@@ -13,9 +13,12 @@
 //                 writes the first/last scores of every vertex into BV
 //   k_pull        one upward hierarchy level (align.hpp:296-314), pull form
 //   k_top         every level of the top region, up and down, in shared memory
-//   k_down        one downward level (align.hpp:317-343) plus the final
-//                 within-vertex propagation (align.hpp:381-396) of the vertices
-//                 it finalises, which only needs the vertex's own first score
+//   k_down        one downward level (align.hpp:317-343). The final
+//                 within-vertex propagation (align.hpp:381-396) only ever
+//                 lowers char c of vertex s to F[s] + (c - first(s)), F[s] the
+//                 swept first score, so it is either written into the row here
+//                 (FIXUP: rows that are kept, i.e. traceback) or applied when
+//                 the next row-step reads the row (score-only: k_row<DEFER>)
 //   k_advance     moves every slot to its next row, harvests finished reads
 //                 and refills slots from the device read queue
 // Row 0 of a read is only the initial match/substitution row
@@ -39,6 +42,8 @@ struct GraphPtrs {
   const uint32_t* vin_off;
   const uint32_t* vin_src;
   const uint32_t* vin_srcv;
+  const int2* vin_fix;  // per first-char in-edge: {hierarchy position of the source's
+                        // vertex, source char - that vertex's first char}
   const uint32_t* dv_first;
   const uint32_t* dv_len;
   const uint32_t* up_off;
@@ -55,6 +60,7 @@ constexpr uint32_t SW_INIT = 1u << 8;       // row 0: match/substitution only
 constexpr uint32_t SW_CLOSURE = 1u << 9;    // row >= 1: hierarchy closure applies
 constexpr uint32_t SW_ENDING = 1u << 10;    // last row of the read: reduce its minimum
 constexpr uint32_t SW_ACTIVE = 1u << 11;
+constexpr uint32_t SW_FIX = 1u << 12;      // row >= 2: previous row had a closure to apply
 
 struct SlotState {
   unsigned long long off;  // first base of the read in the device read buffer
@@ -77,7 +83,8 @@ struct StepCtl {        // device-resident control block
   uint32_t q_count;     // queue entries published by the host
   uint32_t done;        // reads finished
   uint32_t steps;       // row-steps with work
-  uint32_t pad[2];
+  uint32_t error;       // nonzero: a bounded device-side wait gave up
+  uint32_t pad;
 };
 
 template <int R>
@@ -159,6 +166,12 @@ __device__ __forceinline__ uint32_t base_code(int b, int special) {
   }
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 __device__ __forceinline__ unsigned long long pack_min(int score, uint32_t c) {
   return ((unsigned long long)(uint32_t)score << 32) | c;
 }
@@ -176,13 +189,17 @@ __device__ __forceinline__ void flush_min(unsigned long long* sm_best, unsigned 
 // each slot: the first char takes min(D[f]+1, min over in-edges D[u]+delta),
 // every later char c takes min(D[c]+1, D[c-1]+delta, T[c-1]+1): the chain
 // in-edge c-1 -> c plus the within-vertex forward scan. Row 0 takes delta.
+// With DEFER, D holds the previous row before its final within-vertex
+// propagation and BVp the previous row's swept first scores, and every D
+// value is read as min(D[c], BVp[2 d(c)] + c - first(c)).
 // ---------------------------------------------------------------------------
-template <int R>
-__global__ void __launch_bounds__(256) k_row(GraphPtrs g, const int* __restrict__ D,
-                                             int* __restrict__ T, int* __restrict__ BV,
-                                             const uint32_t* __restrict__ slot_word,
-                                             unsigned long long* __restrict__ best,
-                                             const StepCtl* __restrict__ ctl) {
+template <int R, bool DEFER>
+__global__ void __launch_bounds__(256, 3) k_row(GraphPtrs g, const int* __restrict__ D,
+                                                int* __restrict__ T, int* __restrict__ BV,
+                                                const int* __restrict__ BVp,
+                                                const uint32_t* __restrict__ slot_word,
+                                                unsigned long long* __restrict__ best,
+                                                const StepCtl* __restrict__ ctl) {
   constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
   __shared__ unsigned long long sm_best[R];
   const bool ending_any = ctl->any_ending != 0;
@@ -196,17 +213,30 @@ __global__ void __launch_bounds__(256) k_row(GraphPtrs g, const int* __restrict_
   const int lane = (int)(gt % G);
   if (s < g.S) {
     uint32_t code[V];
-    bool init[V], ending[V];
+    bool init[V], ending[V], fix[V];
+    bool any_fix = false;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const uint32_t w = __ldg(slot_word + lane * V + v);
       code[v] = w & SW_CODE;
       init[v] = (w & SW_INIT) != 0;
       ending[v] = (w & SW_ENDING) != 0;
+      fix[v] = DEFER && (w & SW_FIX) != 0;
+      any_fix |= fix[v];
     }
     const uint32_t f = __ldg(g.sv_off + s), e = __ldg(g.sv_off + s + 1);
     const uint32_t d = __ldg(g.sv_dev + s);
     const size_t so = (size_t)lane * V;
+    constexpr int kBig = 0x3fffffff;
+    IV<V> F;  // previous row's swept first score of this vertex
+#pragma unroll
+    for (int v = 0; v < V; ++v) F.v[v] = kBig;
+    if (DEFER && any_fix) {
+      const IV<V> x = ld_nc<V>(BVp + (size_t)(2 * d) * R + so);
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        if (fix[v]) F.v[v] = x.v[v];
+    }
     int bmin[V];
     uint32_t barg[V];
     // first char
@@ -217,13 +247,21 @@ __global__ void __launch_bounds__(256) k_row(GraphPtrs g, const int* __restrict_
       int delta[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
+        if (DEFER) dprev.v[v] = min(dprev.v[v], F.v[v]);
         delta[v] = key == code[v] ? 0 : 1;
         t.v[v] = dprev.v[v] + 1;
       }
       const uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
       for (uint32_t k = k0; k < k1; ++k) {
         const uint32_t u = __ldg(g.vin_src + k);
-        const IV<V> du = ld_nc<V>(D + (size_t)u * R + so);
+        IV<V> du = ld_nc<V>(D + (size_t)u * R + so);
+        if (DEFER && any_fix) {
+          const int2 fx = __ldg(g.vin_fix + k);
+          const IV<V> fu = ld_nc<V>(BVp + (size_t)(2 * fx.x) * R + so);
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            if (fix[v]) du.v[v] = min(du.v[v], fu.v[v] + fx.y);
+        }
 #pragma unroll
         for (int v = 0; v < V; ++v) t.v[v] = min(t.v[v], du.v[v] + delta[v]);
       }
@@ -236,23 +274,36 @@ __global__ void __launch_bounds__(256) k_row(GraphPtrs g, const int* __restrict_
     }
     st<V>(T + (size_t)f * R + so, t);
     st<V>(BV + (size_t)(2 * d) * R + so, t);
-    for (uint32_t c = f + 1; c < e; ++c) {
-      const uint32_t key = label_key(g, c);
-      const IV<V> dc = ld_nc<V>(D + (size_t)c * R + so);
+    // chain chars in groups of four: the four loads go out together so each
+    // warp keeps several row segments in flight
+    for (uint32_t c0 = f + 1; c0 < e; c0 += 4) {
+      const uint32_t n = min(4u, e - c0);
+      IV<V> dq[4];
 #pragma unroll
-      for (int v = 0; v < V; ++v) {
-        const int delta = key == code[v] ? 0 : 1;
-        int x = min(dc.v[v] + 1, dprev.v[v] + delta);
-        x = min(x, t.v[v] + 1);
-        if (init[v]) x = delta;
-        t.v[v] = x;
-        if (x < bmin[v]) {
-          bmin[v] = x;
-          barg[v] = c;
+      for (uint32_t k = 0; k < 4; ++k)
+        if (k < n) dq[k] = ld_nc<V>(D + (size_t)(c0 + k) * R + so);
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k) {
+        if (k < n) {
+          const uint32_t c = c0 + k;
+          const uint32_t key = label_key(g, c);
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            if (DEFER) dq[k].v[v] = min(dq[k].v[v], F.v[v] + (int)(c - f));
+            const int delta = key == code[v] ? 0 : 1;
+            int x = min(dq[k].v[v] + 1, dprev.v[v] + delta);
+            x = min(x, t.v[v] + 1);
+            if (init[v]) x = delta;
+            t.v[v] = x;
+            if (x < bmin[v]) {
+              bmin[v] = x;
+              barg[v] = c;
+            }
+          }
+          dprev = dq[k];
+          st<V>(T + (size_t)c * R + so, t);
         }
       }
-      dprev = dc;
-      st<V>(T + (size_t)c * R + so, t);
     }
     if (e - f > 1) st<V>(BV + (size_t)(2 * d + 1) * R + so, t);
     if (ending_any) {
@@ -308,7 +359,7 @@ __global__ void __launch_bounds__(256) k_pull(int* __restrict__ BV, uint32_t lo,
 // and propagate first + (p - first) forward while it improves
 // (align.hpp:381-396). Slots without closure (row 0, idle) are untouched.
 // ---------------------------------------------------------------------------
-template <int R>
+template <int R, bool FIXUP>
 __global__ void __launch_bounds__(256) k_down(GraphPtrs g, int* __restrict__ BV, int* __restrict__ T,
                                               uint32_t lo, uint32_t mid, uint32_t hi,
                                               const uint32_t* __restrict__ slot_word,
@@ -347,93 +398,229 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, int* __restrict__ BV,
       if (changed) st<V>(p, f);
     }
     const uint32_t first = __ldg(g.dv_first + d), len = __ldg(g.dv_len + d);
-    const IV<V> t0 = ld<V>(T + (size_t)first * R + so);
+    (void)len;
+    if (!FIXUP) {
+      // the row stays raw; a slot on its last row needs min over the final
+      // scores = min(min over raw scores [k_row], min over swept first scores)
+      if (ending_any) {
 #pragma unroll
-    for (int v = 0; v < V; ++v) {
-      if (f.v[v] >= t0.v[v]) continue;
-      const uint32_t w = __ldg(slot_word + so + v);
-      if (!(w & SW_CLOSURE)) continue;
-      const bool ending = (w & SW_ENDING) != 0;
-      const int fv = f.v[v];
-      T[(size_t)first * R + so + v] = fv;
-      if (ending) atomicMin(sm_best + so + v, pack_min(fv, first));
-      for (uint32_t q = 1; q < len; ++q) {
-        int* tp = T + (size_t)(first + q) * R + so + v;
-        const int cand = fv + (int)q;
-        if (cand < *tp) {
-          *tp = cand;
-          if (ending) atomicMin(sm_best + so + v, pack_min(cand, first + q));
-        } else {
-          break;
+        for (int v = 0; v < V; ++v) {
+          const uint32_t w = __ldg(slot_word + so + v);
+          if ((w & SW_CLOSURE) && (w & SW_ENDING))
+            atomicMin(sm_best + so + v, pack_min(f.v[v], first));
         }
       }
+    } else {
+    IV<V> tq = ld<V>(T + (size_t)first * R + so);
+    bool act[V], endg[V];
+    bool any = false;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const uint32_t w = __ldg(slot_word + so + v);
+      act[v] = (w & SW_CLOSURE) && f.v[v] < tq.v[v];
+      endg[v] = act[v] && (w & SW_ENDING);
+      if (act[v]) {
+        tq.v[v] = f.v[v];
+        if (endg[v]) atomicMin(sm_best + so + v, pack_min(f.v[v], first));
+      }
+      any |= act[v];
+    }
+    if (any) {
+      st<V>(T + (size_t)first * R + so, tq);
+      // first + q while it improves, every slot of the lane in one pass per char
+      for (uint32_t q = 1; q < len && any; ++q) {
+        int* tp = T + (size_t)(first + q) * R + so;
+        IV<V> x = ld<V>(tp);
+        any = false;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          if (!act[v]) continue;
+          const int cand = f.v[v] + (int)q;
+          if (cand < x.v[v]) {
+            x.v[v] = cand;
+            if (endg[v]) atomicMin(sm_best + so + v, pack_min(cand, first + q));
+            any = true;
+          } else {
+            act[v] = false;
+          }
+        }
+        st<V>(tp, x);
+      }
+    }
     }
   }
   if (ending_any) flush_min<R>(sm_best, best);
 }
 
 // ---------------------------------------------------------------------------
-// k_top: hierarchy positions [K0, S), one CTA per slot. Stages first/last
-// scores in shared memory, then runs the upward levels low -> high and the
-// downward levels high -> low with a block barrier between levels. Edges
-// from below the region were applied by k_pull before this launch.
+// Bulk asynchronous copies (TMA engine, non-tensor form) into shared memory,
+// completing on an mbarrier. Source and destination 16-byte aligned, size a
+// multiple of 16. Every wait is bounded: on expiry the kernel records an
+// error code in StepCtl::error and stops.
 // ---------------------------------------------------------------------------
+constexpr uint32_t kWaitLimit = 1u << 22;  // try_wait polls (each may suspend briefly)
+constexpr uint32_t ERR_TOP_WAIT = 1;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// One arrival that also announces `bytes` of transaction, then the copy.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Waits for phase `parity` of the barrier; false if the poll budget ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// k_top: hierarchy positions [K0, S), one CTA per slot. The first/last
+// scores of the region are staged in shared memory; the region's upward
+// levels (low -> high) and downward levels (high -> low) then run as a
+// sequence of edge chunks, each chunk a contiguous array of
+// {target << 16 | source, weight} that thread 0 brings into one of two shared
+// buffers with a bulk copy while the block relaxes the previous chunk
+// (atomic min into the target's first score). A chunk never spans two
+// levels and ends with a block barrier, so every level sees its sources
+// final. Edges from below the region were applied by k_pull before launch.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kTopChunk = 1024;  // edges per chunk (8 KiB)
+
 struct TopPtrs {
-  uint32_t K0, K, nlev;
-  const uint32_t* lvl_off;  // nlev+1, local
-  const uint32_t* upl_off;
-  const int2* upl;
-  const uint32_t* dn_off;
-  const int2* dn;
-  const uint32_t* dv_len;   // global, by hierarchy position
+  uint32_t K0, K, nchunks;
+  const int2* chunk;   // nchunks x {first edge, edge count (even)}
+  const int2* edges;   // chunk edges in schedule order, 16-byte aligned chunks
+  const uint32_t* dv_len;  // global, by hierarchy position
 };
+
+__host__ __device__ constexpr size_t top_smem_bytes(uint32_t K) {
+  return ((size_t)(2 * K + 2) * 4 + 15) / 16 * 16 + 2 * kTopChunk * 8 + 16;
+}
 
 template <int R>
 __global__ void __launch_bounds__(1024) k_top(int* __restrict__ BV, TopPtrs t,
                                               const uint32_t* __restrict__ slot_word,
-                                              const StepCtl* __restrict__ ctl) {
-  extern __shared__ int sm[];  // 2*K ints: [2j] first, [2j+1] last
+                                              StepCtl* __restrict__ ctl) {
+  extern __shared__ __align__(16) unsigned char top_smem[];
   if (!ctl->any_active) return;
   const int r = blockIdx.x;
   if (!(slot_word[r] & SW_CLOSURE)) return;
-  for (uint32_t j = threadIdx.x; j < t.K; j += blockDim.x) {
-    const size_t d = t.K0 + j;
-    sm[2 * j] = BV[(2 * d) * R + r];
-    if (__ldg(t.dv_len + d) > 1) sm[2 * j + 1] = BV[(2 * d + 1) * R + r];
+  int* sm = reinterpret_cast<int*>(top_smem);  // [2j] first, [2j+1] last, [2K] scratch
+  int2* ebuf = reinterpret_cast<int2*>(top_smem + ((size_t)(2 * t.K + 2) * 4 + 15) / 16 * 16);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(ebuf + 2 * kTopChunk);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_async_shared();
   }
   __syncthreads();
-  for (uint32_t l = 0; l < t.nlev; ++l) {
-    const uint32_t lo = t.lvl_off[l], hi = t.lvl_off[l + 1];
-    for (uint32_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-      int f = sm[2 * j];
-      for (uint32_t k = t.upl_off[j]; k < t.upl_off[j + 1]; ++k) {
-        const int2 ew = t.upl[k];
-        f = min(f, sm[ew.x] + ew.y);
+  if (threadIdx.x == 0) {
+    for (uint32_t c = 0; c < 2 && c < t.nchunks; ++c) {
+      const int2 ch = t.chunk[c];
+      bulk_load(ebuf + c * kTopChunk, t.edges + ch.x, (uint32_t)ch.y * 8, &bar[c]);
+    }
+  }
+  // stage the region's scores (independent loads, unrolled)
+  const size_t K0 = t.K0;
+  for (uint32_t j0 = threadIdx.x; j0 < t.K; j0 += 4 * blockDim.x) {
+    int fv[4], lv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t j = j0 + u * blockDim.x;
+      if (j < t.K) {
+        const size_t d = K0 + j;
+        if constexpr (R == 1) {
+          const int2 x = *reinterpret_cast<const int2*>(BV + 2 * d);
+          fv[u] = x.x;
+          lv[u] = x.y;
+        } else {
+          fv[u] = BV[(2 * d) * R + r];
+          lv[u] = BV[(2 * d + 1) * R + r];
+        }
       }
-      sm[2 * j] = f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t j = j0 + u * blockDim.x;
+      if (j < t.K) {
+        sm[2 * j] = fv[u];
+        sm[2 * j + 1] = lv[u];
+      }
+    }
+  }
+  __shared__ int s_fail;
+  if (threadIdx.x == 0) {
+    sm[2 * t.K] = 0;
+    s_fail = 0;
+  }
+  __syncthreads();
+  uint32_t c = 0;
+  for (; c < t.nchunks; ++c) {
+    const uint32_t b = c & 1;
+    // a thread whose wait expires flags it and still reaches the barrier
+    // below, so the whole block leaves the loop together
+    if (!mbar_wait(&bar[b], (c >> 1) & 1)) s_fail = 1;
+    const int n = t.chunk[c].y;
+    const int2* e = ebuf + b * kTopChunk;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int2 x = e[i];
+      atomicMin(&sm[2 * (x.x >> 16)], sm[x.x & 0xFFFF] + x.y);
     }
     __syncthreads();
+    if (s_fail) break;
+    if (threadIdx.x == 0 && c + 2 < t.nchunks) {
+      fence_async_shared();
+      const int2 ch = t.chunk[c + 2];
+      bulk_load(ebuf + b * kTopChunk, t.edges + ch.x, (uint32_t)ch.y * 8, &bar[b]);
+    }
   }
-  for (uint32_t l = t.nlev; l-- > 0;) {
-    const uint32_t lo = t.lvl_off[l], hi = t.lvl_off[l + 1];
-    for (uint32_t j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-      int f = sm[2 * j];
-      for (uint32_t k = t.dn_off[j]; k < t.dn_off[j + 1]; ++k) {
-        const int2 ew = t.dn[k];
-        f = min(f, sm[ew.x] + ew.y);
-      }
-      sm[2 * j] = f;
+  if (s_fail) {
+    // record the failure and give the copies still in flight a bounded wait
+    // before the shared memory is released
+    if (threadIdx.x == 0) {
+      atomicOr(&ctl->error, ERR_TOP_WAIT);
+      for (uint32_t k = c; k < c + 2 && k < t.nchunks; ++k) mbar_wait(&bar[k & 1], (k >> 1) & 1);
     }
     __syncthreads();
+    return;
   }
-  for (uint32_t j = threadIdx.x; j < t.K; j += blockDim.x) BV[(2 * (size_t)(t.K0 + j)) * R + r] = sm[2 * j];
+  for (uint32_t j = threadIdx.x; j < t.K; j += blockDim.x) BV[(2 * (K0 + j)) * R + r] = sm[2 * j];
 }
 
 // ---------------------------------------------------------------------------
 // k_advance: one block. Slots that computed their last row hand in their
 // minimum (score and smallest char index reaching it); idle slots admit the
 // next queued reads in order; every slot gets its word for the next step.
-// prime != 0 only recomputes the words (used after the host sets slots).
+// Admission and completion times (device global timer, ns) are recorded per
+// read. prime != 0 only recomputes the words (used after the host sets slots).
 // ---------------------------------------------------------------------------
 template <int R>
 __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
@@ -442,6 +629,8 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
                                                  unsigned long long* __restrict__ best,
                                                  int32_t* __restrict__ res_score,
                                                  uint32_t* __restrict__ res_vertex,
+                                                 unsigned long long* __restrict__ res_t0,
+                                                 unsigned long long* __restrict__ res_t1,
                                                  uint32_t* __restrict__ slot_word,
                                                  StepCtl* __restrict__ ctl, int special,
                                                  int prime) {
@@ -461,6 +650,7 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
         const unsigned long long b = best[r];
         res_score[st.id] = (int32_t)(b >> 32);
         res_vertex[st.id] = (uint32_t)(b & 0xffffffffu);
+        res_t1[st.id] = global_ns();
         atomicAdd(&ctl->done, 1u);
         st.id = -1;
       } else {
@@ -492,11 +682,13 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
       st.row = 0;
       st.id = q.id;
       best[r] = ~0ull;
+      res_t0[q.id] = global_ns();
     }
     uint32_t w = 0;
     if (st.id >= 0) {
       w = base_code(reads[st.off + st.row], special) | SW_ACTIVE;
       w |= st.row == 0 ? SW_INIT : SW_CLOSURE;
+      if (st.row >= 2) w |= SW_FIX;
       if (st.row + 1 == st.len) w |= SW_ENDING;
       atomicOr(&s_active, 1u);
       if (w & SW_ENDING) atomicOr(&s_ending, 1u);

@@ -255,12 +255,25 @@ void chsga_tb_result_free(chsga_tb_result* r);
  * terminator; returns the full length needed (excluding the terminator). */
 uint64_t chsga_ops_to_cigar(const chsga_op* ops, uint64_t n, char* buf, uint64_t cap);
 
-/* Per-phase device time of the last call (CHSGA_FLAG_PROFILE), in ms. */
+/* Device timing of the last score call. total_ms: CUDA-event time of the
+ * whole device sequence (every row-step, reads already resident). With
+ * CHSGA_FLAG_PROFILE (CUDA graphs off, one sync per row-step) the five kernel
+ * groups of every row-step are timed with CUDA events: row_ms (k_row),
+ * sweep_up_ms (upward level kernels), top_ms (top region), sweep_down_ms
+ * (downward levels with the final propagation), other_ms (slot advance). */
 typedef struct {
   double row_ms, sweep_up_ms, top_ms, sweep_down_ms, other_ms, total_ms;
-  uint64_t rows, launches;
+  uint64_t rows;          /* read rows computed */
+  uint64_t steps;         /* row-steps that had work */
+  uint64_t launches;      /* kernels launched by those steps */
+  uint64_t row_launches;  /* k_row launches */
 } chsga_profile;
 chsga_status chsga_get_profile(chsga_ctx* ctx, chsga_profile* out);
+
+/* Per-read admission and completion times of the last score call (device
+ * global timer, ns), in the order of the non-empty reads passed in. No
+ * reference counterpart: used for per-read latency percentiles. */
+chsga_status chsga_get_read_times(chsga_ctx* ctx, uint64_t* admit_ns, uint64_t* done_ns, uint32_t n);
 
 #ifdef __cplusplus
 }

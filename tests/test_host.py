@@ -1,0 +1,154 @@
+"""Host-side logic of libchsga: no GPU needed.
+
+The C-ABI library loads and exports every entry point include/chsga.h
+declares; file formats round-trip; the read loader follows kseq's record
+rules and load_reads' upper-casing and 5-read cap; the generator is
+deterministic; hierarchies satisfy the level invariants the GPU sweeps rely
+on; malformed inputs fail with the documented status codes; the drop-in
+tools keep the reference drivers' argument errors.
+"""
+import ctypes
+import gzip
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import chsga_b200 as cb
+from conftest import ROOT, gen_graph
+
+BIN = os.path.join(ROOT, "chsga_b200", "bin")
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(cb.LIB_PATH)
+    names = cb.exported_symbols()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_file_round_trip(tmp_path):
+    g, files = gen_graph(tmp_path, "a", backbone_len=4000, seed=3)
+    h = cb.HostGraph.read_files(*files)
+    a, b = g.view(), h.view()
+    assert a.num_chars == b.num_chars
+    for attr in ("char_graph", "string_graph"):
+        x, y = getattr(a, attr), getattr(b, attr)
+        assert x.n == y.n and x.m == y.m
+        assert np.array_equal(np.ctypeslib.as_array(x.offset, (x.n + 1,)),
+                              np.ctypeslib.as_array(y.offset, (y.n + 1,)))
+        assert np.array_equal(np.ctypeslib.as_array(x.target, (x.m,)),
+                              np.ctypeslib.as_array(y.target, (y.m,)))
+    assert a.pch.n == b.pch.n and a.pch.m == b.pch.m and a.pch.rm == b.pch.rm
+    # writing the re-read graph reproduces every file byte for byte
+    files2 = h.write_files(str(tmp_path / "b"))
+    for f1, f2 in zip(files, files2):
+        assert open(f1, "rb").read() == open(f2, "rb").read()
+
+
+def test_generator_is_deterministic(tmp_path):
+    _, f1 = gen_graph(tmp_path, "x", backbone_len=3000, seed=9)
+    _, f2 = gen_graph(tmp_path, "y", backbone_len=3000, seed=9)
+    for a, b in zip(f1, f2):
+        assert open(a, "rb").read() == open(b, "rb").read()
+
+
+def test_char_graph_is_the_string_expansion():
+    g = cb.HostGraph.generate(**dict(cb.GRAPH_CONFIGS["cfg1"], backbone_len=3000))
+    v = g.view()
+    S, N = v.string_graph.n, v.num_chars
+    offs = np.ctypeslib.as_array(v.label_offsets, (S + 1,))
+    so = np.ctypeslib.as_array(v.string_graph.offset, (S + 1,))
+    st = np.ctypeslib.as_array(v.string_graph.target, (v.string_graph.m,))
+    co = np.ctypeslib.as_array(v.char_graph.offset, (N + 1,))
+    ct = np.ctypeslib.as_array(v.char_graph.target, (v.char_graph.m,))
+    for s in range(S):
+        for c in range(offs[s], offs[s + 1] - 1):
+            assert list(ct[co[c]:co[c + 1]]) == [c + 1]
+        last = offs[s + 1] - 1
+        assert list(ct[co[last]:co[last + 1]]) == [offs[t] for t in st[so[s]:so[s + 1]]]
+    # char ids are topologically ordered (the exact DP relies on it)
+    for u in range(N):
+        assert all(t > u for t in ct[co[u]:co[u + 1]])
+
+
+def test_hierarchy_invariants():
+    g = cb.HostGraph.generate(**dict(cb.GRAPH_CONFIGS["cfg2"], backbone_len=200_000))
+    g.build_pch()
+    p = g.view().pch
+    n = p.n
+    rank = np.ctypeslib.as_array(p.rank, (n,))
+    level = np.ctypeslib.as_array(p.level, (n,))
+    assert sorted(rank.tolist()) == list(range(n))
+    lo = np.ctypeslib.as_array(p.layer_offset, (p.num_layers + 1,))
+    assert lo[0] == 0 and lo[-1] == n and (np.diff(lo) > 0).all()
+    for off, v, what in ((p.up_offset, p.up_v, "up"), (p.down_offset, p.down_v, "down")):
+        o = np.ctypeslib.as_array(off, (n + 1,))
+        t = np.ctypeslib.as_array(v, (int(o[-1]),))
+        src = np.repeat(np.arange(n), np.diff(o).astype(np.int64))
+        # every edge joins a lower level to a strictly higher one
+        assert (level[t] > level[src]).all(), what
+    st = g.stats()
+    assert st["pch_levels"] >= 10 and st["pch_up_edges"] > 0
+
+
+def test_reads_loader_rules(tmp_path):
+    fa = tmp_path / "r.fa"
+    fa.write_text(">a x\nacgt\nNNac\n\n>b\nTTT\n>c\nG\n>d\nAA\n>e\nC\n>f\nGG\n")
+    assert cb.Reads.load(str(fa)).to_list() == [b"ACGTNNAC", b"TTT", b"G", b"AA", b"C"]
+    assert len(cb.Reads.load(str(fa), max_reads=0)) == 6
+    fq = tmp_path / "r.fq.gz"
+    with gzip.open(fq, "wt") as f:
+        f.write("@r1\nACGTA\n+\nIIIII\n@r2\nGG\n+r2\n!!\n")
+    assert cb.Reads.load(str(fq), max_reads=0).to_list() == [b"ACGTA", b"GG"]
+    with pytest.raises(cb.ChsgaError) as e:
+        cb.Reads.load(str(tmp_path / "missing.fa"))
+    assert e.value.status == cb.ERR_IO
+
+
+def test_malformed_inputs_fail_with_status(tmp_path):
+    _, files = gen_graph(tmp_path, "m", backbone_len=2000, seed=5)
+    bad = list(files)
+    bad[2] = str(tmp_path / "nope.out")
+    with pytest.raises(cb.ChsgaError) as e:
+        cb.HostGraph.read_files(*bad)
+    assert e.value.status == cb.ERR_IO
+    trunc = tmp_path / "t.out"
+    trunc.write_bytes(open(files[2], "rb").read()[:100])
+    bad[2] = str(trunc)
+    with pytest.raises(cb.ChsgaError) as e:
+        cb.HostGraph.read_files(*bad)
+    assert e.value.status == cb.ERR_FORMAT
+    offs = tmp_path / "o.txt"
+    offs.write_text("0 1 2\n")
+    bad = list(files)
+    bad[4] = str(offs)
+    with pytest.raises(cb.ChsgaError) as e:
+        cb.HostGraph.read_files(*bad)
+    assert e.value.status == cb.ERR_FORMAT
+
+
+def test_cli_argument_errors(tmp_path):
+    for tool in ("ConSGA_mismatchN_dag", "ConSGA_traceback_mismatchN_dag"):
+        r = subprocess.run([os.path.join(BIN, tool), "-I", "x"], capture_output=True, text=True)
+        assert r.returncode == 1 and "Error: missing required arguments" in r.stderr
+        r = subprocess.run([os.path.join(BIN, tool), "-Z"], capture_output=True, text=True)
+        assert r.returncode == 1 and "Usage:" in r.stderr
+    r = subprocess.run([os.path.join(BIN, "build_pch")], capture_output=True, text=True)
+    assert r.returncode == 0 and "Usage" in r.stderr
+
+
+def test_build_pch_and_gen_tools(tmp_path):
+    p = str(tmp_path / "w")
+    r = subprocess.run([os.path.join(BIN, "chsga_gen"), "-o", p, "-B", "3000", "-n", "4", "-L", "60"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = str(tmp_path / "again.out")
+    r = subprocess.run([os.path.join(BIN, "build_pch"), "-i", p + ".string.adj", "-o", out, "-v",
+                        p + ".string.label_offsets"], capture_output=True, text=True)
+    assert r.returncode == 0 and "[ build time ]" in r.stdout
+    # the tool and the library build the same hierarchy for the same seed
+    assert open(out, "rb").read() == open(p + ".string.out", "rb").read()
+    assert len(cb.Reads.load(p + ".reads.fa", 0)) == 4

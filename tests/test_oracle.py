@@ -1,0 +1,122 @@
+"""The CPU oracle (oracle/consga_oracle.cpp) pinned against the reference.
+
+Three pins, all on CPU:
+  * golden fixtures made by the reference's own code (tests/golden/),
+  * the reference's align.hpp / traceback.hpp compiled in oracle/_ref, run
+    here on fresh random graphs (scores, every DP row, traceback, checkpoint
+    rows byte for byte),
+  * the reference's exact DP serial_align_CSR: equal to the hierarchy result
+    when every string vertex is a single char (the closure is then exact), and
+    never above it otherwise.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import chsga_b200 as cb
+import oracle as orc
+from conftest import gen_graph
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+needs_ref = pytest.mark.skipif(not orc.ref_available(), reason="oracle/_ref not built")
+
+
+def golden_files(name):
+    return cb.files_for(os.path.join(GOLD, name))
+
+
+def test_hand_dag_known_answers():
+    exp = json.load(open(os.path.join(GOLD, "hand.expected.json")))
+    o = orc.Oracle(golden_files("hand"))
+    reads = [r.encode() for r in exp["reads"]]
+    assert o.scores(reads).tolist() == [0, 0, 1, 1] == exp["scores"]
+    assert o.exact_scores(reads).tolist() == exp["exact"]
+
+
+def test_golden_scores_rows_and_checkpoints(tmp_path):
+    exp = json.load(open(os.path.join(GOLD, "g1.expected.json")))
+    o = orc.Oracle(golden_files("g1"))
+    reads = [r.encode() for r in exp["reads"]]
+    assert o.scores(reads).tolist() == exp["scores"]
+    assert o.exact_scores(reads).tolist() == exp["exact"]
+    rows = np.load(os.path.join(GOLD, "g1.rows0.npz"))["rows"].astype(np.int32)
+    np.testing.assert_array_equal(o.rows(reads[0]), rows)
+    d = tmp_path / "ck"
+    ops, score, ck = o.traceback(reads[0], k=exp["ckpt_k"], fast_cap_bytes=0, ckpt_dir=str(d),
+                                 cleanup=False)
+    assert ck and score == exp["scores"][0]
+    for i, h in exp["ckpt_rows_sha256"].items():
+        assert hashlib.sha256((d / f"row_{i}.bin").read_bytes()).hexdigest() == h
+    labels = open(golden_files("g1")[3], "rb").read()
+    assert orc.rescore(ops, reads[0], labels) == (exp["scores"][0], len(reads[0]) - 1)
+
+
+@needs_ref
+@pytest.mark.parametrize("seed,vmax", [(31, 1), (32, 4), (33, 32), (34, 12)])
+def test_oracle_matches_reference_code(tmp_path, seed, vmax):
+    g, files = gen_graph(tmp_path, f"r{seed}", backbone_len=2500, seed=seed, vlen_max=vmax,
+                         bubble_gap_mean=10.0, p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=3,
+                         alt_max=50)
+    reads = g.gen_reads(10, seed, 10, 120, sub_rate=0.05, indel_rate=0.05, n_rate=0.02).to_list()
+    o, r = orc.Oracle(files), orc.RefHarness(files)
+    np.testing.assert_array_equal(o.scores(reads), r.scores(reads))
+    for rd in reads[:2]:
+        np.testing.assert_array_equal(o.rows(rd), r.rows(rd, o.num_chars))
+
+
+@needs_ref
+def test_single_char_graphs_are_exact(tmp_path):
+    # with one char per string vertex the hierarchy sweeps are an exact
+    # shortest-path closure, so the reference's own CH result equals its
+    # exact DP; the oracle must agree with both
+    for seed in (41, 42, 43):
+        g, files = gen_graph(tmp_path, f"s{seed}", backbone_len=1500, seed=seed, vlen_max=1,
+                             bubble_gap_mean=6.0, p_snp=0.4, p_indel=0.4, p_alt=0.2, alt_min=2,
+                             alt_max=20)
+        reads = g.gen_reads(10, seed, 20, 90, sub_rate=0.06, indel_rate=0.06).to_list()
+        r = orc.RefHarness(files)
+        exact = r.exact_scores(reads)
+        np.testing.assert_array_equal(r.scores(reads), exact)
+        np.testing.assert_array_equal(orc.Oracle(files).scores(reads), exact)
+
+
+@needs_ref
+def test_multi_char_never_below_exact(tmp_path):
+    g, files = gen_graph(tmp_path, "m", backbone_len=4000, seed=51, bubble_gap_mean=12.0,
+                         p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=5, alt_max=80)
+    reads = g.gen_reads(30, 52, 30, 150, sub_rate=0.05, indel_rate=0.05).to_list()
+    ch = orc.Oracle(files).scores(reads)
+    exact = orc.RefHarness(files).exact_scores(reads)
+    assert (ch >= exact).all()
+
+
+@needs_ref
+def test_traceback_paths_rescore(tmp_path):
+    g, files = gen_graph(tmp_path, "t", backbone_len=3000, seed=61, bubble_gap_mean=15.0,
+                         p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=4, alt_max=40)
+    reads = g.gen_reads(6, 62, 40, 140, sub_rate=0.04, indel_rate=0.04, n_rate=0.01).to_list()
+    labels = open(files[3], "rb").read()
+    o, fast, slow = orc.Oracle(files), orc.RefHarness(files), orc.RefHarness(files, True)
+    want = o.scores(reads)
+    for i, rd in enumerate(reads):
+        for ops in (fast.traceback(rd), slow.traceback(rd, k=25, ckpt_dir=str(tmp_path / f"c{i}")),
+                    o.traceback(rd)[0], o.traceback(rd, k=25, fast_cap_bytes=0,
+                                                    ckpt_dir=str(tmp_path / f"o{i}"))[0]):
+            assert orc.rescore(ops, rd, labels) == (want[i], len(rd) - 1)
+
+
+@needs_ref
+def test_checkpoint_rows_byte_identical_to_reference(tmp_path):
+    g, files = gen_graph(tmp_path, "k", backbone_len=2000, seed=71, bubble_gap_mean=15.0,
+                         p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=4, alt_max=40)
+    rd = g.gen_reads(1, 72, 130, sub_rate=0.04, indel_rate=0.04).to_list()[0]
+    a, b = tmp_path / "ref", tmp_path / "orc"
+    orc.RefHarness(files, True).traceback(rd, k=20, ckpt_dir=str(a), cleanup=False)
+    orc.Oracle(files).traceback(rd, k=20, fast_cap_bytes=0, ckpt_dir=str(b), cleanup=False)
+    names = sorted(os.listdir(a))
+    assert names == sorted(os.listdir(b)) and len(names) == 7  # rows 0, 20, ..., 120
+    for n in names:
+        assert (a / n).read_bytes() == (b / n).read_bytes()
