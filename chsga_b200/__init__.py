@@ -87,12 +87,19 @@ class GraphStats(C.Structure):
         "single_char_strings")]
 
 
+class LayoutStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in (
+        "num_levels", "top_first_level", "top_vertices", "tiled", "tiles", "long_tiles",
+        "slot_bytes", "slots_per_block", "smem_bytes")]
+
+
 class OptsT(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_cap_bytes", C.c_uint64), ("flags", C.c_uint32)]
 
 
 class BatchOpts(C.Structure):
-    _fields_ = [("slots", C.c_uint32), ("steps_per_graph", C.c_uint32), ("use_graphs", C.c_uint32)]
+    _fields_ = [("slots", C.c_uint32), ("steps_per_graph", C.c_uint32), ("use_graphs", C.c_uint32),
+                ("row_bits", C.c_uint32)]
 
 
 class TbOpts(C.Structure):
@@ -113,7 +120,8 @@ class TbResult(C.Structure):
 class ProfileT(C.Structure):
     _fields_ = [("row_ms", C.c_double), ("sweep_up_ms", C.c_double), ("top_ms", C.c_double),
                 ("sweep_down_ms", C.c_double), ("other_ms", C.c_double), ("total_ms", C.c_double),
-                ("rows", C.c_uint64), ("steps", C.c_uint64), ("launches", C.c_uint64),
+                ("row_bits", C.c_uint64), ("rows", C.c_uint64), ("steps", C.c_uint64),
+                ("launches", C.c_uint64),
                 ("row_launches", C.c_uint64)]
 
 
@@ -134,6 +142,7 @@ _sig("chsga_graph_write_files", C.c_int32, vp, C.c_char_p)
 _sig("chsga_gen_graph", C.c_int32, C.POINTER(GenGraphCfg), C.POINTER(vp))
 _sig("chsga_build_pch", C.c_int32, vp, C.POINTER(PchOpts))
 _sig("chsga_graph_get_stats", C.c_int32, vp, C.POINTER(GraphStats))
+_sig("chsga_check_layout", C.c_int32, vp, C.c_uint32, C.c_uint32, C.POINTER(LayoutStats))
 _sig("chsga_reads_load", C.c_int32, C.c_char_p, C.c_uint64, C.POINTER(vp))
 _sig("chsga_reads_from_arrays", C.c_int32, C.c_char_p, u64p, C.c_uint64, C.POINTER(vp))
 _sig("chsga_reads_count", C.c_uint64, vp)
@@ -273,6 +282,12 @@ class HostGraph:
         _check(_lib.chsga_graph_get_stats(self._h, C.byref(s)))
         return {k: int(getattr(s, k)) for k, _ in GraphStats._fields_}
 
+    def check_layout(self, slots: int, row_bits: int) -> dict:
+        """Host-side pre-flight of the device layout (chsga_check_layout)."""
+        st = LayoutStats()
+        _check(_lib.chsga_check_layout(self._h, slots, row_bits, C.byref(st)))
+        return {k: int(getattr(st, k)) for k, _ in LayoutStats._fields_}
+
     def view(self) -> GraphHostT:
         v = GraphHostT()
         _check(_lib.chsga_graph_view(self._h, C.byref(v)))
@@ -333,10 +348,10 @@ class Context:
         return out
 
     def align_scores_batched(self, reads: Sequence[bytes], slots: int = 64, steps_per_graph: int = 8,
-                             use_graphs: bool = True) -> np.ndarray:
+                             use_graphs: bool = True, row_bits: int = 0) -> np.ndarray:
         arr, lens = _read_ptrs(reads)
         out = np.zeros(len(reads), dtype=np.int32)
-        o = BatchOpts(slots, steps_per_graph, int(use_graphs))
+        o = BatchOpts(slots, steps_per_graph, int(use_graphs), row_bits)
         self._ck(_lib.chsga_align_scores_batched(self._h, arr, lens.ctypes.data_as(u32p), len(reads),
                                                  C.byref(o), out.ctypes.data_as(i32p)))
         return out

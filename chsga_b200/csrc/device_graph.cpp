@@ -60,6 +60,7 @@ HostLayout build_layout(const chsga_graph_host& g) {
             "string vertex " + std::to_string(s) + " has an empty label");
     require(L.sv_off[s + 1] - L.sv_off[s] < (1u << 29), CHSGA_ERR_UNSUPPORTED,
             "string vertex labels must be shorter than 2^29 chars");
+    L.max_len = std::max(L.max_len, L.sv_off[s + 1] - L.sv_off[s]);
     for (uint32_t c = L.sv_off[s]; c < L.sv_off[s + 1]; ++c) vertex_of[c] = s;
   }
   const chsga_csr& cg = g.char_graph;
@@ -145,18 +146,22 @@ HostLayout build_layout(const chsga_graph_host& g) {
   for (uint32_t d = 0; d < S; ++d) dev[order[d]] = d;
   L.dv_first.resize(S);
   L.dv_len.resize(S);
+  L.dv_s.resize(S);
   for (uint32_t d = 0; d < S; ++d) {
     uint32_t s = og[order[d]];
     L.dv_first[d] = L.sv_off[s];
     L.dv_len[d] = L.sv_off[s + 1] - L.sv_off[s];
+    L.dv_s[d] = s;
   }
   L.sv_dev.resize(S);
   for (uint32_t s = 0; s < S; ++s) L.sv_dev[s] = dev[p.rank[s]];
-  L.vin_fix.resize(L.vin_src.size());
-  for (size_t k = 0; k < L.vin_src.size(); ++k) {
-    const uint32_t sv = L.vin_srcv[k];
-    L.vin_fix[k] = {(int32_t)L.sv_dev[sv], (int32_t)(L.vin_src[k] - L.sv_off[sv])};
-  }
+  // a first char's in-edges come from last chars (the string expansion); the
+  // row kernels read those sources' final scores from the per-vertex array
+  for (size_t k = 0; k < L.vin_src.size(); ++k)
+    require(L.vin_src[k] + 1 == L.sv_off[L.vin_srcv[k] + 1], CHSGA_ERR_UNSUPPORTED,
+            "char " + std::to_string(L.vin_src[k]) +
+                " has an edge to the first char of another string but is not the last char of "
+                "its own string: the char graph must be the expansion of the string graph");
   auto bv_last = [&](uint32_t rank) { return 2 * dev[rank] + (L.dv_len[dev[rank]] > 1 ? 1 : 0); };
   // pull lists
   std::vector<std::vector<EdgeW>> up(S), dn(S);
@@ -166,7 +171,8 @@ HostLayout build_layout(const chsga_graph_host& g) {
       require(v < S, CHSGA_ERR_FORMAT, "hierarchy edge out of range");
       require(cc_of[v] == cc_of[u] && layer_of[v] > layer_of[u], CHSGA_ERR_UNSUPPORTED,
               "upward hierarchy edge does not climb to a later layer of its component");
-      require(p.up_w[j] <= (1u << 30), CHSGA_ERR_UNSUPPORTED, "hierarchy weight too large");
+      require(p.up_w[j] >= 1 && p.up_w[j] <= (1u << 30), CHSGA_ERR_UNSUPPORTED,
+              "hierarchy weights must be in [1, 2^30]");
       up[dev[v]].push_back({(int32_t)bv_last(u), (int32_t)p.up_w[j]});
     }
     for (uint64_t j = p.down_offset[u]; j < p.down_offset[u + 1]; ++j) {
@@ -174,7 +180,8 @@ HostLayout build_layout(const chsga_graph_host& g) {
       require(v < S, CHSGA_ERR_FORMAT, "hierarchy edge out of range");
       require(cc_of[v] == cc_of[u] && layer_of[v] > layer_of[u], CHSGA_ERR_UNSUPPORTED,
               "downward hierarchy edge does not come from a later layer of its component");
-      require(p.down_w[j] <= (1u << 30), CHSGA_ERR_UNSUPPORTED, "hierarchy weight too large");
+      require(p.down_w[j] >= 1 && p.down_w[j] <= (1u << 30), CHSGA_ERR_UNSUPPORTED,
+              "hierarchy weights must be in [1, 2^30]");
       dn[dev[u]].push_back({(int32_t)bv_last(v), (int32_t)p.down_w[j]});
     }
   }
@@ -213,6 +220,146 @@ HostLayout build_layout(const chsga_graph_host& g) {
       for (uint64_t e = sg.offset[u]; e < sg.offset[u + 1]; ++e) L.istr_src[cur[sg.target[e]]++] = (uint32_t)u;
   }
   return L;
+}
+
+size_t row_tiled_smem(const HostRowTiles& t, uint32_t R) {
+  // slots, full and empty barriers, per-slot minima, spare
+  return (size_t)t.nslots * t.slot_bytes() + (size_t)kTileSlotsMax * 16 + (size_t)R * 8 + 16;
+}
+
+HostRowTiles build_row_tiles(const HostLayout& L, uint32_t R, uint32_t sz) {
+  HostRowTiles t;
+  const uint32_t PC = R * sz;  // bytes per char slot-row (and per FL entry)
+  require(R >= 32 && PC % 16 == 0, CHSGA_ERR_INTERNAL, "tiled rows need R >= 32");
+  t.d_cap = std::max<uint32_t>(8192, 32 * PC);
+  t.fl_cap = 2 * kTileMaxVerts * PC;
+  t.desc_cap = (16 * kTileMaxVerts + 4 * kTileMaxEdges + 15) / 16 * 16;
+  t.ext_cap = kTileMaxExt * PC;
+  t.nslots = std::min<uint32_t>(kTileSlotsMax, kTileSmemBudget / t.slot_bytes());
+  if (t.nslots < 2) return t;
+  auto edges_of = [&](uint32_t s) { return L.vin_off[s + 1] - L.vin_off[s]; };
+  auto n_ext = [&](uint32_t s0, uint32_t e1) {
+    uint32_t x = 0;
+    for (uint32_t v = s0; v < e1; ++v)
+      for (uint32_t k = L.vin_off[v]; k < L.vin_off[v + 1]; ++k)
+        x += (L.vin_srcv[k] < s0 || L.vin_srcv[k] >= e1) ? 1 : 0;
+    return x;
+  };
+  uint32_t s = 0;
+  while (s < L.S) {
+    const uint32_t s0 = s, c0 = L.sv_off[s0];
+    const bool lng = (uint64_t)(L.sv_off[s0 + 1] - c0) * PC > t.d_cap;
+    uint32_t s1 = s0 + 1, ne = edges_of(s0);
+    if (ne > kTileMaxEdges || n_ext(s0, s1) > kTileMaxExt) return HostRowTiles{};
+    if (!lng) {
+      while (s1 < L.S && s1 - s0 < kTileMaxVerts &&
+             (uint64_t)(L.sv_off[s1 + 1] - c0) * PC <= t.d_cap &&
+             ne + edges_of(s1) <= kTileMaxEdges && n_ext(s0, s1 + 1) <= kTileMaxExt) {
+        ne += edges_of(s1);
+        ++s1;
+      }
+    }
+    const uint32_t off = (uint32_t)t.desc.size();
+    std::vector<uint32_t> ext;
+    uint32_t eb = 0;
+    for (uint32_t v = s0; v < s1; ++v) {
+      const uint32_t ec = edges_of(v);
+      t.desc.push_back(L.sv_off[v]);
+      t.desc.push_back(L.sv_off[v + 1] - L.sv_off[v]);
+      t.desc.push_back(L.sv_dev[v]);
+      t.desc.push_back((eb << 16) | ec);
+      eb += ec;
+    }
+    for (uint32_t v = s0; v < s1; ++v)
+      for (uint32_t k = L.vin_off[v]; k < L.vin_off[v + 1]; ++k) {
+        const uint32_t su = L.vin_srcv[k];
+        if (su >= s0 && su < s1) {
+          t.desc.push_back(su - s0);
+        } else {
+          t.desc.push_back(0x80000000u | (uint32_t)ext.size());
+          ext.push_back(su);
+        }
+      }
+    while (t.desc.size() % 4) t.desc.push_back(0);
+    const uint32_t bytes = (uint32_t)(t.desc.size() - off) * 4;
+    const uint32_t ext_off = (uint32_t)t.desc.size();
+    t.desc.insert(t.desc.end(), ext.begin(), ext.end());
+    while (t.desc.size() % 4) t.desc.push_back(0);
+    const uint32_t c1 = L.sv_off[s1];
+    const int32_t r0[4] = {(int32_t)s0, (int32_t)s1, (int32_t)c0,
+                           (int32_t)(lng ? (c1 | 0x80000000u) : c1)};
+    const int32_t r1[4] = {(int32_t)off, (int32_t)bytes, (int32_t)ext.size(), (int32_t)ext_off};
+    t.rec.insert(t.rec.end(), r0, r0 + 4);
+    t.rec.insert(t.rec.end(), r1, r1 + 4);
+    t.long_tiles += lng ? 1 : 0;
+    s = s1;
+  }
+  t.ok = true;
+  return t;
+}
+
+void validate_row_tiles(const HostLayout& L, uint32_t R, uint32_t sz, const HostRowTiles& t) {
+  auto bad = [&](uint32_t tile, const std::string& m) {
+    fail(CHSGA_ERR_INTERNAL, "row tile " + std::to_string(tile) + ": " + m);
+  };
+  if (!t.ok) return;
+  const uint64_t PC = (uint64_t)R * sz;
+  const uint64_t row_bytes = ((uint64_t)L.N + 32) * PC;      // score row allocation
+  const uint64_t fl_bytes = 2 * ((uint64_t)L.S + 16) * PC;   // FL allocation
+  if (t.slot_bytes() % 16 || t.d_cap % 16 || t.fl_cap % 16 || t.desc_cap % 16 || t.ext_cap % 16)
+    bad(0, "slot regions must be multiples of 16 bytes");
+  if (row_tiled_smem(t, R) + 16 > kSmemPerBlockMax) bad(0, "shared memory above the per-block limit");
+  if (t.nslots < 2 || t.nslots > kTileSlotsMax) bad(0, "slot count");
+  uint32_t next_s = 0;
+  for (uint32_t i = 0; i < t.ntiles(); ++i) {
+    const int32_t* r0 = &t.rec[8 * i];
+    const int32_t* r1 = r0 + 4;
+    const uint32_t s0 = (uint32_t)r0[0], s1 = (uint32_t)r0[1], c0 = (uint32_t)r0[2];
+    const bool lng = r0[3] < 0;
+    const uint32_t c1 = (uint32_t)r0[3] & 0x7fffffffu;
+    if (s0 != next_s || s1 <= s0 || s1 > L.S) bad(i, "tiles must cover the vertices in order");
+    next_s = s1;
+    const uint32_t nv = s1 - s0;
+    if (nv > kTileMaxVerts || (lng && nv != 1)) bad(i, "vertex count");
+    if (c0 != L.sv_off[s0] || c1 != L.sv_off[s1]) bad(i, "char range");
+    if (!lng) {
+      const uint64_t db = (uint64_t)(c1 - c0) * PC;
+      if (db > t.d_cap || (c0 * PC) % 16 || db % 16 || c0 * PC + db > row_bytes) bad(i, "score copy");
+    }
+    const uint64_t flo = 2 * (uint64_t)s0 * PC, flb = 2 * (uint64_t)nv * PC;
+    if (flb > t.fl_cap || flo % 16 || flb % 16 || flo + flb > fl_bytes) bad(i, "FL copy");
+    const uint32_t off = (uint32_t)r1[0], bytes = (uint32_t)r1[1], next = (uint32_t)r1[2],
+                   eoff = (uint32_t)r1[3];
+    if (off % 4 || bytes % 16 || bytes > t.desc_cap || (uint64_t)off * 4 + bytes > t.desc.size() * 4)
+      bad(i, "descriptor copy");
+    if (next > kTileMaxExt || (uint64_t)next * PC > t.ext_cap || eoff + next > t.desc.size())
+      bad(i, "external list");
+    uint32_t eb = 0, edges = 0;
+    for (uint32_t j = 0; j < nv; ++j) {
+      const uint32_t* vr = &t.desc[off + 4 * j];
+      const uint32_t s = s0 + j;
+      if (vr[0] != L.sv_off[s] || vr[1] != L.sv_off[s + 1] - L.sv_off[s] || vr[2] != L.sv_dev[s] ||
+          (vr[3] >> 16) != eb || (vr[3] & 0xFFFFu) != L.vin_off[s + 1] - L.vin_off[s])
+        bad(i, "vertex record " + std::to_string(j));
+      eb += vr[3] & 0xFFFFu;
+    }
+    edges = eb;
+    if (16ull * nv + 4ull * edges > bytes) bad(i, "descriptor shorter than its records");
+    uint32_t q = 0;
+    for (uint32_t j = 0; j < nv; ++j)
+      for (uint32_t k = L.vin_off[s0 + j]; k < L.vin_off[s0 + j + 1]; ++k, ++q) {
+        const uint32_t loc = t.desc[off + 4 * nv + q];
+        const uint32_t su = L.vin_srcv[k];
+        if (loc & 0x80000000u) {
+          const uint32_t x = loc & 0x7fffffffu;
+          if (x >= next || t.desc[eoff + x] != su || (2ull * su + 2) * PC > fl_bytes)
+            bad(i, "external in-edge record");
+        } else if (loc >= nv || s0 + loc != su) {
+          bad(i, "internal in-edge record");
+        }
+      }
+  }
+  if (next_s != L.S) bad(t.ntiles(), "tiles do not reach the last vertex");
 }
 
 HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edges) {

@@ -44,14 +44,14 @@ struct EdgeW {  // matches the device int2 layout
 
 struct HostLayout {
   uint32_t N = 0, S = 0, levels = 0;
+  uint32_t max_len = 0;  // longest string vertex label
   // label encoding: code 0..3 for A,C,G,T; `special` holds the one other
   // byte that may occur in the labels (usually 'N'), flagged in lab_sp
   int special = -1;
   std::vector<uint32_t> lab2;   // ceil(N/16) words
   std::vector<uint32_t> lab_sp; // ceil(N/32) words
   std::vector<uint32_t> sv_off, sv_dev, vin_off, vin_src, vin_srcv;
-  std::vector<EdgeW> vin_fix;  // {hierarchy position of vertex(src), src - first(vertex(src))}
-  std::vector<uint32_t> dv_first, dv_len;  // by hierarchy order
+  std::vector<uint32_t> dv_first, dv_len, dv_s;  // by hierarchy order
   std::vector<uint32_t> up_off, dn_off;    // S+1, by hierarchy order
   std::vector<EdgeW> up_in, dn_in;
   std::vector<uint32_t> lvl_off;           // levels+1
@@ -74,6 +74,36 @@ struct HostTop {
   std::vector<EdgeW> sched;       // src = target << 16 | local source, w
   std::vector<std::pair<int32_t, int32_t>> chunks;  // {first edge, count}
 };
+
+// Tiles of consecutive string vertices for the shared-memory-staged row
+// kernel (one warp per vertex, R >= 32 slots). Per tile: two int4 records
+// r0 = {s0, s1, c0, c1 | long << 31}, r1 = {descriptor word offset,
+// descriptor bytes, external count, external list word offset}; descriptor
+// = per vertex {first char, length, hierarchy position, first edge << 16 |
+// edge count}, then one word per in-edge (source vertex - s0 inside the tile,
+// else 0x80000000 | external index), padded to 16 bytes, then the external
+// source vertices. Each slot of shared memory holds the tile's scores
+// (d_cap), its per-vertex final first/last scores (fl_cap), the descriptor
+// (desc_cap) and the external sources' last scores (ext_cap).
+constexpr uint32_t kTileMaxVerts = 16, kTileMaxEdges = 48, kTileMaxExt = 4;
+constexpr uint32_t kTileSlotsMax = 16, kTileSmemBudget = 200 * 1024;
+constexpr uint32_t kSmemPerBlockMax = 232448;  // sm_100 opt-in maximum
+
+struct HostRowTiles {
+  bool ok = false;  // false: some vertex cannot fit a tile (use the direct kernel)
+  uint32_t d_cap = 0, fl_cap = 0, desc_cap = 0, ext_cap = 0, nslots = 0;
+  std::vector<int32_t> rec;   // 8 per tile
+  std::vector<uint32_t> desc;
+  uint32_t long_tiles = 0;
+  uint32_t slot_bytes() const { return d_cap + fl_cap + desc_cap + ext_cap; }
+  uint32_t ntiles() const { return (uint32_t)(rec.size() / 8); }
+};
+
+// Shared memory of the tiled row kernel for these tiles.
+size_t row_tiled_smem(const HostRowTiles& t, uint32_t R);
+HostRowTiles build_row_tiles(const HostLayout& L, uint32_t R, uint32_t score_bytes);
+// Checks every bound and alignment the kernel relies on; throws on violation.
+void validate_row_tiles(const HostLayout& L, uint32_t R, uint32_t score_bytes, const HostRowTiles& t);
 
 HostLayout build_layout(const chsga_graph_host& g);
 HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edges);

@@ -10,6 +10,7 @@
 #include <map>
 #include <memory>
 #include <new>
+#include <type_traits>
 
 #include "device_graph.hpp"
 #include "host_graph.hpp"
@@ -77,7 +78,8 @@ struct PinnedArr {
 struct GraphDev {
   DevArr<uint32_t> lab2, lab_sp, sv_off, sv_dev, vin_off, vin_src, vin_srcv, dv_first, dv_len;
   DevArr<uint32_t> up_off, dn_off, istr_off, istr_src;
-  DevArr<int2> up_in, dn_in, vin_fix;
+  DevArr<uint32_t> dv_s;
+  DevArr<int2> up_in, dn_in;
 };
 
 struct TopDev {
@@ -87,18 +89,33 @@ struct TopDev {
   dev::TopPtrs ptrs{};
 };
 
-// Buffers of one slot configuration (R slots).
+// Buffers of one slot configuration (R slots). Score rows and boundary
+// arrays are raw bytes used as int32 or uint16 storage (see scores_with).
 struct SlotBufs {
   int R = 0;
-  DevArr<int> rows[2];
-  DevArr<int> BV, BV2;  // BV2: second boundary buffer of the deferred score-only mode
+  DevArr<unsigned char> rows[2];
+  DevArr<unsigned char> BV;
+  DevArr<unsigned char> FL;  // final first/last score per vertex, char order
   DevArr<dev::SlotState> slots;
   DevArr<uint32_t> word;
   DevArr<unsigned long long> best;
   DevArr<dev::StepCtl> ctl;
 };
 
-constexpr uint32_t kTopMaxVertices = 23000;  // 2 x int32 per vertex in shared memory
+// Row kernel choice: the DPX kernel for 16-bit rows (default), the direct
+// kernel, or the shared-memory tile-staged kernel (CHSGA_ROW_KERNEL=direct |
+// tiled, for comparisons).
+enum class RowKernel { Auto, Direct, Tiled };
+
+struct RowTileDev {
+  DevArr<int4> rec;
+  DevArr<uint32_t> desc;
+  dev::RowTiles rt{};
+  bool ok = false;
+};
+
+constexpr uint32_t kTopMaxVertices = 23000;
+constexpr uint32_t kRow16Max = 65000;  // longest read whose rows fit uint16  // 2 x int32 per vertex in shared memory
 constexpr int kTopThreads = 1024;
 
 }  // namespace chsga
@@ -116,6 +133,10 @@ struct chsga_ctx {
   chsga::dev::GraphPtrs gp{};
   std::unique_ptr<chsga::TopDev> top;
   std::map<int, std::unique_ptr<chsga::SlotBufs>> bufs;
+  std::map<int, std::unique_ptr<chsga::RowTileDev>> row_tiles;  // by R * 8 + sizeof(score)
+  int num_sms = 148;
+  chsga::RowKernel row_kernel = chsga::RowKernel::Auto;
+  size_t pitch = 0;  // traceback matrix row stride (elements), 16-byte aligned rows
   chsga::DevArr<unsigned char> reads;
   chsga::DevArr<chsga::dev::ReadDesc> queue;
   chsga::DevArr<int32_t> res_score;
@@ -139,25 +160,26 @@ void set_device(chsga_ctx& c) { CK(cudaSetDevice(c.device)); }
 
 void check_launch() { CK(cudaGetLastError()); }
 
-template <int R>
+template <int R, typename ST>
 SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
   auto& b = c.bufs[R];
   if (!b) b = std::make_unique<SlotBufs>();
   b->R = R;
   const size_t N = c.L.N, S = c.L.S;
   if (need_rows) {
-    b->rows[0].alloc(N * R);
-    b->rows[1].alloc(N * R);
-    b->BV2.alloc(2 * S * R);
+    // bulk tile copies may read up to 16 bytes past the last char
+    b->rows[0].alloc((N + 32) * R * sizeof(ST));
+    b->rows[1].alloc((N + 32) * R * sizeof(ST));
   }
-  b->BV.alloc(2 * S * R);
+  b->BV.alloc(2 * S * R * sizeof(ST));
+  b->FL.alloc(2 * (S + 16) * R * sizeof(ST));
   b->slots.alloc(R);
   b->word.alloc(R);
   b->best.alloc(R);
   b->ctl.alloc(1);
   static bool attr_set = false;
   if (!attr_set) {
-    CK(cudaFuncSetAttribute(dev::k_top<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CK(cudaFuncSetAttribute(dev::k_top<R, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)dev::top_smem_bytes(kTopMaxVertices)));
     attr_set = true;
   }
@@ -204,6 +226,45 @@ void reset_slots(chsga_ctx& c, SlotBufs& b, uint32_t q_count) {
   CK(cudaStreamSynchronize(c.st));  // host copies above are from stack memory
 }
 
+// Tiles of consecutive string vertices for k_row_tiled (R >= 32): per tile
+// the char range, the FL range, a descriptor of vertex and in-edge records
+// and the list of in-edge source vertices outside the tile (see
+// kernels.cuh). Returns nullptr when some vertex cannot fit a tile (too many
+// in-edges), in which case the direct kernel runs instead.
+template <int R, typename ST>
+const dev::RowTiles* row_tiles(chsga_ctx& c) {
+  if constexpr (R < 32) {
+    return nullptr;
+  } else {
+    auto& slot = c.row_tiles[R * 8 + (int)sizeof(ST)];
+    if (slot) return slot->ok ? &slot->rt : nullptr;
+    slot = std::make_unique<RowTileDev>();
+    const HostRowTiles h = build_row_tiles(c.L, R, sizeof(ST));
+    if (!h.ok) return nullptr;
+    validate_row_tiles(c.L, R, sizeof(ST), h);
+    std::vector<int4> rec(h.ntiles() * 2);
+    std::memcpy(rec.data(), h.rec.data(), h.rec.size() * 4);
+    slot->rec.upload(rec, c.st);
+    slot->desc.upload(h.desc, c.st);
+    CK(cudaStreamSynchronize(c.st));
+    dev::RowTiles rt{};
+    rt.rec = slot->rec.p;
+    rt.desc = slot->desc.p;
+    rt.ntiles = h.ntiles();
+    rt.nslots = h.nslots;
+    rt.d_cap = h.d_cap;
+    rt.fl_cap = h.fl_cap;
+    rt.desc_cap = h.desc_cap;
+    rt.ext_cap = h.ext_cap;
+    slot->rt = rt;
+    slot->ok = true;
+    const int smem = (int)row_tiled_smem(h, R);
+    CK(cudaFuncSetAttribute(dev::k_row_tiled<R, true, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CK(cudaFuncSetAttribute(dev::k_row_tiled<R, false, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return &slot->rt;
+  }
+}
+
 // Fails with CHSGA_ERR_TIMEOUT if a kernel's bounded wait expired.
 void check_device_error(chsga_ctx& c, SlotBufs& b) {
   dev::StepCtl fin{};
@@ -247,41 +308,63 @@ struct StepEvents {
 // BVc = this step's boundary scores. DEFER (score-only): rows stay raw and
 // BVp holds the previous step's swept boundary scores; otherwise every row
 // is written final (rows that are kept for traceback).
-template <int R, bool DEFER>
-void row_step(chsga_ctx& c, SlotBufs& b, const int* D, int* T, int* BVc, const int* BVp,
-              cudaStream_t s, StepEvents* ev = nullptr) {
+template <int R, bool DEFER, typename ST>
+void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
+              StepEvents* ev = nullptr) {
+  ST* BVc = reinterpret_cast<ST*>(b.BV.p);
   const HostLayout& L = c.L;
   const TopDev& top = *c.top;
   constexpr int G = Lanes<R>::G;
   if (ev) CK(cudaEventRecord(ev->e[0], s));
-  dev::k_row<R, DEFER><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(c.gp, D, T, BVc, BVp, b.word.p,
-                                                                   b.best.p, b.ctl.p);
+  ST* FL = reinterpret_cast<ST*>(b.FL.p);
+  bool done = false;
+  if constexpr (std::is_same_v<ST, uint16_t> && R >= 2) {
+    // packed 16-bit DPX kernel; exact while F + (c - first) stays below 2^16
+    if (L.max_len <= 512 && c.row_kernel != RowKernel::Tiled && c.row_kernel != RowKernel::Direct) {
+      dev::k_row_dpx<R, DEFER><<<nblocks((uint64_t)L.S * dev::Pairs<R>::G), 256, 0, s>>>(
+          c.gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+      done = true;
+    }
+  }
+  if constexpr (R >= 32) {
+    if (!done && c.row_kernel == RowKernel::Tiled) {
+      if (const dev::RowTiles* rt = row_tiles<R, ST>(c)) {
+        dev::k_row_tiled<R, DEFER, ST>
+            <<<c.num_sms, dev::kRowThreads, dev::row_smem_bytes(dev::row_slot_bytes(*rt), rt->nslots, R),
+               s>>>(c.gp, *rt, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+        done = true;
+      }
+    }
+  }
+  if (!done)
+    dev::k_row_direct<R, DEFER, ST><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(
+        c.gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
   if (ev) CK(cudaEventRecord(ev->e[1], s));
   const uint32_t fl = top.h.first_level;
   for (uint32_t l = 0; l < fl; ++l) {
     if (L.lvl_up_edges[l] == 0) continue;
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
-    dev::k_pull<R><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
+    dev::k_pull<R, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
         BVc, lo, hi, c.gd.up_off.p, c.gd.up_in.p, 0, b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[2], s));
   if (top.h.K) {
     if (!top.h.upg.empty())
-      dev::k_pull<R><<<nblocks((uint64_t)top.h.K * G), 256, 0, s>>>(
+      dev::k_pull<R, ST><<<nblocks((uint64_t)top.h.K * G), 256, 0, s>>>(
           BVc, top.h.K0, L.S, top.upg_off.p, top.upg.p, top.h.K0, b.ctl.p);
-    dev::k_top<R><<<R, kTopThreads, dev::top_smem_bytes(top.h.K), s>>>(BVc, top.ptrs, b.word.p,
+    dev::k_top<R, ST><<<R, kTopThreads, dev::top_smem_bytes(top.h.K), s>>>(BVc, top.ptrs, b.word.p,
                                                                        b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[3], s));
   if (fl == 0) {
-    dev::k_down<R, !DEFER><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(c.gp, BVc, T, 0, 0, L.S,
-                                                                       b.word.p, b.best.p, b.ctl.p);
+    dev::k_down<R, !DEFER, ST><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(
+        c.gp, BVc, T, FL, 0, 0, L.S, b.word.p, b.best.p, b.ctl.p);
   } else {
     for (int l = (int)fl - 1; l >= 0; --l) {
       const uint32_t lo = L.lvl_off[l], mid = L.lvl_off[l + 1];
       const uint32_t hi = (l == (int)fl - 1) ? L.S : mid;
-      dev::k_down<R, !DEFER><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-          c.gp, BVc, T, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
+      dev::k_down<R, !DEFER, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
+          c.gp, BVc, T, FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
     }
   }
   if (ev) CK(cudaEventRecord(ev->e[4], s));
@@ -301,9 +384,10 @@ uint32_t kernels_per_step(const chsga_ctx& c) {
 // Runs every queued read to completion through R slots. Steps are captured
 // in CUDA graphs of `per_graph` row-steps (even, so the two row buffers
 // alternate identically in every launch).
-template <int R>
+template <int R, typename ST>
 void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, uint32_t per_graph) {
-  SlotBufs& b = get_bufs<R>(c, true);
+  SlotBufs& b = get_bufs<R, ST>(c, true);
+  if (c.row_kernel == RowKernel::Tiled) row_tiles<R, ST>(c);  // allocates: never inside a capture
   reset_slots<R>(c, b, n);
   const bool profile = (c.flags & CHSGA_FLAG_PROFILE) != 0;
   if (profile) use_graphs = false;
@@ -322,10 +406,10 @@ void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, u
   CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
-  int* BVs[2] = {b.BV.p, b.BV2.p};
+  ST* rows[2] = {reinterpret_cast<ST*>(b.rows[0].p), reinterpret_cast<ST*>(b.rows[1].p)};
   auto enqueue_block = [&](cudaStream_t s) {
     for (uint32_t i = 0; i < per_graph; ++i)
-      row_step<R, true>(c, b, b.rows[i & 1].p, b.rows[(i + 1) & 1].p, BVs[(i + 1) & 1], BVs[i & 1], s);
+      row_step<R, true, ST>(c, b, rows[i & 1], rows[(i + 1) & 1], s);
   };
   if (use_graphs) {
     cudaStream_t cap;
@@ -341,8 +425,7 @@ void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, u
       CK(cudaGraphLaunch(exec, c.st));
     } else if (profile) {
       for (uint32_t i = 0; i < per_graph; ++i) {
-        row_step<R, true>(c, b, b.rows[i & 1].p, b.rows[(i + 1) & 1].p, BVs[(i + 1) & 1], BVs[i & 1],
-                          c.st, sev.get());
+        row_step<R, true, ST>(c, b, rows[i & 1], rows[(i + 1) & 1], c.st, sev.get());
         sev->add(c.prof);
       }
     } else {
@@ -413,11 +496,7 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   d.dn_off.upload(L.dn_off, s);
   d.istr_off.upload(L.istr_off, s);
   d.istr_src.upload(L.istr_src, s);
-  {
-    std::vector<int2> vf(L.vin_fix.size());
-    for (size_t i = 0; i < vf.size(); ++i) vf[i] = make_int2(L.vin_fix[i].src, L.vin_fix[i].w);
-    d.vin_fix.upload(vf, s);
-  }
+  d.dv_s.upload(L.dv_s, s);
   std::vector<int2> up(L.up_in.size()), dn(L.dn_in.size());
   for (size_t i = 0; i < up.size(); ++i) up[i] = make_int2(L.up_in[i].src, L.up_in[i].w);
   for (size_t i = 0; i < dn.size(); ++i) dn[i] = make_int2(L.dn_in[i].src, L.dn_in[i].w);
@@ -442,20 +521,22 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   CK(cudaStreamSynchronize(s));
   c.gp = dev::GraphPtrs{L.N,          L.S,          L.special,      d.lab2.p,     d.lab_sp.p,
                         d.sv_off.p,   d.sv_dev.p,   d.vin_off.p,    d.vin_src.p,  d.vin_srcv.p,
-                        d.vin_fix.p,
-                        d.dv_first.p, d.dv_len.p,   d.up_off.p,     d.up_in.p,    d.dn_off.p,
+
+                        d.dv_first.p, d.dv_len.p,   d.dv_s.p,       d.up_off.p,   d.up_in.p,    d.dn_off.p,
                         d.dn_in.p,    d.istr_off.p, d.istr_src.p};
   c.nul_label = false;
   for (uint32_t i = 0; i < g.num_chars && !c.nul_label; ++i) c.nul_label = g.labels[i] == '\0';
+  c.pitch = ((size_t)L.N + 15) / 16 * 16;
   c.L = std::move(L);
   c.top = std::move(top);
   c.bufs.clear();
+  c.row_tiles.clear();
   c.loaded = true;
 }
 
 template <int R>
 void scores_with(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n,
-                 int32_t* out, bool graphs, uint32_t per_graph) {
+                 int32_t* out, bool graphs, uint32_t per_graph, uint32_t row_bits) {
   // length-0 reads never reach the device: the reference scores row 0
   // against read[0] == '\0', i.e. 1 unless a label byte is 0
   std::vector<const char*> rp;
@@ -474,7 +555,19 @@ void scores_with(chsga_ctx& c, const char* const* reads, const uint32_t* lens, u
   c.last_ids = idx;
   if (rp.empty()) return;
   upload_reads(c, rp.data(), rl.data(), (uint32_t)rp.size(), R > 1);
-  run_queue<R>(c, (uint32_t)rp.size(), rows, graphs, per_graph);
+  // every value of row i is at most i + 1 (row 0 is 0/1, a row adds at most
+  // the deletion cost 1, the closure only lowers), so reads shorter than
+  // kRow16Max rows are stored exactly in 16 bits
+  const uint32_t max_len = *std::max_element(rl.begin(), rl.end());
+  const bool narrow = row_bits == 16 || (row_bits == 0 && max_len <= kRow16Max);
+  require(!(row_bits == 16 && max_len > kRow16Max), CHSGA_ERR_INVALID_ARG,
+          "16-bit rows need reads of at most 65000 bases");
+  if (narrow) {
+    run_queue<R, uint16_t>(c, (uint32_t)rp.size(), rows, graphs, per_graph);
+  } else {
+    run_queue<R, int>(c, (uint32_t)rp.size(), rows, graphs, per_graph);
+  }
+  c.prof.row_bits = narrow ? 16 : 32;
   std::vector<int32_t> res(rp.size());
   CK(cudaMemcpy(res.data(), c.res_score.p, res.size() * 4, cudaMemcpyDeviceToHost));
   for (size_t i = 0; i < idx.size(); ++i) out[idx[i]] = res[i];
@@ -490,8 +583,8 @@ struct TbState {
 // device), writing row i to out + (i - a) * N if out_rows, else rotating two
 // buffers; sub-checkpoint rows every `sub_k` rows go to sub + j * N.
 void forward_rows(chsga_ctx& c, SlotBufs& b, uint32_t len, int64_t a, int64_t b_row,
-                  int* matrix /* rows a..b, row a already present */) {
-  const size_t N = c.L.N;
+                  int* matrix /* rows a..b at stride c.pitch, row a already present */) {
+  const size_t N = c.pitch;
   // slot 0 at row a+1 of read 0
   dev::SlotState s{0, len, (uint32_t)(a + 1), 0, 0};
   CK(cudaMemcpyAsync(b.slots.p, &s, sizeof(s), cudaMemcpyHostToDevice, c.st));
@@ -502,8 +595,12 @@ void forward_rows(chsga_ctx& c, SlotBufs& b, uint32_t len, int64_t a, int64_t b_
   CK(cudaMemcpyAsync(b.best.p, &inf, 8, cudaMemcpyHostToDevice, c.st));
   CK(cudaStreamSynchronize(c.st));
   launch_advance<1>(c, b, 1, c.st);
+  // the row-step reads the previous row's per-vertex first/last scores; row a
+  // comes from a checkpoint, so derive them from it
+  dev::k_fl_from_row<<<nblocks(c.L.S), 256, 0, c.st>>>(c.gp, matrix, reinterpret_cast<int*>(b.FL.p));
+  check_launch();
   for (int64_t i = a + 1; i <= b_row; ++i)
-    row_step<1, false>(c, b, matrix + (size_t)(i - 1 - a) * N, matrix + (size_t)(i - a) * N, b.BV.p, nullptr, c.st);
+    row_step<1, false, int>(c, b, matrix + (size_t)(i - 1 - a) * N, matrix + (size_t)(i - a) * N, c.st);
   check_device_error(c, b);
 }
 
@@ -514,7 +611,7 @@ void walk(chsga_ctx& c, const int* M, int64_t lo, int64_t hi, uint32_t start, ui
   ops.alloc(max_ops);
   DevArr<dev::WalkOut> out;
   out.alloc(1);
-  dev::k_walk<<<1, 1, 0, c.st>>>(c.gp, M, lo, hi, start, c.reads.p, ops.p, max_ops, out.p);
+  dev::k_walk<<<1, 1, 0, c.st>>>(c.gp, M, c.pitch, lo, hi, start, c.reads.p, ops.p, max_ops, out.p);
   check_launch();
   dev::WalkOut h{};
   CK(cudaMemcpyAsync(&h, out.p, sizeof(h), cudaMemcpyDeviceToHost, c.st));
@@ -533,15 +630,16 @@ void walk(chsga_ctx& c, const int* M, int64_t lo, int64_t hi, uint32_t start, ui
 void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts* o,
                chsga_tb_result* res) {
   require(len > 0, CHSGA_ERR_INVALID_ARG, "traceback of an empty read");
-  const size_t N = c.L.N;
+  const size_t N = c.pitch;   // row stride of every matrix below
+  const size_t NC = c.L.N;    // chars per row
   const int64_t k = (o && o->k > 0) ? o->k : 500;
   const uint64_t cap = (o && o->cap_bytes) ? o->cap_bytes : c.cap;
   const std::string dir = (o && o->dir) ? o->dir : "";
   const bool keep = o && o->keep_files;
   const char* rp[1] = {read};
   upload_reads(c, rp, &len, 1);
-  SlotBufs& b = get_bufs<1>(c, false);
-  const uint64_t row_bytes = (uint64_t)N * 4;
+  SlotBufs& b = get_bufs<1, int>(c, false);
+  const uint64_t row_bytes = (uint64_t)NC * 4;  // one checkpoint row (the reference's file size)
   const uint64_t store = (uint64_t)len * row_bytes;
   std::vector<dev::WalkOp> path;
   uint32_t best_v = 0;
@@ -561,7 +659,7 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
     reset_slots<1>(c, b, 1);
     launch_advance<1>(c, b, 0, c.st);
     for (uint32_t i = 0; i < len; ++i)
-      row_step<1, false>(c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, b.BV.p, nullptr, c.st);
+      row_step<1, false, int>(c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, c.st);
     harvest();
     uint32_t v = best_v;
     if (len > 1) walk(c, M.p, 0, len - 1, best_v, len, path, &v);
@@ -571,7 +669,7 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
     res->checkpointed = 1;
     const uint64_t nck = (len - 1) / (uint64_t)k + 1;
     res->num_checkpoints = nck;
-    c.h_ckpt.alloc(nck * N);
+    c.h_ckpt.alloc(nck * NC);
     DevArr<int> ring;
     ring.alloc(3 * N);
     cudaEvent_t done_ev[3];
@@ -591,13 +689,13 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
         CK(cudaEventSynchronize(done_ev[cur]));
         busy[cur] = false;
       }
-      row_step<1, false>(c, b, ring.p + (size_t)prev * N, ring.p + (size_t)cur * N, b.BV.p, nullptr, c.st);
+      row_step<1, false, int>(c, b, ring.p + (size_t)prev * N, ring.p + (size_t)cur * N, c.st);
       if (i % k == 0) {
         cudaEvent_t ready;
         CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
         CK(cudaEventRecord(ready, c.st));
         CK(cudaStreamWaitEvent(c.side, ready, 0));
-        CK(cudaMemcpyAsync(c.h_ckpt.p + (size_t)(i / k) * N, ring.p + (size_t)cur * N, row_bytes,
+        CK(cudaMemcpyAsync(c.h_ckpt.p + (size_t)(i / k) * NC, ring.p + (size_t)cur * N, row_bytes,
                            cudaMemcpyDeviceToHost, c.side));
         CK(cudaEventRecord(done_ev[cur], c.side));
         busy[cur] = true;
@@ -611,19 +709,22 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
     ring.release();
     if (!dir.empty())
       for (uint64_t j = 0; j < nck; ++j)
-        write_ckpt_row(dir, (int64_t)(j * k), c.h_ckpt.p + (size_t)j * N, N);
+        write_ckpt_row(dir, (int64_t)(j * k), c.h_ckpt.p + (size_t)j * NC, NC);
     // backward, one segment at a time (src/traceback.hpp:945-1011)
     int64_t cur_row = len - 1;
     uint32_t cur_v = best_v;
-    const uint64_t budget = cap;
+    // like the reference, the cap only decides between the two paths
+    // (traceback.hpp:614-645); segment recompute is sized by device memory
+    const uint64_t budget = std::max<uint64_t>(c.cap, cap);
     while (cur_row > 0) {
       int64_t seg_start = (cur_row % k == 0) ? (cur_row - k) : (cur_row / k * k);
       if (seg_start < 0) seg_start = 0;
       const int64_t seg_end = cur_row;
-      const int* ck = c.h_ckpt.p + (size_t)(seg_start / k) * N;
+      const int* ck = c.h_ckpt.p + (size_t)(seg_start / k) * NC;
       const uint64_t rows = (uint64_t)(seg_end - seg_start + 1);
       uint32_t landing = cur_v;
-      if (rows * row_bytes <= budget || rows <= 2) {
+      const uint64_t pitch_bytes = (uint64_t)N * 4;
+      if (rows * pitch_bytes <= budget || rows <= 2) {
         DevArr<int> seg;
         seg.alloc(rows * N);
         CK(cudaMemcpyAsync(seg.p, ck, row_bytes, cudaMemcpyHostToDevice, c.st));
@@ -634,7 +735,7 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
         const uint64_t span = (uint64_t)(seg_end - seg_start);
         const uint64_t k2 = std::max<uint64_t>(1, (uint64_t)std::ceil(std::sqrt((double)span)));
         const uint64_t nsub = span / k2 + 1;
-        require((nsub + k2 + 1) * row_bytes <= budget, CHSGA_ERR_OOM,
+        require((nsub + k2 + 1) * pitch_bytes <= budget, CHSGA_ERR_OOM,
                 "traceback segment does not fit the byte cap even with two-level checkpoints");
         DevArr<int> sub, seg;
         sub.alloc(nsub * N);
@@ -728,6 +829,11 @@ chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out) {
     CK(cudaGetDeviceProperties(&prop, c->device));
     require(prop.major >= 10, CHSGA_ERR_UNSUPPORTED,
             std::string("libchsga is built for sm_100a; device is ") + prop.name);
+    c->num_sms = prop.multiProcessorCount;
+    if (const char* rk = std::getenv("CHSGA_ROW_KERNEL")) {
+      if (std::string(rk) == "direct") c->row_kernel = RowKernel::Direct;
+      if (std::string(rk) == "tiled") c->row_kernel = RowKernel::Tiled;
+    }
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     size_t free_b = 0, total_b = 0;
@@ -772,7 +878,9 @@ chsga_status chsga_align_scores(chsga_ctx* c, const char* const* reads, const ui
   return guarded_ctx(c, [&] {
     require(c && (n == 0 || (reads && lens && scores_out)), CHSGA_ERR_INVALID_ARG, "null argument");
     require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
-    scores_with<1>(*c, reads, lens, n, scores_out, true, 16);
+    scores_with<1>(*c, reads, lens, n, scores_out, true, 16,
+                   (uint32_t)std::strtoul(std::getenv("CHSGA_ROW_BITS") ? std::getenv("CHSGA_ROW_BITS") : "0",
+                                          nullptr, 10));
   });
 }
 
@@ -785,15 +893,17 @@ chsga_status chsga_align_scores_batched(chsga_ctx* c, const char* const* reads,
     uint32_t slots = o && o->slots ? o->slots : 64;
     const bool graphs = o ? o->use_graphs != 0 : true;
     const uint32_t per = o && o->steps_per_graph ? o->steps_per_graph : 8;
+    const uint32_t rb = o ? o->row_bits : 0;
+    require(rb == 0 || rb == 16 || rb == 32, CHSGA_ERR_INVALID_ARG, "row_bits must be 0, 16 or 32");
     switch (slots) {
-      case 1: scores_with<1>(*c, reads, lens, n, scores_out, graphs, per); break;
-      case 2: scores_with<2>(*c, reads, lens, n, scores_out, graphs, per); break;
-      case 4: scores_with<4>(*c, reads, lens, n, scores_out, graphs, per); break;
-      case 8: scores_with<8>(*c, reads, lens, n, scores_out, graphs, per); break;
-      case 16: scores_with<16>(*c, reads, lens, n, scores_out, graphs, per); break;
-      case 32: scores_with<32>(*c, reads, lens, n, scores_out, graphs, per); break;
-      case 64: scores_with<64>(*c, reads, lens, n, scores_out, graphs, per); break;
-      case 128: scores_with<128>(*c, reads, lens, n, scores_out, graphs, per); break;
+      case 1: scores_with<1>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
+      case 2: scores_with<2>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
+      case 4: scores_with<4>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
+      case 8: scores_with<8>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
+      case 16: scores_with<16>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
+      case 32: scores_with<32>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
+      case 64: scores_with<64>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
+      case 128: scores_with<128>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
       default: fail(CHSGA_ERR_INVALID_ARG, "slots must be 1, 2, 4, 8, 16, 32, 64 or 128");
     }
   });
@@ -803,18 +913,18 @@ chsga_status chsga_align_rows(chsga_ctx* c, const char* read, uint32_t len, int3
   return guarded_ctx(c, [&] {
     require(c && read && rows_out && len > 0, CHSGA_ERR_INVALID_ARG, "bad argument");
     require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
-    const size_t N = c->L.N;
+    const size_t N = c->pitch, NC = c->L.N;
     const char* rp[1] = {read};
     upload_reads(*c, rp, &len, 1);
-    SlotBufs& b = get_bufs<1>(*c, false);
+    SlotBufs& b = get_bufs<1, int>(*c, false);
     DevArr<int> M;
     M.alloc((size_t)(len + 1) * N);
     reset_slots<1>(*c, b, 1);
     launch_advance<1>(*c, b, 0, c->st);
     for (uint32_t i = 0; i < len; ++i)
-      row_step<1, false>(*c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, b.BV.p, nullptr, c->st);
+      row_step<1, false, int>(*c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, c->st);
     check_device_error(*c, b);
-    CK(cudaMemcpy(rows_out, M.p, (size_t)len * N * 4, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy2D(rows_out, NC * 4, M.p, N * 4, NC * 4, len, cudaMemcpyDeviceToHost));
   });
 }
 

@@ -5,6 +5,7 @@
 #include <memory>
 #include <new>
 
+#include "device_graph.hpp"
 #include "host_graph.hpp"
 
 namespace chsga {
@@ -192,6 +193,33 @@ chsga_status chsga_gen_reads(const chsga_host_graph* g, const chsga_gen_reads_cf
     auto r = std::make_unique<chsga_reads>();
     generate_reads(*g, *cfg, r->r);
     *out = r.release();
+  });
+}
+
+chsga_status chsga_check_layout(const chsga_host_graph* g, uint32_t slots, uint32_t row_bits,
+                                chsga_layout_stats* out) {
+  return guarded([&] {
+    require(g && out, CHSGA_ERR_INVALID_ARG, "null argument");
+    require(row_bits == 16 || row_bits == 32, CHSGA_ERR_INVALID_ARG, "row_bits must be 16 or 32");
+    validate_host_graph(*g);
+    chsga_graph_host v{};
+    require(chsga_graph_view(g, &v) == CHSGA_OK, CHSGA_ERR_INTERNAL, "graph view");
+    HostLayout L = build_layout(v);
+    std::memset(out, 0, sizeof(*out));
+    out->num_levels = L.levels;
+    HostTop top = build_top(L, 23000, 1024);
+    out->top_first_level = top.first_level;
+    out->top_vertices = top.K;
+    if (slots >= 32) {
+      HostRowTiles t = build_row_tiles(L, slots, row_bits / 8);
+      validate_row_tiles(L, slots, row_bits / 8, t);
+      out->tiled = t.ok ? 1 : 0;
+      out->tiles = t.ntiles();
+      out->long_tiles = t.long_tiles;
+      out->slot_bytes = t.slot_bytes();
+      out->slots_per_block = t.nslots;
+      out->smem_bytes = t.ok ? row_tiled_smem(t, slots) : 0;
+    }
   });
 }
 

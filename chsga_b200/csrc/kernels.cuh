@@ -29,6 +29,8 @@
 
 #include <cstdint>
 
+#include "device_graph.hpp"  // tile limits shared with the host-side tile builder
+
 namespace chsga {
 namespace dev {
 
@@ -41,11 +43,11 @@ struct GraphPtrs {
   const uint32_t* sv_dev;
   const uint32_t* vin_off;
   const uint32_t* vin_src;
-  const uint32_t* vin_srcv;
-  const int2* vin_fix;  // per first-char in-edge: {hierarchy position of the source's
-                        // vertex, source char - that vertex's first char}
+  const uint32_t* vin_srcv;  // string vertex of each first-char in-edge source (the
+                             // source is that vertex's last char)
   const uint32_t* dv_first;
   const uint32_t* dv_len;
+  const uint32_t* dv_s;  // original id of hierarchy vertex d
   const uint32_t* up_off;
   const int2* up_in;
   const uint32_t* dn_off;
@@ -147,6 +149,59 @@ __device__ __forceinline__ void st(int* p, const IV<V>& x) {
   }
 }
 
+// 16-bit row storage: the same accessors over uint16_t (values widened to
+// int in registers). Every DP value of row i is at most i + 1, so rows of
+// reads shorter than 65535 fit exactly.
+template <int V>
+__device__ __forceinline__ IV<V> ld_nc(const uint16_t* p) {
+  IV<V> o;
+  if constexpr (V == 1) {
+    o.v[0] = __ldg(reinterpret_cast<const unsigned short*>(p));
+  } else if constexpr (V == 2) {
+    const uint32_t t = __ldg(reinterpret_cast<const unsigned int*>(p));
+    o.v[0] = (int)(t & 0xFFFFu);
+    o.v[1] = (int)(t >> 16);
+  } else {
+    const uint2 t = __ldg(reinterpret_cast<const uint2*>(p));
+    o.v[0] = (int)(t.x & 0xFFFFu);
+    o.v[1] = (int)(t.x >> 16);
+    o.v[2] = (int)(t.y & 0xFFFFu);
+    o.v[3] = (int)(t.y >> 16);
+  }
+  return o;
+}
+
+template <int V>
+__device__ __forceinline__ IV<V> ld(const uint16_t* p) {
+  IV<V> o;
+  if constexpr (V == 1) {
+    o.v[0] = *p;
+  } else if constexpr (V == 2) {
+    const uint32_t t = *reinterpret_cast<const uint32_t*>(p);
+    o.v[0] = (int)(t & 0xFFFFu);
+    o.v[1] = (int)(t >> 16);
+  } else {
+    const uint2 t = *reinterpret_cast<const uint2*>(p);
+    o.v[0] = (int)(t.x & 0xFFFFu);
+    o.v[1] = (int)(t.x >> 16);
+    o.v[2] = (int)(t.y & 0xFFFFu);
+    o.v[3] = (int)(t.y >> 16);
+  }
+  return o;
+}
+
+template <int V>
+__device__ __forceinline__ void st(uint16_t* p, const IV<V>& x) {
+  if constexpr (V == 1) {
+    *p = (uint16_t)x.v[0];
+  } else if constexpr (V == 2) {
+    *reinterpret_cast<uint32_t*>(p) = (uint32_t)x.v[0] | ((uint32_t)x.v[1] << 16);
+  } else {
+    *reinterpret_cast<uint2*>(p) = make_uint2((uint32_t)x.v[0] | ((uint32_t)x.v[1] << 16),
+                                              (uint32_t)x.v[2] | ((uint32_t)x.v[3] << 16));
+  }
+}
+
 // Label key of char c: 0..3 for A,C,G,T, 4 for the special byte.
 __device__ __forceinline__ uint32_t label_key(const GraphPtrs& g, uint32_t c) {
   const uint32_t code = (__ldg(g.lab2 + (c >> 4)) >> ((c & 15u) * 2u)) & 3u;
@@ -182,274 +237,6 @@ __device__ __forceinline__ void flush_min(unsigned long long* sm_best, unsigned 
   __syncthreads();
   for (int r = threadIdx.x; r < R; r += blockDim.x)
     if (sm_best[r] != ~0ull) atomicMin(best + r, sm_best[r]);
-}
-
-// ---------------------------------------------------------------------------
-// k_row: one pass over the string vertices in char order. For vertex s and
-// each slot: the first char takes min(D[f]+1, min over in-edges D[u]+delta),
-// every later char c takes min(D[c]+1, D[c-1]+delta, T[c-1]+1): the chain
-// in-edge c-1 -> c plus the within-vertex forward scan. Row 0 takes delta.
-// With DEFER, D holds the previous row before its final within-vertex
-// propagation and BVp the previous row's swept first scores, and every D
-// value is read as min(D[c], BVp[2 d(c)] + c - first(c)).
-// ---------------------------------------------------------------------------
-template <int R, bool DEFER>
-__global__ void __launch_bounds__(256, 3) k_row(GraphPtrs g, const int* __restrict__ D,
-                                                int* __restrict__ T, int* __restrict__ BV,
-                                                const int* __restrict__ BVp,
-                                                const uint32_t* __restrict__ slot_word,
-                                                unsigned long long* __restrict__ best,
-                                                const StepCtl* __restrict__ ctl) {
-  constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
-  __shared__ unsigned long long sm_best[R];
-  const bool ending_any = ctl->any_ending != 0;
-  if (!ctl->any_active) return;
-  if (ending_any) {
-    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
-    __syncthreads();
-  }
-  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t s = (uint32_t)(gt / G);
-  const int lane = (int)(gt % G);
-  if (s < g.S) {
-    uint32_t code[V];
-    bool init[V], ending[V], fix[V];
-    bool any_fix = false;
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const uint32_t w = __ldg(slot_word + lane * V + v);
-      code[v] = w & SW_CODE;
-      init[v] = (w & SW_INIT) != 0;
-      ending[v] = (w & SW_ENDING) != 0;
-      fix[v] = DEFER && (w & SW_FIX) != 0;
-      any_fix |= fix[v];
-    }
-    const uint32_t f = __ldg(g.sv_off + s), e = __ldg(g.sv_off + s + 1);
-    const uint32_t d = __ldg(g.sv_dev + s);
-    const size_t so = (size_t)lane * V;
-    constexpr int kBig = 0x3fffffff;
-    IV<V> F;  // previous row's swept first score of this vertex
-#pragma unroll
-    for (int v = 0; v < V; ++v) F.v[v] = kBig;
-    if (DEFER && any_fix) {
-      const IV<V> x = ld_nc<V>(BVp + (size_t)(2 * d) * R + so);
-#pragma unroll
-      for (int v = 0; v < V; ++v)
-        if (fix[v]) F.v[v] = x.v[v];
-    }
-    int bmin[V];
-    uint32_t barg[V];
-    // first char
-    IV<V> dprev = ld_nc<V>(D + (size_t)f * R + so);
-    IV<V> t;
-    {
-      const uint32_t key = label_key(g, f);
-      int delta[V];
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        if (DEFER) dprev.v[v] = min(dprev.v[v], F.v[v]);
-        delta[v] = key == code[v] ? 0 : 1;
-        t.v[v] = dprev.v[v] + 1;
-      }
-      const uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
-      for (uint32_t k = k0; k < k1; ++k) {
-        const uint32_t u = __ldg(g.vin_src + k);
-        IV<V> du = ld_nc<V>(D + (size_t)u * R + so);
-        if (DEFER && any_fix) {
-          const int2 fx = __ldg(g.vin_fix + k);
-          const IV<V> fu = ld_nc<V>(BVp + (size_t)(2 * fx.x) * R + so);
-#pragma unroll
-          for (int v = 0; v < V; ++v)
-            if (fix[v]) du.v[v] = min(du.v[v], fu.v[v] + fx.y);
-        }
-#pragma unroll
-        for (int v = 0; v < V; ++v) t.v[v] = min(t.v[v], du.v[v] + delta[v]);
-      }
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        if (init[v]) t.v[v] = delta[v];
-        bmin[v] = t.v[v];
-        barg[v] = f;
-      }
-    }
-    st<V>(T + (size_t)f * R + so, t);
-    st<V>(BV + (size_t)(2 * d) * R + so, t);
-    // chain chars in groups of four: the four loads go out together so each
-    // warp keeps several row segments in flight
-    for (uint32_t c0 = f + 1; c0 < e; c0 += 4) {
-      const uint32_t n = min(4u, e - c0);
-      IV<V> dq[4];
-#pragma unroll
-      for (uint32_t k = 0; k < 4; ++k)
-        if (k < n) dq[k] = ld_nc<V>(D + (size_t)(c0 + k) * R + so);
-#pragma unroll
-      for (uint32_t k = 0; k < 4; ++k) {
-        if (k < n) {
-          const uint32_t c = c0 + k;
-          const uint32_t key = label_key(g, c);
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            if (DEFER) dq[k].v[v] = min(dq[k].v[v], F.v[v] + (int)(c - f));
-            const int delta = key == code[v] ? 0 : 1;
-            int x = min(dq[k].v[v] + 1, dprev.v[v] + delta);
-            x = min(x, t.v[v] + 1);
-            if (init[v]) x = delta;
-            t.v[v] = x;
-            if (x < bmin[v]) {
-              bmin[v] = x;
-              barg[v] = c;
-            }
-          }
-          dprev = dq[k];
-          st<V>(T + (size_t)c * R + so, t);
-        }
-      }
-    }
-    if (e - f > 1) st<V>(BV + (size_t)(2 * d + 1) * R + so, t);
-    if (ending_any) {
-#pragma unroll
-      for (int v = 0; v < V; ++v)
-        if (ending[v]) atomicMin(sm_best + lane * V + v, pack_min(bmin[v], barg[v]));
-    }
-  }
-  if (ending_any) flush_min<R>(sm_best, best);
-}
-
-// ---------------------------------------------------------------------------
-// k_pull: hierarchy positions [lo, hi): BV[2d] = min(BV[2d], BV[src] + w)
-// over the list off[d-base]..off[d-base+1]. Every source lies on another
-// level, finished before this launch, so the gathers use the read-only path.
-// ---------------------------------------------------------------------------
-template <int R>
-__global__ void __launch_bounds__(256) k_pull(int* __restrict__ BV, uint32_t lo, uint32_t hi,
-                                              const uint32_t* __restrict__ off,
-                                              const int2* __restrict__ edges, uint32_t base,
-                                              const StepCtl* __restrict__ ctl) {
-  constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
-  if (!ctl->any_active) return;
-  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t d = lo + (uint32_t)(gt / G);
-  const int lane = (int)(gt % G);
-  if (d >= hi) return;
-  const size_t so = (size_t)lane * V;
-  const uint32_t k0 = __ldg(off + (d - base)), k1 = __ldg(off + (d - base) + 1);
-  if (k0 == k1) return;
-  int* p = BV + (size_t)(2 * d) * R + so;
-  IV<V> f = ld<V>(p);
-  bool changed = false;
-  for (uint32_t k = k0; k < k1; ++k) {
-    const int2 ew = __ldg(edges + k);
-    const IV<V> x = ld_nc<V>(BV + (size_t)ew.x * R + so);
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const int c = x.v[v] + ew.y;
-      if (c < f.v[v]) {
-        f.v[v] = c;
-        changed = true;
-      }
-    }
-  }
-  if (changed) st<V>(p, f);
-}
-
-// ---------------------------------------------------------------------------
-// k_down: positions [lo, hi). Those below `mid` first pull their downward
-// in-edges (sources on higher levels, final); every position then finalises
-// its vertex's chars: if the first score fell below the row value, write it
-// and propagate first + (p - first) forward while it improves
-// (align.hpp:381-396). Slots without closure (row 0, idle) are untouched.
-// ---------------------------------------------------------------------------
-template <int R, bool FIXUP>
-__global__ void __launch_bounds__(256) k_down(GraphPtrs g, int* __restrict__ BV, int* __restrict__ T,
-                                              uint32_t lo, uint32_t mid, uint32_t hi,
-                                              const uint32_t* __restrict__ slot_word,
-                                              unsigned long long* __restrict__ best,
-                                              const StepCtl* __restrict__ ctl) {
-  constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
-  __shared__ unsigned long long sm_best[R];
-  const bool ending_any = ctl->any_ending != 0;
-  if (!ctl->any_active) return;
-  if (ending_any) {
-    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
-    __syncthreads();
-  }
-  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t d = lo + (uint32_t)(gt / G);
-  const int lane = (int)(gt % G);
-  if (d < hi) {
-    const size_t so = (size_t)lane * V;
-    int* p = BV + (size_t)(2 * d) * R + so;
-    IV<V> f = ld<V>(p);
-    if (d < mid) {
-      const uint32_t k0 = __ldg(g.dn_off + d), k1 = __ldg(g.dn_off + d + 1);
-      bool changed = false;
-      for (uint32_t k = k0; k < k1; ++k) {
-        const int2 ew = __ldg(g.dn_in + k);
-        const IV<V> x = ld_nc<V>(BV + (size_t)ew.x * R + so);
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const int c = x.v[v] + ew.y;
-          if (c < f.v[v]) {
-            f.v[v] = c;
-            changed = true;
-          }
-        }
-      }
-      if (changed) st<V>(p, f);
-    }
-    const uint32_t first = __ldg(g.dv_first + d), len = __ldg(g.dv_len + d);
-    (void)len;
-    if (!FIXUP) {
-      // the row stays raw; a slot on its last row needs min over the final
-      // scores = min(min over raw scores [k_row], min over swept first scores)
-      if (ending_any) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const uint32_t w = __ldg(slot_word + so + v);
-          if ((w & SW_CLOSURE) && (w & SW_ENDING))
-            atomicMin(sm_best + so + v, pack_min(f.v[v], first));
-        }
-      }
-    } else {
-    IV<V> tq = ld<V>(T + (size_t)first * R + so);
-    bool act[V], endg[V];
-    bool any = false;
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const uint32_t w = __ldg(slot_word + so + v);
-      act[v] = (w & SW_CLOSURE) && f.v[v] < tq.v[v];
-      endg[v] = act[v] && (w & SW_ENDING);
-      if (act[v]) {
-        tq.v[v] = f.v[v];
-        if (endg[v]) atomicMin(sm_best + so + v, pack_min(f.v[v], first));
-      }
-      any |= act[v];
-    }
-    if (any) {
-      st<V>(T + (size_t)first * R + so, tq);
-      // first + q while it improves, every slot of the lane in one pass per char
-      for (uint32_t q = 1; q < len && any; ++q) {
-        int* tp = T + (size_t)(first + q) * R + so;
-        IV<V> x = ld<V>(tp);
-        any = false;
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          if (!act[v]) continue;
-          const int cand = f.v[v] + (int)q;
-          if (cand < x.v[v]) {
-            x.v[v] = cand;
-            if (endg[v]) atomicMin(sm_best + so + v, pack_min(cand, first + q));
-            any = true;
-          } else {
-            act[v] = false;
-          }
-        }
-        st<V>(tp, x);
-      }
-    }
-    }
-  }
-  if (ending_any) flush_min<R>(sm_best, best);
 }
 
 // ---------------------------------------------------------------------------
@@ -502,6 +289,734 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t pari
 }
 
 // ---------------------------------------------------------------------------
+// k_row: one pass over the string vertices in char order. For vertex s and
+// each slot: the first char takes min(D[f]+1, min over in-edges D[u]+delta),
+// every later char c takes min(D[c]+1, D[c-1]+delta, T[c-1]+1): the chain
+// in-edge c-1 -> c plus the within-vertex forward scan. Row 0 takes delta.
+//
+// The previous row's final first and last scores of every string vertex are
+// kept in char order, FL[(2s + j) * R + r] (j = 0 first, 1 last; written by
+// k_down). A first char's in-edge sources are last chars of other vertices,
+// so their final values are read from FL. With DEFER, D holds the previous
+// row before its within-vertex propagation, and every chain value is read as
+// min(D[c], FL_first(s) + c - first(s)).
+// ---------------------------------------------------------------------------
+template <int R, bool DEFER, typename ST>
+__global__ void __launch_bounds__(256, 3) k_row_direct(GraphPtrs g, const ST* __restrict__ D,
+                                                       ST* __restrict__ T, ST* __restrict__ BV,
+                                                       const ST* __restrict__ FL,
+                                                       const uint32_t* __restrict__ slot_word,
+                                                       unsigned long long* __restrict__ best,
+                                                       const StepCtl* __restrict__ ctl) {
+  constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
+  __shared__ unsigned long long sm_best[R];
+  const bool ending_any = ctl->any_ending != 0;
+  if (!ctl->any_active) return;
+  if (ending_any) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
+    __syncthreads();
+  }
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t s = (uint32_t)(gt / G);
+  const int lane = (int)(gt % G);
+  if (s < g.S) {
+    uint32_t code[V];
+    bool init[V], ending[V], fix[V];
+    bool any_fix = false;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const uint32_t w = __ldg(slot_word + lane * V + v);
+      code[v] = w & SW_CODE;
+      init[v] = (w & SW_INIT) != 0;
+      ending[v] = (w & SW_ENDING) != 0;
+      fix[v] = DEFER && (w & SW_FIX) != 0;
+      any_fix |= fix[v];
+    }
+    const uint32_t f = __ldg(g.sv_off + s), e = __ldg(g.sv_off + s + 1);
+    const uint32_t d = __ldg(g.sv_dev + s);
+    const size_t so = (size_t)lane * V;
+    constexpr int kBig = 0x3fffffff;
+    IV<V> F;
+#pragma unroll
+    for (int v = 0; v < V; ++v) F.v[v] = kBig;
+    if (DEFER && any_fix) {
+      const IV<V> x = ld_nc<V>(FL + (size_t)(2 * s) * R + so);
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        if (fix[v]) F.v[v] = x.v[v];
+    }
+    int bmin[V];
+    uint32_t barg[V];
+    IV<V> dprev = ld_nc<V>(D + (size_t)f * R + so);
+    IV<V> t;
+    {
+      const uint32_t key = label_key(g, f);
+      int delta[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        if (DEFER) dprev.v[v] = min(dprev.v[v], F.v[v]);
+        delta[v] = key == code[v] ? 0 : 1;
+        t.v[v] = dprev.v[v] + 1;
+      }
+      const uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
+      for (uint32_t k = k0; k < k1; ++k) {
+        const uint32_t su = __ldg(g.vin_srcv + k);
+        const IV<V> du = ld_nc<V>(FL + (size_t)(2 * su + 1) * R + so);
+#pragma unroll
+        for (int v = 0; v < V; ++v) t.v[v] = min(t.v[v], du.v[v] + delta[v]);
+      }
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        if (init[v]) t.v[v] = delta[v];
+        bmin[v] = t.v[v];
+        barg[v] = f;
+      }
+    }
+    st<V>(T + (size_t)f * R + so, t);
+    st<V>(BV + (size_t)(2 * d) * R + so, t);
+    for (uint32_t c0 = f + 1; c0 < e; c0 += 4) {
+      const uint32_t n = min(4u, e - c0);
+      IV<V> dq[4];
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k)
+        if (k < n) dq[k] = ld_nc<V>(D + (size_t)(c0 + k) * R + so);
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k) {
+        if (k < n) {
+          const uint32_t c = c0 + k;
+          const uint32_t key = label_key(g, c);
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            if (DEFER) dq[k].v[v] = min(dq[k].v[v], F.v[v] + (int)(c - f));
+            const int delta = key == code[v] ? 0 : 1;
+            int x = min(dq[k].v[v] + 1, dprev.v[v] + delta);
+            x = min(x, t.v[v] + 1);
+            if (init[v]) x = delta;
+            t.v[v] = x;
+            if (x < bmin[v]) {
+              bmin[v] = x;
+              barg[v] = c;
+            }
+          }
+          dprev = dq[k];
+          st<V>(T + (size_t)c * R + so, t);
+        }
+      }
+    }
+    if (e - f > 1) st<V>(BV + (size_t)(2 * d + 1) * R + so, t);
+    if (ending_any) {
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        if (ending[v]) atomicMin(sm_best + lane * V + v, pack_min(bmin[v], barg[v]));
+    }
+  }
+  if (ending_any) flush_min<R>(sm_best, best);
+}
+
+// ---------------------------------------------------------------------------
+// k_row_dpx: k_row_direct for 16-bit rows on the DPX units. Two slots share
+// one 32-bit register (one 16-bit score each) and every min/add of the
+// recurrence runs on both at once: the chain char c becomes
+//   x = min(dprev + delta, min(T[c-1] + 1, D[c] + 1))   (two __viaddmin_u16x2)
+// No half ever wraps: every score is at most 65000 (rows are 16-bit only for
+// reads of at most 65000 bases), +1 and +delta stay below 65536, and the
+// deferred term F + (c - first) stays below 65536 because the engine runs
+// this kernel only when every string vertex has at most 512 chars.
+// Lanes: G = min(32, R/2) per vertex, P = R / (2G) register pairs each.
+// ---------------------------------------------------------------------------
+template <int R>
+struct Pairs {
+  static constexpr int G = (R / 2) < 32 ? (R / 2) : 32;
+  static constexpr int P = R / (2 * G);
+};
+
+template <int P>
+struct U2 {
+  uint32_t h[P];
+};
+
+template <int P>
+__device__ __forceinline__ U2<P> ldp_nc(const uint16_t* p) {
+  U2<P> o;
+  if constexpr (P == 1) {
+    o.h[0] = __ldg(reinterpret_cast<const unsigned int*>(p));
+  } else {
+    const uint2 t = __ldg(reinterpret_cast<const uint2*>(p));
+    o.h[0] = t.x;
+    o.h[1] = t.y;
+  }
+  return o;
+}
+
+template <int P>
+__device__ __forceinline__ void stp(uint16_t* p, const U2<P>& x) {
+  if constexpr (P == 1) {
+    *reinterpret_cast<uint32_t*>(p) = x.h[0];
+  } else {
+    *reinterpret_cast<uint2*>(p) = make_uint2(x.h[0], x.h[1]);
+  }
+}
+
+// (a & m) | (b & ~m) in one LOP3
+__device__ __forceinline__ uint32_t sel(uint32_t a, uint32_t b, uint32_t m) {
+  uint32_t r;
+  asm("lop3.b32 %0, %1, %2, %3, 0xE4;" : "=r"(r) : "r"(a), "r"(b), "r"(m));
+  return r;
+}
+
+template <int R, bool DEFER>
+__global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t* __restrict__ D,
+                                                    uint16_t* __restrict__ T,
+                                                    uint16_t* __restrict__ BV,
+                                                    const uint16_t* __restrict__ FL,
+                                                    const uint32_t* __restrict__ slot_word,
+                                                    unsigned long long* __restrict__ best,
+                                                    const StepCtl* __restrict__ ctl) {
+  constexpr int G = Pairs<R>::G, P = Pairs<R>::P;
+  constexpr uint32_t ONES = 0x00010001u;
+  __shared__ unsigned long long sm_best[R];
+  const bool ending_any = ctl->any_ending != 0;
+  if (!ctl->any_active) return;
+  if (ending_any) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
+    __syncthreads();
+  }
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t s = (uint32_t)(gt / G);
+  const int lane = (int)(gt % G);
+  if (s < g.S) {
+    const size_t so = (size_t)lane * 2 * P;  // first slot of this lane
+    // per register pair: delta table over label keys (bit k of each half =
+    // mismatch of key k), row-0 mask, deferred-propagation mask
+    uint32_t dtab[P], imask[P], fmask[P];
+    bool any_fix = false, any_end = false;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      dtab[p] = imask[p] = fmask[p] = 0;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const uint32_t w = __ldg(slot_word + so + 2 * p + h);
+        const uint32_t code = w & SW_CODE;
+        dtab[p] |= ((0x3Fu & ~(1u << code)) & 0x3Fu) << (16 * h);
+        if (w & SW_INIT) imask[p] |= 0xFFFFu << (16 * h);
+        if (DEFER && (w & SW_FIX)) fmask[p] |= 0xFFFFu << (16 * h);
+        any_end |= (w & SW_ENDING) != 0;
+      }
+      any_fix |= fmask[p] != 0;
+    }
+    const uint32_t f = __ldg(g.sv_off + s), e = __ldg(g.sv_off + s + 1);
+    const uint32_t d = __ldg(g.sv_dev + s);
+    U2<P> F;
+    if (DEFER && any_fix) F = ldp_nc<P>(FL + (size_t)(2 * s) * R + so);
+    U2<P> dprev = ldp_nc<P>(D + (size_t)f * R + so);
+    U2<P> t;
+    {
+      const uint32_t key = label_key(g, f);
+      uint32_t delta[P];
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        delta[p] = (dtab[p] >> key) & ONES;
+        if (DEFER && any_fix) dprev.h[p] = sel(__vminu2(dprev.h[p], F.h[p]), dprev.h[p], fmask[p]);
+        t.h[p] = dprev.h[p] + ONES;
+      }
+      const uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
+      for (uint32_t k = k0; k < k1; ++k) {
+        const uint32_t su = __ldg(g.vin_srcv + k);
+        const U2<P> du = ldp_nc<P>(FL + (size_t)(2 * su + 1) * R + so);
+#pragma unroll
+        for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(du.h[p], delta[p], t.h[p]);
+      }
+#pragma unroll
+      for (int p = 0; p < P; ++p) t.h[p] = sel(delta[p], t.h[p], imask[p]);
+    }
+    stp<P>(T + (size_t)f * R + so, t);
+    stp<P>(BV + (size_t)(2 * d) * R + so, t);
+    int bmin[2 * P];
+    uint32_t barg[2 * P];
+    if (ending_any && any_end) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        bmin[2 * p] = (int)(t.h[p] & 0xFFFFu);
+        bmin[2 * p + 1] = (int)(t.h[p] >> 16);
+        barg[2 * p] = barg[2 * p + 1] = f;
+      }
+    }
+    for (uint32_t c0 = f + 1; c0 < e; c0 += 4) {
+      const uint32_t n = min(4u, e - c0);
+      U2<P> dq[4];
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k)
+        if (k < n) dq[k] = ldp_nc<P>(D + (size_t)(c0 + k) * R + so);
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k) {
+        if (k < n) {
+          const uint32_t c = c0 + k;
+          const uint32_t key = label_key(g, c);
+          const uint32_t off2 = (c - f) * ONES;
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            const uint32_t delta = (dtab[p] >> key) & ONES;
+            if (DEFER && any_fix)
+              dq[k].h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq[k].h[p]), dq[k].h[p], fmask[p]);
+            uint32_t x = __viaddmin_u16x2(t.h[p], ONES, dq[k].h[p] + ONES);
+            x = __viaddmin_u16x2(dprev.h[p], delta, x);
+            t.h[p] = sel(delta, x, imask[p]);
+          }
+          dprev = dq[k];
+          stp<P>(T + (size_t)c * R + so, t);
+          if (ending_any && any_end) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+              const int lo = (int)(t.h[p] & 0xFFFFu), hi = (int)(t.h[p] >> 16);
+              if (lo < bmin[2 * p]) {
+                bmin[2 * p] = lo;
+                barg[2 * p] = c;
+              }
+              if (hi < bmin[2 * p + 1]) {
+                bmin[2 * p + 1] = hi;
+                barg[2 * p + 1] = c;
+              }
+            }
+          }
+        }
+      }
+    }
+    if (e - f > 1) stp<P>(BV + (size_t)(2 * d + 1) * R + so, t);
+    if (ending_any && any_end) {
+#pragma unroll
+      for (int q = 0; q < 2 * P; ++q) {
+        const uint32_t w = __ldg(slot_word + so + q);
+        if (w & SW_ENDING) atomicMin(sm_best + so + q, pack_min(bmin[q], barg[q]));
+      }
+    }
+  }
+  if (ending_any) flush_min<R>(sm_best, best);
+}
+
+// ---------------------------------------------------------------------------
+// k_row_tiled (R >= 32, one warp per vertex): the same update with every
+// input of a tile of consecutive vertices staged in shared memory by TMA
+// bulk copies. A producer warp walks the block's tiles and, per tile, copies
+// the previous-row scores of its chars, the FL block of its vertices, the
+// tile's descriptor (vertex and in-edge records, built on the host) and the
+// FL last scores of in-edge sources outside the tile into one of nslots
+// buffers; 16 consumer warps compute tiles from shared memory, so no
+// dependent global load sits on their critical path. full/empty mbarriers
+// hand buffers back and forth; all waits are bounded.
+//
+// Tile record: r0 = {s0, s1, c0, c1 | long << 31}, r1 = {descriptor word
+// offset, descriptor bytes, external count, external list word offset}.
+// Descriptor: per vertex {first char, length, hierarchy position,
+// first edge << 16 | edge count}, then per in-edge one word: source vertex
+// - s0 if inside the tile, else 0x80000000 | external index. A long tile (one
+// vertex longer than the score buffer) reads its chars from global memory.
+// ---------------------------------------------------------------------------
+constexpr int kRowCons = 16;     // consumer warps per block
+constexpr int kRowMaxSlots = (int)kTileSlotsMax;
+constexpr int kRowThreads = (kRowCons + 1) * 32;
+constexpr uint32_t ERR_ROW_WAIT = 2;
+
+struct RowTiles {
+  const int4* rec;          // 2 per tile
+  const uint32_t* desc;     // descriptors (16-byte aligned per tile)
+  uint32_t ntiles;
+  uint32_t nslots;          // buffers per block
+  uint32_t d_cap, fl_cap, desc_cap, ext_cap;  // byte size of each slot region
+};
+
+__host__ __device__ constexpr uint32_t row_slot_bytes(const RowTiles& t) {
+  return t.d_cap + t.fl_cap + t.desc_cap + t.ext_cap;
+}
+__host__ __device__ constexpr size_t row_smem_bytes(uint32_t slot_bytes, uint32_t nslots, int R) {
+  return (size_t)nslots * slot_bytes + (size_t)kRowMaxSlots * 16 + (size_t)R * 8 + 16;
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Bulk copy into shared memory completing on `bar` without an arrival (the
+// arrival with the whole tile's byte count is made separately).
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes,
+                                          unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(unsigned long long* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+template <int R, bool DEFER, typename ST>
+__global__ void __launch_bounds__(kRowThreads, 1) k_row_tiled(GraphPtrs g, RowTiles rt,
+                                                             const ST* __restrict__ D,
+                                                             ST* __restrict__ T, ST* __restrict__ BV,
+                                                             const ST* __restrict__ FL,
+                                                             const uint32_t* __restrict__ slot_word,
+                                                             unsigned long long* __restrict__ best,
+                                                             StepCtl* __restrict__ ctl) {
+  static_assert(R >= 32, "one warp per vertex");
+  constexpr int V = Lanes<R>::V;
+  constexpr uint32_t PC = R * sizeof(ST);  // bytes per char (and per FL entry)
+  extern __shared__ __align__(16) unsigned char row_smem[];
+  __shared__ int s_fail;
+  if (!ctl->any_active) return;
+  const bool ending_any = ctl->any_ending != 0;
+  const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
+  const uint32_t SB = row_slot_bytes(rt);
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(row_smem + (size_t)rt.nslots * SB);
+  unsigned long long* empty = full + kRowMaxSlots;
+  unsigned long long* sm_best = empty + kRowMaxSlots;
+  if (ending_any)
+    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    for (uint32_t k = 0; k < rt.nslots; ++k) {
+      mbar_init(&full[k], 1);
+      mbar_init(&empty[k], 1);
+    }
+    fence_async_shared();
+  }
+  __syncthreads();
+  // this block's tiles: t = blockIdx.x + i * gridDim.x; tile i uses buffer
+  // i % nslots and consumer warp i % nslots (nslots <= kRowCons)
+  const uint32_t nt =
+      rt.ntiles > blockIdx.x ? (rt.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  if (warp == kRowCons) {
+    uint32_t last_parity = 0, used = 0;  // lane 0's record of every buffer's last fill
+    for (uint32_t i = 0; i < nt; ++i) {
+      const uint32_t k = i % rt.nslots;
+      int stop = 0;
+      if (wl == 0) {
+        stop = *(volatile int*)&s_fail;
+        if (!stop && i >= rt.nslots && !mbar_wait(&empty[k], ((i / rt.nslots) - 1) & 1)) {
+          s_fail = 1;
+          stop = 1;
+        }
+      }
+      if (__shfl_sync(0xffffffffu, stop, 0)) break;
+      const uint32_t t = blockIdx.x + i * gridDim.x;
+      const int4 r0 = rt.rec[2 * t], r1 = rt.rec[2 * t + 1];
+      unsigned char* slot = row_smem + (size_t)k * SB;
+      const uint32_t s0 = (uint32_t)r0.x, s1 = (uint32_t)r0.y, c0 = (uint32_t)r0.z;
+      const bool lng = r0.w < 0;
+      const uint32_t c1 = (uint32_t)(r0.w & 0x7fffffff);
+      const uint32_t dbytes = lng ? 0u : (c1 - c0) * PC;
+      const uint32_t flbytes = 2 * (s1 - s0) * PC;
+      const uint32_t total = dbytes + flbytes + (uint32_t)r1.y + (uint32_t)r1.z * PC;
+      if (wl == 0) {
+        fence_async_shared();
+        mbar_expect(&full[k], total);
+        if (dbytes) bulk_copy(slot, D + (size_t)c0 * R, dbytes, &full[k]);
+        bulk_copy(slot + rt.d_cap, FL + (size_t)(2 * s0) * R, flbytes, &full[k]);
+        bulk_copy(slot + rt.d_cap + rt.fl_cap, rt.desc + (size_t)r1.x, (uint32_t)r1.y, &full[k]);
+        last_parity ^= 1u << k;
+        used |= 1u << k;
+      }
+      __syncwarp();
+      if (wl < r1.z) {
+        const uint32_t su = rt.desc[(size_t)r1.w + wl];
+        bulk_copy(slot + rt.d_cap + rt.fl_cap + rt.desc_cap + wl * PC, FL + (size_t)(2 * su + 1) * R,
+                  PC, &full[k]);
+      }
+    }
+    if (wl == 0 && *(volatile int*)&s_fail) {
+      // bounded wait for every buffer's last fill before shared memory goes
+      for (uint32_t k = 0; k < rt.nslots; ++k)
+        if (used & (1u << k)) mbar_wait(&full[k], ((last_parity >> k) & 1) ^ 1);
+    }
+  } else {
+    const int lane = wl;
+    const size_t so = (size_t)lane * V;
+    uint32_t code[V];
+    bool init[V], ending[V], fix[V];
+    bool any_fix = false;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const uint32_t w = __ldg(slot_word + so + v);
+      code[v] = w & SW_CODE;
+      init[v] = (w & SW_INIT) != 0;
+      ending[v] = (w & SW_ENDING) != 0;
+      fix[v] = DEFER && (w & SW_FIX) != 0;
+      any_fix |= fix[v];
+    }
+    int bmin[V];
+    uint32_t barg[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      bmin[v] = 0x7fffffff;
+      barg[v] = 0;
+    }
+    constexpr int kBig = 0x3fffffff;
+    // consumer warp w owns buffer w and takes tiles w, w + nslots, ...: each
+    // buffer's fills are consumed in order, so a parity wait can never be
+    // satisfied by an older fill of the same buffer
+    for (uint32_t i = warp; warp < (int)rt.nslots && i < nt; i += rt.nslots) {
+      const uint32_t k = i % rt.nslots;
+      const bool ok = mbar_wait(&full[k], (i / rt.nslots) & 1);
+      if (__any_sync(0xffffffffu, !ok || *(volatile int*)&s_fail)) {
+        s_fail = 1;
+        break;
+      }
+      const uint32_t t = blockIdx.x + i * gridDim.x;
+      const int4 r0 = rt.rec[2 * t];
+      const uint32_t s0 = (uint32_t)r0.x, nv = (uint32_t)r0.y - s0, c0 = (uint32_t)r0.z;
+      const bool lng = r0.w < 0;
+      const unsigned char* slot = row_smem + (size_t)k * SB;
+      const ST* Dt = lng ? D + (size_t)c0 * R : reinterpret_cast<const ST*>(slot);
+      const ST* FLt = reinterpret_cast<const ST*>(slot + rt.d_cap);
+      const uint32_t* dsc = reinterpret_cast<const uint32_t*>(slot + rt.d_cap + rt.fl_cap);
+      const ST* EXt = reinterpret_cast<const ST*>(slot + rt.d_cap + rt.fl_cap + rt.desc_cap);
+      const uint32_t* erec = dsc + 4 * nv;
+      for (uint32_t j = 0; j < nv; ++j) {
+        const uint4 vr = *reinterpret_cast<const uint4*>(dsc + 4 * j);
+        const uint32_t f = vr.x, len = vr.y, d = vr.z;
+        const uint32_t eb = vr.w >> 16, ec = vr.w & 0xFFFFu;
+        IV<V> F;
+#pragma unroll
+        for (int v = 0; v < V; ++v) F.v[v] = kBig;
+        if (DEFER && any_fix) {
+          const IV<V> x = ld<V>(FLt + (size_t)(2 * j) * R + so);
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            if (fix[v]) F.v[v] = x.v[v];
+        }
+        const ST* Dv = Dt + (size_t)(f - c0) * R + so;
+        IV<V> dprev = ld<V>(Dv);
+        IV<V> tv;
+        {
+          const uint32_t key = label_key(g, f);
+          int delta[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            if (DEFER) dprev.v[v] = min(dprev.v[v], F.v[v]);
+            delta[v] = key == code[v] ? 0 : 1;
+            tv.v[v] = dprev.v[v] + 1;
+          }
+          for (uint32_t q = 0; q < ec; ++q) {
+            const uint32_t loc = erec[eb + q];
+            const ST* src = (loc & 0x80000000u)
+                                ? EXt + (size_t)(loc & 0x7fffffffu) * R + so
+                                : FLt + (size_t)(2 * loc + 1) * R + so;
+            const IV<V> du = ld<V>(src);
+#pragma unroll
+            for (int v = 0; v < V; ++v) tv.v[v] = min(tv.v[v], du.v[v] + delta[v]);
+          }
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            if (init[v]) tv.v[v] = delta[v];
+            if (tv.v[v] < bmin[v]) {
+              bmin[v] = tv.v[v];
+              barg[v] = f;
+            }
+          }
+        }
+        st<V>(T + (size_t)f * R + so, tv);
+        st<V>(BV + (size_t)(2 * d) * R + so, tv);
+        for (uint32_t q0 = 1; q0 < len; q0 += 4) {
+          const uint32_t n = min(4u, len - q0);
+          IV<V> dq[4];
+#pragma unroll
+          for (uint32_t q = 0; q < 4; ++q)
+            if (q < n) dq[q] = ld<V>(Dv + (size_t)(q0 + q) * R);
+#pragma unroll
+          for (uint32_t q = 0; q < 4; ++q) {
+            if (q < n) {
+              const uint32_t c = f + q0 + q;
+              const uint32_t key = label_key(g, c);
+#pragma unroll
+              for (int v = 0; v < V; ++v) {
+                if (DEFER) dq[q].v[v] = min(dq[q].v[v], F.v[v] + (int)(q0 + q));
+                const int delta = key == code[v] ? 0 : 1;
+                int x = min(dq[q].v[v] + 1, dprev.v[v] + delta);
+                x = min(x, tv.v[v] + 1);
+                if (init[v]) x = delta;
+                tv.v[v] = x;
+                if (x < bmin[v]) {
+                  bmin[v] = x;
+                  barg[v] = c;
+                }
+              }
+              dprev = dq[q];
+              st<V>(T + (size_t)c * R + so, tv);
+            }
+          }
+        }
+        if (len > 1) st<V>(BV + (size_t)(2 * d + 1) * R + so, tv);
+      }
+      __syncwarp();
+      if (wl == 0) mbar_arrive(&empty[k]);
+    }
+    if (ending_any) {
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        if (ending[v] && bmin[v] != 0x7fffffff)
+          atomicMin(sm_best + so + v, pack_min(bmin[v], barg[v]));
+    }
+  }
+  __syncthreads();
+  if (s_fail && threadIdx.x == 0) atomicOr(&ctl->error, ERR_ROW_WAIT);
+  if (ending_any)
+    for (int r = threadIdx.x; r < R; r += blockDim.x)
+      if (sm_best[r] != ~0ull) atomicMin(best + r, sm_best[r]);
+}
+
+// ---------------------------------------------------------------------------
+// k_pull: hierarchy positions [lo, hi): BV[2d] = min(BV[2d], BV[src] + w)
+// over the list off[d-base]..off[d-base+1]. Every source lies on another
+// level, finished before this launch, so the gathers use the read-only path.
+// ---------------------------------------------------------------------------
+template <int R, typename ST>
+__global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, uint32_t hi,
+                                              const uint32_t* __restrict__ off,
+                                              const int2* __restrict__ edges, uint32_t base,
+                                              const StepCtl* __restrict__ ctl) {
+  constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
+  if (!ctl->any_active) return;
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  const int lane = (int)(gt % G);
+  if (d >= hi) return;
+  const size_t so = (size_t)lane * V;
+  const uint32_t k0 = __ldg(off + (d - base)), k1 = __ldg(off + (d - base) + 1);
+  if (k0 == k1) return;
+  ST* p = BV + (size_t)(2 * d) * R + so;
+  IV<V> f = ld<V>(p);
+  bool changed = false;
+  for (uint32_t k = k0; k < k1; ++k) {
+    const int2 ew = __ldg(edges + k);
+    const IV<V> x = ld_nc<V>(BV + (size_t)ew.x * R + so);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const int c = x.v[v] + ew.y;
+      if (c < f.v[v]) {
+        f.v[v] = c;
+        changed = true;
+      }
+    }
+  }
+  if (changed) st<V>(p, f);
+}
+
+// ---------------------------------------------------------------------------
+// k_down: positions [lo, hi). Those below `mid` first pull their downward
+// in-edges (sources on higher levels, final); every position then finalises
+// its vertex's chars: if the first score fell below the row value, write it
+// and propagate first + (p - first) forward while it improves
+// (align.hpp:381-396). Slots without closure (row 0, idle) are untouched.
+// ---------------------------------------------------------------------------
+template <int R, bool FIXUP, typename ST>
+__global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, ST* __restrict__ T,
+                                              ST* __restrict__ FL, uint32_t lo, uint32_t mid,
+                                              uint32_t hi,
+                                              const uint32_t* __restrict__ slot_word,
+                                              unsigned long long* __restrict__ best,
+                                              const StepCtl* __restrict__ ctl) {
+  constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
+  __shared__ unsigned long long sm_best[R];
+  const bool ending_any = ctl->any_ending != 0;
+  if (!ctl->any_active) return;
+  if (ending_any) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
+    __syncthreads();
+  }
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  const int lane = (int)(gt % G);
+  if (d < hi) {
+    const size_t so = (size_t)lane * V;
+    ST* p = BV + (size_t)(2 * d) * R + so;
+    IV<V> f = ld<V>(p);
+    if (d < mid) {
+      const uint32_t k0 = __ldg(g.dn_off + d), k1 = __ldg(g.dn_off + d + 1);
+      bool changed = false;
+      for (uint32_t k = k0; k < k1; ++k) {
+        const int2 ew = __ldg(g.dn_in + k);
+        const IV<V> x = ld_nc<V>(BV + (size_t)ew.x * R + so);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const int c = x.v[v] + ew.y;
+          if (c < f.v[v]) {
+            f.v[v] = c;
+            changed = true;
+          }
+        }
+      }
+      if (changed) st<V>(p, f);
+    }
+    const uint32_t first = __ldg(g.dv_first + d), len = __ldg(g.dv_len + d);
+    {
+      // final first and last scores of the vertex, in char order, for the
+      // next row-step (the last char ends at min(raw last, F + len - 1))
+      const uint32_t sv = __ldg(g.dv_s + d);
+      IV<V> lf = f;
+      if (len > 1) {
+        const IV<V> raw = ld<V>(BV + (size_t)(2 * d + 1) * R + so);
+#pragma unroll
+        for (int v = 0; v < V; ++v) lf.v[v] = min(raw.v[v], f.v[v] + (int)(len - 1));
+      }
+      st<V>(FL + (size_t)(2 * sv) * R + so, f);
+      st<V>(FL + (size_t)(2 * sv + 1) * R + so, lf);
+    }
+    if (!FIXUP) {
+      // the row stays raw; a slot on its last row needs min over the final
+      // scores = min(min over raw scores [k_row], min over swept first scores)
+      if (ending_any) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const uint32_t w = __ldg(slot_word + so + v);
+          if ((w & SW_CLOSURE) && (w & SW_ENDING))
+            atomicMin(sm_best + so + v, pack_min(f.v[v], first));
+        }
+      }
+    } else {
+    IV<V> tq = ld<V>(T + (size_t)first * R + so);
+    bool act[V], endg[V];
+    bool any = false;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const uint32_t w = __ldg(slot_word + so + v);
+      act[v] = (w & SW_CLOSURE) && f.v[v] < tq.v[v];
+      endg[v] = act[v] && (w & SW_ENDING);
+      if (act[v]) {
+        tq.v[v] = f.v[v];
+        if (endg[v]) atomicMin(sm_best + so + v, pack_min(f.v[v], first));
+      }
+      any |= act[v];
+    }
+    if (any) {
+      st<V>(T + (size_t)first * R + so, tq);
+      // first + q while it improves, every slot of the lane in one pass per char
+      for (uint32_t q = 1; q < len && any; ++q) {
+        ST* tp = T + (size_t)(first + q) * R + so;
+        IV<V> x = ld<V>(tp);
+        any = false;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          if (!act[v]) continue;
+          const int cand = f.v[v] + (int)q;
+          if (cand < x.v[v]) {
+            x.v[v] = cand;
+            if (endg[v]) atomicMin(sm_best + so + v, pack_min(cand, first + q));
+            any = true;
+          } else {
+            act[v] = false;
+          }
+        }
+        st<V>(tp, x);
+      }
+    }
+    }
+  }
+  if (ending_any) flush_min<R>(sm_best, best);
+}
+
+// ---------------------------------------------------------------------------
 // k_top: hierarchy positions [K0, S), one CTA per slot. The first/last
 // scores of the region are staged in shared memory; the region's upward
 // levels (low -> high) and downward levels (high -> low) then run as a
@@ -525,8 +1040,8 @@ __host__ __device__ constexpr size_t top_smem_bytes(uint32_t K) {
   return ((size_t)(2 * K + 2) * 4 + 15) / 16 * 16 + 2 * kTopChunk * 8 + 16;
 }
 
-template <int R>
-__global__ void __launch_bounds__(1024) k_top(int* __restrict__ BV, TopPtrs t,
+template <int R, typename ST>
+__global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
                                               const uint32_t* __restrict__ slot_word,
                                               StepCtl* __restrict__ ctl) {
   extern __shared__ __align__(16) unsigned char top_smem[];
@@ -557,7 +1072,7 @@ __global__ void __launch_bounds__(1024) k_top(int* __restrict__ BV, TopPtrs t,
       const uint32_t j = j0 + u * blockDim.x;
       if (j < t.K) {
         const size_t d = K0 + j;
-        if constexpr (R == 1) {
+        if constexpr (R == 1 && sizeof(ST) == 4) {
           const int2 x = *reinterpret_cast<const int2*>(BV + 2 * d);
           fv[u] = x.x;
           lv[u] = x.y;
@@ -612,7 +1127,19 @@ __global__ void __launch_bounds__(1024) k_top(int* __restrict__ BV, TopPtrs t,
     __syncthreads();
     return;
   }
-  for (uint32_t j = threadIdx.x; j < t.K; j += blockDim.x) BV[(2 * (K0 + j)) * R + r] = sm[2 * j];
+  for (uint32_t j = threadIdx.x; j < t.K; j += blockDim.x) BV[(2 * (K0 + j)) * R + r] = (ST)sm[2 * j];
+}
+
+// ---------------------------------------------------------------------------
+// k_fl_from_row: FL of a final row that was not produced by the preceding
+// row-step (a checkpoint row a segment restarts from): first and last score
+// of every string vertex, read from the row (R = 1, int32 rows).
+// ---------------------------------------------------------------------------
+__global__ void k_fl_from_row(GraphPtrs g, const int* __restrict__ row, int* __restrict__ FL) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= g.S) return;
+  FL[2 * s] = row[g.sv_off[s]];
+  FL[2 * s + 1] = row[g.sv_off[s + 1] - 1];
 }
 
 // ---------------------------------------------------------------------------
@@ -706,7 +1233,7 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
 
 // ---------------------------------------------------------------------------
 // k_walk: single-thread traceback by score equality over rows
-// [row_lo, row_hi] of a score matrix (row i at M + (i - row_lo) * N),
+// [row_lo, row_hi] of a score matrix (row i at M + (i - row_lo) * pitch),
 // walk_traceback_from_scores (src/traceback.hpp:483-586). Tie order:
 // INSERT from the previous char of the same vertex, INSERT from the last
 // char of the first string in-neighbour (in-CSR order) that fits, DELETE,
@@ -726,11 +1253,11 @@ struct WalkOp {
   uint32_t op;
 };
 
-__global__ void k_walk(GraphPtrs g, const int* __restrict__ M, long long row_lo, long long row_hi,
-                       uint32_t start, const unsigned char* __restrict__ read, WalkOp* __restrict__ ops,
-                       uint32_t max_ops, WalkOut* __restrict__ out) {
+__global__ void k_walk(GraphPtrs g, const int* __restrict__ M, size_t pitch, long long row_lo,
+                       long long row_hi, uint32_t start, const unsigned char* __restrict__ read,
+                       WalkOp* __restrict__ ops, uint32_t max_ops, WalkOut* __restrict__ out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const size_t N = g.N;
+  const size_t N = pitch;
   uint32_t cur = start;
   long long row = row_hi;
   // string vertex of `cur`: binary search over sv_off

@@ -170,6 +170,19 @@ typedef struct {
 } chsga_graph_stats;
 chsga_status chsga_graph_get_stats(const chsga_host_graph* g, chsga_graph_stats* out);
 
+/* Pre-flight check of a graph for the device layout, on the host only:
+ * builds the layout the kernels use (labels, string vertices, hierarchy
+ * order, pull lists, top region) and, for slots >= 32, the shared-memory
+ * tiles of the row kernel, and checks every bound and alignment the kernels
+ * rely on. No reference counterpart. */
+typedef struct {
+  uint64_t num_levels, top_first_level, top_vertices;
+  uint64_t tiled;            /* 1 if the tile-staged row kernel applies */
+  uint64_t tiles, long_tiles, slot_bytes, slots_per_block, smem_bytes;
+} chsga_layout_stats;
+chsga_status chsga_check_layout(const chsga_host_graph* g, uint32_t slots, uint32_t row_bits,
+                                chsga_layout_stats* out);
+
 const char* chsga_last_error_global(void);
 
 /* ------------------------------------------------------------------------- */
@@ -211,9 +224,12 @@ chsga_status chsga_align_rows(chsga_ctx* ctx, const char* read, uint32_t len, in
  * refilled on the device. No reference counterpart (the reference aligns
  * reads serially, src/align.hpp:488); results equal chsga_align_scores. */
 typedef struct {
-  uint32_t slots;         /* reads advanced together: 1,2,4,8,16,32,64,128; 0 = autotune */
+  uint32_t slots;         /* reads advanced together: 1,2,4,8,16,32,64,128; 0 = 64 */
   uint32_t steps_per_graph; /* row-steps captured per CUDA graph launch; 0 = default */
   uint32_t use_graphs;    /* 1 = CUDA-graph capture of the row-step sequence */
+  uint32_t row_bits;      /* storage of the score rows: 0 = 16 when every read is at most
+                             65000 bases (each value of row i is at most i + 1, so this is
+                             exact; arithmetic stays int32), else 32; or force 16 / 32 */
 } chsga_batch_opts;
 chsga_status chsga_align_scores_batched(chsga_ctx* ctx, const char* const* reads,
                                         const uint32_t* lens, uint32_t n,
@@ -263,6 +279,7 @@ uint64_t chsga_ops_to_cigar(const chsga_op* ops, uint64_t n, char* buf, uint64_t
  * (downward levels with the final propagation), other_ms (slot advance). */
 typedef struct {
   double row_ms, sweep_up_ms, top_ms, sweep_down_ms, other_ms, total_ms;
+  uint64_t row_bits;      /* 16 or 32: storage width of the score rows */
   uint64_t rows;          /* read rows computed */
   uint64_t steps;         /* row-steps that had work */
   uint64_t launches;      /* kernels launched by those steps */

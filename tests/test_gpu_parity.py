@@ -38,11 +38,29 @@ def test_every_row_matches_oracle(small_graph, ctx_small, oracle_small):
 
 
 @pytest.mark.parametrize("slots", [2, 8, 32, 64, 128])
-def test_batched_matches_plain(small_graph, ctx_small, oracle_small, slots):
+@pytest.mark.parametrize("row_bits", [16, 32])
+def test_batched_matches_plain(small_graph, ctx_small, oracle_small, slots, row_bits):
     g, files, reads = small_graph
     want = oracle_small.scores(reads)
-    got = ctx_small.align_scores_batched(reads, slots=slots)
+    got = ctx_small.align_scores_batched(reads, slots=slots, row_bits=row_bits)
     np.testing.assert_array_equal(got, want)
+    assert ctx_small.profile()["row_bits"] == row_bits
+
+
+def test_row_width_follows_the_read_length(tmp_path):
+    # rows of a read longer than 65000 bases do not fit 16 bits: the engine
+    # must fall back to 32-bit rows (and refuse a forced 16)
+    g, files = gen_graph(tmp_path, "long", backbone_len=600, seed=81)
+    rd = g.gen_reads(1, 82, 40).to_list()[0] * 1700  # 68000 bases
+    o = orc.Oracle(files)
+    want = o.scores([rd, rd[:300]])
+    ctx = cb.Context(0).load(g)
+    np.testing.assert_array_equal(ctx.align_scores_batched([rd, rd[:300]], slots=2), want)
+    assert ctx.profile()["row_bits"] == 32
+    with pytest.raises(cb.ChsgaError) as e:
+        ctx.align_scores_batched([rd], slots=2, row_bits=16)
+    assert e.value.status == cb.ERR_INVALID_ARG
+    ctx.close()
 
 
 def test_batched_uneven_lengths(small_graph, ctx_small, oracle_small):
@@ -90,8 +108,11 @@ def test_traceback_two_level(small_graph, ctx_small, oracle_small):
     rd = reads[1]
     want = int(oracle_small.scores([rd])[0])
     n = oracle_small.num_chars
-    # a segment of 100 rows does not fit 40 rows: sub-checkpoints inside it
-    ops, score, ck = ctx_small.align_traceback(rd, k=100, cap_bytes=40 * n * 4)
+    # a context whose device budget is 40 rows: a segment of 100 rows does
+    # not fit, so the segment is recomputed from sub-checkpoints
+    ctx = cb.Context(0, hbm_cap_bytes=40 * n * 4).load(g)
+    ops, score, ck = ctx.align_traceback(rd, k=100)
+    ctx.close()
     assert ck and score == want
     ps, last = orc.rescore(ops, rd, labels)
     assert ps == want and last == len(rd) - 1

@@ -152,3 +152,19 @@ def test_build_pch_and_gen_tools(tmp_path):
     # the tool and the library build the same hierarchy for the same seed
     assert open(out, "rb").read() == open(p + ".string.out", "rb").read()
     assert len(cb.Reads.load(p + ".reads.fa", 0)) == 4
+
+
+@pytest.mark.parametrize("slots", [32, 64, 128])
+@pytest.mark.parametrize("row_bits", [16, 32])
+def test_device_layout_preflight(slots, row_bits):
+    # builds the kernels' layout and the row kernel's shared-memory tiles on
+    # the host and checks every copy bound, alignment and record index the
+    # tiled row kernel relies on (chsga_check_layout raises on a violation)
+    for cfg in (dict(cb.GRAPH_CONFIGS["cfg2"], backbone_len=300_000),
+                dict(cb.GRAPH_CONFIGS["cfg1"], backbone_len=20_000, vlen_max=100)):
+        g = cb.HostGraph.generate(**cfg).build_pch()
+        st = g.check_layout(slots, row_bits)
+        assert st["num_levels"] > 5 and st["top_vertices"] > 0
+        if st["tiled"]:
+            assert st["tiles"] > 0 and st["smem_bytes"] <= 232448
+            assert 2 <= st["slots_per_block"] <= 16
