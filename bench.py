@@ -120,15 +120,20 @@ def make_reads(g, n, seed, len_max=10000):
                        indel_len_max=3).to_list()
 
 
-def algorithmic_row_bytes(st, slots, multi):
-    """Bytes one k_row launch must move: the previous and the new score of
-    every char for every slot (8 N R), the first/last boundary scores of
-    every vertex (4 R (S + S_multi)), 2-bit labels plus the special-char map
-    (3N/8), three words per vertex (offset, hierarchy position, in-edge
-    offset: 12 S) and the in-edges of first chars (4 E_first)."""
+def algorithmic_row_bytes(st, slots, multi, score_bytes):
+    """Bytes one row-kernel launch must move, with w = bytes per stored
+    score: the previous and the new score of every char for every slot
+    (2 w N R), the first/last boundary scores of every vertex written for
+    the sweeps (w R (S + S_multi)), the previous row's final first score of
+    every vertex and final last score of every first-char in-edge source
+    (w R (S + E_first)), 2-bit labels plus the special-char map (3N/8), three
+    words per vertex (offset, hierarchy position, in-edge offset: 12 S) and
+    one word per first-char in-edge (4 E_first)."""
     N, S = st["num_chars"], st["num_strings"]
     e_first = st["num_char_edges"] - (N - S)
-    return 8 * N * slots + 4 * slots * (S + multi) + 3 * N / 8 + 12 * S + 4 * e_first
+    w = score_bytes
+    return (2 * w * N * slots + w * slots * (S + multi) + w * slots * (S + e_first)
+            + 3 * N / 8 + 12 * S + 4 * e_first)
 
 
 def measured_peak():
@@ -335,11 +340,12 @@ def main():
         pctx.close()
         row_avg_s = pr["row_ms"] / max(1, pr["row_launches"]) / 1e3
         peak, src = measured_peak()
-        ab = algorithmic_row_bytes(st, args.slots, multi)
+        ab = algorithmic_row_bytes(st, args.slots, multi, pr["row_bits"] // 8)
         tr = ncu_traffic()
         total = pr["row_ms"] + pr["sweep_up_ms"] + pr["top_ms"] + pr["sweep_down_ms"] + pr["other_ms"]
         line["roofline"] = {
-            "bound": "hbm", "kernel": f"k_row<{args.slots}>",
+            "bound": "hbm", "kernel": f"k_row_dpx<{args.slots}>" if pr["row_bits"] == 16
+            else f"k_row_direct<{args.slots}>", "row_bits": int(pr["row_bits"]),
             "achieved": ab / row_avg_s / 1e9, "peak": peak, "unit": "GB/s",
             "frac": ab / row_avg_s / 1e9 / peak, "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)"
             if src == "measured" else "fallback 6.65 TB/s",

@@ -37,6 +37,7 @@ HostLayout build_layout(const chsga_graph_host& g) {
   // --- labels: 2-bit code plus one "special" byte class --------------------
   L.lab2.assign((N + 15) / 16, 0);
   L.lab_sp.assign((N + 31) / 32, 0);
+  L.lab4.assign((N + 7) / 8 + 2, 0);  // two spare words: the kernels read a word ahead
   for (uint32_t c = 0; c < N; ++c) {
     unsigned char ch = (unsigned char)g.labels[c];
     int code = base_code(ch);
@@ -49,6 +50,8 @@ HostLayout build_layout(const chsga_graph_host& g) {
       code = 0;
     }
     L.lab2[c >> 4] |= (uint32_t)code << ((c & 15) * 2);
+    const uint32_t key = ((L.lab_sp[c >> 5] >> (c & 31)) & 1u) ? 4u : (uint32_t)code;
+    L.lab4[c >> 3] |= key << ((c & 7) * 4);
   }
 
   // --- string vertices and the char graph -----------------------------------

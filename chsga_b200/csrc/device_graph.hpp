@@ -50,6 +50,7 @@ struct HostLayout {
   int special = -1;
   std::vector<uint32_t> lab2;   // ceil(N/16) words
   std::vector<uint32_t> lab_sp; // ceil(N/32) words
+  std::vector<uint32_t> lab4;   // ceil(N/8)+2 words: 4-bit label key per char (0..3 ACGT, 4 special)
   std::vector<uint32_t> sv_off, sv_dev, vin_off, vin_src, vin_srcv;
   std::vector<uint32_t> dv_first, dv_len, dv_s;  // by hierarchy order
   std::vector<uint32_t> up_off, dn_off;    // S+1, by hierarchy order

@@ -76,7 +76,7 @@ struct PinnedArr {
 };
 
 struct GraphDev {
-  DevArr<uint32_t> lab2, lab_sp, sv_off, sv_dev, vin_off, vin_src, vin_srcv, dv_first, dv_len;
+  DevArr<uint32_t> lab2, lab_sp, lab4, sv_off, sv_dev, vin_off, vin_src, vin_srcv, dv_first, dv_len;
   DevArr<uint32_t> up_off, dn_off, istr_off, istr_src;
   DevArr<uint32_t> dv_s;
   DevArr<int2> up_in, dn_in;
@@ -485,6 +485,7 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   cudaStream_t s = c.st;
   d.lab2.upload(L.lab2, s);
   d.lab_sp.upload(L.lab_sp, s);
+  d.lab4.upload(L.lab4, s);
   d.sv_off.upload(L.sv_off, s);
   d.sv_dev.upload(L.sv_dev, s);
   d.vin_off.upload(L.vin_off, s);
@@ -520,6 +521,7 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
                            d.dv_len.p};
   CK(cudaStreamSynchronize(s));
   c.gp = dev::GraphPtrs{L.N,          L.S,          L.special,      d.lab2.p,     d.lab_sp.p,
+                        d.lab4.p,
                         d.sv_off.p,   d.sv_dev.p,   d.vin_off.p,    d.vin_src.p,  d.vin_srcv.p,
 
                         d.dv_first.p, d.dv_len.p,   d.dv_s.p,       d.up_off.p,   d.up_in.p,    d.dn_off.p,

@@ -39,6 +39,7 @@ struct GraphPtrs {
   int special;
   const uint32_t* lab2;
   const uint32_t* lab_sp;
+  const uint32_t* lab4;  // 4-bit label key per char, 8 per word
   const uint32_t* sv_off;
   const uint32_t* sv_dev;
   const uint32_t* vin_off;
@@ -464,6 +465,84 @@ __device__ __forceinline__ uint32_t sel(uint32_t a, uint32_t b, uint32_t m) {
   return r;
 }
 
+// Label keys of consecutive chars: a 64-bit window over the 4-bit key array.
+struct KeyWindow {
+  const uint32_t* w;
+  uint64_t win;
+  uint32_t sh;
+  __device__ __forceinline__ KeyWindow(const uint32_t* lab4, uint32_t c) {
+    w = lab4 + (c >> 3);
+    win = (uint64_t)__ldg(w) | ((uint64_t)__ldg(w + 1) << 32);
+    sh = (c & 7u) * 4u;
+  }
+  __device__ __forceinline__ uint32_t next() {
+    const uint32_t k = (uint32_t)(win >> sh) & 0xFu;
+    sh += 4;
+    if (sh == 32) {
+      ++w;
+      win = (win >> 32) | ((uint64_t)__ldg(w + 1) << 32);
+      sh = 0;
+    }
+    return k;
+  }
+};
+
+// The chain chars of one vertex (c = f+1 .. f+len-1); TRACK also keeps the
+// per-slot minimum and its smallest char for slots on their last row.
+template <int R, bool DEFER, bool TRACK, int P>
+__device__ __forceinline__ void dpx_chain(const uint16_t* __restrict__ dp, uint16_t* __restrict__ tp,
+                                          uint32_t len, uint32_t f, KeyWindow& kw, U2<P>& t,
+                                          U2<P>& dprev, const U2<P>& F, bool any_fix,
+                                          const uint32_t (&dtab)[P], const uint32_t (&imask)[P],
+                                          const uint32_t (&fmask)[P], int (&bmin)[2 * P],
+                                          uint32_t (&barg)[2 * P]) {
+  constexpr uint32_t ONES = 0x00010001u;
+  constexpr int DEPTH = 8;
+  uint32_t off2 = 0;
+  for (uint32_t q0 = 1; q0 < len; q0 += DEPTH) {
+    const uint32_t n = min((uint32_t)DEPTH, len - q0);
+    U2<P> dq[DEPTH];
+#pragma unroll
+    for (int k = 0; k < DEPTH; ++k)
+      if (k < (int)n) dq[k] = ldp_nc<P>(dp + (size_t)k * R);
+#pragma unroll
+    for (int k = 0; k < DEPTH; ++k) {
+      if (k < (int)n) {
+        const uint32_t key = kw.next();
+        off2 += ONES;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const uint32_t delta = (dtab[p] >> key) & ONES;
+          if (DEFER && any_fix)
+            dq[k].h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq[k].h[p]), dq[k].h[p], fmask[p]);
+          uint32_t x = __viaddmin_u16x2(t.h[p], ONES, dq[k].h[p] + ONES);
+          x = __viaddmin_u16x2(dprev.h[p], delta, x);
+          t.h[p] = sel(delta, x, imask[p]);
+        }
+        dprev = dq[k];
+        stp<P>(tp + (size_t)k * R, t);
+        if (TRACK) {
+          const uint32_t c = f + q0 + k;
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            const int lo = (int)(t.h[p] & 0xFFFFu), hi = (int)(t.h[p] >> 16);
+            if (lo < bmin[2 * p]) {
+              bmin[2 * p] = lo;
+              barg[2 * p] = c;
+            }
+            if (hi < bmin[2 * p + 1]) {
+              bmin[2 * p + 1] = hi;
+              barg[2 * p + 1] = c;
+            }
+          }
+        }
+      }
+    }
+    dp += (size_t)DEPTH * R;
+    tp += (size_t)DEPTH * R;
+  }
+}
+
 template <int R, bool DEFER>
 __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t* __restrict__ D,
                                                     uint16_t* __restrict__ T,
@@ -506,12 +585,18 @@ __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t*
     }
     const uint32_t f = __ldg(g.sv_off + s), e = __ldg(g.sv_off + s + 1);
     const uint32_t d = __ldg(g.sv_dev + s);
+    const uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
+    KeyWindow kw(g.lab4, f);
     U2<P> F;
+#pragma unroll
+    for (int p = 0; p < P; ++p) F.h[p] = 0;
     if (DEFER && any_fix) F = ldp_nc<P>(FL + (size_t)(2 * s) * R + so);
-    U2<P> dprev = ldp_nc<P>(D + (size_t)f * R + so);
+    const uint16_t* dp = D + (size_t)f * R + so;
+    uint16_t* tp = T + (size_t)f * R + so;
+    U2<P> dprev = ldp_nc<P>(dp);
     U2<P> t;
     {
-      const uint32_t key = label_key(g, f);
+      const uint32_t key = kw.next();
       uint32_t delta[P];
 #pragma unroll
       for (int p = 0; p < P; ++p) {
@@ -519,7 +604,6 @@ __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t*
         if (DEFER && any_fix) dprev.h[p] = sel(__vminu2(dprev.h[p], F.h[p]), dprev.h[p], fmask[p]);
         t.h[p] = dprev.h[p] + ONES;
       }
-      const uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
       for (uint32_t k = k0; k < k1; ++k) {
         const uint32_t su = __ldg(g.vin_srcv + k);
         const U2<P> du = ldp_nc<P>(FL + (size_t)(2 * su + 1) * R + so);
@@ -529,59 +613,25 @@ __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t*
 #pragma unroll
       for (int p = 0; p < P; ++p) t.h[p] = sel(delta[p], t.h[p], imask[p]);
     }
-    stp<P>(T + (size_t)f * R + so, t);
+    stp<P>(tp, t);
     stp<P>(BV + (size_t)(2 * d) * R + so, t);
     int bmin[2 * P];
     uint32_t barg[2 * P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      bmin[2 * p] = (int)(t.h[p] & 0xFFFFu);
+      bmin[2 * p + 1] = (int)(t.h[p] >> 16);
+      barg[2 * p] = barg[2 * p + 1] = f;
+    }
+    const uint32_t len = e - f;
     if (ending_any && any_end) {
-#pragma unroll
-      for (int p = 0; p < P; ++p) {
-        bmin[2 * p] = (int)(t.h[p] & 0xFFFFu);
-        bmin[2 * p + 1] = (int)(t.h[p] >> 16);
-        barg[2 * p] = barg[2 * p + 1] = f;
-      }
+      dpx_chain<R, DEFER, true, P>(dp + R, tp + R, len, f, kw, t, dprev, F, any_fix, dtab, imask,
+                                   fmask, bmin, barg);
+    } else {
+      dpx_chain<R, DEFER, false, P>(dp + R, tp + R, len, f, kw, t, dprev, F, any_fix, dtab, imask,
+                                    fmask, bmin, barg);
     }
-    for (uint32_t c0 = f + 1; c0 < e; c0 += 4) {
-      const uint32_t n = min(4u, e - c0);
-      U2<P> dq[4];
-#pragma unroll
-      for (uint32_t k = 0; k < 4; ++k)
-        if (k < n) dq[k] = ldp_nc<P>(D + (size_t)(c0 + k) * R + so);
-#pragma unroll
-      for (uint32_t k = 0; k < 4; ++k) {
-        if (k < n) {
-          const uint32_t c = c0 + k;
-          const uint32_t key = label_key(g, c);
-          const uint32_t off2 = (c - f) * ONES;
-#pragma unroll
-          for (int p = 0; p < P; ++p) {
-            const uint32_t delta = (dtab[p] >> key) & ONES;
-            if (DEFER && any_fix)
-              dq[k].h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq[k].h[p]), dq[k].h[p], fmask[p]);
-            uint32_t x = __viaddmin_u16x2(t.h[p], ONES, dq[k].h[p] + ONES);
-            x = __viaddmin_u16x2(dprev.h[p], delta, x);
-            t.h[p] = sel(delta, x, imask[p]);
-          }
-          dprev = dq[k];
-          stp<P>(T + (size_t)c * R + so, t);
-          if (ending_any && any_end) {
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-              const int lo = (int)(t.h[p] & 0xFFFFu), hi = (int)(t.h[p] >> 16);
-              if (lo < bmin[2 * p]) {
-                bmin[2 * p] = lo;
-                barg[2 * p] = c;
-              }
-              if (hi < bmin[2 * p + 1]) {
-                bmin[2 * p + 1] = hi;
-                barg[2 * p + 1] = c;
-              }
-            }
-          }
-        }
-      }
-    }
-    if (e - f > 1) stp<P>(BV + (size_t)(2 * d + 1) * R + so, t);
+    if (len > 1) stp<P>(BV + (size_t)(2 * d + 1) * R + so, t);
     if (ending_any && any_end) {
 #pragma unroll
       for (int q = 0; q < 2 * P; ++q) {
