@@ -30,6 +30,7 @@ OK, ERR_INVALID_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, \
     ERR_NO_PATH, ERR_TIMEOUT, ERR_INTERNAL, ERR_BUSY = range(11)
 OP_DELETE, OP_MATCHSUB, OP_INSERT = 0, 1, 2
 FLAG_PROFILE = 1
+NOALLOC_SCRATCH_BYTES = 32 << 20  # CHSGA_NOALLOC_SCRATCH_BYTES
 
 u64p = C.POINTER(C.c_uint64)
 u32p = C.POINTER(C.c_uint32)
@@ -159,6 +160,7 @@ _sig("chsga_load_host_graph", C.c_int32, vp, vp)
 _sig("chsga_align_scores", C.c_int32, vp, C.POINTER(C.c_char_p), u32p, C.c_uint32, i32p)
 _sig("chsga_align_scores_batched", C.c_int32, vp, C.POINTER(C.c_char_p), u32p, C.c_uint32,
      C.POINTER(BatchOpts), i32p)
+_sig("chsga_align_scores_noalloc", C.c_int32, vp, C.POINTER(C.c_char_p), u32p, C.c_uint32, i32p)
 _sig("chsga_align_rows", C.c_int32, vp, C.c_char_p, C.c_uint32, i32p)
 _sig("chsga_align_traceback", C.c_int32, vp, C.c_char_p, C.c_uint32, C.POINTER(TbOpts),
      C.POINTER(TbResult))
@@ -354,6 +356,15 @@ class Context:
         o = BatchOpts(slots, steps_per_graph, int(use_graphs), row_bits)
         self._ck(_lib.chsga_align_scores_batched(self._h, arr, lens.ctypes.data_as(u32p), len(reads),
                                                  C.byref(o), out.ctypes.data_as(i32p)))
+        return out
+
+    def align_scores_noalloc(self, reads: Sequence[bytes]) -> np.ndarray:
+        """Same scores as align_scores, with no device allocation per call: the
+        working memory is a fixed array of NOALLOC_SCRATCH_BYTES in the library."""
+        arr, lens = _read_ptrs(reads)
+        out = np.zeros(len(reads), dtype=np.int32)
+        self._ck(_lib.chsga_align_scores_noalloc(self._h, arr, lens.ctypes.data_as(u32p), len(reads),
+                                                 out.ctypes.data_as(i32p)))
         return out
 
     def align_rows(self, read: bytes, num_chars: int) -> np.ndarray:

@@ -9,6 +9,7 @@
 #include <filesystem>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <type_traits>
 
@@ -790,6 +791,264 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
   res->score = best_s;
 }
 
+// ---- score-only alignment without device allocation -------------------------
+//
+// For callers that may not allocate GPU memory once they are running (a
+// service whose free HBM belongs to its own pool after start-up, a loop that
+// cannot afford the device-wide synchronisation of cudaMalloc): every
+// per-call buffer of the one-read-per-step score path comes from this fixed
+// array. The driver reserves it on each GPU where it loads this file's device
+// code, until the process exits. On the host, `noalloc_scratch` only names
+// the symbol; its device address on the current GPU comes from
+// cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char noalloc_scratch[CHSGA_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoallocMaxDevices = 64;
+
+struct NoallocDevice {
+  std::mutex mu;                  // held for a whole call: calls on a device never overlap
+  unsigned char* base = nullptr;  // device address of noalloc_scratch on this device
+};
+NoallocDevice noalloc_devices[kNoallocMaxDevices];
+
+// Byte offsets of the per-call buffers in the array (each 256-byte aligned).
+struct NoallocLayout {
+  uint64_t rows[2], bv, fl, slots, word, best, ctl, reads, lens, queue, slot_of, res_score,
+      res_vertex, res_t0, res_t1, out, end;
+};
+
+NoallocLayout noalloc_layout(uint64_t N, uint64_t S, uint64_t read_bytes, uint64_t n) {
+  NoallocLayout l{};
+  uint64_t at = 0;
+  auto take = [&](uint64_t bytes) {
+    const uint64_t o = at;
+    at += (std::max<uint64_t>(bytes, 1) + 255) / 256 * 256;
+    return o;
+  };
+  // the same sizes as the context's own buffers for one slot of 16-bit rows
+  l.rows[0] = take((N + 32) * sizeof(uint16_t));
+  l.rows[1] = take((N + 32) * sizeof(uint16_t));
+  l.bv = take(2 * S * sizeof(uint16_t));
+  l.fl = take(2 * (S + 16) * sizeof(uint16_t));
+  l.slots = take(sizeof(dev::SlotState));
+  l.word = take(sizeof(uint32_t));
+  l.best = take(sizeof(unsigned long long));
+  l.ctl = take(sizeof(dev::StepCtl));
+  l.reads = take(read_bytes);
+  l.lens = take(n * sizeof(uint32_t));
+  l.queue = take(n * sizeof(dev::ReadDesc));
+  l.slot_of = take(n * sizeof(int32_t));
+  l.res_score = take(n * sizeof(int32_t));
+  l.res_vertex = take(n * sizeof(uint32_t));
+  l.res_t0 = take(n * sizeof(unsigned long long));
+  l.res_t1 = take(n * sizeof(unsigned long long));
+  l.out = take(n * sizeof(int32_t));
+  l.end = at;
+  return l;
+}
+
+struct NoallocBufs {
+  uint16_t* rows[2];
+  uint16_t* BV;
+  uint16_t* FL;
+  dev::SlotState* slots;
+  uint32_t* word;
+  unsigned long long* best;
+  dev::StepCtl* ctl;
+  unsigned char* reads;
+  uint32_t* lens;
+  dev::ReadDesc* queue;
+  int32_t* slot_of;
+  int32_t* res_score;
+  uint32_t* res_vertex;
+  unsigned long long *res_t0, *res_t1;
+  int32_t* out;
+};
+
+// One block. Builds the read queue from the lengths: the non-empty reads in
+// caller order, ids 0..m-1, offsets = prefix sums of all lengths (where the
+// host copied the bytes); slot_of[i] = queue id of caller read i, -1 when it
+// is empty. Puts the slot idle and the control block at zero with m queued
+// reads: the array holds the previous call's values.
+__global__ void __launch_bounds__(1024) k_noalloc_prepare(const uint32_t* __restrict__ lens, uint32_t n,
+                                                          dev::ReadDesc* __restrict__ queue,
+                                                          int32_t* __restrict__ slot_of,
+                                                          dev::SlotState* __restrict__ slots,
+                                                          dev::StepCtl* __restrict__ ctl,
+                                                          unsigned long long* __restrict__ best) {
+  __shared__ unsigned long long s_off[1024];
+  __shared__ uint32_t s_cnt[1024];
+  const uint64_t per = ((uint64_t)n + 1023) / 1024;
+  const uint64_t a = threadIdx.x * per;
+  const uint64_t lo = a < n ? a : n, hi = lo + per < n ? lo + per : n;
+  unsigned long long off = 0;
+  uint32_t cnt = 0;
+  for (uint64_t i = lo; i < hi; ++i) {
+    off += lens[i];
+    cnt += lens[i] != 0;
+  }
+  s_off[threadIdx.x] = off;
+  s_cnt[threadIdx.x] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long o = 0;
+    uint32_t k = 0;
+    for (int t = 0; t < 1024; ++t) {
+      const unsigned long long a = s_off[t];
+      const uint32_t b = s_cnt[t];
+      s_off[t] = o;
+      s_cnt[t] = k;
+      o += a;
+      k += b;
+    }
+    dev::StepCtl z{};
+    z.q_count = k;
+    *ctl = z;
+    slots[0] = dev::SlotState{0, 0, 0, -1, 0};
+    best[0] = ~0ull;
+  }
+  __syncthreads();
+  off = s_off[threadIdx.x];
+  cnt = s_cnt[threadIdx.x];
+  for (uint64_t i = lo; i < hi; ++i) {
+    const uint32_t len = lens[i];
+    if (len) {
+      queue[cnt] = dev::ReadDesc{off, len, (int32_t)cnt};
+      slot_of[i] = (int32_t)cnt;
+      ++cnt;
+    } else {
+      slot_of[i] = -1;
+    }
+    off += len;
+  }
+}
+
+__global__ void k_noalloc_finish(const int32_t* __restrict__ slot_of,
+                                 const int32_t* __restrict__ res_score, uint32_t n,
+                                 int32_t empty_score, int32_t* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const int32_t q = slot_of[i];
+    out[i] = q < 0 ? empty_score : res_score[q];
+  }
+}
+
+// The row-step of chsga_align_scores (one slot, 16-bit rows, deferred
+// closure) on the buffers of the fixed array.
+void noalloc_row_step(chsga_ctx& c, const NoallocBufs& b, const uint16_t* D, uint16_t* T) {
+  const cudaStream_t s = c.st;
+  const HostLayout& L = c.L;
+  const TopDev& top = *c.top;
+  constexpr int G = Lanes<1>::G;
+  dev::k_row_direct<1, true, uint16_t><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(
+      c.gp, D, T, b.BV, b.FL, b.word, b.best, b.ctl);
+  const uint32_t fl = top.h.first_level;
+  for (uint32_t l = 0; l < fl; ++l) {
+    if (L.lvl_up_edges[l] == 0) continue;
+    const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
+    dev::k_pull<1, uint16_t><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
+        b.BV, lo, hi, c.gd.up_off.p, c.gd.up_in.p, 0, b.ctl);
+  }
+  if (top.h.K) {
+    if (!top.h.upg.empty())
+      dev::k_pull<1, uint16_t><<<nblocks((uint64_t)top.h.K * G), 256, 0, s>>>(
+          b.BV, top.h.K0, L.S, top.upg_off.p, top.upg.p, top.h.K0, b.ctl);
+    dev::k_top<1, uint16_t><<<1, kTopThreads, dev::top_smem_bytes(top.h.K), s>>>(b.BV, top.ptrs,
+                                                                               b.word, b.ctl);
+  }
+  if (fl == 0) {
+    dev::k_down<1, false, uint16_t><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(
+        c.gp, b.BV, T, b.FL, 0, 0, L.S, b.word, b.best, b.ctl);
+  } else {
+    for (int l = (int)fl - 1; l >= 0; --l) {
+      const uint32_t lo = L.lvl_off[l], mid = L.lvl_off[l + 1];
+      const uint32_t hi = (l == (int)fl - 1) ? L.S : mid;
+      dev::k_down<1, false, uint16_t><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
+          c.gp, b.BV, T, b.FL, lo, mid, hi, b.word, b.best, b.ctl);
+    }
+  }
+  dev::k_advance<1><<<1, 128, 0, s>>>(b.slots, b.queue, b.reads, b.best, b.res_score, b.res_vertex,
+                                      b.res_t0, b.res_t1, b.word, b.ctl, L.special, 0);
+  check_launch();
+}
+
+void scores_noalloc(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n,
+                    int32_t* out) {
+  require(c.device >= 0 && c.device < kNoallocMaxDevices, CHSGA_ERR_UNSUPPORTED,
+          "chsga_align_scores_noalloc supports device ordinals below 64");
+  NoallocDevice& d = noalloc_devices[c.device];
+  std::lock_guard<std::mutex> lock(d.mu);
+  if (!d.base) {  // set-up, once per device; the context made this device current
+    unsigned char* ptr = nullptr;
+    CK(cudaGetSymbolAddress((void**)&ptr, noalloc_scratch));
+    CK(cudaFuncSetAttribute(dev::k_top<1, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)dev::top_smem_bytes(kTopMaxVertices)));
+    d.base = ptr;
+  }
+  uint64_t total = 0;
+  uint32_t m = 0, max_len = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    require(reads[i] != nullptr || lens[i] == 0, CHSGA_ERR_INVALID_ARG, "null read");
+    total += lens[i];
+    m += lens[i] != 0;
+    max_len = std::max(max_len, lens[i]);
+  }
+  require(max_len <= kRow16Max, CHSGA_ERR_UNSUPPORTED,
+          "chsga_align_scores_noalloc keeps 16-bit rows: reads of at most 65000 bases");
+  const NoallocLayout l = noalloc_layout(c.L.N, c.L.S, total, n);
+  require(l.end <= CHSGA_NOALLOC_SCRATCH_BYTES, CHSGA_ERR_OOM,
+          "chsga_align_scores_noalloc needs " + std::to_string(l.end) +
+              " bytes of its fixed device array for this graph and these reads; the array holds " +
+              std::to_string((uint64_t)CHSGA_NOALLOC_SCRATCH_BYTES) + " (CHSGA_NOALLOC_SCRATCH_BYTES)");
+  if (n == 0) return;
+  unsigned char* base = d.base;
+  NoallocBufs b{};
+  b.rows[0] = reinterpret_cast<uint16_t*>(base + l.rows[0]);
+  b.rows[1] = reinterpret_cast<uint16_t*>(base + l.rows[1]);
+  b.BV = reinterpret_cast<uint16_t*>(base + l.bv);
+  b.FL = reinterpret_cast<uint16_t*>(base + l.fl);
+  b.slots = reinterpret_cast<dev::SlotState*>(base + l.slots);
+  b.word = reinterpret_cast<uint32_t*>(base + l.word);
+  b.best = reinterpret_cast<unsigned long long*>(base + l.best);
+  b.ctl = reinterpret_cast<dev::StepCtl*>(base + l.ctl);
+  b.reads = base + l.reads;
+  b.lens = reinterpret_cast<uint32_t*>(base + l.lens);
+  b.queue = reinterpret_cast<dev::ReadDesc*>(base + l.queue);
+  b.slot_of = reinterpret_cast<int32_t*>(base + l.slot_of);
+  b.res_score = reinterpret_cast<int32_t*>(base + l.res_score);
+  b.res_vertex = reinterpret_cast<uint32_t*>(base + l.res_vertex);
+  b.res_t0 = reinterpret_cast<unsigned long long*>(base + l.res_t0);
+  b.res_t1 = reinterpret_cast<unsigned long long*>(base + l.res_t1);
+  b.out = reinterpret_cast<int32_t*>(base + l.out);
+  const cudaStream_t s = c.st;
+  // copies from pageable caller memory: each returns once its source is read
+  CK(cudaMemcpyAsync(b.lens, lens, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+  uint64_t off = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (lens[i]) CK(cudaMemcpyAsync(b.reads + off, reads[i], lens[i], cudaMemcpyHostToDevice, s));
+    off += lens[i];
+  }
+  k_noalloc_prepare<<<1, 1024, 0, s>>>(b.lens, n, b.queue, b.slot_of, b.slots, b.ctl, b.best);
+  check_launch();
+  if (m) {
+    // admit the first read, then one row per step: `total` steps finish every read
+    dev::k_advance<1><<<1, 128, 0, s>>>(b.slots, b.queue, b.reads, b.best, b.res_score,
+                                        b.res_vertex, b.res_t0, b.res_t1, b.word, b.ctl,
+                                        c.L.special, 0);
+    check_launch();
+    for (uint64_t k = 0; k < total; ++k) noalloc_row_step(c, b, b.rows[k & 1], b.rows[(k + 1) & 1]);
+  }
+  k_noalloc_finish<<<nblocks(n), 256, 0, s>>>(b.slot_of, b.res_score, n, c.nul_label ? 0 : 1, b.out);
+  check_launch();
+  dev::StepCtl fin{};
+  CK(cudaMemcpyAsync(&fin, b.ctl, sizeof(fin), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(out, b.out, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  require(fin.error == 0, CHSGA_ERR_TIMEOUT,
+          "a bounded device-side wait expired (code " + std::to_string(fin.error) + ")");
+  require(fin.done == m, CHSGA_ERR_INTERNAL, "allocation-free path lost reads");
+}
+
 template <typename F>
 chsga_status guarded_ctx(chsga_ctx* c, F&& f) {
   try {
@@ -908,6 +1167,15 @@ chsga_status chsga_align_scores_batched(chsga_ctx* c, const char* const* reads,
       case 128: scores_with<128>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
       default: fail(CHSGA_ERR_INVALID_ARG, "slots must be 1, 2, 4, 8, 16, 32, 64 or 128");
     }
+  });
+}
+
+chsga_status chsga_align_scores_noalloc(chsga_ctx* c, const char* const* reads,
+                                        const uint32_t* lens, uint32_t n, int32_t* scores_out) {
+  return guarded_ctx(c, [&] {
+    require(c && (n == 0 || (reads && lens && scores_out)), CHSGA_ERR_INVALID_ARG, "null argument");
+    require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
+    scores_noalloc(*c, reads, lens, n, scores_out);
   });
 }
 

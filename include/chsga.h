@@ -235,6 +235,41 @@ chsga_status chsga_align_scores_batched(chsga_ctx* ctx, const char* const* reads
                                         const uint32_t* lens, uint32_t n,
                                         const chsga_batch_opts* opts, int32_t* scores_out);
 
+/* Score-only alignment that allocates no device memory. It has no
+ * counterpart in the reference.
+ *
+ * Some callers may not allocate GPU memory once they are running: a
+ * service that hands the free HBM to its own pool at start-up, or a loop
+ * that cannot afford the device-wide synchronisation cudaMalloc may imply.
+ * They load the graph at start-up (chsga_load_graph allocates the graph's
+ * arrays then) and align with this call. It returns the same scores as
+ * chsga_align_scores for the same reads. Every per-call buffer comes from
+ * one fixed array of CHSGA_NOALLOC_SCRATCH_BYTES inside the library: read
+ * bytes, read queue, two 16-bit score rows, per-vertex boundary scores,
+ * slot state and results. The call makes no cudaMalloc, no cudaFree and no
+ * other allocating call.
+ *
+ * - The CUDA driver reserves the array on each GPU where it loads the
+ *   library's device code, and the GPU keeps it until the process exits.
+ * - The first call on a device looks up the array's device address, so
+ *   make that first call before any stream capture starts.
+ * - The call fails with CHSGA_ERR_OOM, and runs nothing, when the graph and
+ *   the reads need more than the array holds. The need is about
+ *   4 N + 8 S + (read bytes) + 52 n bytes, where N = chars and S = string
+ *   vertices, each part rounded up to 256 bytes.
+ * - It fails with CHSGA_ERR_UNSUPPORTED for a read longer than 65000 bases,
+ *   because its rows are 16-bit.
+ * - All calls on one device share the array, which keeps the last call's
+ *   contents. The call clears the slot, queue and control state before it
+ *   starts. Calls whose GPU work overlapped would race on the array. The
+ *   library holds a per-device lock for the whole call, and the call
+ *   returns only after its GPU work is done, so calls made through it do
+ *   not overlap.
+ * - chsga_get_profile and chsga_get_read_times do not report on this call. */
+#define CHSGA_NOALLOC_SCRATCH_BYTES (32u << 20)
+chsga_status chsga_align_scores_noalloc(chsga_ctx* ctx, const char* const* reads,
+                                        const uint32_t* lens, uint32_t n, int32_t* scores_out);
+
 /* Traceback of one read: align_read_with_traceback<int> (src/traceback.hpp:588-1031).
  * If len x N x 4 bytes fit under the byte cap the full score matrix stays in
  * HBM and the path is walked by score equality (src/traceback.hpp:483-586);
