@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
-from typing import List, Optional, Sequence, Tuple
+from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -29,6 +29,7 @@ _lib = C.CDLL(LIB_PATH)
 OK, ERR_INVALID_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, \
     ERR_NO_PATH, ERR_TIMEOUT, ERR_INTERNAL, ERR_BUSY = range(11)
 OP_DELETE, OP_MATCHSUB, OP_INSERT = 0, 1, 2
+REQ_SCORE, REQ_TRACEBACK = 0, 1
 FLAG_PROFILE = 1
 NOALLOC_SCRATCH_BYTES = 32 << 20  # CHSGA_NOALLOC_SCRATCH_BYTES
 
@@ -126,6 +127,29 @@ class ProfileT(C.Structure):
                 ("row_launches", C.c_uint64)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("steps_per_graph", C.c_uint32),
+                ("queue_capacity", C.c_uint32), ("tb_workers", C.c_uint32),
+                ("arena_bytes", C.c_uint64), ("hbm_budget_bytes", C.c_uint64), ("tb_k", C.c_int64),
+                ("tb_cap_bytes", C.c_uint64), ("row_bits", C.c_uint32), ("max_pending", C.c_uint32)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("status", C.c_int32), ("score", C.c_int32),
+                ("vertex", C.c_uint32), ("mode", C.c_uint32), ("read_len", C.c_uint32),
+                ("pad", C.c_uint32), ("submit_ns", C.c_int64), ("start_ns", C.c_int64),
+                ("done_ns", C.c_int64), ("tb", TbResult)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("pending", C.c_uint64), ("running", C.c_uint64), ("cells", C.c_uint64),
+                ("wall_s", C.c_double), ("gcups", C.c_double), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("score_p50_ms", C.c_double), ("score_p99_ms", C.c_double),
+                ("tb_p50_ms", C.c_double), ("tb_p99_ms", C.c_double), ("peak_tb_bytes", C.c_uint64),
+                ("blocks", C.c_uint64), ("gpu_launches", C.c_uint64)]
+
+
 def _sig(name, res, *args):
     f = getattr(_lib, name)
     f.restype = res
@@ -168,6 +192,15 @@ _sig("chsga_tb_result_free", None, C.POINTER(TbResult))
 _sig("chsga_ops_to_cigar", C.c_uint64, C.POINTER(OpT), C.c_uint64, C.c_char_p, C.c_uint64)
 _sig("chsga_get_profile", C.c_int32, vp, C.POINTER(ProfileT))
 _sig("chsga_get_read_times", C.c_int32, vp, u64p, u64p, C.c_uint32)
+_sig("chsga_server_open", C.c_int32, vp, C.POINTER(ServerOpts), C.POINTER(vp))
+_sig("chsga_server_submit", C.c_int32, vp, C.c_char_p, C.c_uint32, C.c_uint32,
+     C.POINTER(C.c_uint64))
+_sig("chsga_server_poll", C.c_int32, vp, C.POINTER(ServerResult), C.c_uint32,
+     C.POINTER(C.c_uint32), C.c_int32)
+_sig("chsga_server_stats_get", C.c_int32, vp, C.POINTER(ServerStats))
+_sig("chsga_server_drain", C.c_int32, vp)
+_sig("chsga_server_close", None, vp)
+_sig("chsga_server_last_error", C.c_char_p, vp)
 
 
 def _check(status: int, ctx=None):
@@ -424,3 +457,82 @@ def ops_to_cigar(ops: np.ndarray) -> str:
             prev, run = c, 1
     out.append(f"{run}{prev}")
     return "".join(out)
+
+
+class Server:
+    """Serving loop over a loaded Context (chsga_server_*): score requests go
+    through the continuously refilled batched engine, traceback requests to
+    workers admitted by projected device footprint."""
+
+    def __init__(self, ctx: "Context", **opts):
+        o = ServerOpts(**opts)
+        h = vp()
+        _check(_lib.chsga_server_open(ctx._h, C.byref(o), C.byref(h)))
+        self._h = h
+        self._ctx = ctx
+
+    def _ck(self, st):
+        if st != OK:
+            msg = _lib.chsga_server_last_error(self._h) or b""
+            raise ChsgaError(st, msg.decode(errors="replace"))
+
+    def submit(self, read: bytes, mode: int = REQ_SCORE) -> int:
+        t = C.c_uint64()
+        self._ck(_lib.chsga_server_submit(self._h, read, len(read), mode, C.byref(t)))
+        return t.value
+
+    def try_submit(self, read: bytes, mode: int = REQ_SCORE) -> Optional[int]:
+        """submit(), or None when the server answers BUSY."""
+        t = C.c_uint64()
+        st = _lib.chsga_server_submit(self._h, read, len(read), mode, C.byref(t))
+        if st == ERR_BUSY:
+            return None
+        self._ck(st)
+        return t.value
+
+    def poll(self, max_results: int = 256, wait_ms: int = 0) -> List[dict]:
+        buf = (ServerResult * max_results)()
+        n = C.c_uint32()
+        self._ck(_lib.chsga_server_poll(self._h, buf, max_results, C.byref(n), wait_ms))
+        out = []
+        for i in range(n.value):
+            r = buf[i]
+            d = {k: getattr(r, k) for k, _ in ServerResult._fields_ if k not in ("tb", "pad")}
+            if r.mode == REQ_TRACEBACK:
+                m = int(r.tb.num_ops)
+                ops = np.zeros((m, 3), dtype=np.int64)
+                for j in range(m):
+                    x = r.tb.ops[j]
+                    ops[j] = (x.row, x.vertex, x.op)
+                d["ops"] = ops
+                d["checkpointed"] = bool(r.tb.checkpointed)
+                _lib.chsga_tb_result_free(C.byref(r.tb))
+            out.append(d)
+        return out
+
+    def drain(self):
+        self._ck(_lib.chsga_server_drain(self._h))
+
+    def collect(self) -> Dict[int, dict]:
+        """Drains and returns every pending result by ticket."""
+        self.drain()
+        res = {}
+        while True:
+            got = self.poll(1024, 0)
+            if not got:
+                return res
+            for d in got:
+                res[d["ticket"]] = d
+
+    def stats(self) -> dict:
+        t = ServerStats()
+        self._ck(_lib.chsga_server_stats_get(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.chsga_server_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

@@ -14,6 +14,7 @@
 #include <type_traits>
 
 #include "device_graph.hpp"
+#include "engine_api.hpp"
 #include "host_graph.hpp"
 #include "kernels.cuh"
 
@@ -121,6 +122,19 @@ constexpr int kTopThreads = 1024;
 
 }  // namespace chsga
 
+namespace chsga {
+// A graph on the device with its host-side layout. Contexts that work on the
+// same graph (the traceback workers of a server) share one instance.
+struct LoadedGraph {
+  HostLayout L;
+  GraphDev gd;
+  dev::GraphPtrs gp{};
+  std::unique_ptr<TopDev> top;
+  size_t pitch = 0;  // traceback matrix row stride (elements), 16-byte aligned rows
+  bool nul_label = false;
+};
+}  // namespace chsga
+
 struct chsga_ctx {
   int device = 0;
   cudaStream_t st = nullptr, side = nullptr;
@@ -128,18 +142,15 @@ struct chsga_ctx {
   uint64_t cap = 0;
   uint32_t flags = 0;
   bool loaded = false;
-  bool nul_label = false;
-  chsga::HostLayout L;
-  chsga::GraphDev gd;
-  chsga::dev::GraphPtrs gp{};
-  std::unique_ptr<chsga::TopDev> top;
+  std::shared_ptr<chsga::LoadedGraph> g;
   std::map<int, std::unique_ptr<chsga::SlotBufs>> bufs;
   std::map<int, std::unique_ptr<chsga::RowTileDev>> row_tiles;  // by R * 8 + sizeof(score)
   int num_sms = 148;
   chsga::RowKernel row_kernel = chsga::RowKernel::Auto;
-  size_t pitch = 0;  // traceback matrix row stride (elements), 16-byte aligned rows
   chsga::DevArr<unsigned char> reads;
   chsga::DevArr<chsga::dev::ReadDesc> queue;
+  uint32_t qmask = 0xFFFFFFFFu;                      // queue ring mask (serving), else linear
+  chsga::DevArr<chsga::dev::CompletionRec> done_ring;  // serving: finished reads, in order
   chsga::DevArr<int32_t> res_score;
   chsga::DevArr<uint32_t> res_vertex;
   chsga::DevArr<unsigned long long> res_t0, res_t1;  // admission / completion, device ns
@@ -166,7 +177,7 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
   auto& b = c.bufs[R];
   if (!b) b = std::make_unique<SlotBufs>();
   b->R = R;
-  const size_t N = c.L.N, S = c.L.S;
+  const size_t N = c.g->L.N, S = c.g->L.S;
   if (need_rows) {
     // bulk tile copies may read up to 16 bytes past the last char
     b->rows[0].alloc((N + 32) * R * sizeof(ST));
@@ -178,12 +189,13 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
   b->word.alloc(R);
   b->best.alloc(R);
   b->ctl.alloc(1);
-  static bool attr_set = false;
-  if (!attr_set) {
+  // once per process (thread-safe: serving threads may get here together)
+  static const bool attr_set = [] {
     CK(cudaFuncSetAttribute(dev::k_top<R, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)dev::top_smem_bytes(kTopMaxVertices)));
-    attr_set = true;
-  }
+    return true;
+  }();
+  (void)attr_set;
   return *b;
 }
 
@@ -240,9 +252,9 @@ const dev::RowTiles* row_tiles(chsga_ctx& c) {
     auto& slot = c.row_tiles[R * 8 + (int)sizeof(ST)];
     if (slot) return slot->ok ? &slot->rt : nullptr;
     slot = std::make_unique<RowTileDev>();
-    const HostRowTiles h = build_row_tiles(c.L, R, sizeof(ST));
+    const HostRowTiles h = build_row_tiles(c.g->L, R, sizeof(ST));
     if (!h.ok) return nullptr;
-    validate_row_tiles(c.L, R, sizeof(ST), h);
+    validate_row_tiles(c.g->L, R, sizeof(ST), h);
     std::vector<int4> rec(h.ntiles() * 2);
     std::memcpy(rec.data(), h.rec.data(), h.rec.size() * 4);
     slot->rec.upload(rec, c.st);
@@ -279,7 +291,7 @@ template <int R>
 void launch_advance(chsga_ctx& c, SlotBufs& b, int prime, cudaStream_t s) {
   dev::k_advance<R><<<1, 128, 0, s>>>(b.slots.p, c.queue.p, c.reads.p, b.best.p, c.res_score.p,
                                       c.res_vertex.p, c.res_t0.p, c.res_t1.p, b.word.p, b.ctl.p,
-                                      c.L.special, prime);
+                                      c.g->L.special, prime, c.qmask, c.done_ring.p);
   check_launch();
 }
 
@@ -313,8 +325,8 @@ template <int R, bool DEFER, typename ST>
 void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
               StepEvents* ev = nullptr) {
   ST* BVc = reinterpret_cast<ST*>(b.BV.p);
-  const HostLayout& L = c.L;
-  const TopDev& top = *c.top;
+  const HostLayout& L = c.g->L;
+  const TopDev& top = *c.g->top;
   constexpr int G = Lanes<R>::G;
   if (ev) CK(cudaEventRecord(ev->e[0], s));
   ST* FL = reinterpret_cast<ST*>(b.FL.p);
@@ -323,7 +335,7 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
     // packed 16-bit DPX kernel; exact while F + (c - first) stays below 2^16
     if (L.max_len <= 512 && c.row_kernel != RowKernel::Tiled && c.row_kernel != RowKernel::Direct) {
       dev::k_row_dpx<R, DEFER><<<nblocks((uint64_t)L.S * dev::Pairs<R>::G), 256, 0, s>>>(
-          c.gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+          c.g->gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
       done = true;
     }
   }
@@ -332,21 +344,21 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
       if (const dev::RowTiles* rt = row_tiles<R, ST>(c)) {
         dev::k_row_tiled<R, DEFER, ST>
             <<<c.num_sms, dev::kRowThreads, dev::row_smem_bytes(dev::row_slot_bytes(*rt), rt->nslots, R),
-               s>>>(c.gp, *rt, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+               s>>>(c.g->gp, *rt, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
         done = true;
       }
     }
   }
   if (!done)
     dev::k_row_direct<R, DEFER, ST><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(
-        c.gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+        c.g->gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
   if (ev) CK(cudaEventRecord(ev->e[1], s));
   const uint32_t fl = top.h.first_level;
   for (uint32_t l = 0; l < fl; ++l) {
     if (L.lvl_up_edges[l] == 0) continue;
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
     dev::k_pull<R, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-        BVc, lo, hi, c.gd.up_off.p, c.gd.up_in.p, 0, b.ctl.p);
+        BVc, lo, hi, c.g->gd.up_off.p, c.g->gd.up_in.p, 0, b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[2], s));
   if (top.h.K) {
@@ -359,13 +371,13 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   if (ev) CK(cudaEventRecord(ev->e[3], s));
   if (fl == 0) {
     dev::k_down<R, !DEFER, ST><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(
-        c.gp, BVc, T, FL, 0, 0, L.S, b.word.p, b.best.p, b.ctl.p);
+        c.g->gp, BVc, T, FL, 0, 0, L.S, b.word.p, b.best.p, b.ctl.p);
   } else {
     for (int l = (int)fl - 1; l >= 0; --l) {
       const uint32_t lo = L.lvl_off[l], mid = L.lvl_off[l + 1];
       const uint32_t hi = (l == (int)fl - 1) ? L.S : mid;
       dev::k_down<R, !DEFER, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-          c.gp, BVc, T, FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
+          c.g->gp, BVc, T, FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
     }
   }
   if (ev) CK(cudaEventRecord(ev->e[4], s));
@@ -375,9 +387,9 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
 
 uint32_t kernels_per_step(const chsga_ctx& c) {
   uint32_t k = 2;  // k_row + k_advance
-  const uint32_t fl = c.top->h.first_level;
-  for (uint32_t l = 0; l < fl; ++l) k += c.L.lvl_up_edges[l] ? 1 : 0;
-  if (c.top->h.K) k += 1 + (c.top->h.upg.empty() ? 0 : 1);
+  const uint32_t fl = c.g->top->h.first_level;
+  for (uint32_t l = 0; l < fl; ++l) k += c.g->L.lvl_up_edges[l] ? 1 : 0;
+  if (c.g->top->h.K) k += 1 + (c.g->top->h.upg.empty() ? 0 : 1);
   k += fl == 0 ? 1 : fl;
   return k;
 }
@@ -482,7 +494,9 @@ void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, u
 
 void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   HostLayout L = build_layout(g);
-  GraphDev& d = c.gd;
+  // the previous graph (if any) stays alive while another context shares it
+  auto lg = std::make_shared<LoadedGraph>();
+  GraphDev& d = lg->gd;
   cudaStream_t s = c.st;
   d.lab2.upload(L.lab2, s);
   d.lab_sp.upload(L.lab_sp, s);
@@ -521,17 +535,16 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   top->ptrs = dev::TopPtrs{h.K0, h.K, (uint32_t)h.chunks.size(), top->chunks.p, top->sched.p,
                            d.dv_len.p};
   CK(cudaStreamSynchronize(s));
-  c.gp = dev::GraphPtrs{L.N,          L.S,          L.special,      d.lab2.p,     d.lab_sp.p,
-                        d.lab4.p,
-                        d.sv_off.p,   d.sv_dev.p,   d.vin_off.p,    d.vin_src.p,  d.vin_srcv.p,
-
-                        d.dv_first.p, d.dv_len.p,   d.dv_s.p,       d.up_off.p,   d.up_in.p,    d.dn_off.p,
-                        d.dn_in.p,    d.istr_off.p, d.istr_src.p};
-  c.nul_label = false;
-  for (uint32_t i = 0; i < g.num_chars && !c.nul_label; ++i) c.nul_label = g.labels[i] == '\0';
-  c.pitch = ((size_t)L.N + 15) / 16 * 16;
-  c.L = std::move(L);
-  c.top = std::move(top);
+  lg->gp = dev::GraphPtrs{L.N,          L.S,          L.special,    d.lab2.p,     d.lab_sp.p,
+                          d.lab4.p,     d.sv_off.p,   d.sv_dev.p,   d.vin_off.p,  d.vin_src.p,
+                          d.vin_srcv.p, d.dv_first.p, d.dv_len.p,   d.dv_s.p,     d.up_off.p,
+                          d.up_in.p,    d.dn_off.p,   d.dn_in.p,    d.istr_off.p, d.istr_src.p};
+  lg->nul_label = false;
+  for (uint32_t i = 0; i < g.num_chars && !lg->nul_label; ++i) lg->nul_label = g.labels[i] == '\0';
+  lg->pitch = ((size_t)L.N + 15) / 16 * 16;
+  lg->L = std::move(L);
+  lg->top = std::move(top);
+  c.g = std::move(lg);
   c.bufs.clear();
   c.row_tiles.clear();
   c.loaded = true;
@@ -547,7 +560,7 @@ void scores_with(chsga_ctx& c, const char* const* reads, const uint32_t* lens, u
   uint64_t rows = 0;
   for (uint32_t i = 0; i < n; ++i) {
     if (lens[i] == 0) {
-      out[i] = c.nul_label ? 0 : 1;
+      out[i] = c.g->nul_label ? 0 : 1;
       continue;
     }
     rp.push_back(reads[i]);
@@ -586,8 +599,8 @@ struct TbState {
 // device), writing row i to out + (i - a) * N if out_rows, else rotating two
 // buffers; sub-checkpoint rows every `sub_k` rows go to sub + j * N.
 void forward_rows(chsga_ctx& c, SlotBufs& b, uint32_t len, int64_t a, int64_t b_row,
-                  int* matrix /* rows a..b at stride c.pitch, row a already present */) {
-  const size_t N = c.pitch;
+                  int* matrix /* rows a..b at stride c.g->pitch, row a already present */) {
+  const size_t N = c.g->pitch;
   // slot 0 at row a+1 of read 0
   dev::SlotState s{0, len, (uint32_t)(a + 1), 0, 0};
   CK(cudaMemcpyAsync(b.slots.p, &s, sizeof(s), cudaMemcpyHostToDevice, c.st));
@@ -600,7 +613,7 @@ void forward_rows(chsga_ctx& c, SlotBufs& b, uint32_t len, int64_t a, int64_t b_
   launch_advance<1>(c, b, 1, c.st);
   // the row-step reads the previous row's per-vertex first/last scores; row a
   // comes from a checkpoint, so derive them from it
-  dev::k_fl_from_row<<<nblocks(c.L.S), 256, 0, c.st>>>(c.gp, matrix, reinterpret_cast<int*>(b.FL.p));
+  dev::k_fl_from_row<<<nblocks(c.g->L.S), 256, 0, c.st>>>(c.g->gp, matrix, reinterpret_cast<int*>(b.FL.p));
   check_launch();
   for (int64_t i = a + 1; i <= b_row; ++i)
     row_step<1, false, int>(c, b, matrix + (size_t)(i - 1 - a) * N, matrix + (size_t)(i - a) * N, c.st);
@@ -614,7 +627,7 @@ void walk(chsga_ctx& c, const int* M, int64_t lo, int64_t hi, uint32_t start, ui
   ops.alloc(max_ops);
   DevArr<dev::WalkOut> out;
   out.alloc(1);
-  dev::k_walk<<<1, 1, 0, c.st>>>(c.gp, M, c.pitch, lo, hi, start, c.reads.p, ops.p, max_ops, out.p);
+  dev::k_walk<<<1, 1, 0, c.st>>>(c.g->gp, M, c.g->pitch, lo, hi, start, c.reads.p, ops.p, max_ops, out.p);
   check_launch();
   dev::WalkOut h{};
   CK(cudaMemcpyAsync(&h, out.p, sizeof(h), cudaMemcpyDeviceToHost, c.st));
@@ -633,8 +646,8 @@ void walk(chsga_ctx& c, const int* M, int64_t lo, int64_t hi, uint32_t start, ui
 void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts* o,
                chsga_tb_result* res) {
   require(len > 0, CHSGA_ERR_INVALID_ARG, "traceback of an empty read");
-  const size_t N = c.pitch;   // row stride of every matrix below
-  const size_t NC = c.L.N;    // chars per row
+  const size_t N = c.g->pitch;   // row stride of every matrix below
+  const size_t NC = c.g->L.N;    // chars per row
   const int64_t k = (o && o->k > 0) ? o->k : 500;
   const uint64_t cap = (o && o->cap_bytes) ? o->cap_bytes : c.cap;
   const std::string dir = (o && o->dir) ? o->dir : "";
@@ -937,17 +950,17 @@ __global__ void k_noalloc_finish(const int32_t* __restrict__ slot_of,
 // closure) on the buffers of the fixed array.
 void noalloc_row_step(chsga_ctx& c, const NoallocBufs& b, const uint16_t* D, uint16_t* T) {
   const cudaStream_t s = c.st;
-  const HostLayout& L = c.L;
-  const TopDev& top = *c.top;
+  const HostLayout& L = c.g->L;
+  const TopDev& top = *c.g->top;
   constexpr int G = Lanes<1>::G;
   dev::k_row_direct<1, true, uint16_t><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(
-      c.gp, D, T, b.BV, b.FL, b.word, b.best, b.ctl);
+      c.g->gp, D, T, b.BV, b.FL, b.word, b.best, b.ctl);
   const uint32_t fl = top.h.first_level;
   for (uint32_t l = 0; l < fl; ++l) {
     if (L.lvl_up_edges[l] == 0) continue;
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
     dev::k_pull<1, uint16_t><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-        b.BV, lo, hi, c.gd.up_off.p, c.gd.up_in.p, 0, b.ctl);
+        b.BV, lo, hi, c.g->gd.up_off.p, c.g->gd.up_in.p, 0, b.ctl);
   }
   if (top.h.K) {
     if (!top.h.upg.empty())
@@ -958,13 +971,13 @@ void noalloc_row_step(chsga_ctx& c, const NoallocBufs& b, const uint16_t* D, uin
   }
   if (fl == 0) {
     dev::k_down<1, false, uint16_t><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(
-        c.gp, b.BV, T, b.FL, 0, 0, L.S, b.word, b.best, b.ctl);
+        c.g->gp, b.BV, T, b.FL, 0, 0, L.S, b.word, b.best, b.ctl);
   } else {
     for (int l = (int)fl - 1; l >= 0; --l) {
       const uint32_t lo = L.lvl_off[l], mid = L.lvl_off[l + 1];
       const uint32_t hi = (l == (int)fl - 1) ? L.S : mid;
       dev::k_down<1, false, uint16_t><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-          c.gp, b.BV, T, b.FL, lo, mid, hi, b.word, b.best, b.ctl);
+          c.g->gp, b.BV, T, b.FL, lo, mid, hi, b.word, b.best, b.ctl);
     }
   }
   dev::k_advance<1><<<1, 128, 0, s>>>(b.slots, b.queue, b.reads, b.best, b.res_score, b.res_vertex,
@@ -995,7 +1008,7 @@ void scores_noalloc(chsga_ctx& c, const char* const* reads, const uint32_t* lens
   }
   require(max_len <= kRow16Max, CHSGA_ERR_UNSUPPORTED,
           "chsga_align_scores_noalloc keeps 16-bit rows: reads of at most 65000 bases");
-  const NoallocLayout l = noalloc_layout(c.L.N, c.L.S, total, n);
+  const NoallocLayout l = noalloc_layout(c.g->L.N, c.g->L.S, total, n);
   require(l.end <= CHSGA_NOALLOC_SCRATCH_BYTES, CHSGA_ERR_OOM,
           "chsga_align_scores_noalloc needs " + std::to_string(l.end) +
               " bytes of its fixed device array for this graph and these reads; the array holds " +
@@ -1034,11 +1047,11 @@ void scores_noalloc(chsga_ctx& c, const char* const* reads, const uint32_t* lens
     // admit the first read, then one row per step: `total` steps finish every read
     dev::k_advance<1><<<1, 128, 0, s>>>(b.slots, b.queue, b.reads, b.best, b.res_score,
                                         b.res_vertex, b.res_t0, b.res_t1, b.word, b.ctl,
-                                        c.L.special, 0);
+                                        c.g->L.special, 0);
     check_launch();
     for (uint64_t k = 0; k < total; ++k) noalloc_row_step(c, b, b.rows[k & 1], b.rows[(k + 1) & 1]);
   }
-  k_noalloc_finish<<<nblocks(n), 256, 0, s>>>(b.slot_of, b.res_score, n, c.nul_label ? 0 : 1, b.out);
+  k_noalloc_finish<<<nblocks(n), 256, 0, s>>>(b.slot_of, b.res_score, n, c.g->nul_label ? 0 : 1, b.out);
   check_launch();
   dev::StepCtl fin{};
   CK(cudaMemcpyAsync(&fin, b.ctl, sizeof(fin), cudaMemcpyDeviceToHost, s));
@@ -1069,7 +1082,236 @@ chsga_status guarded_ctx(chsga_ctx* c, F&& f) {
   }
 }
 
+// ---- continuous score lane (serving) -----------------------------------------
+
+__global__ void k_publish(dev::StepCtl* ctl, uint32_t q_count) { ctl->q_count = q_count; }
+
+__global__ void k_clock(unsigned long long* out) { *out = dev::global_ns(); }
+
+int64_t host_ns() {
+  return std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+template <int R, typename ST>
+class ScoreLaneImpl final : public ScoreLane {
+ public:
+  ScoreLaneImpl(chsga_ctx& parent, uint32_t per_graph, uint32_t cap, uint64_t arena)
+      : c_(fork_context(parent)), cap_(cap), arena_(arena) {
+    chsga_ctx& c = *c_;
+    per_ = std::max<uint32_t>(2, per_graph + (per_graph & 1));
+    c.qmask = cap - 1;
+    c.reads.alloc(arena + 64);
+    c.queue.alloc(cap);
+    c.res_score.alloc(cap);
+    c.res_vertex.alloc(cap);
+    c.res_t0.alloc(cap);
+    c.res_t1.alloc(cap);
+    c.done_ring.alloc(cap);
+    b_ = &get_bufs<R, ST>(c, true);
+    if (c.row_kernel == RowKernel::Tiled) row_tiles<R, ST>(c);  // allocates: before the capture
+    reset_slots<R>(c, *b_, 0);
+    launch_advance<R>(c, *b_, 0, c.st);  // every slot idle
+    harena_.alloc(arena + 64);
+    hq_.alloc(cap);
+    hctl_.alloc(2);
+    hring_.alloc(2 * (size_t)cap);
+    for (auto& e : ev_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaStream_t cap_st;
+    CK(cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(cap_st, cudaStreamCaptureModeThreadLocal));
+    ST* rows[2] = {reinterpret_cast<ST*>(b_->rows[0].p), reinterpret_cast<ST*>(b_->rows[1].p)};
+    for (uint32_t i = 0; i < per_; ++i) row_step<R, true, ST>(c, *b_, rows[i & 1], rows[(i + 1) & 1], cap_st);
+    CK(cudaStreamEndCapture(cap_st, &graph_));
+    CK(cudaGraphInstantiate(&exec_, graph_, 0));
+    CK(cudaStreamDestroy(cap_st));
+    calibrate_clock();
+  }
+
+  ~ScoreLaneImpl() override {
+    cudaStreamSynchronize(c_->st);
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    for (auto& e : ev_) cudaEventDestroy(e);
+    chsga_close(c_);
+  }
+
+  uint32_t capacity() const override { return cap_; }
+  uint64_t arena_bytes() const override { return arena_; }
+  unsigned char* staging() override { return harena_.p; }
+  uint64_t blocks() const override { return launched_; }
+  uint32_t kernels_per_block() const override { return kernels_per_step(*c_) * per_; }
+
+  void publish(uint64_t lo, uint64_t hi, const LaneRead* reads, uint32_t n) override {
+    chsga_ctx& c = *c_;
+    require(hi <= arena_ && lo <= hi, CHSGA_ERR_INTERNAL, "arena range");
+    if (hi > lo)
+      CK(cudaMemcpyAsync(c.reads.p + lo, harena_.p + lo, hi - lo, cudaMemcpyHostToDevice, c.st));
+    const uint32_t mask = cap_ - 1;
+    for (uint32_t i = 0; i < n; ++i) {
+      require(reads[i].id < cap_ && reads[i].off + reads[i].len <= arena_, CHSGA_ERR_INTERNAL,
+              "lane read out of range");
+      hq_.p[(qpub_ + i) & mask] = dev::ReadDesc{reads[i].off, reads[i].len, (int32_t)reads[i].id};
+    }
+    const uint32_t first = qpub_ & mask;
+    const uint32_t n1 = std::min<uint32_t>(n, cap_ - first);
+    if (n1)
+      CK(cudaMemcpyAsync(c.queue.p + first, hq_.p + first, n1 * sizeof(dev::ReadDesc),
+                         cudaMemcpyHostToDevice, c.st));
+    if (n > n1)
+      CK(cudaMemcpyAsync(c.queue.p, hq_.p, (n - n1) * sizeof(dev::ReadDesc), cudaMemcpyHostToDevice,
+                         c.st));
+    qpub_ += n;
+    k_publish<<<1, 1, 0, c.st>>>(b_->ctl.p, qpub_);
+    check_launch();
+  }
+
+  void step(std::vector<LaneDone>& out) override {
+    chsga_ctx& c = *c_;
+    const int k = (int)(launched_ & 1);
+    CK(cudaGraphLaunch(exec_, c.st));
+    CK(cudaMemcpyAsync(hctl_.p + k, b_->ctl.p, sizeof(dev::StepCtl), cudaMemcpyDeviceToHost, c.st));
+    CK(cudaMemcpyAsync(hring_.p + (size_t)k * cap_, c.done_ring.p, (size_t)cap_ * sizeof(dev::CompletionRec),
+                       cudaMemcpyDeviceToHost, c.st));
+    CK(cudaEventRecord(ev_[k], c.st));
+    ++launched_;
+    if (launched_ >= 2) harvest((int)((launched_ - 2) & 1), out);
+  }
+
+  void drain(std::vector<LaneDone>& out) override {
+    if (launched_ == 0) return;
+    CK(cudaStreamSynchronize(c_->st));
+    harvest((int)((launched_ - 1) & 1), out);
+  }
+
+ private:
+  void harvest(int k, std::vector<LaneDone>& out) {
+    CK(cudaEventSynchronize(ev_[k]));
+    const dev::StepCtl& s = hctl_.p[k];
+    require(s.error == 0, CHSGA_ERR_TIMEOUT,
+            "a bounded device-side wait expired (code " + std::to_string(s.error) + ")");
+    const uint32_t mask = cap_ - 1;
+    for (uint32_t i = hdone_; i != s.done; ++i) {
+      const dev::CompletionRec& r = hring_.p[(size_t)k * cap_ + (i & mask)];
+      out.push_back(LaneDone{(uint32_t)r.id, r.score, r.vertex, (int64_t)r.t0 - clock_off_,
+                             (int64_t)r.t1 - clock_off_});
+    }
+    hdone_ = s.done;
+  }
+
+  // device global timer minus host steady clock, from the tightest of a few
+  // round trips
+  void calibrate_clock() {
+    DevArr<unsigned long long> t;
+    t.alloc(1);
+    int64_t best_rt = INT64_MAX;
+    for (int i = 0; i < 8; ++i) {
+      CK(cudaStreamSynchronize(c_->st));
+      const int64_t a = host_ns();
+      k_clock<<<1, 1, 0, c_->st>>>(t.p);
+      unsigned long long d = 0;
+      CK(cudaMemcpyAsync(&d, t.p, 8, cudaMemcpyDeviceToHost, c_->st));
+      CK(cudaStreamSynchronize(c_->st));
+      const int64_t b = host_ns();
+      if (b - a < best_rt) {
+        best_rt = b - a;
+        clock_off_ = (int64_t)d - (a + b) / 2;
+      }
+    }
+  }
+
+  chsga_ctx* c_;
+  SlotBufs* b_ = nullptr;
+  uint32_t cap_;
+  uint64_t arena_;
+  uint32_t per_ = 8;
+  uint32_t qpub_ = 0, hdone_ = 0;
+  uint64_t launched_ = 0;
+  int64_t clock_off_ = 0;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
+  PinnedArr<unsigned char> harena_;
+  PinnedArr<dev::ReadDesc> hq_;
+  PinnedArr<dev::StepCtl> hctl_;
+  PinnedArr<dev::CompletionRec> hring_;
+};
+
+template <typename ST>
+std::unique_ptr<ScoreLane> lane_for(chsga_ctx& p, uint32_t slots, uint32_t per, uint32_t cap,
+                                    uint64_t arena) {
+  switch (slots) {
+    case 2: return std::make_unique<ScoreLaneImpl<2, ST>>(p, per, cap, arena);
+    case 4: return std::make_unique<ScoreLaneImpl<4, ST>>(p, per, cap, arena);
+    case 8: return std::make_unique<ScoreLaneImpl<8, ST>>(p, per, cap, arena);
+    case 16: return std::make_unique<ScoreLaneImpl<16, ST>>(p, per, cap, arena);
+    case 32: return std::make_unique<ScoreLaneImpl<32, ST>>(p, per, cap, arena);
+    case 64: return std::make_unique<ScoreLaneImpl<64, ST>>(p, per, cap, arena);
+    case 128: return std::make_unique<ScoreLaneImpl<128, ST>>(p, per, cap, arena);
+    default: fail(CHSGA_ERR_INVALID_ARG, "slots must be 2, 4, 8, 16, 32, 64 or 128");
+  }
+}
+
 }  // namespace
+
+chsga_ctx* fork_context(chsga_ctx& p) {
+  require(p.loaded && p.g, CHSGA_ERR_INVALID_ARG, "no graph loaded");
+  auto c = std::make_unique<chsga_ctx>();
+  c->device = p.device;
+  c->flags = p.flags & ~(uint32_t)CHSGA_FLAG_PROFILE;
+  c->cap = p.cap;
+  c->num_sms = p.num_sms;
+  c->row_kernel = p.row_kernel;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+  c->g = p.g;
+  c->loaded = true;
+  return c.release();
+}
+
+uint64_t traceback_device_bytes(const chsga_ctx& c, uint32_t len, const chsga_tb_opts* o) {
+  const uint64_t pb = (uint64_t)c.g->pitch * 4, row_bytes = (uint64_t)c.g->L.N * 4;
+  const int64_t k = (o && o->k > 0) ? o->k : 500;
+  const uint64_t cap = (o && o->cap_bytes) ? o->cap_bytes : c.cap;
+  const uint64_t read = (len + 255) / 256 * 256;
+  if ((uint64_t)len * row_bytes <= cap) return ((uint64_t)len + 1) * pb + read;
+  // checkpointed: three forward rows, then the largest recompute segment
+  const uint64_t budget = std::max<uint64_t>(c.cap, cap);
+  const uint64_t seg = std::min<uint64_t>((uint64_t)k, len ? len - 1 : 0) + 1;
+  uint64_t peak = seg * pb;
+  if (!(seg * pb <= budget || seg <= 2)) {
+    const uint64_t span = seg - 1;
+    const uint64_t k2 = std::max<uint64_t>(1, (uint64_t)std::ceil(std::sqrt((double)span)));
+    peak = (span / k2 + 1 + k2 + 1) * pb;
+  }
+  return std::max<uint64_t>(3 * pb, peak) + read;
+}
+
+uint64_t graph_chars(const chsga_ctx& c) { return c.g->L.N; }
+uint64_t graph_string_vertices(const chsga_ctx& c) { return c.g->L.S; }
+int32_t empty_read_score(const chsga_ctx& c) { return c.g->nul_label ? 0 : 1; }
+
+void bind_device(const chsga_ctx& c) { CK(cudaSetDevice(c.device)); }
+
+uint64_t device_free_bytes(const chsga_ctx& c) {
+  CK(cudaSetDevice(c.device));
+  size_t f = 0, t = 0;
+  CK(cudaMemGetInfo(&f, &t));
+  return f;
+}
+
+std::unique_ptr<ScoreLane> make_score_lane(chsga_ctx& parent, uint32_t slots, uint32_t per_graph,
+                                           uint32_t capacity, uint64_t arena_bytes,
+                                           uint32_t row_bits) {
+  require(capacity >= 2 && (capacity & (capacity - 1)) == 0, CHSGA_ERR_INVALID_ARG,
+          "queue capacity must be a power of two");
+  require(row_bits == 16 || row_bits == 32, CHSGA_ERR_INVALID_ARG, "row_bits must be 16 or 32");
+  if (row_bits == 16) return lane_for<uint16_t>(parent, slots, per_graph, capacity, arena_bytes);
+  return lane_for<int>(parent, slots, per_graph, capacity, arena_bytes);
+}
+
 }  // namespace chsga
 
 using namespace chsga;
@@ -1109,7 +1351,7 @@ void chsga_close(chsga_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->st);
   c->bufs.clear();
-  c->top.reset();
+  c->g.reset();
   if (c->st) cudaStreamDestroy(c->st);
   if (c->side) cudaStreamDestroy(c->side);
   delete c;
@@ -1183,7 +1425,7 @@ chsga_status chsga_align_rows(chsga_ctx* c, const char* read, uint32_t len, int3
   return guarded_ctx(c, [&] {
     require(c && read && rows_out && len > 0, CHSGA_ERR_INVALID_ARG, "bad argument");
     require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
-    const size_t N = c->pitch, NC = c->L.N;
+    const size_t N = c->g->pitch, NC = c->g->L.N;
     const char* rp[1] = {read};
     upload_reads(*c, rp, &len, 1);
     SlotBufs& b = get_bufs<1, int>(*c, false);

@@ -79,6 +79,15 @@ struct ReadDesc {
   int32_t id;
 };
 
+// One finished read, appended by k_advance to a completion ring (serving).
+struct CompletionRec {
+  int32_t id;
+  int32_t score;
+  uint32_t vertex;
+  uint32_t pad;
+  unsigned long long t0, t1;  // admission / completion, device global timer ns
+};
+
 struct StepCtl {        // device-resident control block
   uint32_t any_active;  // some slot has a row to compute
   uint32_t any_ending;  // some slot is on its last row
@@ -1198,6 +1207,9 @@ __global__ void k_fl_from_row(GraphPtrs g, const int* __restrict__ row, int* __r
 // next queued reads in order; every slot gets its word for the next step.
 // Admission and completion times (device global timer, ns) are recorded per
 // read. prime != 0 only recomputes the words (used after the host sets slots).
+// Serving: the queue is a ring (entry i at queue[i & qmask]) that the host
+// refills while the engine runs, ids index the result arrays, and every
+// finished read is also appended to done_ring (entry ctl->done & qmask).
 // ---------------------------------------------------------------------------
 template <int R>
 __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
@@ -1210,7 +1222,8 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
                                                  unsigned long long* __restrict__ res_t1,
                                                  uint32_t* __restrict__ slot_word,
                                                  StepCtl* __restrict__ ctl, int special,
-                                                 int prime) {
+                                                 int prime, uint32_t qmask = 0xFFFFFFFFu,
+                                                 CompletionRec* __restrict__ done_ring = nullptr) {
   __shared__ uint32_t s_need[128];
   __shared__ uint32_t s_base, s_take, s_active, s_ending;
   const int r = threadIdx.x;
@@ -1225,10 +1238,14 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
     if (!prime && st.id >= 0) {
       if (st.row + 1 >= st.len) {
         const unsigned long long b = best[r];
+        const unsigned long long t1 = global_ns();
         res_score[st.id] = (int32_t)(b >> 32);
         res_vertex[st.id] = (uint32_t)(b & 0xffffffffu);
-        res_t1[st.id] = global_ns();
-        atomicAdd(&ctl->done, 1u);
+        res_t1[st.id] = t1;
+        const uint32_t k = atomicAdd(&ctl->done, 1u);
+        if (done_ring)
+          done_ring[k & qmask] = CompletionRec{st.id, (int32_t)(b >> 32), (uint32_t)(b & 0xffffffffu), 0u,
+                                               res_t0[st.id], t1};
         st.id = -1;
       } else {
         st.row += 1;
@@ -1253,7 +1270,7 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
   __syncthreads();
   if (r < R) {
     if (need && s_need[r] < s_take) {
-      const ReadDesc q = queue[s_base + s_need[r]];
+      const ReadDesc q = queue[(s_base + s_need[r]) & qmask];
       st.off = q.off;
       st.len = q.len;
       st.row = 0;

@@ -327,6 +327,84 @@ chsga_status chsga_get_profile(chsga_ctx* ctx, chsga_profile* out);
  * reference counterpart: used for per-read latency percentiles. */
 chsga_status chsga_get_read_times(chsga_ctx* ctx, uint64_t* admit_ns, uint64_t* done_ns, uint32_t n);
 
+/* ------------------------------------------------------------------------- */
+/* Serving loop (no reference counterpart: the reference aligns a fixed read */
+/* set serially, src/align.hpp:488)                                          */
+/* ------------------------------------------------------------------------- */
+
+/* A server takes reads as they arrive and keeps the context's graph and
+ * hierarchy resident. Score requests run through a continuously refilled
+ * batched engine: `slots` reads advance together, a finished slot takes the
+ * next queued read on the device, and reads submitted while others run are
+ * published between CUDA-graph blocks of row-steps. Traceback requests run
+ * on `tb_workers` worker contexts that share the graph; each is admitted
+ * when its projected device footprint (full matrix, or the checkpointed
+ * path's rows) fits what the running ones leave of `hbm_budget_bytes`.
+ * Results are the same as chsga_align_scores / chsga_align_traceback on
+ * the same read, whatever else is in flight. The server is internally
+ * synchronised: any thread may submit and poll. The context must outlive
+ * the server and must not be reloaded while it runs. */
+typedef struct chsga_server chsga_server;
+
+typedef struct {
+  uint32_t slots;            /* score reads advanced together: 2..128 (power of 2); 0 = 128 */
+  uint32_t steps_per_graph;  /* row-steps per CUDA-graph launch; 0 = 8 */
+  uint32_t queue_capacity;   /* score reads queued or running on the device (power of 2); 0 = 4096 */
+  uint32_t tb_workers;       /* traceback requests running at once; 0 = 2 */
+  uint64_t arena_bytes;      /* device bytes for the bases of queued score reads; 0 = 64 MiB */
+  uint64_t hbm_budget_bytes; /* device bytes running traceback requests may hold; 0 = 50% of free */
+  int64_t tb_k;              /* checkpoint interval of traceback requests; 0 = 500 */
+  uint64_t tb_cap_bytes;     /* full-matrix byte cap of a traceback request; 0 = the context's */
+  uint32_t row_bits;         /* score rows: 16 (reads <= 65000 bases) or 32; 0 = 16 */
+  uint32_t max_pending;      /* requests waiting for admission before submit says BUSY; 0 = 2^20 */
+} chsga_server_opts;
+
+enum { CHSGA_REQ_SCORE = 0, CHSGA_REQ_TRACEBACK = 1 };
+
+typedef struct {
+  uint64_t ticket;       /* from chsga_server_submit */
+  int32_t status;        /* chsga_status of this request */
+  int32_t score;
+  uint32_t vertex;       /* score requests: smallest char index reaching the score */
+  uint32_t mode;         /* CHSGA_REQ_* */
+  uint32_t read_len;
+  uint32_t pad;
+  int64_t submit_ns;     /* host steady-clock ns: submitted, */
+  int64_t start_ns;      /* admitted to the device, */
+  int64_t done_ns;       /* finished */
+  chsga_tb_result tb;    /* traceback requests; free with chsga_tb_result_free */
+} chsga_server_result;
+
+typedef struct {
+  uint64_t submitted, completed, failed, pending, running;
+  uint64_t cells;            /* sum over completed requests of read length x N */
+  double wall_s;             /* first submit to last completion */
+  double gcups;              /* cells / wall_s / 1e9 */
+  double p50_ms, p99_ms;     /* latency submit -> done, all completed requests */
+  double score_p50_ms, score_p99_ms, tb_p50_ms, tb_p99_ms;
+  uint64_t peak_tb_bytes;    /* largest projected footprint held by running tracebacks */
+  uint64_t blocks;           /* CUDA-graph blocks launched by the score lane */
+  uint64_t gpu_launches;     /* kernels launched by the score lane */
+} chsga_server_stats;
+
+chsga_status chsga_server_open(chsga_ctx* ctx, const chsga_server_opts* opts, chsga_server** out);
+/* Queues one request (the read is copied). CHSGA_ERR_BUSY when max_pending
+ * requests already wait; CHSGA_ERR_OOM when a traceback could never fit the
+ * budget; CHSGA_ERR_UNSUPPORTED for a score read over 65000 bases with
+ * 16-bit rows. */
+chsga_status chsga_server_submit(chsga_server* s, const char* read, uint32_t len, uint32_t mode,
+                                 uint64_t* ticket);
+/* Moves up to `max` finished results to `out`; waits up to wait_ms (-1 =
+ * until one is ready, 0 = not at all) when none is ready. */
+chsga_status chsga_server_poll(chsga_server* s, chsga_server_result* out, uint32_t max,
+                               uint32_t* n_out, int32_t wait_ms);
+chsga_status chsga_server_stats_get(chsga_server* s, chsga_server_stats* out);
+/* Waits until every submitted request has finished (results stay pollable). */
+chsga_status chsga_server_drain(chsga_server* s);
+/* Drains, stops the engine and workers, frees unpolled results. */
+void chsga_server_close(chsga_server* s);
+const char* chsga_server_last_error(chsga_server* s);
+
 #ifdef __cplusplus
 }
 #endif
