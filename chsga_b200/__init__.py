@@ -30,6 +30,7 @@ OK, ERR_INVALID_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, \
     ERR_NO_PATH, ERR_TIMEOUT, ERR_INTERNAL, ERR_BUSY = range(11)
 OP_DELETE, OP_MATCHSUB, OP_INSERT = 0, 1, 2
 REQ_SCORE, REQ_TRACEBACK = 0, 1
+FP_PLAN, FP_MODEL, FP_ANALYTIC = 0, 1, 2
 FLAG_PROFILE = 1
 NOALLOC_SCRATCH_BYTES = 32 << 20  # CHSGA_NOALLOC_SCRATCH_BYTES
 
@@ -131,14 +132,16 @@ class ServerOpts(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("steps_per_graph", C.c_uint32),
                 ("queue_capacity", C.c_uint32), ("tb_workers", C.c_uint32),
                 ("arena_bytes", C.c_uint64), ("hbm_budget_bytes", C.c_uint64), ("tb_k", C.c_int64),
-                ("tb_cap_bytes", C.c_uint64), ("row_bits", C.c_uint32), ("max_pending", C.c_uint32)]
+                ("tb_cap_bytes", C.c_uint64), ("row_bits", C.c_uint32), ("max_pending", C.c_uint32),
+                ("cost_model", C.c_void_p), ("footprint", C.c_uint32), ("pad", C.c_uint32)]
 
 
 class ServerResult(C.Structure):
     _fields_ = [("ticket", C.c_uint64), ("status", C.c_int32), ("score", C.c_int32),
                 ("vertex", C.c_uint32), ("mode", C.c_uint32), ("read_len", C.c_uint32),
                 ("pad", C.c_uint32), ("submit_ns", C.c_int64), ("start_ns", C.c_int64),
-                ("done_ns", C.c_int64), ("tb", TbResult)]
+                ("done_ns", C.c_int64), ("projected_bytes", C.c_uint64), ("peak_bytes", C.c_uint64),
+                ("predicted_ms", C.c_float), ("pad2", C.c_uint32), ("tb", TbResult)]
 
 
 class ServerStats(C.Structure):
@@ -148,6 +151,11 @@ class ServerStats(C.Structure):
                 ("p99_ms", C.c_double), ("score_p50_ms", C.c_double), ("score_p99_ms", C.c_double),
                 ("tb_p50_ms", C.c_double), ("tb_p99_ms", C.c_double), ("peak_tb_bytes", C.c_uint64),
                 ("blocks", C.c_uint64), ("gpu_launches", C.c_uint64)]
+
+
+class CmTrainOpts(C.Structure):
+    _fields_ = [("epochs", C.c_uint32), ("batch", C.c_uint32), ("lr", C.c_float),
+                ("keep_norm", C.c_uint32), ("seed", C.c_uint64)]
 
 
 def _sig(name, res, *args):
@@ -192,6 +200,20 @@ _sig("chsga_tb_result_free", None, C.POINTER(TbResult))
 _sig("chsga_ops_to_cigar", C.c_uint64, C.POINTER(OpT), C.c_uint64, C.c_char_p, C.c_uint64)
 _sig("chsga_get_profile", C.c_int32, vp, C.POINTER(ProfileT))
 _sig("chsga_get_read_times", C.c_int32, vp, u64p, u64p, C.c_uint32)
+f32p = C.POINTER(C.c_float)
+_sig("chsga_cm_create", C.c_int32, C.c_int, C.c_uint64, C.POINTER(vp))
+_sig("chsga_cm_free", None, vp)
+_sig("chsga_cm_last_error", C.c_char_p, vp)
+_sig("chsga_cm_num_params", C.c_uint32)
+_sig("chsga_cm_get_params", C.c_int32, vp, f32p, f32p)
+_sig("chsga_cm_set_params", C.c_int32, vp, f32p, f32p)
+_sig("chsga_cm_loss_grad", C.c_int32, vp, f32p, f32p, C.c_uint32, f32p, f32p)
+_sig("chsga_cm_train", C.c_int32, vp, f32p, f32p, C.c_uint32, C.POINTER(CmTrainOpts), f32p)
+_sig("chsga_cm_predict", C.c_int32, vp, f32p, C.c_uint32, f32p)
+_sig("chsga_cm_save", C.c_int32, vp, C.c_char_p)
+_sig("chsga_cm_load", C.c_int32, vp, C.c_char_p)
+_sig("chsga_cm_features", C.c_int32, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int64, C.c_uint64,
+     f32p)
 _sig("chsga_server_open", C.c_int32, vp, C.POINTER(ServerOpts), C.POINTER(vp))
 _sig("chsga_server_submit", C.c_int32, vp, C.c_char_p, C.c_uint32, C.c_uint32,
      C.POINTER(C.c_uint64))
@@ -464,8 +486,11 @@ class Server:
     through the continuously refilled batched engine, traceback requests to
     workers admitted by projected device footprint."""
 
-    def __init__(self, ctx: "Context", **opts):
+    def __init__(self, ctx: "Context", cost_model: Optional["CostModel"] = None, **opts):
         o = ServerOpts(**opts)
+        if cost_model is not None:
+            o.cost_model = cost_model._h
+        self._cm = cost_model
         h = vp()
         _check(_lib.chsga_server_open(ctx._h, C.byref(o), C.byref(h)))
         self._h = h
@@ -497,7 +522,7 @@ class Server:
         out = []
         for i in range(n.value):
             r = buf[i]
-            d = {k: getattr(r, k) for k, _ in ServerResult._fields_ if k not in ("tb", "pad")}
+            d = {k: getattr(r, k) for k, _ in ServerResult._fields_ if k not in ("tb", "pad", "pad2")}
             if r.mode == REQ_TRACEBACK:
                 m = int(r.tb.num_ops)
                 ops = np.zeros((m, 3), dtype=np.int64)
@@ -536,3 +561,88 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+CM_FEATURES, CM_OUTPUTS, CM_NUM_NORM = 8, 2, 20
+
+
+def _f32(a, shape=None) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+class CostModel:
+    """The FP32 MLP cost model (chsga_cm_*): trained and run on the GPU by the
+    library's own kernels. Targets: (time ms, peak device bytes) per read."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        h = vp()
+        _check(_lib.chsga_cm_create(device, seed, C.byref(h)))
+        self._h = h
+
+    def _ck(self, st):
+        if st != OK:
+            msg = _lib.chsga_cm_last_error(self._h) or b""
+            raise ChsgaError(st, msg.decode(errors="replace"))
+
+    @staticmethod
+    def num_params() -> int:
+        return int(_lib.chsga_cm_num_params())
+
+    def params(self):
+        p = np.zeros(self.num_params(), np.float32)
+        nm = np.zeros(CM_NUM_NORM, np.float32)
+        self._ck(_lib.chsga_cm_get_params(self._h, p.ctypes.data_as(f32p), nm.ctypes.data_as(f32p)))
+        return p, nm
+
+    def set_params(self, params=None, norm=None):
+        pp = None if params is None else _f32(params)
+        nn = None if norm is None else _f32(norm)
+        self._ck(_lib.chsga_cm_set_params(self._h, pp.ctypes.data_as(f32p) if pp is not None else None,
+                                          nn.ctypes.data_as(f32p) if nn is not None else None))
+
+    def loss_grad(self, x, y):
+        x, y = _f32(x, (-1, CM_FEATURES)), _f32(y, (-1, CM_OUTPUTS))
+        loss = C.c_float()
+        g = np.zeros(self.num_params(), np.float32)
+        self._ck(_lib.chsga_cm_loss_grad(self._h, x.ctypes.data_as(f32p), y.ctypes.data_as(f32p), len(x),
+                                         C.byref(loss), g.ctypes.data_as(f32p)))
+        return float(loss.value), g
+
+    def train(self, x, y, epochs=200, batch=256, lr=3e-3, seed=0, keep_norm=False) -> float:
+        x, y = _f32(x, (-1, CM_FEATURES)), _f32(y, (-1, CM_OUTPUTS))
+        o = CmTrainOpts(epochs, batch, lr, int(keep_norm), seed)
+        loss = C.c_float()
+        self._ck(_lib.chsga_cm_train(self._h, x.ctypes.data_as(f32p), y.ctypes.data_as(f32p), len(x),
+                                     C.byref(o), C.byref(loss)))
+        return float(loss.value)
+
+    def predict(self, x) -> np.ndarray:
+        x = _f32(x, (-1, CM_FEATURES))
+        out = np.zeros((len(x), CM_OUTPUTS), np.float32)
+        self._ck(_lib.chsga_cm_predict(self._h, x.ctypes.data_as(f32p), len(x), out.ctypes.data_as(f32p)))
+        return out
+
+    def save(self, path: str):
+        self._ck(_lib.chsga_cm_save(self._h, path.encode()))
+
+    def load(self, path: str):
+        self._ck(_lib.chsga_cm_load(self._h, path.encode()))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.chsga_cm_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def cm_features(ctx: "Context", read_len: int, mode: int = REQ_SCORE, slots: int = 1, k: int = 500,
+                cap_bytes: int = 0) -> np.ndarray:
+    x = np.zeros(CM_FEATURES, np.float32)
+    _check(_lib.chsga_cm_features(ctx._h, read_len, mode, slots, k, cap_bytes, x.ctypes.data_as(f32p)),
+           ctx._h)
+    return x

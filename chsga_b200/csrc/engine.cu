@@ -31,6 +31,11 @@ void validate_host_graph(const chsga_host_graph& g);
            std::string(#x) + ": " + cudaGetErrorString(e_));                                 \
   } while (0)
 
+// Device bytes held by DevArr allocations made on this thread, and their
+// peak since the last meter_reset (the serving loop logs a traceback
+// request's peak from it).
+thread_local int64_t t_live_bytes = 0, t_peak_bytes = 0;
+
 template <typename T>
 struct DevArr {
   T* p = nullptr;
@@ -40,7 +45,10 @@ struct DevArr {
   DevArr& operator=(const DevArr&) = delete;
   ~DevArr() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaFree(p);
+      t_live_bytes -= (int64_t)(n * sizeof(T));
+    }
     p = nullptr;
     n = 0;
   }
@@ -50,6 +58,8 @@ struct DevArr {
     if (count == 0) count = 1;
     CK(cudaMalloc((void**)&p, count * sizeof(T)));
     n = count;
+    t_live_bytes += (int64_t)(count * sizeof(T));
+    t_peak_bytes = std::max(t_peak_bytes, t_live_bytes);
   }
   void upload(const std::vector<T>& v, cudaStream_t s) {
     alloc(v.size());
@@ -1295,6 +1305,29 @@ int32_t empty_read_score(const chsga_ctx& c) { return c.g->nul_label ? 0 : 1; }
 
 void bind_device(const chsga_ctx& c) { CK(cudaSetDevice(c.device)); }
 
+int64_t meter_reset() {
+  t_peak_bytes = t_live_bytes;
+  return t_live_bytes;
+}
+
+uint64_t meter_peak_since(int64_t base) { return (uint64_t)std::max<int64_t>(0, t_peak_bytes - base); }
+
+void request_features(const chsga_ctx& c, uint32_t len, uint32_t mode, uint32_t slots, int64_t k,
+                      uint64_t cap_bytes, float* x) {
+  const HostLayout& L = c.g->L;
+  const uint64_t cap = cap_bytes ? cap_bytes : c.cap;
+  const bool tb = mode == CHSGA_REQ_TRACEBACK;
+  const bool ck = tb && (uint64_t)len * L.N * 4 > cap;
+  x[0] = (float)std::log2((double)len + 1);
+  x[1] = (float)std::log2((double)std::max<uint32_t>(L.N, 1));
+  x[2] = (float)std::log2((double)std::max<uint32_t>(L.S, 1));
+  x[3] = (float)std::log2((double)(L.up_in.size() + L.dn_in.size()) + 1);
+  x[4] = (float)std::log2((double)L.levels + 1);
+  x[5] = (float)std::log2((double)std::max<uint32_t>(slots, 1));
+  x[6] = tb ? 1.f : 0.f;
+  x[7] = ck ? (float)std::log2((double)std::max<int64_t>(k > 0 ? k : 500, 1)) : 0.f;
+}
+
 uint64_t device_free_bytes(const chsga_ctx& c) {
   CK(cudaSetDevice(c.device));
   size_t f = 0, t = 0;
@@ -1500,6 +1533,15 @@ chsga_status chsga_get_read_times(chsga_ctx* c, uint64_t* admit_ns, uint64_t* do
       admit_ns[i] = a[i];
       done_ns[i] = d[i];
     }
+  });
+}
+
+chsga_status chsga_cm_features(chsga_ctx* c, uint32_t read_len, uint32_t mode, uint32_t slots,
+                               int64_t k, uint64_t cap_bytes, float* x_out) {
+  return guarded_ctx(c, [&] {
+    require(c && x_out, CHSGA_ERR_INVALID_ARG, "null argument");
+    require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
+    request_features(*c, read_len, mode, slots, k, cap_bytes, x_out);
   });
 }
 

@@ -30,6 +30,14 @@ int32_t empty_read_score(const chsga_ctx& c);
 void bind_device(const chsga_ctx& c);
 // Free device memory now (cudaMemGetInfo) on the context's device.
 uint64_t device_free_bytes(const chsga_ctx& c);
+// Device bytes the library allocated on this thread: meter_reset starts a
+// window (returns its base), meter_peak_since(base) is the window's peak
+// above the base.
+int64_t meter_reset();
+uint64_t meter_peak_since(int64_t base);
+// Cost-model features of one request (chsga_cm_features).
+void request_features(const chsga_ctx& c, uint32_t len, uint32_t mode, uint32_t slots, int64_t k,
+                      uint64_t cap_bytes, float* x);
 
 // Queue entry of the score lane: bytes at `off` in the lane's arena.
 struct LaneRead {

@@ -93,6 +93,7 @@ struct Request {
   std::string read;
   int64_t submit_ns = 0;
   uint64_t footprint = 0;  // traceback: projected device bytes
+  float predicted_ms = 0;
 };
 
 struct Running {  // a score read on the lane
@@ -130,6 +131,7 @@ struct chsga_server {
   std::vector<std::thread> workers;
 
   std::mutex mu;
+  std::mutex cm_mu;  // the cost model is not re-entrant
   std::condition_variable cv_engine, cv_tb, cv_done;
   std::deque<Request> pend_score, pend_tb;
   std::deque<chsga_server_result> done;
@@ -327,9 +329,13 @@ struct chsga_server {
       r.read_len = (uint32_t)q.read.size();
       r.mode = CHSGA_REQ_TRACEBACK;
       r.submit_ns = q.submit_ns;
+      r.projected_bytes = q.footprint;
+      r.predicted_ms = q.predicted_ms;
       r.start_ns = now_ns();
       chsga_tb_opts t{o.tb_k, nullptr, 0, o.tb_cap_bytes};
+      const int64_t base = meter_reset();
       r.status = chsga_align_traceback(c, q.read.data(), (uint32_t)q.read.size(), &t, &r.tb);
+      r.peak_bytes = meter_peak_since(base);
       r.score = r.tb.score;
       r.done_ns = now_ns();
       std::lock_guard<std::mutex> lk(mu);
@@ -395,6 +401,9 @@ chsga_status chsga_server_open(chsga_ctx* ctx, const chsga_server_opts* opts, ch
     if (!o.tb_k) o.tb_k = 500;
     if (!o.row_bits) o.row_bits = 16;
     if (!o.max_pending) o.max_pending = 1u << 20;
+    require(o.footprint <= CHSGA_FP_ANALYTIC, CHSGA_ERR_INVALID_ARG, "footprint must be CHSGA_FP_*");
+    require(o.footprint != CHSGA_FP_MODEL || o.cost_model, CHSGA_ERR_INVALID_ARG,
+            "CHSGA_FP_MODEL needs a cost model");
     require(o.tb_workers <= 16, CHSGA_ERR_INVALID_ARG, "at most 16 traceback workers");
     s->ctx = ctx;
     s->num_chars = graph_chars(*ctx);
@@ -436,6 +445,16 @@ chsga_status chsga_server_submit(chsga_server* s, const char* read, uint32_t len
       require(len > 0, CHSGA_ERR_INVALID_ARG, "traceback of an empty read");
       chsga_tb_opts t{s->o.tb_k, nullptr, 0, s->o.tb_cap_bytes};
       q.footprint = traceback_device_bytes(*s->tb_ctx[0], len, &t);
+      if (s->o.cost_model) {
+        float x[CHSGA_CM_FEATURES], y[CHSGA_CM_OUTPUTS];
+        request_features(*s->tb_ctx[0], len, mode, 1, s->o.tb_k, s->o.tb_cap_bytes, x);
+        std::lock_guard<std::mutex> lk(s->cm_mu);
+        const chsga_status st = chsga_cm_predict(s->o.cost_model, x, 1, y);
+        require(st == CHSGA_OK, st, "cost model prediction failed");
+        q.predicted_ms = y[0];
+        if (s->o.footprint == CHSGA_FP_MODEL) q.footprint = (uint64_t)std::max(0.f, y[1]);
+      }
+      if (s->o.footprint == CHSGA_FP_ANALYTIC) q.footprint = 4ull * len * s->num_chars;
       require(q.footprint <= s->o.hbm_budget_bytes, CHSGA_ERR_OOM,
               "traceback footprint " + std::to_string(q.footprint) + " bytes exceeds the budget");
     }

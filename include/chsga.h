@@ -357,7 +357,17 @@ typedef struct {
   uint64_t tb_cap_bytes;     /* full-matrix byte cap of a traceback request; 0 = the context's */
   uint32_t row_bits;         /* score rows: 16 (reads <= 65000 bases) or 32; 0 = 16 */
   uint32_t max_pending;      /* requests waiting for admission before submit says BUSY; 0 = 2^20 */
+  struct chsga_cost_model* cost_model; /* predicts traceback time and footprint (may be NULL) */
+  uint32_t footprint;        /* projection used for admission, CHSGA_FP_*; 0 = PLAN */
+  uint32_t pad;
 } chsga_server_opts;
+
+/* How a traceback request's device footprint is projected for admission:
+ * PLAN     the allocation plan of the traceback (full matrix, or the
+ *          checkpointed path's row ring and largest recompute segment);
+ * MODEL    the cost model's prediction (cost_model must be set);
+ * ANALYTIC the |V| x |read| fallback, 4 N len bytes (a full matrix). */
+enum { CHSGA_FP_PLAN = 0, CHSGA_FP_MODEL = 1, CHSGA_FP_ANALYTIC = 2 };
 
 enum { CHSGA_REQ_SCORE = 0, CHSGA_REQ_TRACEBACK = 1 };
 
@@ -372,6 +382,10 @@ typedef struct {
   int64_t submit_ns;     /* host steady-clock ns: submitted, */
   int64_t start_ns;      /* admitted to the device, */
   int64_t done_ns;       /* finished */
+  uint64_t projected_bytes; /* traceback: footprint admission counted */
+  uint64_t peak_bytes;      /* traceback: device bytes the request allocated at its peak */
+  float predicted_ms;       /* traceback with a cost model: predicted time, else 0 */
+  uint32_t pad2;
   chsga_tb_result tb;    /* traceback requests; free with chsga_tb_result_free */
 } chsga_server_result;
 
@@ -404,6 +418,57 @@ chsga_status chsga_server_drain(chsga_server* s);
 /* Drains, stops the engine and workers, frees unpolled results. */
 void chsga_server_close(chsga_server* s);
 const char* chsga_server_last_error(chsga_server* s);
+
+/* ------------------------------------------------------------------------- */
+/* Learned cost model (no reference counterpart)                             */
+/* ------------------------------------------------------------------------- */
+
+/* FP32 MLP, 8 features -> 64 -> 64 -> 2 outputs (ReLU), trained and run by
+ * the library's own CUDA kernels. Outputs: per-read device time in ms and
+ * peak device bytes, learned in log space. It feeds the serving loop's
+ * admission control (chsga_server_opts.cost_model) and the autotuner; the
+ * fallback without it is the analytic |V| x |read| model; it never changes
+ * a score. Parameters: W1[8][64] b1[64] W2[64][64] b2[64] W3[64][2] b3[2];
+ * normalisation: x mean[8], x std[8], log-target mean[2], log-target std[2]. */
+#define CHSGA_CM_FEATURES 8
+#define CHSGA_CM_HIDDEN 64
+#define CHSGA_CM_OUTPUTS 2
+#define CHSGA_CM_NUM_PARAMS 4866
+#define CHSGA_CM_NUM_NORM 20
+typedef struct chsga_cost_model chsga_cost_model;
+
+typedef struct {
+  uint32_t epochs;     /* 0 = 200 */
+  uint32_t batch;      /* mini-batch size, 0 = 256 */
+  float lr;            /* Adam step, 0 = 3e-3 */
+  uint32_t keep_norm;  /* 1: keep the current normalisation instead of fitting it */
+  uint64_t seed;       /* shuffling */
+} chsga_cm_train_opts;
+
+chsga_status chsga_cm_create(int device, uint64_t seed, chsga_cost_model** out);
+void chsga_cm_free(chsga_cost_model* m);
+const char* chsga_cm_last_error(chsga_cost_model* m);
+uint32_t chsga_cm_num_params(void);
+chsga_status chsga_cm_get_params(chsga_cost_model* m, float* params, float* norm);
+chsga_status chsga_cm_set_params(chsga_cost_model* m, const float* params, const float* norm);
+/* x: n x 8 features; y: n x 2 targets (time ms, bytes; both > 0). Loss
+ * 1/(2n) sum (o - t)^2 over standardised log targets t, and its gradient
+ * with respect to the parameters (for gradient checks). */
+chsga_status chsga_cm_loss_grad(chsga_cost_model* m, const float* x, const float* y, uint32_t n,
+                                float* loss, float* grad);
+/* Adam on mini-batches; fits the normalisation first unless keep_norm. */
+chsga_status chsga_cm_train(chsga_cost_model* m, const float* x, const float* y, uint32_t n,
+                            const chsga_cm_train_opts* opts, float* final_loss);
+/* y_out: n x 2 predictions (time ms, bytes). */
+chsga_status chsga_cm_predict(chsga_cost_model* m, const float* x, uint32_t n, float* y_out);
+chsga_status chsga_cm_save(chsga_cost_model* m, const char* path);
+chsga_status chsga_cm_load(chsga_cost_model* m, const char* path);
+/* Features of one request on the context's graph: log2(len + 1), log2 N,
+ * log2 S, log2(hierarchy edges + 1), log2(hierarchy levels + 1),
+ * log2(slots), traceback (0/1), log2(k) when the traceback is checkpointed
+ * under cap_bytes (0 = the context's cap) else 0. */
+chsga_status chsga_cm_features(chsga_ctx* ctx, uint32_t read_len, uint32_t mode, uint32_t slots,
+                               int64_t k, uint64_t cap_bytes, float* x_out);
 
 #ifdef __cplusplus
 }
