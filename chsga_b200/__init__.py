@@ -31,6 +31,7 @@ OK, ERR_INVALID_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, \
 OP_DELETE, OP_MATCHSUB, OP_INSERT = 0, 1, 2
 REQ_SCORE, REQ_TRACEBACK = 0, 1
 FP_PLAN, FP_MODEL, FP_ANALYTIC = 0, 1, 2
+ROW_AUTO, ROW_DIRECT, ROW_TILED = 0, 1, 2
 FLAG_PROFILE = 1
 NOALLOC_SCRATCH_BYTES = 32 << 20  # CHSGA_NOALLOC_SCRATCH_BYTES
 
@@ -102,7 +103,17 @@ class OptsT(C.Structure):
 
 class BatchOpts(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("steps_per_graph", C.c_uint32), ("use_graphs", C.c_uint32),
-                ("row_bits", C.c_uint32)]
+                ("row_bits", C.c_uint32), ("row_kernel", C.c_uint32), ("top_vertices", C.c_uint32)]
+
+
+class TuneTrial(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("steps_per_graph", C.c_uint32), ("row_kernel", C.c_uint32),
+                ("top_vertices", C.c_uint32), ("predicted_gcups", C.c_double),
+                ("measured_gcups", C.c_double)]
+
+
+class TuneOpts(C.Structure):
+    _fields_ = [("cost_model", C.c_void_p), ("measure_top", C.c_uint32), ("repeats", C.c_uint32)]
 
 
 class TbOpts(C.Structure):
@@ -193,6 +204,8 @@ _sig("chsga_align_scores", C.c_int32, vp, C.POINTER(C.c_char_p), u32p, C.c_uint3
 _sig("chsga_align_scores_batched", C.c_int32, vp, C.POINTER(C.c_char_p), u32p, C.c_uint32,
      C.POINTER(BatchOpts), i32p)
 _sig("chsga_align_scores_noalloc", C.c_int32, vp, C.POINTER(C.c_char_p), u32p, C.c_uint32, i32p)
+_sig("chsga_autotune", C.c_int32, vp, C.POINTER(C.c_char_p), u32p, C.c_uint32, C.POINTER(TuneOpts),
+     C.POINTER(BatchOpts), C.POINTER(TuneTrial), C.c_uint32, C.POINTER(C.c_uint32))
 _sig("chsga_align_rows", C.c_int32, vp, C.c_char_p, C.c_uint32, i32p)
 _sig("chsga_align_traceback", C.c_int32, vp, C.c_char_p, C.c_uint32, C.POINTER(TbOpts),
      C.POINTER(TbResult))
@@ -405,10 +418,11 @@ class Context:
         return out
 
     def align_scores_batched(self, reads: Sequence[bytes], slots: int = 64, steps_per_graph: int = 8,
-                             use_graphs: bool = True, row_bits: int = 0) -> np.ndarray:
+                             use_graphs: bool = True, row_bits: int = 0, row_kernel: int = 0,
+                             top_vertices: int = 0) -> np.ndarray:
         arr, lens = _read_ptrs(reads)
         out = np.zeros(len(reads), dtype=np.int32)
-        o = BatchOpts(slots, steps_per_graph, int(use_graphs), row_bits)
+        o = BatchOpts(slots, steps_per_graph, int(use_graphs), row_bits, row_kernel, top_vertices)
         self._ck(_lib.chsga_align_scores_batched(self._h, arr, lens.ctypes.data_as(u32p), len(reads),
                                                  C.byref(o), out.ctypes.data_as(i32p)))
         return out
@@ -421,6 +435,19 @@ class Context:
         self._ck(_lib.chsga_align_scores_noalloc(self._h, arr, lens.ctypes.data_as(u32p), len(reads),
                                                  out.ctypes.data_as(i32p)))
         return out
+
+    def autotune(self, reads: Sequence[bytes], cost_model: Optional["CostModel"] = None,
+                 measure_top: int = 0, repeats: int = 0):
+        """(best batch options as a dict, list of trial dicts)."""
+        arr, lens = _read_ptrs(reads)
+        o = TuneOpts(cost_model._h if cost_model is not None else None, measure_top, repeats)
+        best = BatchOpts()
+        trials = (TuneTrial * 64)()
+        nt = C.c_uint32()
+        self._ck(_lib.chsga_autotune(self._h, arr, lens.ctypes.data_as(u32p), len(reads), C.byref(o),
+                                     C.byref(best), trials, 64, C.byref(nt)))
+        tr = [{k: getattr(trials[i], k) for k, _ in TuneTrial._fields_} for i in range(min(nt.value, 64))]
+        return {k: getattr(best, k) for k, _ in BatchOpts._fields_}, tr
 
     def align_rows(self, read: bytes, num_chars: int) -> np.ndarray:
         out = np.zeros((len(read), num_chars), dtype=np.int32)

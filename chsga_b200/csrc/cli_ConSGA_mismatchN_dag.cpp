@@ -73,7 +73,7 @@ int main(int argc, char** argv) {
   const uint32_t slots = (uint32_t)cli::env_u64("CHSGA_SLOTS", 0);
   auto t0 = std::chrono::high_resolution_clock::now();
   if (slots > 1) {
-    chsga_batch_opts b{slots, 8, 1, 0};
+    chsga_batch_opts b{slots, 8, 1, 0, 0, 0};
     cli::check(chsga_align_scores_batched(ctx, ptrs.data(), lens.data(), (uint32_t)n, &b,
                                           scores.data()),
                ctx, "chsga_align_scores_batched");

@@ -155,6 +155,9 @@ struct chsga_ctx {
   std::shared_ptr<chsga::LoadedGraph> g;
   std::map<int, std::unique_ptr<chsga::SlotBufs>> bufs;
   std::map<int, std::unique_ptr<chsga::RowTileDev>> row_tiles;  // by R * 8 + sizeof(score)
+  // top regions other than the graph's default, by their vertex limit
+  std::map<uint32_t, std::unique_ptr<chsga::TopDev>> tops;
+  const chsga::TopDev* top_sel = nullptr;  // this call's top region (nullptr: the default)
   int num_sms = 148;
   chsga::RowKernel row_kernel = chsga::RowKernel::Auto;
   chsga::DevArr<unsigned char> reads;
@@ -207,6 +210,42 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
   }();
   (void)attr_set;
   return *b;
+}
+
+const TopDev& cur_top(const chsga_ctx& c) { return c.top_sel ? *c.top_sel : *c.g->top; }
+
+// The top region of the hierarchy with at most K vertices (levels from the
+// highest down, while they fit) and its chunk schedule, on the device.
+std::unique_ptr<TopDev> make_top(const HostLayout& L, const GraphDev& d, uint32_t K, cudaStream_t s) {
+  auto top = std::make_unique<TopDev>();
+  top->h = build_top(L, K, dev::kTopChunk);
+  const HostTop& h = top->h;
+  auto to2 = [](const std::vector<EdgeW>& v) {
+    std::vector<int2> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) o[i] = make_int2(v[i].src, v[i].w);
+    return o;
+  };
+  top->upg_off.upload(h.upg_off, s);
+  top->upg.upload(to2(h.upg), s);
+  top->sched.upload(to2(h.sched), s);
+  std::vector<int2> ch(h.chunks.size());
+  for (size_t i = 0; i < ch.size(); ++i) ch[i] = make_int2(h.chunks[i].first, h.chunks[i].second);
+  top->chunks.upload(ch, s);
+  top->ptrs = dev::TopPtrs{h.K0, h.K, (uint32_t)h.chunks.size(), top->chunks.p, top->sched.p,
+                           d.dv_len.p};
+  CK(cudaStreamSynchronize(s));
+  return top;
+}
+
+// The top region for a vertex limit (0 = the graph's default), built once
+// per context and limit.
+const TopDev* top_for(chsga_ctx& c, uint32_t K) {
+  if (K == 0 || K == kTopMaxVertices) return nullptr;
+  require(K <= kTopMaxVertices, CHSGA_ERR_INVALID_ARG,
+          "top_vertices above " + std::to_string(kTopMaxVertices) + " do not fit shared memory");
+  auto& t = c.tops[K];
+  if (!t) t = make_top(c.g->L, c.g->gd, K, c.st);
+  return t.get();
 }
 
 // Uploads reads (raw bytes) and their queue descriptors; ids are 0..n-1.
@@ -336,7 +375,7 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
               StepEvents* ev = nullptr) {
   ST* BVc = reinterpret_cast<ST*>(b.BV.p);
   const HostLayout& L = c.g->L;
-  const TopDev& top = *c.g->top;
+  const TopDev& top = cur_top(c);
   constexpr int G = Lanes<R>::G;
   if (ev) CK(cudaEventRecord(ev->e[0], s));
   ST* FL = reinterpret_cast<ST*>(b.FL.p);
@@ -397,9 +436,10 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
 
 uint32_t kernels_per_step(const chsga_ctx& c) {
   uint32_t k = 2;  // k_row + k_advance
-  const uint32_t fl = c.g->top->h.first_level;
+  const TopDev& top = cur_top(c);
+  const uint32_t fl = top.h.first_level;
   for (uint32_t l = 0; l < fl; ++l) k += c.g->L.lvl_up_edges[l] ? 1 : 0;
-  if (c.g->top->h.K) k += 1 + (c.g->top->h.upg.empty() ? 0 : 1);
+  if (top.h.K) k += 1 + (top.h.upg.empty() ? 0 : 1);
   k += fl == 0 ? 1 : fl;
   return k;
 }
@@ -528,23 +568,7 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   for (size_t i = 0; i < dn.size(); ++i) dn[i] = make_int2(L.dn_in[i].src, L.dn_in[i].w);
   d.up_in.upload(up, s);
   d.dn_in.upload(dn, s);
-  auto top = std::make_unique<TopDev>();
-  top->h = build_top(L, kTopMaxVertices, dev::kTopChunk);
-  const HostTop& h = top->h;
-  auto to2 = [](const std::vector<EdgeW>& v) {
-    std::vector<int2> o(v.size());
-    for (size_t i = 0; i < v.size(); ++i) o[i] = make_int2(v[i].src, v[i].w);
-    return o;
-  };
-  top->upg_off.upload(h.upg_off, s);
-  top->upg.upload(to2(h.upg), s);
-  top->sched.upload(to2(h.sched), s);
-  std::vector<int2> ch(h.chunks.size());
-  for (size_t i = 0; i < ch.size(); ++i) ch[i] = make_int2(h.chunks[i].first, h.chunks[i].second);
-  top->chunks.upload(ch, s);
-  top->ptrs = dev::TopPtrs{h.K0, h.K, (uint32_t)h.chunks.size(), top->chunks.p, top->sched.p,
-                           d.dv_len.p};
-  CK(cudaStreamSynchronize(s));
+  auto top = make_top(L, d, kTopMaxVertices, s);
   lg->gp = dev::GraphPtrs{L.N,          L.S,          L.special,    d.lab2.p,     d.lab_sp.p,
                           d.lab4.p,     d.sv_off.p,   d.sv_dev.p,   d.vin_off.p,  d.vin_src.p,
                           d.vin_srcv.p, d.dv_first.p, d.dv_len.p,   d.dv_s.p,     d.up_off.p,
@@ -557,6 +581,8 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   c.g = std::move(lg);
   c.bufs.clear();
   c.row_tiles.clear();
+  c.tops.clear();
+  c.top_sel = nullptr;
   c.loaded = true;
 }
 
@@ -1072,6 +1098,138 @@ void scores_noalloc(chsga_ctx& c, const char* const* reads, const uint32_t* lens
   require(fin.done == m, CHSGA_ERR_INTERNAL, "allocation-free path lost reads");
 }
 
+// Applies a call's row-kernel and level-grouping choices to the context
+// and puts the previous ones back when the call ends.
+struct CallKnobs {
+  chsga_ctx& c;
+  RowKernel rk;
+  const TopDev* ts;
+  CallKnobs(chsga_ctx& cx, uint32_t row_kernel, uint32_t top_vertices)
+      : c(cx), rk(cx.row_kernel), ts(cx.top_sel) {
+    require(row_kernel <= CHSGA_ROW_TILED, CHSGA_ERR_INVALID_ARG, "row_kernel must be CHSGA_ROW_*");
+    if (row_kernel == CHSGA_ROW_DIRECT) c.row_kernel = RowKernel::Direct;
+    if (row_kernel == CHSGA_ROW_TILED) c.row_kernel = RowKernel::Tiled;
+    c.top_sel = top_for(c, top_vertices);
+  }
+  ~CallKnobs() {
+    c.row_kernel = rk;
+    c.top_sel = ts;
+  }
+};
+
+void scores_batched(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n,
+                    const chsga_batch_opts* o, int32_t* out) {
+  const uint32_t slots = o && o->slots ? o->slots : 64;
+  const bool graphs = o ? o->use_graphs != 0 : true;
+  const uint32_t per = o && o->steps_per_graph ? o->steps_per_graph : 8;
+  const uint32_t rb = o ? o->row_bits : 0;
+  require(rb == 0 || rb == 16 || rb == 32, CHSGA_ERR_INVALID_ARG, "row_bits must be 0, 16 or 32");
+  CallKnobs knobs(c, o ? o->row_kernel : 0, o ? o->top_vertices : 0);
+  switch (slots) {
+    case 1: scores_with<1>(c, reads, lens, n, out, graphs, per, rb); break;
+    case 2: scores_with<2>(c, reads, lens, n, out, graphs, per, rb); break;
+    case 4: scores_with<4>(c, reads, lens, n, out, graphs, per, rb); break;
+    case 8: scores_with<8>(c, reads, lens, n, out, graphs, per, rb); break;
+    case 16: scores_with<16>(c, reads, lens, n, out, graphs, per, rb); break;
+    case 32: scores_with<32>(c, reads, lens, n, out, graphs, per, rb); break;
+    case 64: scores_with<64>(c, reads, lens, n, out, graphs, per, rb); break;
+    case 128: scores_with<128>(c, reads, lens, n, out, graphs, per, rb); break;
+    default: fail(CHSGA_ERR_INVALID_ARG, "slots must be 1, 2, 4, 8, 16, 32, 64 or 128");
+  }
+}
+
+// Coordinate search over the batched engine's knobs on a read sample:
+// slots, then steps per graph, then the row kernel, then the level
+// grouping, each stage keeping the fastest by device time. With a cost
+// model, the slot stage only runs the candidates of highest predicted
+// throughput. Every run must return the first run's scores.
+chsga_batch_opts autotune(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n,
+                          const chsga_tune_opts* o, std::vector<chsga_tune_trial>& trials) {
+  const uint32_t repeats = o && o->repeats ? o->repeats : 2;
+  uint64_t sum_len = 0;
+  for (uint32_t i = 0; i < n; ++i) sum_len += lens[i];
+  const double cells = (double)sum_len * c.g->L.N;
+  std::vector<int32_t> ref(n), got(n);
+  bool have_ref = false;
+  auto run = [&](const chsga_batch_opts& b, double predicted) {
+    double best_ms = 1e300;
+    for (uint32_t r = 0; r < repeats; ++r) {
+      scores_batched(c, reads, lens, n, &b, got.data());
+      best_ms = std::min(best_ms, (double)c.prof.total_ms);
+      if (!have_ref) {
+        ref = got;
+        have_ref = true;
+      }
+      require(got == ref, CHSGA_ERR_INTERNAL, "autotune candidates disagree on the scores");
+    }
+    const double g = cells / (best_ms * 1e-3) / 1e9;
+    trials.push_back(chsga_tune_trial{b.slots, b.steps_per_graph, b.row_kernel, b.top_vertices, predicted, g});
+    return g;
+  };
+  chsga_batch_opts cur{};
+  cur.slots = 64;
+  cur.steps_per_graph = 8;
+  cur.use_graphs = 1;
+  // slots
+  std::vector<std::pair<double, uint32_t>> cand;  // (predicted gcups, slots)
+  for (uint32_t R : {16u, 32u, 64u, 128u}) {
+    double pred = 0;
+    if (o && o->cost_model) {
+      // per-read time at R slots; R reads run at once
+      std::vector<float> x((size_t)n * CHSGA_CM_FEATURES), y((size_t)n * CHSGA_CM_OUTPUTS);
+      for (uint32_t i = 0; i < n; ++i)
+        request_features(c, lens[i], CHSGA_REQ_SCORE, R, 0, 0, &x[(size_t)i * CHSGA_CM_FEATURES]);
+      const chsga_status st = chsga_cm_predict(o->cost_model, x.data(), n, y.data());
+      require(st == CHSGA_OK, st, "cost model prediction failed");
+      double t_ms = 0;
+      for (uint32_t i = 0; i < n; ++i) t_ms += y[(size_t)i * CHSGA_CM_OUTPUTS];
+      pred = cells / (t_ms / R * 1e-3) / 1e9;
+    }
+    cand.push_back({pred, R});
+  }
+  if (o && o->cost_model) {
+    std::stable_sort(cand.begin(), cand.end(), [](auto& a, auto& b) { return a.first > b.first; });
+    const uint32_t top = o->measure_top ? o->measure_top : 4;
+    for (size_t i = top; i < cand.size(); ++i)
+      trials.push_back(chsga_tune_trial{cand[i].second, 8, 0, 0, cand[i].first, 0.0});
+    cand.resize(std::min<size_t>(cand.size(), top));
+  }
+  double best_g = -1;
+  chsga_batch_opts best = cur;
+  for (auto& [pred, R] : cand) {
+    chsga_batch_opts b = cur;
+    b.slots = R;
+    const double g = run(b, pred);
+    if (g > best_g) best_g = g, best = b;
+  }
+  // steps per graph
+  cur = best;
+  for (uint32_t per : {4u, 16u}) {
+    chsga_batch_opts b = cur;
+    b.steps_per_graph = per;
+    const double g = run(b, 0);
+    if (g > best_g) best_g = g, best = b;
+  }
+  // row kernel
+  cur = best;
+  for (uint32_t rk : {(uint32_t)CHSGA_ROW_DIRECT, (uint32_t)CHSGA_ROW_TILED}) {
+    if (rk == CHSGA_ROW_TILED && cur.slots < 32) continue;
+    chsga_batch_opts b = cur;
+    b.row_kernel = rk;
+    const double g = run(b, 0);
+    if (g > best_g) best_g = g, best = b;
+  }
+  // level grouping
+  cur = best;
+  for (uint32_t K : {8000u, 2000u}) {
+    chsga_batch_opts b = cur;
+    b.top_vertices = K;
+    const double g = run(b, 0);
+    if (g > best_g) best_g = g, best = b;
+  }
+  return best;
+}
+
 template <typename F>
 chsga_status guarded_ctx(chsga_ctx* c, F&& f) {
   try {
@@ -1426,22 +1584,22 @@ chsga_status chsga_align_scores_batched(chsga_ctx* c, const char* const* reads,
   return guarded_ctx(c, [&] {
     require(c && (n == 0 || (reads && lens && scores_out)), CHSGA_ERR_INVALID_ARG, "null argument");
     require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
-    uint32_t slots = o && o->slots ? o->slots : 64;
-    const bool graphs = o ? o->use_graphs != 0 : true;
-    const uint32_t per = o && o->steps_per_graph ? o->steps_per_graph : 8;
-    const uint32_t rb = o ? o->row_bits : 0;
-    require(rb == 0 || rb == 16 || rb == 32, CHSGA_ERR_INVALID_ARG, "row_bits must be 0, 16 or 32");
-    switch (slots) {
-      case 1: scores_with<1>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
-      case 2: scores_with<2>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
-      case 4: scores_with<4>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
-      case 8: scores_with<8>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
-      case 16: scores_with<16>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
-      case 32: scores_with<32>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
-      case 64: scores_with<64>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
-      case 128: scores_with<128>(*c, reads, lens, n, scores_out, graphs, per, rb); break;
-      default: fail(CHSGA_ERR_INVALID_ARG, "slots must be 1, 2, 4, 8, 16, 32, 64 or 128");
-    }
+    scores_batched(*c, reads, lens, n, o, scores_out);
+  });
+}
+
+chsga_status chsga_autotune(chsga_ctx* c, const char* const* reads, const uint32_t* lens,
+                            uint32_t n, const chsga_tune_opts* opts, chsga_batch_opts* best,
+                            chsga_tune_trial* trials, uint32_t max_trials, uint32_t* n_trials) {
+  return guarded_ctx(c, [&] {
+    require(c && reads && lens && n > 0 && best, CHSGA_ERR_INVALID_ARG, "bad argument");
+    require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
+    std::vector<chsga_tune_trial> t;
+    *best = autotune(*c, reads, lens, n, opts, t);
+    const uint32_t m = std::min<uint32_t>(max_trials, (uint32_t)t.size());
+    if (trials)
+      for (uint32_t i = 0; i < m; ++i) trials[i] = t[i];
+    if (n_trials) *n_trials = (uint32_t)t.size();
   });
 }
 

@@ -230,7 +230,16 @@ typedef struct {
   uint32_t row_bits;      /* storage of the score rows: 0 = 16 when every read is at most
                              65000 bases (each value of row i is at most i + 1, so this is
                              exact; arithmetic stays int32), else 32; or force 16 / 32 */
+  uint32_t row_kernel;    /* CHSGA_ROW_*: which row kernel runs; 0 = AUTO */
+  uint32_t top_vertices;  /* level grouping: hierarchy vertices (highest levels first) swept
+                             by the one-CTA-per-slot top kernel, the levels below one grid
+                             launch each; 0 = 23000 (the most shared memory holds) */
 } chsga_batch_opts;
+/* Row kernels: AUTO = the packed 16-bit DPX kernel when rows are 16-bit,
+ * slots >= 2 and no string vertex label exceeds 512 chars, else DIRECT;
+ * DIRECT = one thread group per string vertex; TILED = shared-memory tiles
+ * of consecutive string vertices staged by TMA bulk copies (slots >= 32). */
+enum { CHSGA_ROW_AUTO = 0, CHSGA_ROW_DIRECT = 1, CHSGA_ROW_TILED = 2 };
 chsga_status chsga_align_scores_batched(chsga_ctx* ctx, const char* const* reads,
                                         const uint32_t* lens, uint32_t n,
                                         const chsga_batch_opts* opts, int32_t* scores_out);
@@ -326,6 +335,32 @@ chsga_status chsga_get_profile(chsga_ctx* ctx, chsga_profile* out);
  * global timer, ns), in the order of the non-empty reads passed in. No
  * reference counterpart: used for per-read latency percentiles. */
 chsga_status chsga_get_read_times(chsga_ctx* ctx, uint64_t* admit_ns, uint64_t* done_ns, uint32_t n);
+
+/* ------------------------------------------------------------------------- */
+/* Autotuner (no reference counterpart)                                      */
+/* ------------------------------------------------------------------------- */
+
+/* Chooses chsga_batch_opts for a read mix: reads per launch (slots),
+ * row-steps per CUDA graph, the row kernel and the level grouping
+ * (top_vertices). Candidates run chsga_align_scores_batched on the given
+ * sample and the fastest (device time) wins; every candidate must return
+ * the same scores (else CHSGA_ERR_INTERNAL). With a trained cost model only
+ * the `measure_top` candidates of highest predicted throughput are run. */
+typedef struct {
+  uint32_t slots, steps_per_graph, row_kernel, top_vertices;
+  double predicted_gcups;  /* cost model's estimate; 0 without one */
+  double measured_gcups;   /* 0 when not run */
+} chsga_tune_trial;
+
+typedef struct {
+  struct chsga_cost_model* cost_model;  /* optional ranking of the candidates */
+  uint32_t measure_top;                 /* with a cost model: candidates run; 0 = 4 */
+  uint32_t repeats;                     /* timed runs per candidate, fastest kept; 0 = 2 */
+} chsga_tune_opts;
+
+chsga_status chsga_autotune(chsga_ctx* ctx, const char* const* reads, const uint32_t* lens,
+                            uint32_t n, const chsga_tune_opts* opts, chsga_batch_opts* best,
+                            chsga_tune_trial* trials, uint32_t max_trials, uint32_t* n_trials);
 
 /* ------------------------------------------------------------------------- */
 /* Serving loop (no reference counterpart: the reference aligns a fixed read */
