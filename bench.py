@@ -11,9 +11,14 @@ completion through the slot-interleaved engine (score-only, int32).
 
   value   GCUPS over the K timed steps: sum(read_len * num_chars) / device
           time (CUDA events around the device sequence, reads resident)
-  e2e     the same cells / wall time of chsga_align_scores_batched with host
-          buffers (read upload and score download inside), barrier + sync
-          on both sides, max over ranks
+  e2e     batched + served: the same K batches streamed through the serving
+          loop (chsga_server_submit / _poll with host buffers: reads copied
+          in, scores copied out, continuous batching across batches), cells
+          / wall time from the first submit to the last result
+  served  a Poisson arrival stream at ~80% of that capacity (80% 150 bp at
+          1% error, 20% log-uniform 1-10 kbp at 5%): p50/p99 latency from
+          submission to result, and the cost model's per-read time error
+          against the analytic |V| x |read| model on those logs
 The score rows of one step (slots x 25.5 MB per row buffer) exceed the 126 MB
 L2, so no flush is needed between steps.
 
@@ -50,6 +55,8 @@ def parse():
     p.add_argument("--warmup-batch", type=int, default=128,
                    help="reads per warm-up step (lengths capped at 1 kbp)")
     p.add_argument("--no-profile", action="store_true")
+    p.add_argument("--no-tune", action="store_true", help="skip the autotuner (use --slots)")
+    p.add_argument("--served-s", type=float, default=12.0, help="Poisson arrival window, seconds")
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
     return p.parse_args()
 
@@ -190,6 +197,82 @@ def cpu_baseline(g, reads, budget_s):
                       f"shortest first, {dt:.1f} s on {cores} host threads"}
 
 
+def served_mix(g, n, seed):
+    """80% 150 bp at 1% error, 20% log-uniform 1-10 kbp at 5% error."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    longs = int(round(0.2 * n))
+    short = g.gen_reads(n - longs, seed, 150, 150, sub_rate=0.006, indel_rate=0.003,
+                        n_rate=0.001).to_list()
+    lng = make_reads(g, 3 * longs, seed + 1, len_max=10000) if longs else []
+    lng = [r for r in lng if len(r) >= 1000][:longs] or lng[:longs]
+    out = short + lng
+    rng.shuffle(out)
+    return out
+
+
+def served_run(cb, ctx, g, N, opts, capacity_gcups, window_s):
+    """Poisson arrivals at ~80% of the measured served capacity for window_s
+    seconds; latency = result time - submit time (host clock)."""
+    import numpy as np
+    reads = served_mix(g, 4096, 4242)
+    mean_len = float(np.mean([len(r) for r in reads]))
+    rate = 0.8 * capacity_gcups * 1e9 / (mean_len * N)  # reads per second
+    n = max(32, min(len(reads), int(rate * window_s)))
+    reads = reads[:n]
+    rng = np.random.default_rng(7)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    srv = cb.Server(ctx, slots=opts["slots"], steps_per_graph=opts["steps_per_graph"],
+                    queue_capacity=4096, arena_bytes=64 << 20, tb_workers=1)
+    res = {}
+    tickets = [None] * n
+
+    def producer():
+        t0 = time.perf_counter()
+        for i, (r, at) in enumerate(zip(reads, arrivals)):
+            d = at - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            tickets[i] = srv.submit(r)
+
+    th = threading.Thread(target=producer)
+    th.start()
+    while th.is_alive() or len(res) < n:
+        for d in srv.poll(1024, 50):
+            res[d["ticket"]] = d
+    th.join()
+    st = srv.stats()
+    srv.close()
+    lat = np.array([(res[t]["done_ns"] - res[t]["submit_ns"]) / 1e6 for t in tickets])
+    lens = np.array([len(r) for r in reads])
+    short = lens <= 150
+    # cost model: trained on the first half of the served logs (per-read
+    # device time, and the slot share of the engine's buffers), tested on
+    # the second half against the analytic |V| x |read| model
+    feats = np.array([cb.cm_features(ctx, int(L), cb.REQ_SCORE, opts["slots"]) for L in lens])
+    t_ms = np.array([max(1e-3, (res[t]["done_ns"] - res[t]["start_ns"]) / 1e6) for t in tickets])
+    y = np.stack([t_ms, 4.0 * (N + 32) + lens], 1)
+    half = n // 2
+    m = cb.CostModel(0, seed=1)
+    m.train(feats[:half], y[:half], epochs=200, batch=min(64, half), seed=2)
+    pred = m.predict(feats[half:])[:, 0]
+    m.close()
+    cells = lens * float(N)
+    a = np.exp(np.mean(np.log(t_ms[:half] / cells[:half])))
+    ana = a * cells[half:]
+    return {
+        "arrivals": "Poisson", "reads": n, "rate_reads_per_s": rate, "load": 0.8,
+        "mix": "80% 150 bp @1% error, 20% log-uniform 1-10 kbp @5% error",
+        "gcups": st["gcups"], "p50_ms": float(np.percentile(lat, 50)),
+        "p99_ms": float(np.percentile(lat, 99)),
+        "short_p50_ms": float(np.percentile(lat[short], 50)) if short.any() else None,
+        "short_p99_ms": float(np.percentile(lat[short], 99)) if short.any() else None,
+        "cost_model": {"train_reads": half, "test_reads": n - half,
+                       "mean_abs_log_err_time": float(np.mean(np.abs(np.log(pred / t_ms[half:])))),
+                       "analytic_mean_abs_log_err_time": float(np.mean(np.abs(np.log(ana / t_ms[half:]))))},
+    }
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -276,12 +359,24 @@ def main():
     def max_over_ranks(x):
         return replicas.max_over_ranks(x, ws, device=f"cuda:{local}")
 
+    # autotuner on a sample of the distribution (reads capped at 2 kbp)
+    opts = dict(slots=args.slots, steps_per_graph=8, row_kernel=0, top_vertices=0)
+    tune = None
+    if not args.no_tune:
+        tsample = make_reads(g, 2 * args.slots, 60_000 + rank, len_max=2000)
+        best, trials = ctx.autotune(tsample, repeats=1)
+        opts = {k: best[k] for k in opts}
+        tune = {"chosen": opts, "trials": [
+            {k: (round(t[k], 1) if isinstance(t[k], float) else t[k]) for k in
+             ("slots", "steps_per_graph", "row_kernel", "top_vertices", "measured_gcups")}
+            for t in trials]}
+
     # warm-up: full passes of the engine (CUDA-graph instantiation, caches) on
     # batches of the same distribution capped at 1 kbp, so a warm-up step is
     # not held up by one 10 kbp read
     for w in range(args.warmup):
         reads = make_reads(g, wb, 50_000 + 1000 * rank + w, len_max=1000)
-        ctx.align_scores_batched(reads, slots=args.slots)
+        ctx.align_scores_batched(reads, **opts)
     batches = [make_reads(g, args.batch, 1000 * rank + s) for s in range(args.steps)]
     cells = sum(len(r) for b in batches for r in b) * N
     h2d = sum(len(r) for b in batches for r in b) // args.steps + 16 * args.batch
@@ -292,7 +387,7 @@ def main():
     dev_ms, lat, launches, steps_work = 0.0, [], 0, 0
     t0 = time.perf_counter()
     for b in batches:
-        ctx.align_scores_batched(b, slots=args.slots)
+        ctx.align_scores_batched(b, **opts)
         p = ctx.profile()
         dev_ms += p["total_ms"]
         launches += int(p["launches"])
@@ -300,27 +395,47 @@ def main():
         a, d = ctx.read_times(len(b))
         lat.extend(((d - a).astype(np.float64) / 1e6).tolist())
     wall = time.perf_counter() - t0
+    # batched + served: the same batches streamed through the serving loop
+    srv = cb.Server(ctx, slots=opts["slots"], steps_per_graph=opts["steps_per_graph"],
+                    queue_capacity=4096, arena_bytes=64 << 20, tb_workers=1)
+    barrier()
+    t1 = time.perf_counter()
+    for b in batches:
+        for r in b:
+            srv.submit(r)
+    got = 0
+    while got < len(batches) * args.batch:
+        got += len(srv.poll(4096, 100))
+    srv_wall = time.perf_counter() - t1
+    sst = srv.stats()
+    srv.close()
     barrier()
     ck = clocks.stop()
     dev_s = max_over_ranks(dev_ms / 1e3)
-    wall_s = max_over_ranks(wall)
+    srv_s = max_over_ranks(srv_wall)
     total_cells = cells * ws
     value = total_cells / dev_s / 1e9
-    e2e = total_cells / wall_s / 1e9
+    e2e = total_cells / srv_s / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "num_chars": N, "num_strings": st["num_strings"],
                    "hierarchy_levels": st["pch_levels"], "batch_reads": args.batch,
-                   "slots": args.slots, "parallelism": f"replicas x{ws}",
+                   "engine": opts, "parallelism": f"replicas x{ws}",
                    "l2": "score rows exceed L2 (no flush needed)"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                       "what": "device admission-to-completion per read"},
-        "e2e": {"value": e2e, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                       "what": "batched steps: device admission-to-completion per read"},
+        "e2e": {"value": e2e, "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "what": "batched+served: the timed batches streamed through chsga_server, "
+                        "first submit to last result, host buffers",
+                "batched_call_gcups": total_cells / max_over_ranks(wall) / 1e9,
+                "server_launches": int(sst["gpu_launches"])},
         "gpu_launches": launches,
         "clocks": ck,
     }
+    if tune:
+        line["autotune"] = tune
     if rank == 0:
         # plain one-read-per-launch path on a sample of the first batch
         sample = sorted(batches[0], key=len)[: max(2, min(6, len(batches[0])))]
@@ -330,22 +445,26 @@ def main():
         line["plain"] = {"value": pc / (pp["total_ms"] / 1e3) / 1e9, "unit": "GCUPS",
                          "sample": f"{len(sample)} shortest reads of the first batch"}
         line["batched_over_plain"] = value / line["plain"]["value"]
+        line["served_over_plain"] = e2e / line["plain"]["value"]
+        line["served"] = served_run(cb, ctx, g, N, opts, e2e, args.served_s)
     if rank == 0 and not args.no_profile:
         # profiled pass: CUDA events around every kernel group of every row-step
         pctx = cb.Context(local, flags=cb.FLAG_PROFILE)
         pctx.load(g)
-        sample = make_reads(g, args.slots, 77_777, len_max=1000)
-        pctx.align_scores_batched(sample, slots=args.slots)
+        R = opts["slots"]
+        sample = make_reads(g, R, 77_777, len_max=1000)
+        pctx.align_scores_batched(sample, **opts)
         pr = pctx.profile()
         pctx.close()
         row_avg_s = pr["row_ms"] / max(1, pr["row_launches"]) / 1e3
         peak, src = measured_peak()
-        ab = algorithmic_row_bytes(st, args.slots, multi, pr["row_bits"] // 8)
+        ab = algorithmic_row_bytes(st, R, multi, pr["row_bits"] // 8)
+        kname = {cb.ROW_DIRECT: "k_row_direct", cb.ROW_TILED: "k_row_tiled"}.get(
+            opts["row_kernel"], "k_row_dpx" if pr["row_bits"] == 16 else "k_row_direct")
         tr = ncu_traffic()
         total = pr["row_ms"] + pr["sweep_up_ms"] + pr["top_ms"] + pr["sweep_down_ms"] + pr["other_ms"]
         line["roofline"] = {
-            "bound": "hbm", "kernel": f"k_row_dpx<{args.slots}>" if pr["row_bits"] == 16
-            else f"k_row_direct<{args.slots}>", "row_bits": int(pr["row_bits"]),
+            "bound": "hbm", "kernel": f"{kname}<{R}>", "row_bits": int(pr["row_bits"]),
             "achieved": ab / row_avg_s / 1e9, "peak": peak, "unit": "GB/s",
             "frac": ab / row_avg_s / 1e9 / peak, "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)"
             if src == "measured" else "fallback 6.65 TB/s",
