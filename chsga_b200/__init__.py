@@ -31,7 +31,7 @@ OK, ERR_INVALID_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, \
 OP_DELETE, OP_MATCHSUB, OP_INSERT = 0, 1, 2
 REQ_SCORE, REQ_TRACEBACK = 0, 1
 FP_PLAN, FP_MODEL, FP_ANALYTIC = 0, 1, 2
-ROW_AUTO, ROW_DIRECT, ROW_TILED = 0, 1, 2
+ROW_AUTO, ROW_DIRECT, ROW_TILED, ROW_DPX, ROW_STREAM = 0, 1, 2, 3, 4
 FLAG_PROFILE = 1
 NOALLOC_SCRATCH_BYTES = 32 << 20  # CHSGA_NOALLOC_SCRATCH_BYTES
 

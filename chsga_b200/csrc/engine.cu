@@ -117,7 +117,7 @@ struct SlotBufs {
 // Row kernel choice: the DPX kernel for 16-bit rows (default), the direct
 // kernel, or the shared-memory tile-staged kernel (CHSGA_ROW_KERNEL=direct |
 // tiled, for comparisons).
-enum class RowKernel { Auto, Direct, Tiled };
+enum class RowKernel { Auto, Direct, Tiled, Dpx, Stream };
 
 struct RowTileDev {
   DevArr<int4> rec;
@@ -209,6 +209,15 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
     return true;
   }();
   (void)attr_set;
+  if constexpr (std::is_same_v<ST, uint16_t> && R >= 64) {
+    static const bool stream_set = [] {
+      for (auto k : {dev::k_row_stream<R, true>, dev::k_row_stream<R, false>})
+        CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)dev::stream_smem_bytes(R)));
+      return true;
+    }();
+    (void)stream_set;
+  }
   return *b;
 }
 
@@ -381,11 +390,22 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   ST* FL = reinterpret_cast<ST*>(b.FL.p);
   bool done = false;
   if constexpr (std::is_same_v<ST, uint16_t> && R >= 2) {
-    // packed 16-bit DPX kernel; exact while F + (c - first) stays below 2^16
+    // packed 16-bit DPX kernels; exact while F + (c - first) stays below 2^16
     if (L.max_len <= 512 && c.row_kernel != RowKernel::Tiled && c.row_kernel != RowKernel::Direct) {
-      dev::k_row_dpx<R, DEFER><<<nblocks((uint64_t)L.S * dev::Pairs<R>::G), 256, 0, s>>>(
-          c.g->gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
-      done = true;
+      if constexpr (R >= 64) {
+        if (c.row_kernel != RowKernel::Dpx) {
+          const uint64_t runs = ((uint64_t)L.S + 31) / 32;
+          constexpr unsigned tpb = dev::kStreamWarps * 32;
+          dev::k_row_stream<R, DEFER><<<nblocks(runs * 32, tpb), tpb, dev::stream_smem_bytes(R), s>>>(
+              c.g->gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+          done = true;
+        }
+      }
+      if (!done) {
+        dev::k_row_dpx<R, DEFER><<<nblocks((uint64_t)L.S * dev::Pairs<R>::G), 256, 0, s>>>(
+            c.g->gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+        done = true;
+      }
     }
   }
   if constexpr (R >= 32) {
@@ -1106,9 +1126,11 @@ struct CallKnobs {
   const TopDev* ts;
   CallKnobs(chsga_ctx& cx, uint32_t row_kernel, uint32_t top_vertices)
       : c(cx), rk(cx.row_kernel), ts(cx.top_sel) {
-    require(row_kernel <= CHSGA_ROW_TILED, CHSGA_ERR_INVALID_ARG, "row_kernel must be CHSGA_ROW_*");
+    require(row_kernel <= CHSGA_ROW_STREAM, CHSGA_ERR_INVALID_ARG, "row_kernel must be CHSGA_ROW_*");
     if (row_kernel == CHSGA_ROW_DIRECT) c.row_kernel = RowKernel::Direct;
     if (row_kernel == CHSGA_ROW_TILED) c.row_kernel = RowKernel::Tiled;
+    if (row_kernel == CHSGA_ROW_DPX) c.row_kernel = RowKernel::Dpx;
+    if (row_kernel == CHSGA_ROW_STREAM) c.row_kernel = RowKernel::Stream;
     c.top_sel = top_for(c, top_vertices);
   }
   ~CallKnobs() {
@@ -1212,8 +1234,9 @@ chsga_batch_opts autotune(chsga_ctx& c, const char* const* reads, const uint32_t
   }
   // row kernel
   cur = best;
-  for (uint32_t rk : {(uint32_t)CHSGA_ROW_DIRECT, (uint32_t)CHSGA_ROW_TILED}) {
+  for (uint32_t rk : {(uint32_t)CHSGA_ROW_DPX, (uint32_t)CHSGA_ROW_DIRECT, (uint32_t)CHSGA_ROW_TILED}) {
     if (rk == CHSGA_ROW_TILED && cur.slots < 32) continue;
+    if (rk == CHSGA_ROW_DPX && cur.slots < 64) continue;  // AUTO already is DPX there
     chsga_batch_opts b = cur;
     b.row_kernel = rk;
     const double g = run(b, 0);
@@ -1527,6 +1550,8 @@ chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out) {
     if (const char* rk = std::getenv("CHSGA_ROW_KERNEL")) {
       if (std::string(rk) == "direct") c->row_kernel = RowKernel::Direct;
       if (std::string(rk) == "tiled") c->row_kernel = RowKernel::Tiled;
+      if (std::string(rk) == "dpx") c->row_kernel = RowKernel::Dpx;
+      if (std::string(rk) == "stream") c->row_kernel = RowKernel::Stream;
     }
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));

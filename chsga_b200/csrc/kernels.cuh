@@ -479,6 +479,7 @@ struct KeyWindow {
   const uint32_t* w;
   uint64_t win;
   uint32_t sh;
+  KeyWindow() = default;
   __device__ __forceinline__ KeyWindow(const uint32_t* lab4, uint32_t c) {
     w = lab4 + (c >> 3);
     win = (uint64_t)__ldg(w) | ((uint64_t)__ldg(w + 1) << 32);
@@ -646,6 +647,260 @@ __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t*
       for (int q = 0; q < 2 * P; ++q) {
         const uint32_t w = __ldg(slot_word + so + q);
         if (w & SW_ENDING) atomicMin(sm_best + so + q, pack_min(bmin[q], barg[q]));
+      }
+    }
+  }
+  if (ending_any) flush_min<R>(sm_best, best);
+}
+
+// ---------------------------------------------------------------------------
+// k_row_stream (R >= 64): k_row_dpx with one warp walking a run of 32
+// consecutive string vertices, whose chars are consecutive too. The warp's
+// previous-row scores stream through a ring of kStreamRing rows in shared
+// memory: every lane copies its own 2P scores of a row with cp.async
+// (kStreamRing rows in flight per lane, one commit group per row) and reads
+// back only what it copied, so no lane waits for another. The next vertex's
+// final first score F and the final last scores of its first two in-edge
+// sources are loaded into registers while the current vertex computes; the
+// run's vertex words and first 64 in-edge sources come in coalesced loads,
+// one vertex per lane, broadcast by shuffles. Every branch depends only on
+// warp-uniform values. Slots on their last row keep one running minimum
+// per warp; chars are visited in increasing order, so a strict comparison
+// keeps the smallest char among equal scores.
+// ---------------------------------------------------------------------------
+// Measured on B200 (6.4 M-char graph, 128 slots): 16 rows in flight per lane
+// with 4-warp blocks, 6 per SM, beat deeper rings (32 or 48 rows take the
+// shared memory the L1 needs for the in-edge and label loads) and 8-warp
+// blocks.
+#ifndef CHSGA_STREAM_RING
+#define CHSGA_STREAM_RING 16  // rows in flight per warp (build-time tuning)
+#endif
+#ifndef CHSGA_STREAM_WARPS
+#define CHSGA_STREAM_WARPS 4  // warps per block (build-time tuning)
+#endif
+#ifndef CHSGA_STREAM_BLOCKS
+#define CHSGA_STREAM_BLOCKS 6  // blocks per SM the register budget is sized for
+#endif
+constexpr int kStreamRing = CHSGA_STREAM_RING;
+constexpr int kStreamWarps = CHSGA_STREAM_WARPS;
+
+__host__ __device__ constexpr size_t stream_smem_bytes(int R) {
+  return (size_t)kStreamWarps * kStreamRing * R * 2;
+}
+
+template <int P>
+__device__ __forceinline__ void cp_async_row(uint16_t* dst, const uint16_t* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_addr(dst)), "l"(src),
+               "n"(4 * P)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int P>
+struct StreamVertex {
+  uint32_t f, len, d, k0, k1;
+  U2<P> F;
+  U2<P> u[2];  // final last scores of the first two in-edge sources
+};
+
+template <int P>
+__device__ __forceinline__ U2<P> lds_u2(const uint16_t* p) {
+  U2<P> o;
+  if constexpr (P == 1) {
+    o.h[0] = *reinterpret_cast<const uint32_t*>(p);
+  } else {
+    const uint2 t = *reinterpret_cast<const uint2*>(p);
+    o.h[0] = t.x;
+    o.h[1] = t.y;
+  }
+  return o;
+}
+
+template <int R, bool DEFER>
+__global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_stream(
+    GraphPtrs g, const uint16_t* __restrict__ D, uint16_t* __restrict__ T, uint16_t* __restrict__ BV,
+    const uint16_t* __restrict__ FL, const uint32_t* __restrict__ slot_word,
+    unsigned long long* __restrict__ best, const StepCtl* __restrict__ ctl) {
+  static_assert(Pairs<R>::G == 32, "one full warp per vertex");
+  constexpr int P = Pairs<R>::P;
+  constexpr int W = kStreamRing;
+  constexpr uint32_t ONES = 0x00010001u;
+  constexpr unsigned FULL = 0xFFFFFFFFu;
+  extern __shared__ __align__(16) uint16_t ring_smem[];
+  __shared__ unsigned long long sm_best[R];
+  const bool ending_any = ctl->any_ending != 0;
+  if (!ctl->any_active) return;
+  if (ending_any) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const uint32_t run = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+  const uint32_t s0 = run * 32;
+  if (s0 < g.S) {
+    const size_t so = (size_t)lane * 2 * P;
+    // this lane's ring: row slot k at ring + k * R (the warp's 32 lanes side by side)
+    uint16_t* ring = ring_smem + (size_t)(threadIdx.x >> 5) * W * R + so;
+    uint32_t dtab[P], imask[P], fmask[P];
+    bool any_fix = false, any_end = false;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      dtab[p] = imask[p] = fmask[p] = 0;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const uint32_t w = __ldg(slot_word + so + 2 * p + h);
+        dtab[p] |= ((0x3Fu & ~(1u << (w & SW_CODE))) & 0x3Fu) << (16 * h);
+        if (w & SW_INIT) imask[p] |= 0xFFFFu << (16 * h);
+        if (DEFER && (w & SW_FIX)) fmask[p] |= 0xFFFFu << (16 * h);
+        any_end |= (w & SW_ENDING) != 0;
+      }
+      any_fix |= fmask[p] != 0;
+    }
+    any_fix = __any_sync(FULL, any_fix);
+    const bool track = ending_any && __any_sync(FULL, any_end);
+    // the run's vertex words, vertex s0 + lane on each lane
+    const uint32_t nv = min(32u, g.S - s0);
+    uint32_t mf = 0, me = 0, md = 0, mk0 = 0, mk1 = 0;
+    if ((uint32_t)lane < nv) {
+      const uint32_t s = s0 + lane;
+      mf = __ldg(g.sv_off + s);
+      me = __ldg(g.sv_off + s + 1);
+      md = __ldg(g.sv_dev + s);
+      mk0 = __ldg(g.vin_off + s);
+      mk1 = __ldg(g.vin_off + s + 1);
+    }
+    const uint32_t cb = __shfl_sync(FULL, mf, 0), ce = __shfl_sync(FULL, me, nv - 1);
+    // previous-row scores of the run's chars cb .. ce-1: row c goes to slot
+    // (c - cb) % W; one commit group per row, empty past the run
+    const uint16_t* dsrc = D + so;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      if (cb + k < ce) cp_async_row<P>(ring + (size_t)k * R, dsrc + (size_t)(cb + k) * R);
+      cp_async_commit();
+    }
+    const uint32_t kb = __shfl_sync(FULL, mk0, 0), ke = __shfl_sync(FULL, mk1, nv - 1);
+    const uint32_t src_a = kb + lane < ke ? __ldg(g.vin_srcv + kb + lane) : 0u;
+    const uint32_t src_b = kb + 32 + lane < ke ? __ldg(g.vin_srcv + kb + 32 + lane) : 0u;
+    // source vertex of in-edge k (k warp-uniform)
+    auto src_at = [&](uint32_t k) -> uint32_t {
+      const uint32_t i = k - kb;
+      const uint32_t a = __shfl_sync(FULL, src_a, i & 31), b = __shfl_sync(FULL, src_b, i & 31);
+      return i < 32 ? a : i < 64 ? b : __ldg(g.vin_srcv + k);
+    };
+    auto prefetch = [&](uint32_t i, StreamVertex<P>& v) {
+      v.f = __shfl_sync(FULL, mf, i);
+      v.len = __shfl_sync(FULL, me, i) - v.f;
+      v.d = __shfl_sync(FULL, md, i);
+      v.k0 = __shfl_sync(FULL, mk0, i);
+      v.k1 = __shfl_sync(FULL, mk1, i);
+#pragma unroll
+      for (int p = 0; p < P; ++p) v.F.h[p] = v.u[0].h[p] = v.u[1].h[p] = 0;
+      if (DEFER && any_fix) v.F = ldp_nc<P>(FL + (size_t)(2 * (s0 + i)) * R + so);
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        if (v.k0 + j < v.k1) v.u[j] = ldp_nc<P>(FL + (size_t)(2 * src_at(v.k0 + j) + 1) * R + so);
+    };
+    // row c from the ring (its copy is the oldest of W pending groups);
+    // refill() then reuses the slot for row c + W once the value is used
+    auto take = [&](uint32_t c) -> U2<P> {
+      cp_async_wait<W - 1>();
+      return lds_u2<P>(ring + (size_t)((c - cb) % W) * R);
+    };
+    auto refill = [&](uint32_t c) {
+      const uint32_t n = c + W;
+      if (n < ce) cp_async_row<P>(ring + (size_t)((c - cb) % W) * R, dsrc + (size_t)n * R);
+      cp_async_commit();
+    };
+    int bmin[2 * P];
+    uint32_t barg[2 * P];
+#pragma unroll
+    for (int q = 0; q < 2 * P; ++q) {
+      bmin[q] = 0x7fffffff;
+      barg[q] = 0;
+    }
+    auto track_char = [&](const U2<P>& t, uint32_t c) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const int lo = (int)(t.h[p] & 0xFFFFu), hi = (int)(t.h[p] >> 16);
+        if (lo < bmin[2 * p]) {
+          bmin[2 * p] = lo;
+          barg[2 * p] = c;
+        }
+        if (hi < bmin[2 * p + 1]) {
+          bmin[2 * p + 1] = hi;
+          barg[2 * p + 1] = c;
+        }
+      }
+    };
+    KeyWindow kw(g.lab4, cb);
+    StreamVertex<P> cur, nxt;
+    prefetch(0, cur);
+    for (uint32_t i = 0; i < nv; ++i) {
+      if (i + 1 < nv) prefetch(i + 1, nxt);
+      const uint32_t f = cur.f, len = cur.len;
+      const U2<P> F = cur.F;
+      U2<P> t, dprev = take(f);
+      // first char: min(D[f] + 1, min over in-edges of last(u) + delta)
+      {
+        const uint32_t key = kw.next();
+        uint32_t delta[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          delta[p] = (dtab[p] >> key) & ONES;
+          if (DEFER && any_fix) dprev.h[p] = sel(__vminu2(dprev.h[p], F.h[p]), dprev.h[p], fmask[p]);
+          t.h[p] = dprev.h[p] + ONES;
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+          if (cur.k0 + j < cur.k1)
+#pragma unroll
+            for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(cur.u[j].h[p], delta[p], t.h[p]);
+        for (uint32_t k = cur.k0 + 2; k < cur.k1; ++k) {
+          const U2<P> du = ldp_nc<P>(FL + (size_t)(2 * src_at(k) + 1) * R + so);
+#pragma unroll
+          for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(du.h[p], delta[p], t.h[p]);
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) t.h[p] = sel(delta[p], t.h[p], imask[p]);
+      }
+      refill(f);
+      stp<P>(T + (size_t)f * R + so, t);
+      stp<P>(BV + (size_t)(2 * cur.d) * R + so, t);
+      if (track) track_char(t, f);
+      // chain chars
+      for (uint32_t q = 1; q < len; ++q) {
+        const uint32_t c = f + q;
+        U2<P> dq = take(c);
+        const uint32_t key = kw.next();
+        const uint32_t off2 = q * ONES;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const uint32_t delta = (dtab[p] >> key) & ONES;
+          if (DEFER && any_fix)
+            dq.h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq.h[p]), dq.h[p], fmask[p]);
+          uint32_t x = __viaddmin_u16x2(t.h[p], ONES, dq.h[p] + ONES);
+          x = __viaddmin_u16x2(dprev.h[p], delta, x);
+          t.h[p] = sel(delta, x, imask[p]);
+        }
+        dprev = dq;
+        refill(c);
+        stp<P>(T + (size_t)c * R + so, t);
+        if (track) track_char(t, c);
+      }
+      if (len > 1) stp<P>(BV + (size_t)(2 * cur.d + 1) * R + so, t);
+      cur = nxt;
+    }
+    cp_async_wait<0>();
+    if (track) {
+#pragma unroll
+      for (int q = 0; q < 2 * P; ++q) {
+        const uint32_t w = __ldg(slot_word + so + q);
+        if ((w & SW_ENDING) && bmin[q] != 0x7fffffff)
+          atomicMin(sm_best + so + q, pack_min(bmin[q], barg[q]));
       }
     }
   }

@@ -235,11 +235,21 @@ typedef struct {
                              by the one-CTA-per-slot top kernel, the levels below one grid
                              launch each; 0 = 23000 (the most shared memory holds) */
 } chsga_batch_opts;
-/* Row kernels: AUTO = the packed 16-bit DPX kernel when rows are 16-bit,
- * slots >= 2 and no string vertex label exceeds 512 chars, else DIRECT;
- * DIRECT = one thread group per string vertex; TILED = shared-memory tiles
- * of consecutive string vertices staged by TMA bulk copies (slots >= 32). */
-enum { CHSGA_ROW_AUTO = 0, CHSGA_ROW_DIRECT = 1, CHSGA_ROW_TILED = 2 };
+/* Row kernels. With 16-bit rows, slots >= 2 and no string vertex label over
+ * 512 chars, AUTO runs STREAM for slots >= 64 and DPX below, else DIRECT.
+ * DIRECT = one thread group per string vertex, 16- or 32-bit rows;
+ * TILED = shared-memory tiles of consecutive string vertices staged by TMA
+ * bulk copies (slots >= 32); DPX = two 16-bit scores per register on the
+ * DPX min/add units, one thread group per string vertex; STREAM = DPX with
+ * one warp per run of 32 consecutive string vertices, loading the next
+ * vertex's inputs while the current one computes (slots >= 64). */
+enum {
+  CHSGA_ROW_AUTO = 0,
+  CHSGA_ROW_DIRECT = 1,
+  CHSGA_ROW_TILED = 2,
+  CHSGA_ROW_DPX = 3,
+  CHSGA_ROW_STREAM = 4
+};
 chsga_status chsga_align_scores_batched(chsga_ctx* ctx, const char* const* reads,
                                         const uint32_t* lens, uint32_t n,
                                         const chsga_batch_opts* opts, int32_t* scores_out);

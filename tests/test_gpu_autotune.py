@@ -22,14 +22,33 @@ def _mix(g, seed, n):
             for i, L in enumerate(lens)]
 
 
-@pytest.mark.parametrize("row_kernel", [cb.ROW_AUTO, cb.ROW_DIRECT, cb.ROW_TILED])
-@pytest.mark.parametrize("top_vertices", [0, 2000, 300])
-def test_knobs_keep_scores(small_graph, ctx, row_kernel, top_vertices):
+@pytest.mark.parametrize("row_kernel", [cb.ROW_AUTO, cb.ROW_DIRECT, cb.ROW_TILED, cb.ROW_DPX,
+                                        cb.ROW_STREAM])
+@pytest.mark.parametrize("top_vertices", [0, 300])
+@pytest.mark.parametrize("slots", [32, 128])
+def test_knobs_keep_scores(small_graph, ctx, row_kernel, top_vertices, slots):
     g = small_graph[0]
     reads = _mix(g, 3, 40)
     want = ctx.align_scores(reads)
-    got = ctx.align_scores_batched(reads, slots=32, row_kernel=row_kernel, top_vertices=top_vertices)
+    got = ctx.align_scores_batched(reads, slots=slots, row_kernel=row_kernel,
+                                   top_vertices=top_vertices)
     np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("row_kernel", [cb.ROW_DPX, cb.ROW_STREAM])
+def test_row_kernels_on_long_vertices(tmp_path, row_kernel):
+    # vertices up to 300 chars (several prefetch blocks), N in the reads
+    from conftest import gen_graph
+    g, files = gen_graph(tmp_path, "lv", backbone_len=6000, seed=17, vlen_min=40, vlen_max=300,
+                         bubble_gap_mean=30.0, p_snp=0.3, p_indel=0.3, p_alt=0.4, alt_min=20,
+                         alt_max=200)
+    reads = g.gen_reads(64, 18, 20, 800, sub_rate=0.04, indel_rate=0.03, n_rate=0.01).to_list()
+    c = cb.Context(0).load(g)
+    want = c.align_scores(reads)
+    for slots in (64, 128):
+        got = c.align_scores_batched(reads, slots=slots, row_kernel=row_kernel)
+        np.testing.assert_array_equal(got, want)
+    c.close()
 
 
 def test_autotune_picks_a_correct_config(small_graph, ctx):
