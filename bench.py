@@ -13,8 +13,9 @@ completion through the slot-interleaved engine (score-only, int32).
           time (CUDA events around the device sequence, reads resident)
   e2e     batched + served: the same K batches streamed through the serving
           loop (chsga_server_submit / _poll with host buffers: reads copied
-          in, scores copied out, continuous batching across batches), cells
-          / wall time from the first submit to the last result
+          in, scores copied out, continuous batching across batches, longest
+          waiting read admitted first), cells / wall time from the first
+          submit to the last result
   served  a Poisson arrival stream at ~80% of that capacity (80% 150 bp at
           1% error, 20% log-uniform 1-10 kbp at 5%): p50/p99 latency from
           submission to result, and the cost model's per-read time error
@@ -397,7 +398,8 @@ def main():
     wall = time.perf_counter() - t0
     # batched + served: the same batches streamed through the serving loop
     srv = cb.Server(ctx, slots=opts["slots"], steps_per_graph=opts["steps_per_graph"],
-                    queue_capacity=4096, arena_bytes=64 << 20, tb_workers=1)
+                    queue_capacity=4096, arena_bytes=64 << 20, tb_workers=1,
+                    order=cb.ORDER_LONGEST)
     barrier()
     t1 = time.perf_counter()
     for b in batches:

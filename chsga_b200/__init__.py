@@ -31,6 +31,7 @@ OK, ERR_INVALID_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, \
 OP_DELETE, OP_MATCHSUB, OP_INSERT = 0, 1, 2
 REQ_SCORE, REQ_TRACEBACK = 0, 1
 FP_PLAN, FP_MODEL, FP_ANALYTIC = 0, 1, 2
+ORDER_FIFO, ORDER_LONGEST = 0, 1
 ROW_AUTO, ROW_DIRECT, ROW_TILED, ROW_DPX, ROW_STREAM = 0, 1, 2, 3, 4
 FLAG_PROFILE = 1
 NOALLOC_SCRATCH_BYTES = 32 << 20  # CHSGA_NOALLOC_SCRATCH_BYTES
@@ -144,7 +145,7 @@ class ServerOpts(C.Structure):
                 ("queue_capacity", C.c_uint32), ("tb_workers", C.c_uint32),
                 ("arena_bytes", C.c_uint64), ("hbm_budget_bytes", C.c_uint64), ("tb_k", C.c_int64),
                 ("tb_cap_bytes", C.c_uint64), ("row_bits", C.c_uint32), ("max_pending", C.c_uint32),
-                ("cost_model", C.c_void_p), ("footprint", C.c_uint32), ("pad", C.c_uint32)]
+                ("cost_model", C.c_void_p), ("footprint", C.c_uint32), ("order", C.c_uint32)]
 
 
 class ServerResult(C.Structure):

@@ -134,6 +134,7 @@ struct chsga_server {
   std::mutex cm_mu;  // the cost model is not re-entrant
   std::condition_variable cv_engine, cv_tb, cv_done;
   std::deque<Request> pend_score, pend_tb;
+  bool pend_dirty = false;  // score requests arrived since the last ordering
   std::deque<chsga_server_result> done;
   bool stop = false;
   chsga_status broken = CHSGA_OK;  // the score lane failed: score requests fail with this
@@ -198,6 +199,12 @@ struct chsga_server {
     std::vector<Request> batch;
     {
       std::lock_guard<std::mutex> lk(mu);
+      if (o.order == CHSGA_ORDER_LONGEST && pend_dirty) {
+        std::stable_sort(pend_score.begin(), pend_score.end(), [](const Request& a, const Request& b) {
+          return a.read.size() > b.read.size();
+        });
+        pend_dirty = false;
+      }
       uint64_t bytes = 0;
       while (!pend_score.empty() && batch.size() < free_ids.size()) {
         const uint64_t b = round_up(pend_score.front().read.size(), 16);
@@ -402,6 +409,7 @@ chsga_status chsga_server_open(chsga_ctx* ctx, const chsga_server_opts* opts, ch
     if (!o.row_bits) o.row_bits = 16;
     if (!o.max_pending) o.max_pending = 1u << 20;
     require(o.footprint <= CHSGA_FP_ANALYTIC, CHSGA_ERR_INVALID_ARG, "footprint must be CHSGA_FP_*");
+    require(o.order <= CHSGA_ORDER_LONGEST, CHSGA_ERR_INVALID_ARG, "order must be CHSGA_ORDER_*");
     require(o.footprint != CHSGA_FP_MODEL || o.cost_model, CHSGA_ERR_INVALID_ARG,
             "CHSGA_FP_MODEL needs a cost model");
     require(o.tb_workers <= 16, CHSGA_ERR_INVALID_ARG, "at most 16 traceback workers");
@@ -482,6 +490,7 @@ chsga_status chsga_server_submit(chsga_server* s, const char* read, uint32_t len
     }
     if (mode == CHSGA_REQ_SCORE) {
       s->pend_score.push_back(std::move(q));
+      s->pend_dirty = true;
       s->cv_engine.notify_all();
     } else {
       s->pend_tb.push_back(std::move(q));

@@ -404,8 +404,13 @@ typedef struct {
   uint32_t max_pending;      /* requests waiting for admission before submit says BUSY; 0 = 2^20 */
   struct chsga_cost_model* cost_model; /* predicts traceback time and footprint (may be NULL) */
   uint32_t footprint;        /* projection used for admission, CHSGA_FP_*; 0 = PLAN */
-  uint32_t pad;
+  uint32_t order;            /* admission order of waiting score reads, CHSGA_ORDER_*; 0 = FIFO */
 } chsga_server_opts;
+
+/* FIFO: arrival order (latency-fair). LONGEST: the longest waiting read
+ * first (throughput: long reads start early and the engine does not end a
+ * stream with a few long reads running alone in mostly idle slots). */
+enum { CHSGA_ORDER_FIFO = 0, CHSGA_ORDER_LONGEST = 1 };
 
 /* How a traceback request's device footprint is projected for admission:
  * PLAN     the allocation plan of the traceback (full matrix, or the

@@ -26,13 +26,14 @@ def _mix(g, seed, n, lo, hi):
     return g.gen_reads(n, seed, lo, hi, sub_rate=0.03, indel_rate=0.02, n_rate=0.005).to_list()
 
 
-def test_server_scores_equal_plain_and_oracle(small_graph, ctx, oracle_small):
+@pytest.mark.parametrize("order", [cb.ORDER_FIFO, cb.ORDER_LONGEST])
+def test_server_scores_equal_plain_and_oracle(small_graph, ctx, oracle_small, order):
     g, files, reads = small_graph
     mix = list(reads) + _mix(g, 41, 60, 20, 1500) + [b""]
     want = ctx.align_scores(mix)
     np.testing.assert_array_equal(want[:-1], oracle_small.scores(mix[:-1]))
     # fewer result slots than reads: ids and queue entries are reused
-    srv = cb.Server(ctx, slots=32, queue_capacity=64, arena_bytes=1 << 20)
+    srv = cb.Server(ctx, slots=32, queue_capacity=64, arena_bytes=1 << 20, order=order)
     tickets = [srv.submit(r) for r in mix]
     res = srv.collect()
     st = srv.stats()
