@@ -461,8 +461,10 @@ def main():
         row_avg_s = pr["row_ms"] / max(1, pr["row_launches"]) / 1e3
         peak, src = measured_peak()
         ab = algorithmic_row_bytes(st, R, multi, pr["row_bits"] // 8)
-        kname = {cb.ROW_DIRECT: "k_row_direct", cb.ROW_TILED: "k_row_tiled"}.get(
-            opts["row_kernel"], "k_row_dpx" if pr["row_bits"] == 16 else "k_row_direct")
+        auto16 = "k_row_stream" if R >= 64 else "k_row_dpx"
+        kname = {cb.ROW_DIRECT: "k_row_direct", cb.ROW_TILED: "k_row_tiled", cb.ROW_DPX: "k_row_dpx",
+                 cb.ROW_STREAM: "k_row_stream"}.get(
+            opts["row_kernel"], auto16 if pr["row_bits"] == 16 else "k_row_direct")
         tr = ncu_traffic()
         total = pr["row_ms"] + pr["sweep_up_ms"] + pr["top_ms"] + pr["sweep_down_ms"] + pr["other_ms"]
         line["roofline"] = {
