@@ -58,6 +58,11 @@ def parse():
     p.add_argument("--no-profile", action="store_true")
     p.add_argument("--no-tune", action="store_true", help="skip the autotuner (use --slots)")
     p.add_argument("--served-s", type=float, default=12.0, help="Poisson arrival window, seconds")
+    p.add_argument("--backbone", type=int, default=0,
+                   help="backbone length of the config-2-mix graph (0 = 5 Mbp); for small profiling captures")
+    p.add_argument("--kernels-only", action="store_true",
+                   help="time the batched steps only (no server, served run, plain sample, profiled "
+                        "pass or CPU baseline): the command profiling captures run under ncu")
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
     return p.parse_args()
 
@@ -115,9 +120,12 @@ class Clocks:
                 "samples": len(self.rows)}
 
 
-def make_graph():
+def make_graph(backbone=0):
     import chsga_b200 as cb
-    g = cb.HostGraph.generate(**cb.GRAPH_CONFIGS["cfg2"])
+    cfg = dict(cb.GRAPH_CONFIGS["cfg2"])
+    if backbone:
+        cfg["backbone_len"] = backbone
+    g = cb.HostGraph.generate(**cfg)
     g.build_pch()
     return g
 
@@ -278,7 +286,7 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    g = make_graph()
+    g = make_graph(args.backbone)
     st = g.stats()
     N = st["num_chars"]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -342,7 +350,7 @@ def main():
     import numpy as np
 
     import chsga_b200 as cb
-    g = make_graph()
+    g = make_graph(args.backbone)
     st = g.stats()
     N = st["num_chars"]
     multi = st["num_strings"] - st["single_char_strings"]
@@ -396,21 +404,23 @@ def main():
         a, d = ctx.read_times(len(b))
         lat.extend(((d - a).astype(np.float64) / 1e6).tolist())
     wall = time.perf_counter() - t0
-    # batched + served: the same batches streamed through the serving loop
-    srv = cb.Server(ctx, slots=opts["slots"], steps_per_graph=opts["steps_per_graph"],
-                    queue_capacity=4096, arena_bytes=64 << 20, tb_workers=1,
-                    order=cb.ORDER_LONGEST)
-    barrier()
-    t1 = time.perf_counter()
-    for b in batches:
-        for r in b:
-            srv.submit(r)
-    got = 0
-    while got < len(batches) * args.batch:
-        got += len(srv.poll(4096, 100))
-    srv_wall = time.perf_counter() - t1
-    sst = srv.stats()
-    srv.close()
+    srv_wall, sst = wall, {"gpu_launches": 0}
+    if not args.kernels_only:
+        # batched + served: the same batches streamed through the serving loop
+        srv = cb.Server(ctx, slots=opts["slots"], steps_per_graph=opts["steps_per_graph"],
+                        queue_capacity=4096, arena_bytes=64 << 20, tb_workers=1,
+                        order=cb.ORDER_LONGEST)
+        barrier()
+        t1 = time.perf_counter()
+        for b in batches:
+            for r in b:
+                srv.submit(r)
+        got = 0
+        while got < len(batches) * args.batch:
+            got += len(srv.poll(4096, 100))
+        srv_wall = time.perf_counter() - t1
+        sst = srv.stats()
+        srv.close()
     barrier()
     ck = clocks.stop()
     dev_s = max_over_ranks(dev_ms / 1e3)
@@ -438,7 +448,9 @@ def main():
     }
     if tune:
         line["autotune"] = tune
-    if rank == 0:
+    if args.kernels_only:
+        line["e2e"]["what"] = "kernels-only run: wall time of the batched calls"
+    if rank == 0 and not args.kernels_only:
         # plain one-read-per-launch path on a sample of the first batch
         sample = sorted(batches[0], key=len)[: max(2, min(6, len(batches[0])))]
         ctx.align_scores(sample)
@@ -449,7 +461,7 @@ def main():
         line["batched_over_plain"] = value / line["plain"]["value"]
         line["served_over_plain"] = e2e / line["plain"]["value"]
         line["served"] = served_run(cb, ctx, g, N, opts, e2e, args.served_s)
-    if rank == 0 and not args.no_profile:
+    if rank == 0 and not args.no_profile and not args.kernels_only:
         # profiled pass: CUDA events around every kernel group of every row-step
         pctx = cb.Context(local, flags=cb.FLAG_PROFILE)
         pctx.load(g)
