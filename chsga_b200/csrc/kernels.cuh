@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "device_graph.hpp"  // tile limits shared with the host-side tile builder
 
@@ -804,16 +805,28 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
       for (int j = 0; j < 2; ++j)
         if (v.k0 + j < v.k1) v.u[j] = ldp_nc<P>(FL + (size_t)(2 * src_at(v.k0 + j) + 1) * R + so);
     };
-    // row c from the ring (its copy is the oldest of W pending groups);
-    // refill() then reuses the slot for row c + W once the value is used
-    auto take = [&](uint32_t c) -> U2<P> {
+    // The char stream cb .. ce-1: `slot` is the ring row of the current char
+    // (its copy is the oldest of W pending groups), `gnext` the global row
+    // W chars ahead that refills the slot once the current value is used,
+    // `left` how many chars remain to be fetched, `tp` the current char's
+    // row of T.
+    uint16_t* slot = ring;
+    uint16_t* const ring_end = ring + (size_t)W * R;
+    const uint16_t* gnext = dsrc + (size_t)(cb + W) * R;
+    int32_t left = (int32_t)(ce - cb) - W;
+    uint16_t* tp = T + (size_t)cb * R + so;
+    auto take = [&]() -> U2<P> {
       cp_async_wait<W - 1>();
-      return lds_u2<P>(ring + (size_t)((c - cb) % W) * R);
+      return lds_u2<P>(slot);
     };
-    auto refill = [&](uint32_t c) {
-      const uint32_t n = c + W;
-      if (n < ce) cp_async_row<P>(ring + (size_t)((c - cb) % W) * R, dsrc + (size_t)n * R);
+    auto refill = [&]() {
+      if (left > 0) cp_async_row<P>(slot, gnext);
       cp_async_commit();
+      gnext += R;
+      --left;
+      slot += R;
+      if (slot == ring_end) slot = ring;
+      tp += R;
     };
     int bmin[2 * P];
     uint32_t barg[2 * P];
@@ -839,61 +852,69 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
     KeyWindow kw(g.lab4, cb);
     StreamVertex<P> cur, nxt;
     prefetch(0, cur);
-    for (uint32_t i = 0; i < nv; ++i) {
-      if (i + 1 < nv) prefetch(i + 1, nxt);
-      const uint32_t f = cur.f, len = cur.len;
-      const U2<P> F = cur.F;
-      U2<P> t, dprev = take(f);
-      // first char: min(D[f] + 1, min over in-edges of last(u) + delta)
-      {
-        const uint32_t key = kw.next();
-        uint32_t delta[P];
+    // the vertex loop, once with and once without the last-row minimum
+    auto run = [&](auto track_tag) {
+      constexpr bool TRACK = decltype(track_tag)::value;
+      for (uint32_t i = 0; i < nv; ++i) {
+        if (i + 1 < nv) prefetch(i + 1, nxt);
+        const uint32_t f = cur.f, len = cur.len;
+        const U2<P> F = cur.F;
+        U2<P> t, dprev = take();
+        // first char: min(D[f] + 1, min over in-edges of last(u) + delta)
+        {
+          const uint32_t key = kw.next();
+          uint32_t delta[P];
 #pragma unroll
-        for (int p = 0; p < P; ++p) {
-          delta[p] = (dtab[p] >> key) & ONES;
-          if (DEFER && any_fix) dprev.h[p] = sel(__vminu2(dprev.h[p], F.h[p]), dprev.h[p], fmask[p]);
-          t.h[p] = dprev.h[p] + ONES;
+          for (int p = 0; p < P; ++p) {
+            delta[p] = (dtab[p] >> key) & ONES;
+            if (DEFER && any_fix) dprev.h[p] = sel(__vminu2(dprev.h[p], F.h[p]), dprev.h[p], fmask[p]);
+            t.h[p] = dprev.h[p] + ONES;
+          }
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            if (cur.k0 + j < cur.k1)
+#pragma unroll
+              for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(cur.u[j].h[p], delta[p], t.h[p]);
+          for (uint32_t k = cur.k0 + 2; k < cur.k1; ++k) {
+            const U2<P> du = ldp_nc<P>(FL + (size_t)(2 * src_at(k) + 1) * R + so);
+#pragma unroll
+            for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(du.h[p], delta[p], t.h[p]);
+          }
+#pragma unroll
+          for (int p = 0; p < P; ++p) t.h[p] = sel(delta[p], t.h[p], imask[p]);
         }
+        stp<P>(tp, t);
+        stp<P>(BV + (size_t)(2 * cur.d) * R + so, t);
+        if (TRACK) track_char(t, f);
+        refill();
+        // chain chars: off2 = q in both halves
+        uint32_t off2 = 0;
+        for (uint32_t q = 1; q < len; ++q) {
+          U2<P> dq = take();
+          const uint32_t key = kw.next();
+          off2 += ONES;
 #pragma unroll
-        for (int j = 0; j < 2; ++j)
-          if (cur.k0 + j < cur.k1)
-#pragma unroll
-            for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(cur.u[j].h[p], delta[p], t.h[p]);
-        for (uint32_t k = cur.k0 + 2; k < cur.k1; ++k) {
-          const U2<P> du = ldp_nc<P>(FL + (size_t)(2 * src_at(k) + 1) * R + so);
-#pragma unroll
-          for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(du.h[p], delta[p], t.h[p]);
+          for (int p = 0; p < P; ++p) {
+            const uint32_t delta = (dtab[p] >> key) & ONES;
+            if (DEFER && any_fix)
+              dq.h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq.h[p]), dq.h[p], fmask[p]);
+            uint32_t x = __viaddmin_u16x2(t.h[p], ONES, dq.h[p] + ONES);
+            x = __viaddmin_u16x2(dprev.h[p], delta, x);
+            t.h[p] = sel(delta, x, imask[p]);
+          }
+          dprev = dq;
+          stp<P>(tp, t);
+          if (TRACK) track_char(t, f + q);
+          refill();
         }
-#pragma unroll
-        for (int p = 0; p < P; ++p) t.h[p] = sel(delta[p], t.h[p], imask[p]);
+        if (len > 1) stp<P>(BV + (size_t)(2 * cur.d + 1) * R + so, t);
+        cur = nxt;
       }
-      refill(f);
-      stp<P>(T + (size_t)f * R + so, t);
-      stp<P>(BV + (size_t)(2 * cur.d) * R + so, t);
-      if (track) track_char(t, f);
-      // chain chars
-      for (uint32_t q = 1; q < len; ++q) {
-        const uint32_t c = f + q;
-        U2<P> dq = take(c);
-        const uint32_t key = kw.next();
-        const uint32_t off2 = q * ONES;
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-          const uint32_t delta = (dtab[p] >> key) & ONES;
-          if (DEFER && any_fix)
-            dq.h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq.h[p]), dq.h[p], fmask[p]);
-          uint32_t x = __viaddmin_u16x2(t.h[p], ONES, dq.h[p] + ONES);
-          x = __viaddmin_u16x2(dprev.h[p], delta, x);
-          t.h[p] = sel(delta, x, imask[p]);
-        }
-        dprev = dq;
-        refill(c);
-        stp<P>(T + (size_t)c * R + so, t);
-        if (track) track_char(t, c);
-      }
-      if (len > 1) stp<P>(BV + (size_t)(2 * cur.d + 1) * R + so, t);
-      cur = nxt;
-    }
+    };
+    if (track)
+      run(std::true_type{});
+    else
+      run(std::false_type{});
     cp_async_wait<0>();
     if (track) {
 #pragma unroll
