@@ -197,6 +197,26 @@ HostLayout build_layout(const chsga_graph_host& g) {
   };
   flatten(up, L.up_off, L.up_in);
   flatten(dn, L.dn_off, L.dn_in);
+  auto heads = [&](const std::vector<uint32_t>& off, const std::vector<EdgeW>& in,
+                   std::vector<uint32_t>& h) {
+    h.assign((size_t)4 * S, 0);
+    for (uint32_t d = 0; d < S; ++d) {
+      h[4 * d] = off[d];
+      h[4 * d + 1] = off[d + 1];
+      if (off[d + 1] > off[d]) {
+        h[4 * d + 2] = (uint32_t)in[off[d]].src;
+        h[4 * d + 3] = (uint32_t)in[off[d]].w;
+      }
+    }
+  };
+  heads(L.up_off, L.up_in, L.up_head);
+  heads(L.dn_off, L.dn_in, L.dn_head);
+  L.fin.assign((size_t)4 * S, 0);
+  for (uint32_t d = 0; d < S; ++d) {
+    L.fin[4 * d] = L.dv_first[d];
+    L.fin[4 * d + 1] = L.dv_len[d];
+    L.fin[4 * d + 2] = L.dv_s[d];
+  }
   // levels in hierarchy order
   L.lvl_off.push_back(0);
   for (uint32_t d = 1; d < S; ++d)

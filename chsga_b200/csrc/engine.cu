@@ -92,6 +92,7 @@ struct GraphDev {
   DevArr<uint32_t> up_off, dn_off, istr_off, istr_src;
   DevArr<uint32_t> dv_s;
   DevArr<int2> up_in, dn_in;
+  DevArr<uint4> dn_head, up_head, fin;
 };
 
 struct TopDev {
@@ -426,8 +427,8 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   for (uint32_t l = 0; l < fl; ++l) {
     if (L.lvl_up_edges[l] == 0) continue;
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
-    dev::k_pull<R, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-        BVc, lo, hi, c.g->gd.up_off.p, c.g->gd.up_in.p, 0, b.ctl.p);
+    dev::k_pull_lv<R, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
+        BVc, lo, hi, c.g->gd.up_head.p, c.g->gd.up_in.p, b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[2], s));
   if (top.h.K) {
@@ -588,11 +589,20 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   for (size_t i = 0; i < dn.size(); ++i) dn[i] = make_int2(L.dn_in[i].src, L.dn_in[i].w);
   d.up_in.upload(up, s);
   d.dn_in.upload(dn, s);
+  auto to4 = [](const std::vector<uint32_t>& v) {
+    std::vector<uint4> o(v.size() / 4);
+    std::memcpy(o.data(), v.data(), o.size() * sizeof(uint4));
+    return o;
+  };
+  d.dn_head.upload(to4(L.dn_head), s);
+  d.up_head.upload(to4(L.up_head), s);
+  d.fin.upload(to4(L.fin), s);
   auto top = make_top(L, d, kTopMaxVertices, s);
   lg->gp = dev::GraphPtrs{L.N,          L.S,          L.special,    d.lab2.p,     d.lab_sp.p,
                           d.lab4.p,     d.sv_off.p,   d.sv_dev.p,   d.vin_off.p,  d.vin_src.p,
                           d.vin_srcv.p, d.dv_first.p, d.dv_len.p,   d.dv_s.p,     d.up_off.p,
-                          d.up_in.p,    d.dn_off.p,   d.dn_in.p,    d.istr_off.p, d.istr_src.p};
+                          d.up_in.p,    d.dn_off.p,   d.dn_in.p,    d.istr_off.p, d.istr_src.p,
+                          d.dn_head.p,  d.up_head.p,  d.fin.p};
   lg->nul_label = false;
   for (uint32_t i = 0; i < g.num_chars && !lg->nul_label; ++i) lg->nul_label = g.labels[i] == '\0';
   lg->pitch = ((size_t)L.N + 15) / 16 * 16;

@@ -56,6 +56,12 @@ struct GraphPtrs {
   const int2* dn_in;
   const uint32_t* istr_off;
   const uint32_t* istr_src;
+  // per hierarchy position: {list begin, list end, first source, first
+  // weight} of the down / up pull lists, and {first char, length, string
+  // vertex, 0} -- one 16-byte load each instead of a chain of word loads
+  const uint4* dn_head;
+  const uint4* up_head;
+  const uint4* fin;
 };
 
 // Per-slot word for the current row-step, written by k_advance.
@@ -1239,6 +1245,46 @@ __global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, 
 }
 
 // ---------------------------------------------------------------------------
+// k_pull_lv: one upward level [lo, hi) below the top region, the k_pull
+// update with the list head of each position in one 16-byte load (the
+// first source is gathered without waiting for an edge load).
+// ---------------------------------------------------------------------------
+template <int R, typename ST>
+__global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t lo, uint32_t hi,
+                                                 const uint4* __restrict__ head,
+                                                 const int2* __restrict__ edges,
+                                                 const StepCtl* __restrict__ ctl) {
+  constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
+  if (!ctl->any_active) return;
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  const int lane = (int)(gt % G);
+  if (d >= hi) return;
+  const uint4 h = __ldg(head + d);
+  if (h.x == h.y) return;
+  const size_t so = (size_t)lane * V;
+  ST* p = BV + (size_t)(2 * d) * R + so;
+  IV<V> f = ld<V>(p);
+  bool changed = false;
+  auto relax = [&](const IV<V>& x, int w) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const int c = x.v[v] + w;
+      if (c < f.v[v]) {
+        f.v[v] = c;
+        changed = true;
+      }
+    }
+  };
+  relax(ld_nc<V>(BV + (size_t)h.z * R + so), (int)h.w);
+  for (uint32_t k = h.x + 1; k < h.y; ++k) {
+    const int2 ew = __ldg(edges + k);
+    relax(ld_nc<V>(BV + (size_t)ew.x * R + so), ew.y);
+  }
+  if (changed) st<V>(p, f);
+}
+
+// ---------------------------------------------------------------------------
 // k_down: positions [lo, hi). Those below `mid` first pull their downward
 // in-edges (sources on higher levels, final); every position then finalises
 // its vertex's chars: if the first score fell below the row value, write it
@@ -1266,32 +1312,39 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
   if (d < hi) {
     const size_t so = (size_t)lane * V;
     ST* p = BV + (size_t)(2 * d) * R + so;
+    // independent loads first: the list head, the vertex words, the first
+    // score and the raw last score (the last entry is never written here;
+    // for a one-char vertex it is unused)
+    const uint4 h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
+    const uint4 m = __ldg(g.fin + d);
     IV<V> f = ld<V>(p);
-    if (d < mid) {
-      const uint32_t k0 = __ldg(g.dn_off + d), k1 = __ldg(g.dn_off + d + 1);
+    const IV<V> raw = ld<V>(BV + (size_t)(2 * d + 1) * R + so);
+    if (h.y > h.x) {
       bool changed = false;
-      for (uint32_t k = k0; k < k1; ++k) {
-        const int2 ew = __ldg(g.dn_in + k);
-        const IV<V> x = ld_nc<V>(BV + (size_t)ew.x * R + so);
+      auto relax = [&](const IV<V>& x, int w) {
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-          const int c = x.v[v] + ew.y;
+          const int c = x.v[v] + w;
           if (c < f.v[v]) {
             f.v[v] = c;
             changed = true;
           }
         }
+      };
+      relax(ld_nc<V>(BV + (size_t)h.z * R + so), (int)h.w);
+      for (uint32_t k = h.x + 1; k < h.y; ++k) {
+        const int2 ew = __ldg(g.dn_in + k);
+        relax(ld_nc<V>(BV + (size_t)ew.x * R + so), ew.y);
       }
       if (changed) st<V>(p, f);
     }
-    const uint32_t first = __ldg(g.dv_first + d), len = __ldg(g.dv_len + d);
+    const uint32_t first = m.x, len = m.y;
     {
       // final first and last scores of the vertex, in char order, for the
       // next row-step (the last char ends at min(raw last, F + len - 1))
-      const uint32_t sv = __ldg(g.dv_s + d);
+      const uint32_t sv = m.z;
       IV<V> lf = f;
       if (len > 1) {
-        const IV<V> raw = ld<V>(BV + (size_t)(2 * d + 1) * R + so);
 #pragma unroll
         for (int v = 0; v < V; ++v) lf.v[v] = min(raw.v[v], f.v[v] + (int)(len - 1));
       }
