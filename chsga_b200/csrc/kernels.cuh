@@ -1409,13 +1409,17 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
 // scores of the region are staged in shared memory; the region's upward
 // levels (low -> high) and downward levels (high -> low) then run as a
 // sequence of edge chunks, each chunk a contiguous array of
-// {target << 16 | source, weight} that thread 0 brings into one of two shared
-// buffers with a bulk copy while the block relaxes the previous chunk
-// (atomic min into the target's first score). A chunk never spans two
-// levels and ends with a block barrier, so every level sees its sources
-// final. Edges from below the region were applied by k_pull before launch.
+// {target << 16 | source, weight} that thread 0 brings into one of
+// kTopBufs shared buffers with a bulk copy, kTopBufs - 1 chunks ahead of
+// the one the block relaxes (atomic min into the target's first score).
+// Every thread reads the next chunk's edge count while the current one
+// runs, so no global load sits between two chunks. A chunk never spans
+// two levels and ends with a block barrier, so every level sees its
+// sources final. Edges from below the region were applied by k_pull
+// before launch.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kTopChunk = 1024;  // edges per chunk (8 KiB)
+constexpr uint32_t kTopBufs = 4;      // chunk buffers (copies in flight + the one in use)
 
 struct TopPtrs {
   uint32_t K0, K, nchunks;
@@ -1425,7 +1429,7 @@ struct TopPtrs {
 };
 
 __host__ __device__ constexpr size_t top_smem_bytes(uint32_t K) {
-  return ((size_t)(2 * K + 2) * 4 + 15) / 16 * 16 + 2 * kTopChunk * 8 + 16;
+  return ((size_t)(2 * K + 2) * 4 + 15) / 16 * 16 + kTopBufs * kTopChunk * 8 + kTopBufs * 8;
 }
 
 template <int R, typename ST>
@@ -1438,19 +1442,19 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
   if (!(slot_word[r] & SW_CLOSURE)) return;
   int* sm = reinterpret_cast<int*>(top_smem);  // [2j] first, [2j+1] last, [2K] scratch
   int2* ebuf = reinterpret_cast<int2*>(top_smem + ((size_t)(2 * t.K + 2) * 4 + 15) / 16 * 16);
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(ebuf + 2 * kTopChunk);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(ebuf + kTopBufs * kTopChunk);
   if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (uint32_t b = 0; b < kTopBufs; ++b) mbar_init(&bar[b], 1);
     fence_async_shared();
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (uint32_t c = 0; c < 2 && c < t.nchunks; ++c) {
+    for (uint32_t c = 0; c < kTopBufs && c < t.nchunks; ++c) {
       const int2 ch = t.chunk[c];
       bulk_load(ebuf + c * kTopChunk, t.edges + ch.x, (uint32_t)ch.y * 8, &bar[c]);
     }
   }
+  int n_next = t.nchunks ? __ldg(&t.chunk[0].y) : 0;
   // stage the region's scores (independent loads, unrolled)
   const size_t K0 = t.K0;
   for (uint32_t j0 = threadIdx.x; j0 < t.K; j0 += 4 * blockDim.x) {
@@ -1487,11 +1491,12 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
   __syncthreads();
   uint32_t c = 0;
   for (; c < t.nchunks; ++c) {
-    const uint32_t b = c & 1;
+    const uint32_t b = c % kTopBufs;
+    const int n = n_next;
+    if (c + 1 < t.nchunks) n_next = __ldg(&t.chunk[c + 1].y);
     // a thread whose wait expires flags it and still reaches the barrier
     // below, so the whole block leaves the loop together
-    if (!mbar_wait(&bar[b], (c >> 1) & 1)) s_fail = 1;
-    const int n = t.chunk[c].y;
+    if (!mbar_wait(&bar[b], (c / kTopBufs) & 1)) s_fail = 1;
     const int2* e = ebuf + b * kTopChunk;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const int2 x = e[i];
@@ -1499,9 +1504,9 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
     }
     __syncthreads();
     if (s_fail) break;
-    if (threadIdx.x == 0 && c + 2 < t.nchunks) {
+    if (threadIdx.x == 0 && c + kTopBufs < t.nchunks) {
       fence_async_shared();
-      const int2 ch = t.chunk[c + 2];
+      const int2 ch = t.chunk[c + kTopBufs];
       bulk_load(ebuf + b * kTopChunk, t.edges + ch.x, (uint32_t)ch.y * 8, &bar[b]);
     }
   }
@@ -1510,7 +1515,8 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
     // before the shared memory is released
     if (threadIdx.x == 0) {
       atomicOr(&ctl->error, ERR_TOP_WAIT);
-      for (uint32_t k = c; k < c + 2 && k < t.nchunks; ++k) mbar_wait(&bar[k & 1], (k >> 1) & 1);
+      for (uint32_t k = c; k < c + kTopBufs && k < t.nchunks; ++k)
+        mbar_wait(&bar[k % kTopBufs], (k / kTopBufs) & 1);
     }
     __syncthreads();
     return;
