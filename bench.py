@@ -152,6 +152,24 @@ def algorithmic_row_bytes(st, slots, multi, score_bytes):
             + 3 * N / 8 + 12 * S + 4 * e_first)
 
 
+def algorithmic_sweep_bytes(st, lay, slots, score_bytes):
+    """Bytes per row-step of the grid-wide sweep kernels below the top
+    region (16-byte pull-list heads and vertex words, w bytes per score):
+    up (k_pull_lv): per target its head, first score read and written, one
+    gathered score per edge, 8 bytes per edge after the first;
+    down (k_down): per position its vertex words, first and raw last score
+    read, final first and last written to FL; per target below the top its
+    head, first score written, one gathered score per edge, 8 bytes per edge
+    after the first."""
+    S = st["num_strings"]
+    wr = score_bytes * slots
+    ut, ue = lay["sweep_up_targets"], lay["sweep_up_edges"]
+    dt, de = lay["sweep_down_targets"], lay["sweep_down_edges"]
+    up = ut * (16 + 2 * wr) + ue * wr + (ue - ut) * 8
+    down = S * (16 + 4 * wr) + dt * (16 + wr) + de * wr + (de - dt) * 8
+    return up, down
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -489,6 +507,19 @@ def main():
             "traffic_source": tr.get("source") if tr else None,
             "kernel_share": {k: pr[k] / total for k in
                              ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")},
+        }
+        # sweep kernels below the top region (default top region of the layout)
+        lay = g.check_layout(R, 16, opts["top_vertices"])
+        up_b, down_b = algorithmic_sweep_bytes(st, lay, R, pr["row_bits"] // 8)
+        up_s = pr["sweep_up_ms"] / max(1, pr["row_launches"]) / 1e3
+        down_s = pr["sweep_down_ms"] / max(1, pr["row_launches"]) / 1e3
+        line["roofline"]["sweeps"] = {
+            "k_pull_lv": {"algorithmic_bytes_per_step": up_b, "avg_step_ms": up_s * 1e3,
+                          "achieved": up_b / up_s / 1e9, "frac": up_b / up_s / 1e9 / peak},
+            "k_down": {"algorithmic_bytes_per_step": down_b, "avg_step_ms": down_s * 1e3,
+                       "achieved": down_b / down_s / 1e9, "frac": down_b / down_s / 1e9 / peak},
+            "top_region": "levels >= %d (%d vertices) run in k_top, latency-bound" % (
+                lay["top_first_level"], lay["top_vertices"]),
         }
         line["cpu_baseline"] = cpu_baseline(g, batches[0], args.cpu_sample_s)
     if rank == 0:

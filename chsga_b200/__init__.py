@@ -95,7 +95,8 @@ class GraphStats(C.Structure):
 class LayoutStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in (
         "num_levels", "top_first_level", "top_vertices", "tiled", "tiles", "long_tiles",
-        "slot_bytes", "slots_per_block", "smem_bytes")]
+        "slot_bytes", "slots_per_block", "smem_bytes", "sweep_up_targets", "sweep_up_edges",
+        "sweep_down_targets", "sweep_down_edges")]
 
 
 class OptsT(C.Structure):
@@ -187,7 +188,7 @@ _sig("chsga_graph_write_files", C.c_int32, vp, C.c_char_p)
 _sig("chsga_gen_graph", C.c_int32, C.POINTER(GenGraphCfg), C.POINTER(vp))
 _sig("chsga_build_pch", C.c_int32, vp, C.POINTER(PchOpts))
 _sig("chsga_graph_get_stats", C.c_int32, vp, C.POINTER(GraphStats))
-_sig("chsga_check_layout", C.c_int32, vp, C.c_uint32, C.c_uint32, C.POINTER(LayoutStats))
+_sig("chsga_check_layout", C.c_int32, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(LayoutStats))
 _sig("chsga_reads_load", C.c_int32, C.c_char_p, C.c_uint64, C.POINTER(vp))
 _sig("chsga_reads_from_arrays", C.c_int32, C.c_char_p, u64p, C.c_uint64, C.POINTER(vp))
 _sig("chsga_reads_count", C.c_uint64, vp)
@@ -353,10 +354,10 @@ class HostGraph:
         _check(_lib.chsga_graph_get_stats(self._h, C.byref(s)))
         return {k: int(getattr(s, k)) for k, _ in GraphStats._fields_}
 
-    def check_layout(self, slots: int, row_bits: int) -> dict:
+    def check_layout(self, slots: int, row_bits: int, top_vertices: int = 0) -> dict:
         """Host-side pre-flight of the device layout (chsga_check_layout)."""
         st = LayoutStats()
-        _check(_lib.chsga_check_layout(self._h, slots, row_bits, C.byref(st)))
+        _check(_lib.chsga_check_layout(self._h, slots, row_bits, top_vertices, C.byref(st)))
         return {k: int(getattr(st, k)) for k, _ in LayoutStats._fields_}
 
     def view(self) -> GraphHostT:

@@ -209,8 +209,19 @@ HostLayout build_layout(const chsga_graph_host& g) {
       }
     }
   };
-  heads(L.up_off, L.up_in, L.up_head);
   heads(L.dn_off, L.dn_in, L.dn_head);
+  // upward lists average about two edges: their head carries the first two
+  // (8 words: begin, end, src0, w0, src1, w1, 0, 0)
+  L.up_head.assign((size_t)8 * S, 0);
+  for (uint32_t d = 0; d < S; ++d) {
+    uint32_t* h = &L.up_head[(size_t)8 * d];
+    h[0] = L.up_off[d];
+    h[1] = L.up_off[d + 1];
+    for (uint32_t j = 0; j < 2 && L.up_off[d] + j < L.up_off[d + 1]; ++j) {
+      h[2 + 2 * j] = (uint32_t)L.up_in[L.up_off[d] + j].src;
+      h[3 + 2 * j] = (uint32_t)L.up_in[L.up_off[d] + j].w;
+    }
+  }
   L.fin.assign((size_t)4 * S, 0);
   for (uint32_t d = 0; d < S; ++d) {
     L.fin[4 * d] = L.dv_first[d];

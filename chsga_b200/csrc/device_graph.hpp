@@ -55,7 +55,8 @@ struct HostLayout {
   std::vector<uint32_t> dv_first, dv_len, dv_s;  // by hierarchy order
   std::vector<uint32_t> up_off, dn_off;    // S+1, by hierarchy order
   std::vector<EdgeW> up_in, dn_in;
-  std::vector<uint32_t> dn_head, up_head;  // 4 words per position: begin, end, first src, first w
+  std::vector<uint32_t> dn_head;  // 4 words per position: begin, end, first src, first w
+  std::vector<uint32_t> up_head;  // 8 words per position: begin, end, src0, w0, src1, w1, 0, 0
   std::vector<uint32_t> fin;               // 4 words per position: first char, length, string vertex, 0
   std::vector<uint32_t> lvl_off;           // levels+1
   std::vector<uint32_t> lvl_up_edges;      // per level: number of up_in entries

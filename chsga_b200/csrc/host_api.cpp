@@ -197,6 +197,7 @@ chsga_status chsga_gen_reads(const chsga_host_graph* g, const chsga_gen_reads_cf
 }
 
 chsga_status chsga_check_layout(const chsga_host_graph* g, uint32_t slots, uint32_t row_bits,
+                                uint32_t top_vertices,
                                 chsga_layout_stats* out) {
   return guarded([&] {
     require(g && out, CHSGA_ERR_INVALID_ARG, "null argument");
@@ -207,9 +208,17 @@ chsga_status chsga_check_layout(const chsga_host_graph* g, uint32_t slots, uint3
     HostLayout L = build_layout(v);
     std::memset(out, 0, sizeof(*out));
     out->num_levels = L.levels;
-    HostTop top = build_top(L, 23000, 1024);
+    require(top_vertices <= 23000, CHSGA_ERR_INVALID_ARG, "top_vertices above 23000");
+    HostTop top = build_top(L, top_vertices ? top_vertices : 23000, 1024);
     out->top_first_level = top.first_level;
     out->top_vertices = top.K;
+    for (uint32_t d = 0; d < top.K0; ++d) {
+      const uint32_t nu = L.up_off[d + 1] - L.up_off[d], nd = L.dn_off[d + 1] - L.dn_off[d];
+      out->sweep_up_targets += nu > 0;
+      out->sweep_up_edges += nu;
+      out->sweep_down_targets += nd > 0;
+      out->sweep_down_edges += nd;
+    }
     if (slots >= 32) {
       HostRowTiles t = build_row_tiles(L, slots, row_bits / 8);
       validate_row_tiles(L, slots, row_bits / 8, t);

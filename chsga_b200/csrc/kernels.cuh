@@ -57,8 +57,9 @@ struct GraphPtrs {
   const uint32_t* istr_off;
   const uint32_t* istr_src;
   // per hierarchy position: {list begin, list end, first source, first
-  // weight} of the down / up pull lists, and {first char, length, string
-  // vertex, 0} -- one 16-byte load each instead of a chain of word loads
+  // weight} of the down pull list; two uint4 {begin, end, src0, w0},
+  // {src1, w1, 0, 0} of the up pull list; and {first char, length, string
+  // vertex, 0} -- 16-byte loads instead of a chain of word loads
   const uint4* dn_head;
   const uint4* up_head;
   const uint4* fin;
@@ -1246,8 +1247,8 @@ __global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, 
 
 // ---------------------------------------------------------------------------
 // k_pull_lv: one upward level [lo, hi) below the top region, the k_pull
-// update with the list head of each position in one 16-byte load (the
-// first source is gathered without waiting for an edge load).
+// update with the list head of each position in two 16-byte loads (the
+// first two sources are gathered without waiting for an edge load).
 // ---------------------------------------------------------------------------
 template <int R, typename ST>
 __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t lo, uint32_t hi,
@@ -1260,8 +1261,9 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
   const uint32_t d = lo + (uint32_t)(gt / G);
   const int lane = (int)(gt % G);
   if (d >= hi) return;
-  const uint4 h = __ldg(head + d);
+  const uint4 h = __ldg(head + 2 * (size_t)d);
   if (h.x == h.y) return;
+  const uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
   const size_t so = (size_t)lane * V;
   ST* p = BV + (size_t)(2 * d) * R + so;
   IV<V> f = ld<V>(p);
@@ -1276,8 +1278,15 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
       }
     }
   };
-  relax(ld_nc<V>(BV + (size_t)h.z * R + so), (int)h.w);
-  for (uint32_t k = h.x + 1; k < h.y; ++k) {
+  const IV<V> x0 = ld_nc<V>(BV + (size_t)h.z * R + so);
+  if (h.y - h.x > 1) {
+    const IV<V> x1 = ld_nc<V>(BV + (size_t)h2.x * R + so);
+    relax(x0, (int)h.w);
+    relax(x1, (int)h2.y);
+  } else {
+    relax(x0, (int)h.w);
+  }
+  for (uint32_t k = h.x + 2; k < h.y; ++k) {
     const int2 ew = __ldg(edges + k);
     relax(ld_nc<V>(BV + (size_t)ew.x * R + so), ew.y);
   }

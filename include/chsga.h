@@ -179,8 +179,12 @@ typedef struct {
   uint64_t num_levels, top_first_level, top_vertices;
   uint64_t tiled;            /* 1 if the tile-staged row kernel applies */
   uint64_t tiles, long_tiles, slot_bytes, slots_per_block, smem_bytes;
+  /* below the top region: positions with a non-empty upward / downward pull
+   * list and the edges of those lists (the grid-wide sweep kernels' work) */
+  uint64_t sweep_up_targets, sweep_up_edges, sweep_down_targets, sweep_down_edges;
 } chsga_layout_stats;
 chsga_status chsga_check_layout(const chsga_host_graph* g, uint32_t slots, uint32_t row_bits,
+                                uint32_t top_vertices /* 0 = 23000, as chsga_batch_opts */,
                                 chsga_layout_stats* out);
 
 const char* chsga_last_error_global(void);
