@@ -34,6 +34,7 @@ FP_PLAN, FP_MODEL, FP_ANALYTIC = 0, 1, 2
 ORDER_FIFO, ORDER_LONGEST = 0, 1
 ROW_AUTO, ROW_DIRECT, ROW_TILED, ROW_DPX, ROW_STREAM = 0, 1, 2, 3, 4
 FLAG_PROFILE = 1
+FLAG_MATCH_N = 2
 NOALLOC_SCRATCH_BYTES = 32 << 20  # CHSGA_NOALLOC_SCRATCH_BYTES
 
 u64p = C.POINTER(C.c_uint64)

@@ -1,5 +1,6 @@
 // Drop-in for ConSGA_mismatchN_dag (src/ConSGA.cpp): score-only alignment of
-// every read against the graph, printed as the reference prints it.
+// every read against the graph, printed as the reference prints it. Built a
+// second time with -DCHSGA_MATCH_N as ConSGA_matchN_dag (matchN scoring).
 //
 //   ConSGA_mismatchN_dag -I char.adj -i string.adj -c string.out
 //                        -r reads -l char.labels -o string.label_offsets
@@ -50,6 +51,7 @@ int main(int argc, char** argv) {
   if (s != CHSGA_OK) cli::die("Cannot load inputs", chsga_last_error_global());
   chsga_opts o{};
   o.device = (int)cli::env_u64("CHSGA_DEVICE", 0);
+  o.flags = cli::scoring_flags();
   chsga_ctx* ctx = nullptr;
   cli::check(chsga_open(&o, &ctx), nullptr, "chsga_open");
   auto t_ch = std::chrono::steady_clock::now();

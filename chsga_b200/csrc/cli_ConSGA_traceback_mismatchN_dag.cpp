@@ -1,4 +1,5 @@
 // Drop-in for ConSGA_traceback_mismatchN_dag (src/ConSGA_traceback.cpp).
+// Built a second time with -DCHSGA_MATCH_N as ConSGA_traceback_matchN_dag.
 //
 //   ConSGA_traceback_mismatchN_dag [-b] -I char.adj -i string.adj -c string.out
 //       -r reads -l char.labels -o string.label_offsets [-k rows] [-d dir]
@@ -57,6 +58,7 @@ int main(int argc, char** argv) {
   chsga_graph_view(g, &view);
   chsga_opts o{};
   o.device = (int)cli::env_u64("CHSGA_DEVICE", 0);
+  o.flags = cli::scoring_flags();
   o.hbm_cap_bytes = cli::env_u64("CHSGA_HBM_CAP_BYTES", 0);
   chsga_ctx* ctx = nullptr;
   cli::check(chsga_open(&o, &ctx), nullptr, "chsga_open");
@@ -135,6 +137,8 @@ int main(int argc, char** argv) {
         path_score += 1;
         read_pos = (int)op.row;
       } else if (op.op == CHSGA_OP_MATCHSUB) {
+        // byte equality, as the reference's check (ConSGA_traceback.cpp:198-199),
+        // in its matchN build too: an N-matched step counts as a substitution
         path_score += view.labels[op.vertex] == rd[op.row] ? 0 : 1;
         read_pos = (int)op.row;
       } else {

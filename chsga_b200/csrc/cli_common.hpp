@@ -74,4 +74,15 @@ inline void check(chsga_status s, chsga_ctx* ctx, const char* what) {
   if (s != CHSGA_OK) die(what, ctx ? chsga_last_error(ctx) : chsga_last_error_global());
 }
 
+// Scoring of this binary: the ConSGA_*matchN_dag builds define
+// CHSGA_MATCH_N (the reference's ALPHABET_SIZE=4), the *mismatchN_dag builds
+// do not (ALPHABET_SIZE=5).
+inline uint32_t scoring_flags() {
+#ifdef CHSGA_MATCH_N
+  return CHSGA_FLAG_MATCH_N;
+#else
+  return 0;
+#endif
+}
+
 }  // namespace cli

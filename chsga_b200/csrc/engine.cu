@@ -143,6 +143,7 @@ struct LoadedGraph {
   std::unique_ptr<TopDev> top;
   size_t pitch = 0;  // traceback matrix row stride (elements), 16-byte aligned rows
   bool nul_label = false;
+  bool n_label = false;  // some label byte is 'N'
 };
 }  // namespace chsga
 
@@ -183,6 +184,15 @@ using dev::Lanes;
 unsigned nblocks(uint64_t items, unsigned tpb = 256) { return (unsigned)((items + tpb - 1) / tpb); }
 
 void set_device(chsga_ctx& c) { CK(cudaSetDevice(c.device)); }
+
+// 1 when the context scores with matchN (an 'N' matches every base).
+int match_n(const chsga_ctx& c) { return (c.flags & CHSGA_FLAG_MATCH_N) ? 1 : 0; }
+
+// Score of a length-0 read: row 0 against the byte '\0' (the reference
+// reads read[0] of an empty string), 0 if some label matches it.
+int32_t empty_score(const chsga_ctx& c) {
+  return (c.g->nul_label || (match_n(c) && c.g->n_label)) ? 0 : 1;
+}
 
 void check_launch() { CK(cudaGetLastError()); }
 
@@ -350,7 +360,7 @@ template <int R>
 void launch_advance(chsga_ctx& c, SlotBufs& b, int prime, cudaStream_t s) {
   dev::k_advance<R><<<1, 128, 0, s>>>(b.slots.p, c.queue.p, c.reads.p, b.best.p, c.res_score.p,
                                       c.res_vertex.p, c.res_t0.p, c.res_t1.p, b.word.p, b.ctl.p,
-                                      c.g->L.special, prime, c.qmask, c.done_ring.p);
+                                      c.g->L.special, prime, c.qmask, c.done_ring.p, match_n(c));
   check_launch();
 }
 
@@ -604,7 +614,10 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
                           d.up_in.p,    d.dn_off.p,   d.dn_in.p,    d.istr_off.p, d.istr_src.p,
                           d.dn_head.p,  d.up_head.p,  d.fin.p};
   lg->nul_label = false;
-  for (uint32_t i = 0; i < g.num_chars && !lg->nul_label; ++i) lg->nul_label = g.labels[i] == '\0';
+  for (uint32_t i = 0; i < g.num_chars; ++i) {
+    lg->nul_label |= g.labels[i] == '\0';
+    lg->n_label |= g.labels[i] == 'N';
+  }
   lg->pitch = ((size_t)L.N + 15) / 16 * 16;
   lg->L = std::move(L);
   lg->top = std::move(top);
@@ -626,7 +639,7 @@ void scores_with(chsga_ctx& c, const char* const* reads, const uint32_t* lens, u
   uint64_t rows = 0;
   for (uint32_t i = 0; i < n; ++i) {
     if (lens[i] == 0) {
-      out[i] = c.g->nul_label ? 0 : 1;
+      out[i] = empty_score(c);
       continue;
     }
     rp.push_back(reads[i]);
@@ -693,7 +706,8 @@ void walk(chsga_ctx& c, const int* M, int64_t lo, int64_t hi, uint32_t start, ui
   ops.alloc(max_ops);
   DevArr<dev::WalkOut> out;
   out.alloc(1);
-  dev::k_walk<<<1, 1, 0, c.st>>>(c.g->gp, M, c.g->pitch, lo, hi, start, c.reads.p, ops.p, max_ops, out.p);
+  dev::k_walk<<<1, 1, 0, c.st>>>(c.g->gp, M, c.g->pitch, lo, hi, start, c.reads.p, ops.p, max_ops, out.p,
+                                 match_n(c));
   check_launch();
   dev::WalkOut h{};
   CK(cudaMemcpyAsync(&h, out.p, sizeof(h), cudaMemcpyDeviceToHost, c.st));
@@ -1047,7 +1061,8 @@ void noalloc_row_step(chsga_ctx& c, const NoallocBufs& b, const uint16_t* D, uin
     }
   }
   dev::k_advance<1><<<1, 128, 0, s>>>(b.slots, b.queue, b.reads, b.best, b.res_score, b.res_vertex,
-                                      b.res_t0, b.res_t1, b.word, b.ctl, L.special, 0);
+                                      b.res_t0, b.res_t1, b.word, b.ctl, L.special, 0, 0xFFFFFFFFu,
+                                      nullptr, match_n(c));
   check_launch();
 }
 
@@ -1113,11 +1128,11 @@ void scores_noalloc(chsga_ctx& c, const char* const* reads, const uint32_t* lens
     // admit the first read, then one row per step: `total` steps finish every read
     dev::k_advance<1><<<1, 128, 0, s>>>(b.slots, b.queue, b.reads, b.best, b.res_score,
                                         b.res_vertex, b.res_t0, b.res_t1, b.word, b.ctl,
-                                        c.g->L.special, 0);
+                                        c.g->L.special, 0, 0xFFFFFFFFu, nullptr, match_n(c));
     check_launch();
     for (uint64_t k = 0; k < total; ++k) noalloc_row_step(c, b, b.rows[k & 1], b.rows[(k + 1) & 1]);
   }
-  k_noalloc_finish<<<nblocks(n), 256, 0, s>>>(b.slot_of, b.res_score, n, c.g->nul_label ? 0 : 1, b.out);
+  k_noalloc_finish<<<nblocks(n), 256, 0, s>>>(b.slot_of, b.res_score, n, empty_score(c), b.out);
   check_launch();
   dev::StepCtl fin{};
   CK(cudaMemcpyAsync(&fin, b.ctl, sizeof(fin), cudaMemcpyDeviceToHost, s));
@@ -1492,7 +1507,7 @@ uint64_t traceback_device_bytes(const chsga_ctx& c, uint32_t len, const chsga_tb
 
 uint64_t graph_chars(const chsga_ctx& c) { return c.g->L.N; }
 uint64_t graph_string_vertices(const chsga_ctx& c) { return c.g->L.S; }
-int32_t empty_read_score(const chsga_ctx& c) { return c.g->nul_label ? 0 : 1; }
+int32_t empty_read_score(const chsga_ctx& c) { return empty_score(c); }
 
 void bind_device(const chsga_ctx& c) { CK(cudaSetDevice(c.device)); }
 

@@ -72,6 +72,8 @@ constexpr uint32_t SW_CLOSURE = 1u << 9;    // row >= 1: hierarchy closure appli
 constexpr uint32_t SW_ENDING = 1u << 10;    // last row of the read: reduce its minimum
 constexpr uint32_t SW_ACTIVE = 1u << 11;
 constexpr uint32_t SW_FIX = 1u << 12;      // row >= 2: previous row had a closure to apply
+constexpr uint32_t SW_MASK_SHIFT = 16;     // bits 16..20: mismatch mask over label keys
+constexpr uint32_t SW_MASK = 0x1Fu;
 
 struct SlotState {
   unsigned long long off;  // first base of the read in the device read buffer
@@ -239,6 +241,17 @@ __device__ __forceinline__ uint32_t base_code(int b, int special) {
   }
 }
 
+// Bit k set: a label of key k (0..3 A,C,G,T, 4 the special byte) scores a
+// substitution against read byte b, i.e. match_sub (csr_align.hpp:41-50):
+// mismatchN (ALPHABET_SIZE 5) matches equal bytes only; matchN
+// (ALPHABET_SIZE 4, match_n != 0) also matches an 'N' on either side.
+__device__ __forceinline__ uint32_t mismatch_mask(int b, int special, int match_n) {
+  if (match_n && b == 'N') return 0u;
+  uint32_t m = SW_MASK & ~(1u << base_code(b, special));
+  if (match_n && special == 'N') m &= ~(1u << 4);
+  return m;
+}
+
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -344,7 +357,7 @@ __global__ void __launch_bounds__(256, 3) k_row_direct(GraphPtrs g, const ST* __
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const uint32_t w = __ldg(slot_word + lane * V + v);
-      code[v] = w & SW_CODE;
+      code[v] = (w >> SW_MASK_SHIFT) & SW_MASK;  // mismatch mask
       init[v] = (w & SW_INIT) != 0;
       ending[v] = (w & SW_ENDING) != 0;
       fix[v] = DEFER && (w & SW_FIX) != 0;
@@ -373,7 +386,7 @@ __global__ void __launch_bounds__(256, 3) k_row_direct(GraphPtrs g, const ST* __
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         if (DEFER) dprev.v[v] = min(dprev.v[v], F.v[v]);
-        delta[v] = key == code[v] ? 0 : 1;
+        delta[v] = (int)((code[v] >> key) & 1u);
         t.v[v] = dprev.v[v] + 1;
       }
       const uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
@@ -406,7 +419,7 @@ __global__ void __launch_bounds__(256, 3) k_row_direct(GraphPtrs g, const ST* __
 #pragma unroll
           for (int v = 0; v < V; ++v) {
             if (DEFER) dq[k].v[v] = min(dq[k].v[v], F.v[v] + (int)(c - f));
-            const int delta = key == code[v] ? 0 : 1;
+            const int delta = (int)((code[v] >> key) & 1u);
             int x = min(dq[k].v[v] + 1, dprev.v[v] + delta);
             x = min(x, t.v[v] + 1);
             if (init[v]) x = delta;
@@ -593,8 +606,7 @@ __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t*
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const uint32_t w = __ldg(slot_word + so + 2 * p + h);
-        const uint32_t code = w & SW_CODE;
-        dtab[p] |= ((0x3Fu & ~(1u << code)) & 0x3Fu) << (16 * h);
+        dtab[p] |= ((w >> SW_MASK_SHIFT) & SW_MASK) << (16 * h);
         if (w & SW_INIT) imask[p] |= 0xFFFFu << (16 * h);
         if (DEFER && (w & SW_FIX)) fmask[p] |= 0xFFFFu << (16 * h);
         any_end |= (w & SW_ENDING) != 0;
@@ -761,7 +773,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const uint32_t w = __ldg(slot_word + so + 2 * p + h);
-        dtab[p] |= ((0x3Fu & ~(1u << (w & SW_CODE))) & 0x3Fu) << (16 * h);
+        dtab[p] |= ((w >> SW_MASK_SHIFT) & SW_MASK) << (16 * h);
         if (w & SW_INIT) imask[p] |= 0xFFFFu << (16 * h);
         if (DEFER && (w & SW_FIX)) fmask[p] |= 0xFFFFu << (16 * h);
         any_end |= (w & SW_ENDING) != 0;
@@ -1081,7 +1093,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_row_tiled(GraphPtrs g, RowTi
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const uint32_t w = __ldg(slot_word + so + v);
-      code[v] = w & SW_CODE;
+      code[v] = (w >> SW_MASK_SHIFT) & SW_MASK;  // mismatch mask
       init[v] = (w & SW_INIT) != 0;
       ending[v] = (w & SW_ENDING) != 0;
       fix[v] = DEFER && (w & SW_FIX) != 0;
@@ -1137,7 +1149,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_row_tiled(GraphPtrs g, RowTi
 #pragma unroll
           for (int v = 0; v < V; ++v) {
             if (DEFER) dprev.v[v] = min(dprev.v[v], F.v[v]);
-            delta[v] = key == code[v] ? 0 : 1;
+            delta[v] = (int)((code[v] >> key) & 1u);
             tv.v[v] = dprev.v[v] + 1;
           }
           for (uint32_t q = 0; q < ec; ++q) {
@@ -1174,7 +1186,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_row_tiled(GraphPtrs g, RowTi
 #pragma unroll
               for (int v = 0; v < V; ++v) {
                 if (DEFER) dq[q].v[v] = min(dq[q].v[v], F.v[v] + (int)(q0 + q));
-                const int delta = key == code[v] ? 0 : 1;
+                const int delta = (int)((code[v] >> key) & 1u);
                 int x = min(dq[q].v[v] + 1, dprev.v[v] + delta);
                 x = min(x, tv.v[v] + 1);
                 if (init[v]) x = delta;
@@ -1567,7 +1579,8 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
                                                  uint32_t* __restrict__ slot_word,
                                                  StepCtl* __restrict__ ctl, int special,
                                                  int prime, uint32_t qmask = 0xFFFFFFFFu,
-                                                 CompletionRec* __restrict__ done_ring = nullptr) {
+                                                 CompletionRec* __restrict__ done_ring = nullptr,
+                                                 int match_n = 0) {
   __shared__ uint32_t s_need[128];
   __shared__ uint32_t s_base, s_take, s_active, s_ending;
   const int r = threadIdx.x;
@@ -1624,7 +1637,9 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
     }
     uint32_t w = 0;
     if (st.id >= 0) {
-      w = base_code(reads[st.off + st.row], special) | SW_ACTIVE;
+      const int byte = reads[st.off + st.row];
+      w = base_code(byte, special) | (mismatch_mask(byte, special, match_n) << SW_MASK_SHIFT) |
+          SW_ACTIVE;
       w |= st.row == 0 ? SW_INIT : SW_CLOSURE;
       if (st.row >= 2) w |= SW_FIX;
       if (st.row + 1 == st.len) w |= SW_ENDING;
@@ -1666,7 +1681,8 @@ struct WalkOp {
 
 __global__ void k_walk(GraphPtrs g, const int* __restrict__ M, size_t pitch, long long row_lo,
                        long long row_hi, uint32_t start, const unsigned char* __restrict__ read,
-                       WalkOp* __restrict__ ops, uint32_t max_ops, WalkOut* __restrict__ out) {
+                       WalkOp* __restrict__ ops, uint32_t max_ops, WalkOut* __restrict__ out,
+                       int match_n) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const size_t N = pitch;
   uint32_t cur = start;
@@ -1710,7 +1726,7 @@ __global__ void k_walk(GraphPtrs g, const int* __restrict__ M, size_t pitch, lon
     if (op == 255 && Pw[cur] + 1 == s) op = 0;
     if (op == 255) {
       const uint32_t key = label_key(g, cur);
-      const int delta = key == base_code(read[row], g.special) ? 0 : 1;
+      const int delta = (int)((mismatch_mask(read[row], g.special, match_n) >> key) & 1u);
       if (cur > first) {
         if (Pw[cur - 1] + delta == s) {
           op = 1;

@@ -200,7 +200,14 @@ typedef struct {
   uint64_t hbm_cap_bytes;  /* byte cap for the full score matrix; 0 = 85% of free HBM */
   uint32_t flags;          /* CHSGA_FLAG_* */
 } chsga_opts;
-enum { CHSGA_FLAG_PROFILE = 1u /* per-phase CUDA-event timing into chsga_profile */ };
+enum {
+  CHSGA_FLAG_PROFILE = 1u, /* per-phase CUDA-event timing into chsga_profile */
+  /* matchN scoring, the reference's ALPHABET_SIZE=4 builds (ConSGA_matchN_dag,
+   * ConSGA_traceback_matchN_dag): an 'N' in the read or in a label matches
+   * every base (csr_align.hpp:45-46). Default: mismatchN, ALPHABET_SIZE=5,
+   * where only equal bytes match. */
+  CHSGA_FLAG_MATCH_N = 2u
+};
 
 /* Context with its own streams. One context per host thread. */
 chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out);

@@ -160,7 +160,14 @@ Pch read_pch(const std::string& p) {
   return g;
 }
 
-inline LogScore match_sub(char a, char b) { return a == b ? 0 : 1; }  // csr_align.hpp:41-50, ALPHABET_SIZE 5
+// csr_align.hpp:41-50: ALPHABET_SIZE 5 (mismatchN, this build by default)
+// matches equal bytes only; ALPHABET_SIZE 4 (matchN, built with
+// -DORACLE_MATCH_N) also matches an 'N' on either side.
+#ifdef ORACLE_MATCH_N
+inline LogScore match_sub(char a, char b) { return (a == 'N' || b == 'N' || a == b) ? 0 : 1; }
+#else
+inline LogScore match_sub(char a, char b) { return a == b ? 0 : 1; }
+#endif
 
 inline void cas_min(LogScore* t, LogScore nv) {  // csr_align.hpp:386-402
   LogScore prev = __atomic_load_n(t, __ATOMIC_RELAXED);

@@ -19,10 +19,15 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "bin", "libconsga_oracle.so")
+ORACLE_MATCHN_SO = os.path.join(HERE, "bin", "libconsga_oracle_matchN.so")
 REF_FAST_SO = os.path.join(HERE, "_ref", "libref_fast.so")
 REF_CKPT_SO = os.path.join(HERE, "_ref", "libref_ckpt.so")
+REF_FAST_MATCHN_SO = os.path.join(HERE, "_ref", "libref_fast_matchN.so")
+REF_CKPT_MATCHN_SO = os.path.join(HERE, "_ref", "libref_ckpt_matchN.so")
 REF_CONSGA = os.path.join(HERE, "_ref", "ConSGA_mismatchN_dag")
 REF_CONSGA_TB = os.path.join(HERE, "_ref", "ConSGA_traceback_mismatchN_dag")
+REF_CONSGA_MATCHN = os.path.join(HERE, "_ref", "ConSGA_matchN_dag")
+REF_CONSGA_TB_MATCHN = os.path.join(HERE, "_ref", "ConSGA_traceback_matchN_dag")
 REFERENCE_TREE = "/root/reference"
 
 u64p = C.POINTER(C.c_uint64)
@@ -40,7 +45,9 @@ def build(with_ref: Optional[bool] = None) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "-j8"] + targets, check=True)
 
 
-def ref_available() -> bool:
+def ref_available(match_n: bool = False) -> bool:
+    if match_n:
+        return os.path.exists(REF_FAST_MATCHN_SO) and os.path.exists(REF_CKPT_MATCHN_SO)
     return os.path.exists(REF_FAST_SO) and os.path.exists(REF_CKPT_SO)
 
 
@@ -59,8 +66,8 @@ def _pack(reads: Sequence[bytes]):
 class Oracle:
     """The restatement (consga_oracle.cpp) over the five ConSGA input files."""
 
-    def __init__(self, files, threads: int = 0):
-        self.lib = C.CDLL(ORACLE_SO)
+    def __init__(self, files, threads: int = 0, match_n: bool = False):
+        self.lib = C.CDLL(ORACLE_MATCHN_SO if match_n else ORACLE_SO)
         L = self.lib
         L.oracle_load.argtypes = [C.c_char_p] * 5 + [C.POINTER(C.c_void_p)]
         L.oracle_last_error.restype = C.c_char_p
@@ -129,8 +136,11 @@ class Oracle:
 class RefHarness:
     """The reference's own align.hpp / traceback.hpp (oracle/_ref)."""
 
-    def __init__(self, files, checkpointed: bool = False, threads: int = 0):
-        self.lib = C.CDLL(REF_CKPT_SO if checkpointed else REF_FAST_SO)
+    def __init__(self, files, checkpointed: bool = False, threads: int = 0, match_n: bool = False):
+        if match_n:
+            self.lib = C.CDLL(REF_CKPT_MATCHN_SO if checkpointed else REF_FAST_MATCHN_SO)
+        else:
+            self.lib = C.CDLL(REF_CKPT_SO if checkpointed else REF_FAST_SO)
         L = self.lib
         L.ref_load.argtypes = [C.c_char_p] * 5 + [C.POINTER(C.c_void_p)]
         L.ref_last_error.restype = C.c_char_p
@@ -186,16 +196,19 @@ class RefHarness:
             self.h = None
 
 
-def rescore(ops: np.ndarray, read: bytes, labels: bytes) -> tuple:
+def rescore(ops: np.ndarray, read: bytes, labels: bytes, match_n: bool = False) -> tuple:
     """The verification of src/ConSGA_traceback.cpp:190-209: path score under
-    the fixed costs and the last read row the path consumes."""
+    the fixed costs and the last read row the path consumes; match_n scores
+    substitutions as the ALPHABET_SIZE=4 build (csr_align.hpp:45-46)."""
     score, read_pos = 0, -1
+    N = ord("N")
     for row, v, op in ops:
         if op == 0:
             score += 1
             read_pos = int(row)
         elif op == 1:
-            score += 0 if labels[int(v)] == read[int(row)] else 1
+            a, b = labels[int(v)], read[int(row)]
+            score += 0 if (a == b or (match_n and (a == N or b == N))) else 1
             read_pos = int(row)
         else:
             score += 1

@@ -42,6 +42,21 @@ def gen_graph(tmpdir, name, **over):
     return g, files
 
 
+def sprinkle_n(files, rate, seed):
+    """Replaces a fraction `rate` of the label bytes with 'N' in the labels
+    file of `files` (the hierarchy does not depend on label bytes) and
+    returns the graph read back from the files."""
+    import numpy as np
+    path = files[3]
+    raw = bytearray(open(path, "rb").read())
+    rng = np.random.default_rng(seed)
+    pos = [i for i, b in enumerate(raw) if b in b"ACGT"]
+    for i in rng.choice(pos, max(1, int(rate * len(pos))), replace=False):
+        raw[int(i)] = ord("N")
+    open(path, "wb").write(bytes(raw))
+    return cb.HostGraph.read_files(*files)
+
+
 @pytest.fixture(scope="session")
 def small_graph(tmp_path_factory):
     """cfg1 mix on a 20 kbp backbone: ~20k chars, ~1.7k string vertices."""

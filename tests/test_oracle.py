@@ -120,3 +120,30 @@ def test_checkpoint_rows_byte_identical_to_reference(tmp_path):
     assert names == sorted(os.listdir(b)) and len(names) == 7  # rows 0, 20, ..., 120
     for n in names:
         assert (a / n).read_bytes() == (b / n).read_bytes()
+
+
+needs_ref_matchn = pytest.mark.skipif(not orc.ref_available(match_n=True),
+                                      reason="oracle/_ref matchN builds not built")
+
+
+@needs_ref_matchn
+@pytest.mark.parametrize("seed,vmax", [(51, 1), (52, 12), (53, 32)])
+def test_matchn_oracle_matches_reference_code(tmp_path, seed, vmax):
+    # matchN (ALPHABET_SIZE=4): 'N' in labels and reads matches every base
+    from conftest import sprinkle_n
+    g, files = gen_graph(tmp_path, f"m{seed}", backbone_len=2500, seed=seed, vlen_max=vmax,
+                         bubble_gap_mean=10.0, p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=3,
+                         alt_max=50)
+    g = sprinkle_n(files, 0.03, seed)
+    reads = g.gen_reads(10, seed, 10, 120, sub_rate=0.05, indel_rate=0.05, n_rate=0.05).to_list()
+    o, r = orc.Oracle(files, match_n=True), orc.RefHarness(files, match_n=True)
+    want = r.scores(reads)
+    np.testing.assert_array_equal(o.scores(reads), want)
+    # the scheme matters on these inputs
+    assert (orc.Oracle(files).scores(reads) > want).any()
+    for rd in reads[:2]:
+        np.testing.assert_array_equal(o.rows(rd), r.rows(rd, o.num_chars))
+    labels = open(files[3], "rb").read().replace(b"\n", b"")
+    for rd, w in zip(reads[:3], want):
+        ops, score, _ = o.traceback(rd)
+        assert score == w and orc.rescore(ops, rd, labels, match_n=True) == (w, len(rd) - 1)
