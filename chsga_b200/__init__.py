@@ -184,6 +184,10 @@ _sig("chsga_last_error_global", C.c_char_p)
 _sig("chsga_graph_read_files", C.c_int32, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p,
      C.c_char_p, C.POINTER(vp))
 _sig("chsga_graph_view", C.c_int32, vp, C.POINTER(GraphHostT))
+_sig("chsga_gfa_to_csr_text", C.c_int32, C.c_char_p, C.c_char_p, C.c_char_p)
+_sig("chsga_csr_text_to_adj", C.c_int32, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p)
+_sig("chsga_graph_from_gfa", C.c_int32, C.c_char_p, C.POINTER(vp))
+_sig("chsga_graph_from_csr_text", C.c_int32, C.c_char_p, C.c_char_p, C.POINTER(vp))
 _sig("chsga_graph_free", None, vp)
 _sig("chsga_graph_write_files", C.c_int32, vp, C.c_char_p)
 _sig("chsga_gen_graph", C.c_int32, C.POINTER(GenGraphCfg), C.POINTER(vp))
@@ -331,6 +335,20 @@ class HostGraph:
     @classmethod
     def read_prefix(cls, prefix: str) -> "HostGraph":
         return cls.read_files(*files_for(prefix))
+
+    @classmethod
+    def from_gfa(cls, path: str) -> "HostGraph":
+        """Both orientations of a GFA v1 graph (handlegraph_to_csr); no hierarchy."""
+        h = vp()
+        _check(_lib.chsga_graph_from_gfa(path.encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_csr_text(cls, string_csr: str, char_csr: str) -> "HostGraph":
+        """handlegraph_to_csr's two CSR text files; no hierarchy."""
+        h = vp()
+        _check(_lib.chsga_graph_from_csr_text(string_csr.encode(), char_csr.encode(), C.byref(h)))
+        return cls(h)
 
     @classmethod
     def generate(cls, **cfg) -> "HostGraph":
@@ -676,3 +694,11 @@ def cm_features(ctx: "Context", read_len: int, mode: int = REQ_SCORE, slots: int
     _check(_lib.chsga_cm_features(ctx._h, read_len, mode, slots, k, cap_bytes, x.ctypes.data_as(f32p)),
            ctx._h)
     return x
+
+
+def gfa_to_csr_text(gfa: str, string_csr: str, char_csr: str) -> None:
+    _check(_lib.chsga_gfa_to_csr_text(gfa.encode(), string_csr.encode(), char_csr.encode()))
+
+
+def csr_text_to_adj(csr: str, adj: str, labels: str, label_offsets: str) -> None:
+    _check(_lib.chsga_csr_text_to_adj(csr.encode(), adj.encode(), labels.encode(), label_offsets.encode()))

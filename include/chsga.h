@@ -105,6 +105,25 @@ void chsga_graph_free(chsga_host_graph* g);
  * (src/csr_to_adj.cpp:46-114); ".string.out" is the hierarchy file. */
 chsga_status chsga_graph_write_files(const chsga_host_graph* g, const char* prefix);
 
+/* Graph ingest, the reference's handlegraph_to_csr -> csr_to_adj pipeline
+ * (src/handlegraph_to_csr.cpp:44-247, src/csr_to_adj.cpp). libbdsg's
+ * PackedGraph is not available, so the bidirected graph is read from GFA v1
+ * (numeric segment ids, blunt links): node i becomes string vertex 2i
+ * (forward) and 2i + 1 (reverse complement), the out-edges of an oriented
+ * handle are the handles its right side links to (sorted), sequences are
+ * upper-cased with other bytes as N, and the char graph is the expansion.
+ * chsga_gfa_to_csr_text writes handlegraph_to_csr's two CSR text files;
+ * chsga_csr_text_to_adj is csr_to_adj (AdjacencyGraph, labels, label
+ * offsets, byte-identical); chsga_graph_from_gfa / _from_csr_text build a
+ * host graph without a hierarchy (call chsga_build_pch). */
+chsga_status chsga_gfa_to_csr_text(const char* gfa_path, const char* string_csr_out,
+                                   const char* char_csr_out);
+chsga_status chsga_csr_text_to_adj(const char* csr_path, const char* adj_out, const char* labels_out,
+                                   const char* label_offsets_out);
+chsga_status chsga_graph_from_gfa(const char* gfa_path, chsga_host_graph** out);
+chsga_status chsga_graph_from_csr_text(const char* string_csr, const char* char_csr,
+                                       chsga_host_graph** out);
+
 /* Seeded variant-bubble DAG (backbone + SNP / indel / alternative-allele
  * bubbles, string vertices split to [vlen_min, vlen_max] chars). The char
  * graph is the expansion of src/handlegraph_to_csr.cpp:165-247; ids are in

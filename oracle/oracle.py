@@ -28,6 +28,7 @@ REF_CONSGA = os.path.join(HERE, "_ref", "ConSGA_mismatchN_dag")
 REF_CONSGA_TB = os.path.join(HERE, "_ref", "ConSGA_traceback_mismatchN_dag")
 REF_CONSGA_MATCHN = os.path.join(HERE, "_ref", "ConSGA_matchN_dag")
 REF_CONSGA_TB_MATCHN = os.path.join(HERE, "_ref", "ConSGA_traceback_matchN_dag")
+REF_CSR_TO_ADJ = os.path.join(HERE, "_ref", "csr_to_adj")
 REFERENCE_TREE = "/root/reference"
 
 u64p = C.POINTER(C.c_uint64)
