@@ -60,6 +60,9 @@ def parse():
     p.add_argument("--served-s", type=float, default=12.0, help="Poisson arrival window, seconds")
     p.add_argument("--backbone", type=int, default=0,
                    help="backbone length of the config-2-mix graph (0 = 5 Mbp); for small profiling captures")
+    p.add_argument("--scale-cfg4", action="store_true",
+                   help="config-3 scale run instead of the contract line: the 100 Mbp graph, "
+                        "checkpointed tracebacks (-k 500) and batched score-only GCUPS")
     p.add_argument("--kernels-only", action="store_true",
                    help="time the batched steps only (no server, served run, plain sample, profiled "
                         "pass or CPU baseline): the command profiling captures run under ncu")
@@ -281,7 +284,7 @@ def served_run(cb, ctx, g, N, opts, capacity_gcups, window_s):
     y = np.stack([t_ms, 4.0 * (N + 32) + lens], 1)
     half = n // 2
     m = cb.CostModel(0, seed=1)
-    m.train(feats[:half], y[:half], epochs=200, batch=min(64, half), seed=2)
+    m.train(feats[:half], y[:half], epochs=1000, batch=min(64, half), lr=2e-3, seed=2)
     pred = m.predict(feats[half:])[:, 0]
     m.close()
     cells = lens * float(N)
@@ -355,10 +358,77 @@ def run_reference(args):
     return 0
 
 
+def run_scale_cfg4(args):
+    """The 100 Mbp config-4 graph (about 139 M chars): checkpointed tracebacks
+    of 10 kbp reads at 5% error with -k 500 (a full int32 matrix would take
+    5.6 TB), each checked by rescoring its path against the score-only
+    result, then batched score-only GCUPS with 128 slots (two 16-bit rows of
+    35.6 GB). Prints one JSON line."""
+    import numpy as np
+
+    import chsga_b200 as cb
+    t0 = time.time()
+    g = cb.HostGraph.generate(**cb.GRAPH_CONFIGS["cfg4"])
+    g.build_pch()
+    st = g.stats()
+    N = st["num_chars"]
+    prep_s = time.time() - t0
+    ctx = cb.Context(0).load(g)
+    labels = ctypes_labels(g)
+    reads = g.gen_reads(2, 44, 10000, 10000, sub_rate=0.02, indel_rate=0.03, indel_len_max=3).to_list()
+    want = ctx.align_scores(reads)
+    tb = []
+    for r, w in zip(reads, want):
+        t = time.perf_counter()
+        ops, score, ck = ctx.align_traceback(r, k=500)
+        dt = time.perf_counter() - t
+        ps, last = path_score(ops, r, labels)
+        tb.append({"len": len(r), "seconds": dt, "checkpointed": ck, "score": score,
+                   "score_only": int(w), "rescored": ps, "last_row": last,
+                   "ok": bool(score == w == ps and last == len(r) - 1),
+                   "gcups_forward_cells": len(r) * N / dt / 1e9})
+    batch = make_reads(g, 256, 4545, len_max=2000)
+    ctx.align_scores_batched(batch[:128], slots=128)  # warm-up
+    ctx.align_scores_batched(batch, slots=128)
+    p = ctx.profile()
+    cells = sum(len(r) for r in batch) * N
+    line = {"mode": "scale-cfg4", "num_chars": N, "num_strings": st["num_strings"],
+            "hierarchy_levels": st["pch_levels"], "graph_prep_s": prep_s,
+            "traceback": tb, "batched": {"reads": len(batch), "slots": 128,
+                                         "gcups": cells / p["total_ms"] / 1e6,
+                                         "device_ms": p["total_ms"]}}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+def path_score(ops, read, labels):
+    """The traceback drivers' own check (src/ConSGA_traceback.cpp:190-209):
+    the path's score under the unit costs and the last read row it uses."""
+    score, last = 0, -1
+    for row, v, op in ops:
+        if op == 1:
+            score += 0 if labels[int(v)] == read[int(row)] else 1
+            last = int(row)
+        else:
+            score += 1
+            if op == 0:
+                last = int(row)
+    return score, last
+
+
+def ctypes_labels(g):
+    import ctypes
+    v = g.view()
+    return ctypes.string_at(v.labels, v.num_chars)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.scale_cfg4:
+        return run_scale_cfg4(args)
     ws, rank, local = dist_env()
     if ws > 1:
         import torch
