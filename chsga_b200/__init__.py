@@ -220,6 +220,7 @@ _sig("chsga_tb_result_free", None, C.POINTER(TbResult))
 _sig("chsga_ops_to_cigar", C.c_uint64, C.POINTER(OpT), C.c_uint64, C.c_char_p, C.c_uint64)
 _sig("chsga_get_profile", C.c_int32, vp, C.POINTER(ProfileT))
 _sig("chsga_get_read_times", C.c_int32, vp, u64p, u64p, C.c_uint32)
+_sig("chsga_selftest_wait", C.c_int32, vp, C.c_uint32)
 f32p = C.POINTER(C.c_float)
 _sig("chsga_cm_create", C.c_int32, C.c_int, C.c_uint64, C.POINTER(vp))
 _sig("chsga_cm_free", None, vp)
@@ -497,6 +498,11 @@ class Context:
         d = np.zeros(n, dtype=np.uint64)
         self._ck(_lib.chsga_get_read_times(self._h, a.ctypes.data_as(u64p), d.ctypes.data_as(u64p), n))
         return a, d
+
+    def selftest_wait(self, polls: int = 4096) -> None:
+        """Runs a bounded device wait that cannot succeed (chsga_selftest_wait):
+        raises ChsgaError with ERR_TIMEOUT."""
+        self._ck(_lib.chsga_selftest_wait(self._h, polls))
 
     def profile(self) -> dict:
         p = ProfileT()

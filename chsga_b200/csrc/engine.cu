@@ -1753,6 +1753,18 @@ chsga_status chsga_cm_features(chsga_ctx* c, uint32_t read_len, uint32_t mode, u
   });
 }
 
+chsga_status chsga_selftest_wait(chsga_ctx* c, uint32_t polls) {
+  return guarded_ctx(c, [&] {
+    require(c != nullptr, CHSGA_ERR_INVALID_ARG, "null argument");
+    SlotBufs b;
+    b.ctl.alloc(1);
+    CK(cudaMemsetAsync(b.ctl.p, 0, sizeof(dev::StepCtl), c->st));
+    dev::k_wait_selftest<<<1, 32, 0, c->st>>>(b.ctl.p, polls);
+    check_launch();
+    check_device_error(*c, b);
+  });
+}
+
 chsga_status chsga_get_profile(chsga_ctx* c, chsga_profile* out) {
   return guarded_ctx(c, [&] {
     require(c && out, CHSGA_ERR_INVALID_ARG, "null argument");

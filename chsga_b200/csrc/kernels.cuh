@@ -305,8 +305,9 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
 }
 
 // Waits for phase `parity` of the barrier; false if the poll budget ran out.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity,
+                                          uint32_t limit = kWaitLimit) {
+  for (uint32_t i = 0; i < limit; ++i) {
     uint32_t ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -1543,6 +1544,22 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
     return;
   }
   for (uint32_t j = threadIdx.x; j < t.K; j += blockDim.x) BV[(2 * (K0 + j)) * R + r] = (ST)sm[2 * j];
+}
+
+// ---------------------------------------------------------------------------
+// k_wait_selftest: the bounded mbarrier wait of k_top on a barrier that
+// nothing completes. It gives up after `polls` polls and reports through the
+// control block as k_top does, so the host's timeout path can be checked
+// without any real wait failing.
+// ---------------------------------------------------------------------------
+__global__ void k_wait_selftest(StepCtl* __restrict__ ctl, uint32_t polls) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_async_shared();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0, polls)) atomicOr(&ctl->error, ERR_TOP_WAIT);
 }
 
 // ---------------------------------------------------------------------------

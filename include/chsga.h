@@ -376,6 +376,13 @@ chsga_status chsga_get_profile(chsga_ctx* ctx, chsga_profile* out);
  * reference counterpart: used for per-read latency percentiles. */
 chsga_status chsga_get_read_times(chsga_ctx* ctx, uint64_t* admit_ns, uint64_t* done_ns, uint32_t n);
 
+/* Self-test of the device-side failure path, no reference counterpart: one
+ * kernel runs the hierarchy sweep's bounded mbarrier wait on a barrier that
+ * nothing completes, gives up after `polls` polls and flags the control
+ * block; the call then returns CHSGA_ERR_TIMEOUT exactly as an alignment
+ * whose wait expired would, and the context stays usable. */
+chsga_status chsga_selftest_wait(chsga_ctx* ctx, uint32_t polls);
+
 /* ------------------------------------------------------------------------- */
 /* Autotuner (no reference counterpart)                                      */
 /* ------------------------------------------------------------------------- */
