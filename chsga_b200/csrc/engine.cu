@@ -11,6 +11,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <set>
 #include <type_traits>
 
 #include "device_graph.hpp"
@@ -196,6 +197,19 @@ int32_t empty_score(const chsga_ctx& c) {
 
 void check_launch() { CK(cudaGetLastError()); }
 
+// Runs f once for each (key, device) pair: kernel attributes such as the
+// dynamic shared-memory limit are per device, and several threads (serving
+// lane, traceback workers) may ask at once.
+template <typename F>
+void once_per_device(const void* key, int device, F&& f) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({key, device})) return;
+  f();
+  done.insert({key, device});
+}
+
 template <int R, typename ST>
 SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
   auto& b = c.bufs[R];
@@ -213,21 +227,17 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
   b->word.alloc(R);
   b->best.alloc(R);
   b->ctl.alloc(1);
-  // once per process (thread-safe: serving threads may get here together)
-  static const bool attr_set = [] {
+  // the large dynamic shared memory of these kernels, once per device
+  once_per_device((const void*)dev::k_top<R, ST>, c.device, [] {
     CK(cudaFuncSetAttribute(dev::k_top<R, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)dev::top_smem_bytes(kTopMaxVertices)));
-    return true;
-  }();
-  (void)attr_set;
+  });
   if constexpr (std::is_same_v<ST, uint16_t> && R >= 64) {
-    static const bool stream_set = [] {
+    once_per_device((const void*)dev::k_row_stream<R, true>, c.device, [] {
       for (auto k : {dev::k_row_stream<R, true>, dev::k_row_stream<R, false>})
         CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)dev::stream_smem_bytes(R)));
-      return true;
-    }();
-    (void)stream_set;
+    });
   }
   return *b;
 }
