@@ -240,7 +240,9 @@ chsga_status chsga_load_graph(chsga_ctx* ctx, const chsga_graph_host* g);
 chsga_status chsga_load_host_graph(chsga_ctx* ctx, const chsga_host_graph* g);
 
 /* Score-only, one read per launch sequence: align_combo<int> (src/align.hpp:470-531).
- * scores_out[i] = min over the last row of read i. Reads of length 0 are rejected. */
+ * scores_out[i] = min over the last row of read i. A read of length 0 gets
+ * what the reference computes for it, row 0 against the byte '\0': 0 if a
+ * label matches that byte (a '\0' label, or an 'N' under matchN), else 1. */
 chsga_status chsga_align_scores(chsga_ctx* ctx, const char* const* reads, const uint32_t* lens,
                                 uint32_t n, int32_t* scores_out);
 
