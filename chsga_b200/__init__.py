@@ -217,6 +217,8 @@ _sig("chsga_align_rows", C.c_int32, vp, C.c_char_p, C.c_uint32, i32p)
 _sig("chsga_align_traceback", C.c_int32, vp, C.c_char_p, C.c_uint32, C.POINTER(TbOpts),
      C.POINTER(TbResult))
 _sig("chsga_tb_result_free", None, C.POINTER(TbResult))
+_sig("chsga_align_traceback_batched", C.c_int32, vp, C.POINTER(C.c_char_p), u32p, C.c_uint32,
+     C.POINTER(TbOpts), C.c_uint32, C.POINTER(TbResult))
 _sig("chsga_ops_to_cigar", C.c_uint64, C.POINTER(OpT), C.c_uint64, C.c_char_p, C.c_uint64)
 _sig("chsga_get_profile", C.c_int32, vp, C.POINTER(ProfileT))
 _sig("chsga_get_read_times", C.c_int32, vp, u64p, u64p, C.c_uint32)
@@ -491,6 +493,26 @@ class Context:
             return ops, int(r.score), bool(r.checkpointed)
         finally:
             _lib.chsga_tb_result_free(C.byref(r))
+
+    def align_traceback_batched(self, reads: Sequence[bytes], slots: int = 32, k: int = 500,
+                                cap_bytes: int = 0):
+        """[(ops ndarray, score, checkpointed)] per read, as align_traceback."""
+        arr, lens = _read_ptrs(reads)
+        o = TbOpts(k, None, 0, cap_bytes)
+        res = (TbResult * max(1, len(reads)))()
+        self._ck(_lib.chsga_align_traceback_batched(self._h, arr, lens.ctypes.data_as(u32p), len(reads),
+                                                    C.byref(o), slots, res))
+        out = []
+        for i in range(len(reads)):
+            r = res[i]
+            n = int(r.num_ops)
+            ops = np.zeros((n, 3), dtype=np.int64)
+            for j in range(n):
+                x = r.ops[j]
+                ops[j] = (x.row, x.vertex, x.op)
+            out.append((ops, int(r.score), bool(r.checkpointed)))
+            _lib.chsga_tb_result_free(C.byref(r))
+        return out
 
     def read_times(self, n: int):
         """(admit_ns, done_ns) per non-empty read of the last score call."""

@@ -400,9 +400,16 @@ struct StepEvents {
 // BVc = this step's boundary scores. DEFER (score-only): rows stay raw and
 // BVp holds the previous step's swept boundary scores; otherwise every row
 // is written final (rows that are kept for traceback).
+// Per-read matrices of the batched traceback: every active slot's final row
+// is copied there after the sweeps, before k_advance.
+struct RowSink {
+  uint16_t* const* mats;  // device array, one matrix per read id
+  size_t pitch;
+};
+
 template <int R, bool DEFER, typename ST>
 void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
-              StepEvents* ev = nullptr) {
+              StepEvents* ev = nullptr, const RowSink* sink = nullptr) {
   ST* BVc = reinterpret_cast<ST*>(b.BV.p);
   const HostLayout& L = c.g->L;
   const TopDev& top = cur_top(c);
@@ -469,6 +476,11 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
       dev::k_down<R, !DEFER, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
           c.g->gp, BVc, T, FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
     }
+  }
+  if constexpr (std::is_same_v<ST, uint16_t> && !DEFER && R >= 2) {
+    if (sink)
+      dev::k_store_rows<R><<<(L.N + 63) / 64, 256, 0, s>>>(T, b.slots.p, sink->mats, sink->pitch, L.N,
+                                                          b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[4], s));
   launch_advance<R>(c, b, 0, s);
@@ -716,7 +728,7 @@ void walk(chsga_ctx& c, const int* M, int64_t lo, int64_t hi, uint32_t start, ui
   ops.alloc(max_ops);
   DevArr<dev::WalkOut> out;
   out.alloc(1);
-  dev::k_walk<<<1, 1, 0, c.st>>>(c.g->gp, M, c.g->pitch, lo, hi, start, c.reads.p, ops.p, max_ops, out.p,
+  dev::k_walk<int><<<1, 1, 0, c.st>>>(c.g->gp, M, c.g->pitch, lo, hi, start, c.reads.p, ops.p, max_ops, out.p,
                                  match_n(c));
   check_launch();
   dev::WalkOut h{};
@@ -731,6 +743,21 @@ void walk(chsga_ctx& c, const int* M, int64_t lo, int64_t hi, uint32_t start, ui
   if (h.nops)
     CK(cudaMemcpy(path.data() + old, ops.p, h.nops * sizeof(dev::WalkOp), cudaMemcpyDeviceToHost));
   *landing = h.vertex;
+}
+
+// ops of a walked path (collected end first) into a caller-owned result
+void fill_result(chsga_tb_result* res, std::vector<dev::WalkOp>& path, int32_t score) {
+  std::reverse(path.begin(), path.end());
+  res->num_ops = path.size();
+  res->ops = (chsga_op*)std::malloc(std::max<size_t>(1, path.size()) * sizeof(chsga_op));
+  require(res->ops != nullptr, CHSGA_ERR_OOM, "host out of memory");
+  for (size_t i = 0; i < path.size(); ++i) {
+    res->ops[i].row = path[i].row;
+    res->ops[i].vertex = path[i].vertex;
+    res->ops[i].op = (uint8_t)path[i].op;
+    std::memset(res->ops[i].pad, 0, 3);
+  }
+  res->score = score;
 }
 
 void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts* o,
@@ -881,17 +908,165 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
     path.push_back(dev::WalkOp{0, cur_v, CHSGA_OP_MATCHSUB});
     if (!dir.empty() && !keep) std::filesystem::remove(ckpt_row_path(dir, 0));
   }
-  std::reverse(path.begin(), path.end());
-  res->num_ops = path.size();
-  res->ops = (chsga_op*)std::malloc(std::max<size_t>(1, path.size()) * sizeof(chsga_op));
-  require(res->ops != nullptr, CHSGA_ERR_OOM, "host out of memory");
-  for (size_t i = 0; i < path.size(); ++i) {
-    res->ops[i].row = path[i].row;
-    res->ops[i].vertex = path[i].vertex;
-    res->ops[i].op = (uint8_t)path[i].op;
-    std::memset(res->ops[i].pad, 0, 3);
+  fill_result(res, path, best_s);
+}
+
+// Publishes queue entries [0, q_count) to k_advance (one thread, stream-ordered).
+__global__ void k_publish(dev::StepCtl* ctl, uint32_t q_count) { ctl->q_count = q_count; }
+
+// ---- batched full-matrix traceback --------------------------------------------
+//
+// Reads whose full matrix fits the cap run together as the slots of the
+// batched engine in FIXUP mode (every row final); after each row-step
+// k_store_rows copies each active slot's row into that read's own 16-bit
+// matrix (stream-ordered allocations, published to the device queue only
+// once the matrix exists and fits the device budget). A finished read is
+// walked on the side stream, one engine block behind, while the next block
+// runs; its matrix is then freed. Same matrix values and the same walk as
+// the one-read path, so the same ops.
+template <int R>
+void traceback_batched(chsga_ctx& parent, const char* const* reads, const uint32_t* lens,
+                       const std::vector<uint32_t>& idx, chsga_tb_result* out) {
+  std::unique_ptr<chsga_ctx, void (*)(chsga_ctx*)> hold(fork_context(parent), chsga_close);
+  chsga_ctx& c = *hold;
+  const uint32_t nf = (uint32_t)idx.size();
+  std::vector<const char*> rp(nf);
+  std::vector<uint32_t> rl(nf);
+  std::vector<uint64_t> roff(nf);
+  uint64_t off = 0, max_ops = 16;
+  for (uint32_t i = 0; i < nf; ++i) {
+    rp[i] = reads[idx[i]];
+    rl[i] = lens[idx[i]];
+    roff[i] = off;
+    off += rl[i];
+    max_ops = std::max<uint64_t>(max_ops, 4ull * rl[i] + 16);
   }
-  res->score = best_s;
+  upload_reads(c, rp.data(), rl.data(), nf);  // queue entry i = read i, published below
+  c.done_ring.alloc(nf);
+  SlotBufs& b = get_bufs<R, uint16_t>(c, true);
+  reset_slots<R>(c, b, 0);
+  launch_advance<R>(c, b, 0, c.st);
+  DevArr<uint16_t*> mats;
+  mats.alloc(nf);
+  CK(cudaMemsetAsync(mats.p, 0, nf * sizeof(uint16_t*), c.st));
+  const size_t pitch = c.g->pitch;
+  const RowSink sink{mats.p, pitch};
+  constexpr uint32_t per = 8;
+  uint16_t* rows[2] = {reinterpret_cast<uint16_t*>(b.rows[0].p), reinterpret_cast<uint16_t*>(b.rows[1].p)};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  {
+    cudaStream_t cap;
+    CK(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    for (uint32_t i = 0; i < per; ++i)
+      row_step<R, false, uint16_t>(c, b, rows[i & 1], rows[(i + 1) & 1], cap, nullptr, &sink);
+    CK(cudaStreamEndCapture(cap, &graph));
+    CK(cudaGraphInstantiate(&exec, graph, 0));
+    CK(cudaStreamDestroy(cap));
+  }
+  struct GraphHold {
+    cudaGraph_t g;
+    cudaGraphExec_t e;
+    ~GraphHold() {
+      if (e) cudaGraphExecDestroy(e);
+      if (g) cudaGraphDestroy(g);
+    }
+  } gh{graph, exec};
+  PinnedArr<dev::StepCtl> hctl;
+  hctl.alloc(2);
+  PinnedArr<dev::CompletionRec> hring;
+  hring.alloc(2 * (size_t)nf);
+  cudaEvent_t ev[2];
+  for (auto& e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  struct EvHold {
+    cudaEvent_t* e;
+    ~EvHold() {
+      cudaEventDestroy(e[0]);
+      cudaEventDestroy(e[1]);
+    }
+  } eh{ev};
+  DevArr<dev::WalkOp> ops_buf;
+  ops_buf.alloc(max_ops);
+  DevArr<dev::WalkOut> wout;
+  wout.alloc(1);
+  std::vector<dev::WalkOp> hops(max_ops);
+  // matrices held at once: what is free once the engine's buffers exist
+  const uint64_t budget = (uint64_t)(device_free_bytes(c) * 0.8);
+  std::vector<uint16_t*> hm(nf, nullptr);
+  uint64_t used = 0;
+  uint32_t next = 0, hdone = 0;
+  uint64_t launched = 0;
+  auto finish = [&](const dev::CompletionRec& r) {
+    const uint32_t id = (uint32_t)r.id, len = rl[id];
+    std::vector<dev::WalkOp> path;
+    uint32_t v = r.vertex;
+    if (len > 1) {
+      dev::k_walk<uint16_t><<<1, 1, 0, c.side>>>(c.g->gp, hm[id], pitch, 0, (long long)len - 1, r.vertex,
+                                                  c.reads.p + roff[id], ops_buf.p, (uint32_t)max_ops,
+                                                  wout.p, match_n(c));
+      check_launch();
+      dev::WalkOut h{};
+      CK(cudaMemcpyAsync(&h, wout.p, sizeof(h), cudaMemcpyDeviceToHost, c.side));
+      CK(cudaStreamSynchronize(c.side));
+      if (h.status == 7)
+        fail(CHSGA_ERR_NO_PATH, "score-matrix traceback: no valid predecessor at row " +
+                                    std::to_string(h.fail_row));
+      require(h.status == 0, CHSGA_ERR_INTERNAL, "traceback walk exceeded its op budget");
+      if (h.nops)
+        CK(cudaMemcpy(hops.data(), ops_buf.p, h.nops * sizeof(dev::WalkOp), cudaMemcpyDeviceToHost));
+      path.assign(hops.begin(), hops.begin() + h.nops);
+      v = h.vertex;
+    }
+    path.push_back(dev::WalkOp{0, v, CHSGA_OP_MATCHSUB});
+    fill_result(&out[idx[id]], path, r.score);
+    CK(cudaFreeAsync(hm[id], c.side));
+    hm[id] = nullptr;
+    used -= (uint64_t)len * pitch * 2;
+  };
+  auto harvest = [&](int k) {
+    CK(cudaEventSynchronize(ev[k]));
+    const dev::StepCtl& st = hctl.p[k];
+    require(st.error == 0, CHSGA_ERR_TIMEOUT,
+            "a bounded device-side wait expired (code " + std::to_string(st.error) + ")");
+    for (uint32_t i = hdone; i < st.done; ++i) finish(hring.p[(size_t)k * nf + i]);
+    hdone = st.done;
+  };
+  try {
+    while (hdone < nf) {
+      const uint32_t pub0 = next;
+      while (next < nf) {
+        const uint64_t mb = (uint64_t)rl[next] * pitch * 2;
+        // always admit when nothing else holds a matrix, so the loop progresses
+        if (used + mb > budget && used > 0) break;
+        void* p = nullptr;
+        CK(cudaMallocAsync(&p, mb, c.st));
+        hm[next] = static_cast<uint16_t*>(p);
+        dev::k_set_ptr<<<1, 1, 0, c.st>>>(mats.p, next, hm[next]);
+        used += mb;
+        ++next;
+      }
+      if (next > pub0) k_publish<<<1, 1, 0, c.st>>>(b.ctl.p, next);
+      const int k = (int)(launched & 1);
+      CK(cudaGraphLaunch(exec, c.st));
+      CK(cudaMemcpyAsync(hctl.p + k, b.ctl.p, sizeof(dev::StepCtl), cudaMemcpyDeviceToHost, c.st));
+      CK(cudaMemcpyAsync(hring.p + (size_t)k * nf, c.done_ring.p, nf * sizeof(dev::CompletionRec),
+                         cudaMemcpyDeviceToHost, c.st));
+      CK(cudaEventRecord(ev[k], c.st));
+      ++launched;
+      if (launched >= 2) harvest((int)((launched - 2) & 1));
+      require(launched < 4ull * (off + 16) + 64, CHSGA_ERR_INTERNAL, "batched traceback made no progress");
+    }
+    CK(cudaStreamSynchronize(c.st));
+    CK(cudaStreamSynchronize(c.side));
+  } catch (...) {
+    cudaStreamSynchronize(c.st);
+    cudaStreamSynchronize(c.side);
+    for (auto* p : hm)
+      if (p) cudaFreeAsync(p, c.st);
+    cudaStreamSynchronize(c.st);
+    throw;
+  }
 }
 
 // ---- score-only alignment without device allocation -------------------------
@@ -1310,7 +1485,6 @@ chsga_status guarded_ctx(chsga_ctx* c, F&& f) {
 
 // ---- continuous score lane (serving) -----------------------------------------
 
-__global__ void k_publish(dev::StepCtl* ctl, uint32_t q_count) { ctl->q_count = q_count; }
 
 __global__ void k_clock(unsigned long long* out) { *out = dev::global_ns(); }
 
@@ -1698,6 +1872,48 @@ chsga_status chsga_align_traceback(chsga_ctx* c, const char* read, uint32_t len,
     require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
     std::memset(out, 0, sizeof(*out));
     traceback(*c, read, len, opts, out);
+  });
+}
+
+chsga_status chsga_align_traceback_batched(chsga_ctx* c, const char* const* reads,
+                                           const uint32_t* lens, uint32_t n,
+                                           const chsga_tb_opts* opts, uint32_t slots,
+                                           chsga_tb_result* out) {
+  return guarded_ctx(c, [&] {
+    require(c && (n == 0 || (reads && lens && out)), CHSGA_ERR_INVALID_ARG, "null argument");
+    require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
+    if (!slots) slots = 32;
+    require(slots == 16 || slots == 32 || slots == 64, CHSGA_ERR_INVALID_ARG, "slots must be 16, 32 or 64");
+    for (uint32_t i = 0; i < n; ++i) {
+      require(reads[i] && lens[i] > 0, CHSGA_ERR_INVALID_ARG, "traceback of an empty read");
+      std::memset(&out[i], 0, sizeof(out[i]));
+    }
+    // the one-read path's choice between the full matrix and checkpoints
+    const uint64_t cap = (opts && opts->cap_bytes) ? opts->cap_bytes : c->cap;
+    const uint64_t row_bytes = (uint64_t)c->g->L.N * 4;
+    std::vector<uint32_t> full, rest;
+    for (uint32_t i = 0; i < n; ++i) {
+      if (lens[i] <= kRow16Max && (uint64_t)lens[i] * row_bytes <= cap && !(opts && opts->dir))
+        full.push_back(i);
+      else
+        rest.push_back(i);
+    }
+    std::stable_sort(full.begin(), full.end(), [&](uint32_t a, uint32_t b) { return lens[a] > lens[b]; });
+    try {
+      if (full.size() > 1) {
+        switch (slots) {
+          case 16: traceback_batched<16>(*c, reads, lens, full, out); break;
+          case 32: traceback_batched<32>(*c, reads, lens, full, out); break;
+          default: traceback_batched<64>(*c, reads, lens, full, out); break;
+        }
+      } else {
+        rest.insert(rest.end(), full.begin(), full.end());
+      }
+      for (uint32_t i : rest) traceback(*c, reads[i], lens[i], opts, &out[i]);
+    } catch (...) {
+      for (uint32_t i = 0; i < n; ++i) chsga_tb_result_free(&out[i]);
+      throw;
+    }
   });
 }
 

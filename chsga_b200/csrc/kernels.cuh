@@ -1547,6 +1547,44 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
 }
 
 // ---------------------------------------------------------------------------
+// k_store_rows: after a FIXUP row-step (rows final), copies the row every
+// active slot just computed from the slot-interleaved row T into that read's
+// own matrix: row slots[r].row of mats[slots[r].id], `pitch` elements per
+// row. A block moves a tile of 64 chars x R slots through shared memory, so
+// the read of T and each slot's 64-char write are both coalesced. Runs
+// before k_advance moves the slots on.
+// ---------------------------------------------------------------------------
+template <int R>
+__global__ void __launch_bounds__(256) k_store_rows(const uint16_t* __restrict__ T,
+                                                    const SlotState* __restrict__ slots,
+                                                    uint16_t* const* __restrict__ mats,
+                                                    size_t pitch, uint32_t N,
+                                                    const StepCtl* __restrict__ ctl) {
+  constexpr int C = 64;
+  __shared__ uint16_t tile[C][R + 2];
+  __shared__ uint16_t* dst[R];
+  if (!ctl->any_active) return;
+  const uint32_t c0 = blockIdx.x * C;
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    const SlotState st = slots[r];
+    dst[r] = st.id >= 0 ? mats[st.id] + (size_t)st.row * pitch : nullptr;
+  }
+  for (int k = threadIdx.x; k < C * R; k += blockDim.x) {
+    const int i = k / R, r = k % R;
+    const uint32_t c = c0 + i;
+    tile[i][r] = c < N ? T[(size_t)c * R + r] : (uint16_t)0;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < C * R; k += blockDim.x) {
+    const int r = k / C, i = k % C;
+    const uint32_t c = c0 + i;
+    if (dst[r] && c < N) dst[r][c] = tile[i][r];
+  }
+}
+
+__global__ void k_set_ptr(uint16_t** mats, uint32_t i, uint16_t* p) { mats[i] = p; }
+
+// ---------------------------------------------------------------------------
 // k_wait_selftest: the bounded mbarrier wait of k_top on a barrier that
 // nothing completes. It gives up after `polls` polls and reports through the
 // control block as k_top does, so the host's timeout path can be checked
@@ -1696,7 +1734,8 @@ struct WalkOp {
   uint32_t op;
 };
 
-__global__ void k_walk(GraphPtrs g, const int* __restrict__ M, size_t pitch, long long row_lo,
+template <typename MT>
+__global__ void k_walk(GraphPtrs g, const MT* __restrict__ M, size_t pitch, long long row_lo,
                        long long row_hi, uint32_t start, const unsigned char* __restrict__ read,
                        WalkOp* __restrict__ ops, uint32_t max_ops, WalkOut* __restrict__ out,
                        int match_n) {
@@ -1719,9 +1758,9 @@ __global__ void k_walk(GraphPtrs g, const int* __restrict__ M, size_t pitch, lon
       out->fail_row = (int)row;
       break;
     }
-    const int* Rw = M + (size_t)(row - row_lo) * N;
-    const int* Pw = M + (size_t)(row - 1 - row_lo) * N;
-    const int s = Rw[cur];
+    const MT* Rw = M + (size_t)(row - row_lo) * N;
+    const MT* Pw = M + (size_t)(row - 1 - row_lo) * N;
+    const int s = (int)Rw[cur];
     const uint32_t first = g.sv_off[sv];
     uint32_t op = 255, src = cur, src_sv = sv;
     if (cur > first && Rw[cur - 1] + 1 == s) {

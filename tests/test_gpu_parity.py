@@ -130,3 +130,21 @@ def test_random_graphs(tmp_path, seed, vmax):
     np.testing.assert_array_equal(ctx.align_scores(reads), want)
     np.testing.assert_array_equal(ctx.align_scores_batched(reads, slots=4), want)
     ctx.close()
+
+
+@pytest.mark.parametrize("slots", [16, 64])
+def test_traceback_batched_equals_one_by_one(small_graph, ctx_small, oracle_small, slots):
+    g, files, reads = small_graph
+    labels = open(files[3], "rb").read().replace(b"\n", b"")
+    mix = list(reads[:10]) + g.gen_reads(30, 17, 10, 700, sub_rate=0.03, indel_rate=0.02,
+                                          n_rate=0.005).to_list()
+    n = oracle_small.num_chars
+    want = oracle_small.scores(mix)
+    # a cap that sends the longer reads to the checkpointed path
+    cap = 400 * n * 4
+    got = ctx_small.align_traceback_batched(mix, slots=slots, k=60, cap_bytes=cap)
+    for rd, w, (ops, score, ck) in zip(mix, want, got):
+        one = ctx_small.align_traceback(rd, k=60, cap_bytes=cap)
+        assert score == w == one[1] and ck == one[2] == (len(rd) > 400)
+        np.testing.assert_array_equal(ops, one[0])
+        assert orc.rescore(ops, rd, labels) == (w, len(rd) - 1)
