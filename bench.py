@@ -63,6 +63,11 @@ def parse():
     p.add_argument("--scale-cfg4", action="store_true",
                    help="config-3 scale run instead of the contract line: the 100 Mbp graph, "
                         "checkpointed tracebacks (-k 500) and batched score-only GCUPS")
+    p.add_argument("--traceback-cfg1", action="store_true",
+                   help="config-1 run instead of the contract line: tracebacks of 2,000 x 150 bp and "
+                        "200 x 2 kbp reads with full score matrices, batched and one by one")
+    p.add_argument("--tb-sample", type=int, default=0,
+                   help="with --traceback-cfg1: that many 150 bp reads and a tenth as many 2 kbp ones")
     p.add_argument("--kernels-only", action="store_true",
                    help="time the batched steps only (no server, served run, plain sample, profiled "
                         "pass or CPU baseline): the command profiling captures run under ncu")
@@ -417,6 +422,47 @@ def path_score(ops, read, labels):
     return score, last
 
 
+def run_traceback_cfg1(args):
+    """Config 1: the 5 Mbp config-2 graph, 2,000 x 150 bp plus 200 x 2 kbp
+    reads at 1% / 0.5% / 0.1% substitution / indel / N, full int32-sized
+    matrices under the cap (the batched path keeps them 16-bit), every path
+    rescored against the score-only result. The one-read path is timed on a
+    sample for comparison. Prints one JSON line."""
+    import chsga_b200 as cb
+    g = make_graph(args.backbone)
+    N = g.stats()["num_chars"]
+    labels = ctypes_labels(g)
+    n150, n2k = (2000, 200) if not args.tb_sample else (args.tb_sample, max(1, args.tb_sample // 10))
+    reads = (g.gen_reads(n150, 11, 150, 150, sub_rate=0.01, indel_rate=0.005, n_rate=0.001).to_list() +
+             g.gen_reads(n2k, 12, 2000, 2000, sub_rate=0.01, indel_rate=0.005, n_rate=0.001).to_list())
+    ctx = cb.Context(0).load(g)
+    want = ctx.align_scores_batched(reads, slots=128)
+    ctx.align_traceback_batched(reads[:64], slots=64)  # warm-up
+    t = time.perf_counter()
+    got = ctx.align_traceback_batched(reads, slots=64)
+    dt = time.perf_counter() - t
+    bad = 0
+    for r, w, (ops, score, ck) in zip(reads, want, got):
+        ps, last = path_score(ops, r, labels)
+        bad += int(not (score == w == ps and last == len(r) - 1 and not ck))
+    cells = sum(len(r) for r in reads) * N
+    sample = reads[:20] + reads[n150:n150 + 4]
+    t = time.perf_counter()
+    for r in sample:
+        ctx.align_traceback(r)
+    dt1 = time.perf_counter() - t
+    cells1 = sum(len(r) for r in sample) * N
+    line = {"mode": "traceback-cfg1", "num_chars": N, "reads": len(reads), "mismatches": bad,
+            "batched": {"seconds": dt, "reads_per_s": len(reads) / dt, "gcups": cells / dt / 1e9,
+                        "slots": "up to 64, by matrix memory"},
+            "one_by_one": {"sample": f"{len(sample)} reads (20 x 150 bp, 4 x 2 kbp)", "seconds": dt1,
+                           "gcups": cells1 / dt1 / 1e9},
+            "speedup": (cells / dt) / (cells1 / dt1)}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def ctypes_labels(g):
     import ctypes
     v = g.view()
@@ -429,6 +475,8 @@ def main():
         return run_reference(args)
     if args.scale_cfg4:
         return run_scale_cfg4(args)
+    if args.traceback_cfg1:
+        return run_traceback_cfg1(args)
     ws, rank, local = dist_env()
     if ws > 1:
         import torch

@@ -986,50 +986,75 @@ void traceback_batched(chsga_ctx& parent, const char* const* reads, const uint32
       cudaEventDestroy(e[1]);
     }
   } eh{ev};
+  // walk outputs of one harvest (at most R reads finish per row-step)
+  const uint32_t wcap = R * per + R;
   DevArr<dev::WalkOp> ops_buf;
-  ops_buf.alloc(max_ops);
+  ops_buf.alloc(max_ops * wcap);
   DevArr<dev::WalkOut> wout;
-  wout.alloc(1);
+  wout.alloc(wcap);
+  std::vector<dev::WalkOut> hout(wcap);
   std::vector<dev::WalkOp> hops(max_ops);
-  // matrices held at once: what is free once the engine's buffers exist
+  // matrices held at once: what is free once the engine's buffers exist;
+  // the stream-ordered pool keeps freed matrices for the next reads instead
+  // of unmapping them at every synchronisation
   const uint64_t budget = (uint64_t)(device_free_bytes(c) * 0.8);
+  {
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, c.device));
+    uint64_t keep = budget;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   std::vector<uint16_t*> hm(nf, nullptr);
   uint64_t used = 0;
   uint32_t next = 0, hdone = 0;
   uint64_t launched = 0;
-  auto finish = [&](const dev::CompletionRec& r) {
-    const uint32_t id = (uint32_t)r.id, len = rl[id];
-    std::vector<dev::WalkOp> path;
-    uint32_t v = r.vertex;
-    if (len > 1) {
-      dev::k_walk<uint16_t><<<1, 1, 0, c.side>>>(c.g->gp, hm[id], pitch, 0, (long long)len - 1, r.vertex,
-                                                  c.reads.p + roff[id], ops_buf.p, (uint32_t)max_ops,
-                                                  wout.p, match_n(c));
-      check_launch();
-      dev::WalkOut h{};
-      CK(cudaMemcpyAsync(&h, wout.p, sizeof(h), cudaMemcpyDeviceToHost, c.side));
-      CK(cudaStreamSynchronize(c.side));
-      if (h.status == 7)
-        fail(CHSGA_ERR_NO_PATH, "score-matrix traceback: no valid predecessor at row " +
-                                    std::to_string(h.fail_row));
-      require(h.status == 0, CHSGA_ERR_INTERNAL, "traceback walk exceeded its op budget");
-      if (h.nops)
-        CK(cudaMemcpy(hops.data(), ops_buf.p, h.nops * sizeof(dev::WalkOp), cudaMemcpyDeviceToHost));
-      path.assign(hops.begin(), hops.begin() + h.nops);
-      v = h.vertex;
-    }
-    path.push_back(dev::WalkOp{0, v, CHSGA_OP_MATCHSUB});
-    fill_result(&out[idx[id]], path, r.score);
-    CK(cudaFreeAsync(hm[id], c.side));
-    hm[id] = nullptr;
-    used -= (uint64_t)len * pitch * 2;
-  };
+  // the walks of every read finished by a harvested block, launched back to
+  // back on the side stream (the engine stream runs the next block), then
+  // one synchronisation for all of them
   auto harvest = [&](int k) {
     CK(cudaEventSynchronize(ev[k]));
     const dev::StepCtl& st = hctl.p[k];
     require(st.error == 0, CHSGA_ERR_TIMEOUT,
             "a bounded device-side wait expired (code " + std::to_string(st.error) + ")");
-    for (uint32_t i = hdone; i < st.done; ++i) finish(hring.p[(size_t)k * nf + i]);
+    for (uint32_t i0 = hdone; i0 < st.done; i0 += wcap) {
+      const uint32_t i1 = std::min<uint32_t>(st.done, i0 + wcap);
+      for (uint32_t i = i0; i < i1; ++i) {
+        const dev::CompletionRec& r = hring.p[(size_t)k * nf + i];
+        const uint32_t id = (uint32_t)r.id, len = rl[id], j = i - i0;
+        if (len > 1)
+          dev::k_walk<uint16_t><<<1, 1, 0, c.side>>>(c.g->gp, hm[id], pitch, 0, (long long)len - 1,
+                                                      r.vertex, c.reads.p + roff[id],
+                                                      ops_buf.p + (size_t)j * max_ops, (uint32_t)max_ops,
+                                                      wout.p + j, match_n(c));
+      }
+      check_launch();
+      CK(cudaMemcpyAsync(hout.data(), wout.p, (i1 - i0) * sizeof(dev::WalkOut), cudaMemcpyDeviceToHost,
+                         c.side));
+      CK(cudaStreamSynchronize(c.side));
+      for (uint32_t i = i0; i < i1; ++i) {
+        const dev::CompletionRec& r = hring.p[(size_t)k * nf + i];
+        const uint32_t id = (uint32_t)r.id, len = rl[id], j = i - i0;
+        std::vector<dev::WalkOp> path;
+        uint32_t v = r.vertex;
+        if (len > 1) {
+          const dev::WalkOut& h = hout[j];
+          if (h.status == 7)
+            fail(CHSGA_ERR_NO_PATH, "score-matrix traceback: no valid predecessor at row " +
+                                        std::to_string(h.fail_row));
+          require(h.status == 0, CHSGA_ERR_INTERNAL, "traceback walk exceeded its op budget");
+          if (h.nops)
+            CK(cudaMemcpy(hops.data(), ops_buf.p + (size_t)j * max_ops, h.nops * sizeof(dev::WalkOp),
+                          cudaMemcpyDeviceToHost));
+          path.assign(hops.begin(), hops.begin() + h.nops);
+          v = h.vertex;
+        }
+        path.push_back(dev::WalkOp{0, v, CHSGA_OP_MATCHSUB});
+        fill_result(&out[idx[id]], path, r.score);
+        CK(cudaFreeAsync(hm[id], c.side));
+        hm[id] = nullptr;
+        used -= (uint64_t)len * pitch * 2;
+      }
+    }
     hdone = st.done;
   };
   try {
@@ -1882,8 +1907,9 @@ chsga_status chsga_align_traceback_batched(chsga_ctx* c, const char* const* read
   return guarded_ctx(c, [&] {
     require(c && (n == 0 || (reads && lens && out)), CHSGA_ERR_INVALID_ARG, "null argument");
     require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
-    if (!slots) slots = 32;
-    require(slots == 16 || slots == 32 || slots == 64, CHSGA_ERR_INVALID_ARG, "slots must be 16, 32 or 64");
+    if (!slots) slots = 64;
+    require(slots == 4 || slots == 8 || slots == 16 || slots == 32 || slots == 64, CHSGA_ERR_INVALID_ARG,
+            "slots must be 4, 8, 16, 32 or 64");
     for (uint32_t i = 0; i < n; ++i) {
       require(reads[i] && lens[i] > 0, CHSGA_ERR_INVALID_ARG, "traceback of an empty read");
       std::memset(&out[i], 0, sizeof(out[i]));
@@ -1900,14 +1926,33 @@ chsga_status chsga_align_traceback_batched(chsga_ctx* c, const char* const* read
     }
     std::stable_sort(full.begin(), full.end(), [&](uint32_t a, uint32_t b) { return lens[a] > lens[b]; });
     try {
-      if (full.size() > 1) {
-        switch (slots) {
-          case 16: traceback_batched<16>(*c, reads, lens, full, out); break;
-          case 32: traceback_batched<32>(*c, reads, lens, full, out); break;
-          default: traceback_batched<64>(*c, reads, lens, full, out); break;
+      // groups of reads (longest first) whose 16-bit matrices fit together
+      // `slots` at a time; a group whose matrices are large runs with fewer
+      // slots (idle slots would still cost a full row-step each)
+      const uint64_t mem = (uint64_t)(device_free_bytes(*c) * 0.6);
+      const uint64_t pitch_b = (uint64_t)c->g->pitch * 2;
+      size_t g0 = 0;
+      while (g0 < full.size()) {
+        const uint64_t mb = (uint64_t)lens[full[g0]] * pitch_b;  // the group's largest matrix
+        uint32_t fit = (uint32_t)std::min<uint64_t>(slots, std::max<uint64_t>(1, mem / std::max<uint64_t>(mb, 1)));
+        uint32_t R = 64;
+        while (R > fit && R > 4) R >>= 1;
+        // the group: reads while a matrix at most half as large cannot run with more slots
+        size_t g1 = g0 + 1;
+        while (g1 < full.size() && (uint64_t)lens[full[g1]] * pitch_b * 2 > mb) ++g1;
+        std::vector<uint32_t> grp(full.begin() + g0, full.begin() + g1);
+        if (grp.size() == 1) {
+          rest.push_back(grp[0]);
+        } else {
+          switch (std::min(R, slots)) {
+            case 4: traceback_batched<4>(*c, reads, lens, grp, out); break;
+            case 8: traceback_batched<8>(*c, reads, lens, grp, out); break;
+            case 16: traceback_batched<16>(*c, reads, lens, grp, out); break;
+            case 32: traceback_batched<32>(*c, reads, lens, grp, out); break;
+            default: traceback_batched<64>(*c, reads, lens, grp, out); break;
+          }
         }
-      } else {
-        rest.insert(rest.end(), full.begin(), full.end());
+        g0 = g1;
       }
       for (uint32_t i : rest) traceback(*c, reads[i], lens[i], opts, &out[i]);
     } catch (...) {

@@ -354,11 +354,13 @@ void chsga_tb_result_free(chsga_tb_result* r);
 
 /* Tracebacks of many reads; each result equals chsga_align_traceback on that
  * read. Reads whose full matrix fits the cap (and are at most 65000 bases,
- * with no checkpoint directory requested) run together as the `slots`
- * (16, 32 or 64; 0 = 32) of the batched engine with every row final: after
- * each row-step the rows are copied into one 16-bit matrix per read, and a
- * read is walked as soon as it finishes. The others take the one-read
- * checkpointed path. Batching has no reference counterpart (the reference
+ * with no checkpoint directory requested) run together as slots of the
+ * batched engine with every row final: after each row-step the rows are
+ * copied into one 16-bit matrix per read, and a read is walked as soon as it
+ * finishes. Reads are taken longest first in groups of similar length, each
+ * group with as many slots (4 to `slots`, a power of two; 0 = 64) as its
+ * matrices fit in device memory together. The others take the one-read
+ * path. Batching has no reference counterpart (the reference
  * traces reads one after another, src/ConSGA_traceback.cpp:160-180). */
 chsga_status chsga_align_traceback_batched(chsga_ctx* ctx, const char* const* reads,
                                            const uint32_t* lens, uint32_t n,
