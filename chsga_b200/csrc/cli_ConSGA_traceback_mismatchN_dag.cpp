@@ -4,6 +4,9 @@
 //   ConSGA_traceback_mismatchN_dag [-b] -I char.adj -i string.adj -c string.out
 //       -r reads -l char.labels -o string.label_offsets [-k rows] [-d dir]
 //
+// CHSGA_SLOTS >= 4 traces all reads through chsga_align_traceback_batched
+// (same paths; unless CHSGA_CKPT_FILES asks for checkpoint row files).
+//
 // Default mode verifies: forward scores, traceback of every read, then each
 // path is rescored under the fixed costs and must equal the forward score and
 // end on the last read row; exit status 0 iff all checks pass. -b times the
@@ -121,7 +124,16 @@ int main(int argc, char** argv) {
   std::cout << "  (checkpoint every k=" << k << " rows, dir=" << dir << ")\n";
   auto t0 = std::chrono::high_resolution_clock::now();
   std::vector<chsga_tb_result> res(n);
-  for (uint64_t ri = 0; ri < n; ++ri) run_tb(ri, &res[ri]);
+  const uint32_t slots = (uint32_t)cli::env_u64("CHSGA_SLOTS", 0);
+  if (slots >= 4 && !files) {
+    // every read at once: full-matrix reads through the batched engine
+    chsga_tb_opts t{k, nullptr, keep ? 1 : 0, 0};
+    cli::check(chsga_align_traceback_batched(ctx, ptrs.data(), lens.data(), (uint32_t)n, &t,
+                                             std::min<uint32_t>(slots, 64), res.data()),
+               ctx, "chsga_align_traceback_batched");
+  } else {
+    for (uint64_t ri = 0; ri < n; ++ri) run_tb(ri, &res[ri]);
+  }
   const double ms = std::chrono::duration<double, std::milli>(
                         std::chrono::high_resolution_clock::now() - t0).count();
   bool all_ok = true;

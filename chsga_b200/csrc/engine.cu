@@ -1919,7 +1919,9 @@ chsga_status chsga_align_traceback_batched(chsga_ctx* c, const char* const* read
     const uint64_t row_bytes = (uint64_t)c->g->L.N * 4;
     std::vector<uint32_t> full, rest;
     for (uint32_t i = 0; i < n; ++i) {
-      if (lens[i] <= kRow16Max && (uint64_t)lens[i] * row_bytes <= cap && !(opts && opts->dir))
+      // (a full-matrix traceback never writes checkpoint files, so a
+      // checkpoint directory does not keep a read off the batched path)
+      if (lens[i] <= kRow16Max && (uint64_t)lens[i] * row_bytes <= cap)
         full.push_back(i);
       else
         rest.push_back(i);
