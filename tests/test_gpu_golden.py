@@ -113,8 +113,8 @@ def test_cli_traceback_verification_matches_reference_driver(tmp_path):
                              ["-d", str(tmp_path / "c")], capture_output=True, text=True, timeout=300,
                              env=dict(os.environ, CHSGA_SLOTS="8"))
     assert batched.returncode == 0, batched.stdout + batched.stderr
-    for pat in (pat, r"^  CIGAR      : .*$", r"score_ok   : \w+"):
-        assert re.findall(pat, batched.stdout, re.M) == re.findall(pat, ours.stdout, re.M)
+    for line in (pat, r"^  CIGAR      : .*$", r"score_ok   : \w+"):
+        assert re.findall(line, batched.stdout, re.M) == re.findall(line, ours.stdout, re.M)
     # -b benchmark mode prints the reference's summary lines
     b = subprocess.run([os.path.join(BIN, "ConSGA_traceback_mismatchN_dag"), "-b"] + args,
                        capture_output=True, text=True, timeout=300)
