@@ -397,7 +397,7 @@ void validate_row_tiles(const HostLayout& L, uint32_t R, uint32_t sz, const Host
 }
 
 HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edges) {
-  require(max_vertices < 32768 && chunk_edges >= 2 && chunk_edges % 2 == 0, CHSGA_ERR_INTERNAL,
+  require(max_vertices < 32768 && chunk_edges >= 32 && chunk_edges % 32 == 0, CHSGA_ERR_INTERNAL,
           "top region limits");
   HostTop t;
   uint32_t first = L.levels;
@@ -414,6 +414,15 @@ HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edg
     t.upg_off[j + 1] = (uint32_t)t.upg.size();
   }
   const EdgeW pad{(int32_t)(t.K << 16), 0};  // scratch target K, source 0
+  // a run of small levels (<= kTopWarpLevelMax edges each) forms one warp
+  // chunk: every level padded to whole rounds of 32 edges, count negative
+  std::vector<EdgeW> warp;
+  auto flush_warp = [&] {
+    if (warp.empty()) return;
+    t.chunks.push_back({(int32_t)t.sched.size(), -(int32_t)warp.size()});
+    t.sched.insert(t.sched.end(), warp.begin(), warp.end());
+    warp.clear();
+  };
   auto emit_level = [&](uint32_t l, bool up) {
     std::vector<EdgeW> es;
     for (uint32_t d = L.lvl_off[l]; d < L.lvl_off[l + 1]; ++d) {
@@ -428,6 +437,15 @@ HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edg
         es.push_back({(int32_t)((j << 16) | (uint32_t)(in[e].src - lo)), in[e].w});
       }
     }
+    if (es.empty()) return;
+    if (es.size() <= kTopWarpLevelMax) {
+      const size_t rounds = (es.size() + 31) / 32;
+      if (warp.size() + 32 * rounds > chunk_edges) flush_warp();
+      warp.insert(warp.end(), es.begin(), es.end());
+      warp.resize(warp.size() + (32 * rounds - es.size()), pad);
+      return;
+    }
+    flush_warp();
     for (size_t i = 0; i < es.size(); i += chunk_edges) {
       const size_t n = std::min<size_t>(chunk_edges, es.size() - i);
       t.chunks.push_back({(int32_t)t.sched.size(), (int32_t)(n + (n & 1))});
@@ -437,6 +455,7 @@ HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edg
   };
   for (uint32_t l = first; l < L.levels; ++l) emit_level(l, true);
   for (uint32_t l = L.levels; l-- > first;) emit_level(l, false);
+  flush_warp();
   return t;
 }
 

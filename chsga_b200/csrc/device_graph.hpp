@@ -70,13 +70,17 @@ struct HostLayout {
 // own edges run as a chunk schedule: upward levels low -> high, then
 // downward levels high -> low, each chunk at most kTopChunk edges of one
 // level, padded to an even count with a no-op edge into the scratch slot K.
+// Consecutive levels of at most kTopWarpLevelMax edges share one warp chunk
+// instead (count stored negated): each level padded with no-op edges to
+// whole rounds of 32, the rounds run in order by one warp.
+constexpr uint32_t kTopWarpLevelMax = 64;
 struct HostTop {
   uint32_t first_level = 0;  // level index where the top region starts
   uint32_t K0 = 0, K = 0;    // hierarchy positions [K0, K0+K)
   std::vector<uint32_t> upg_off;  // K+1
   std::vector<EdgeW> upg;         // global source index
   std::vector<EdgeW> sched;       // src = target << 16 | local source, w
-  std::vector<std::pair<int32_t, int32_t>> chunks;  // {first edge, count}
+  std::vector<std::pair<int32_t, int32_t>> chunks;  // {first edge, count (< 0: warp chunk)}
 };
 
 // Tiles of consecutive string vertices for the shared-memory-staged row

@@ -454,8 +454,12 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   for (uint32_t l = 0; l < fl; ++l) {
     if (L.lvl_up_edges[l] == 0) continue;
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
-    dev::k_pull_lv<R, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-        BVc, lo, hi, c.g->gd.up_head.p, c.g->gd.up_in.p, b.ctl.p);
+    if constexpr (std::is_same_v<ST, uint16_t> && R >= 8)
+      dev::k_pull_lv16<R><<<nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s>>>(
+          BVc, lo, hi, c.g->gd.up_head.p, c.g->gd.up_in.p, b.ctl.p);
+    else
+      dev::k_pull_lv<R, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
+          BVc, lo, hi, c.g->gd.up_head.p, c.g->gd.up_in.p, b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[2], s));
   if (top.h.K) {

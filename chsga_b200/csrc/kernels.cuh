@@ -1307,6 +1307,69 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
 }
 
 // ---------------------------------------------------------------------------
+// k_pull_lv16: k_pull_lv for 16-bit rows and R >= 8 slots. A lane holds 8
+// slots (16 bytes) as four u16x2 words and relaxes them with a saturating
+// add and a min, so a position takes R / 8 lanes and a warp keeps twice the
+// bytes in flight of the one-word-per-slot form. Saturation is exact here:
+// every stored score is below 65535, so a sum that clamps never wins the
+// min, as in the int form. Edges beyond the two in the head are fetched four
+// at a time, their sources gathered together.
+// ---------------------------------------------------------------------------
+template <int R>
+__global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, uint32_t lo,
+                                                   uint32_t hi, const uint4* __restrict__ head,
+                                                   const int2* __restrict__ edges,
+                                                   const StepCtl* __restrict__ ctl) {
+  static_assert(R >= 8 && R % 8 == 0, "8 slots per lane");
+  constexpr int G = R / 8, B = 4;
+  if (!ctl->any_active) return;
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  const int lane = (int)(gt % G);
+  if (d >= hi) return;
+  const uint4 h = __ldg(head + 2 * (size_t)d);
+  const uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
+  if (h.x == h.y) return;
+  const size_t so = (size_t)lane * 8;
+  uint4* p = reinterpret_cast<uint4*>(BV + (size_t)(2 * d) * R + so);
+  auto src = [&](uint32_t i) { return __ldg(reinterpret_cast<const uint4*>(BV + (size_t)i * R + so)); };
+  const uint4 f0 = *p;
+  uint4 f = f0;
+  auto relax = [&](const uint4& x, uint32_t w) {
+    const uint32_t ww = min(w, 0xFFFFu) * 0x10001u;
+    f.x = __vminu2(f.x, __vaddus2(x.x, ww));
+    f.y = __vminu2(f.y, __vaddus2(x.y, ww));
+    f.z = __vminu2(f.z, __vaddus2(x.z, ww));
+    f.w = __vminu2(f.w, __vaddus2(x.w, ww));
+  };
+  const bool two = h.y - h.x > 1;
+  const uint4 x0 = src(h.z);
+  uint4 x1 = x0;
+  if (two) x1 = src(h2.x);
+  uint32_t k = h.x + 2;
+  int2 e[B];
+#pragma unroll
+  for (int q = 0; q < B; ++q) e[q] = k + q < h.y ? __ldg(edges + k + q) : make_int2(0, 0);
+  relax(x0, h.w);
+  if (two) relax(x1, h2.y);
+  for (; k < h.y; k += B) {
+    uint4 x[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q)
+      if (k + q < h.y) x[q] = src((uint32_t)e[q].x);
+#pragma unroll
+    for (int q = 0; q < B; ++q)
+      if (k + q < h.y) relax(x[q], (uint32_t)e[q].y);
+    if (k + B < h.y) {
+#pragma unroll
+      for (int q = 0; q < B; ++q)
+        e[q] = k + B + q < h.y ? __ldg(edges + k + B + q) : make_int2(0, 0);
+    }
+  }
+  if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
+}
+
+// ---------------------------------------------------------------------------
 // k_down: positions [lo, hi). Those below `mid` first pull their downward
 // in-edges (sources on higher levels, final); every position then finalises
 // its vertex's chars: if the first score fell below the row value, write it
@@ -1473,7 +1536,7 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
   if (threadIdx.x == 0) {
     for (uint32_t c = 0; c < kTopBufs && c < t.nchunks; ++c) {
       const int2 ch = t.chunk[c];
-      bulk_load(ebuf + c * kTopChunk, t.edges + ch.x, (uint32_t)ch.y * 8, &bar[c]);
+      bulk_load(ebuf + c * kTopChunk, t.edges + ch.x, (uint32_t)abs(ch.y) * 8, &bar[c]);
     }
   }
   int n_next = t.nchunks ? __ldg(&t.chunk[0].y) : 0;
@@ -1516,20 +1579,31 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
     const uint32_t b = c % kTopBufs;
     const int n = n_next;
     if (c + 1 < t.nchunks) n_next = __ldg(&t.chunk[c + 1].y);
-    // a thread whose wait expires flags it and still reaches the barrier
-    // below, so the whole block leaves the loop together
-    if (!mbar_wait(&bar[b], (c / kTopBufs) & 1)) s_fail = 1;
+    // a thread whose wait expires flags it, skips the chunk and still
+    // reaches the barrier below, so the whole block leaves the loop together
+    const bool ok = mbar_wait(&bar[b], (c / kTopBufs) & 1);
+    if (!ok) s_fail = 1;
     const int2* e = ebuf + b * kTopChunk;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const int2 x = e[i];
-      atomicMin(&sm[2 * (x.x >> 16)], sm[x.x & 0xFFFF] + x.y);
+    if (ok && n >= 0) {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int2 x = e[i];
+        atomicMin(&sm[2 * (x.x >> 16)], sm[x.x & 0xFFFF] + x.y);
+      }
+    } else if (ok && threadIdx.x < 32) {
+      // warp chunk: a run of small levels in rounds of 32 edges, each level
+      // whole rounds, the rounds ordered by the warp barrier
+      for (int i = threadIdx.x; i < -n; i += 32) {
+        const int2 x = e[i];
+        atomicMin(&sm[2 * (x.x >> 16)], sm[x.x & 0xFFFF] + x.y);
+        __syncwarp();
+      }
     }
     __syncthreads();
     if (s_fail) break;
     if (threadIdx.x == 0 && c + kTopBufs < t.nchunks) {
       fence_async_shared();
       const int2 ch = t.chunk[c + kTopBufs];
-      bulk_load(ebuf + b * kTopChunk, t.edges + ch.x, (uint32_t)ch.y * 8, &bar[b]);
+      bulk_load(ebuf + b * kTopChunk, t.edges + ch.x, (uint32_t)abs(ch.y) * 8, &bar[b]);
     }
   }
   if (s_fail) {
