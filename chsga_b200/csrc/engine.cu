@@ -248,7 +248,9 @@ const TopDev& cur_top(const chsga_ctx& c) { return c.top_sel ? *c.top_sel : *c.g
 // highest down, while they fit) and its chunk schedule, on the device.
 std::unique_ptr<TopDev> make_top(const HostLayout& L, const GraphDev& d, uint32_t K, cudaStream_t s) {
   auto top = std::make_unique<TopDev>();
-  top->h = build_top(L, K, dev::kTopChunk);
+  const uint32_t cap = dev::top_chunk_for(
+      (uint32_t)std::min<size_t>(K, L.S), dev::top_smem_bytes(kTopMaxVertices));
+  top->h = build_top(L, K, cap);
   const HostTop& h = top->h;
   auto to2 = [](const std::vector<EdgeW>& v) {
     std::vector<int2> o(v.size());
@@ -262,7 +264,7 @@ std::unique_ptr<TopDev> make_top(const HostLayout& L, const GraphDev& d, uint32_
   for (size_t i = 0; i < ch.size(); ++i) ch[i] = make_int2(h.chunks[i].first, h.chunks[i].second);
   top->chunks.upload(ch, s);
   top->ptrs = dev::TopPtrs{h.K0, h.K, (uint32_t)h.chunks.size(), top->chunks.p, top->sched.p,
-                           d.dv_len.p};
+                           d.dv_len.p, cap};
   CK(cudaStreamSynchronize(s));
   return top;
 }
@@ -466,19 +468,24 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
     if (!top.h.upg.empty())
       dev::k_pull<R, ST><<<nblocks((uint64_t)top.h.K * G), 256, 0, s>>>(
           BVc, top.h.K0, L.S, top.upg_off.p, top.upg.p, top.h.K0, b.ctl.p);
-    dev::k_top<R, ST><<<R, kTopThreads, dev::top_smem_bytes(top.h.K), s>>>(BVc, top.ptrs, b.word.p,
+    dev::k_top<R, ST><<<R, kTopThreads, dev::top_smem_bytes(top.h.K, top.ptrs.chunk_cap), s>>>(BVc, top.ptrs, b.word.p,
                                                                        b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[3], s));
+  auto down = [&](uint32_t lo, uint32_t mid, uint32_t hi) {
+    if constexpr (std::is_same_v<ST, uint16_t> && DEFER && R >= 8)
+      dev::k_down16<R><<<nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s>>>(
+          c.g->gp, BVc, FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
+    else
+      dev::k_down<R, !DEFER, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
+          c.g->gp, BVc, T, FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
+  };
   if (fl == 0) {
-    dev::k_down<R, !DEFER, ST><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(
-        c.g->gp, BVc, T, FL, 0, 0, L.S, b.word.p, b.best.p, b.ctl.p);
+    down(0, 0, L.S);
   } else {
     for (int l = (int)fl - 1; l >= 0; --l) {
       const uint32_t lo = L.lvl_off[l], mid = L.lvl_off[l + 1];
-      const uint32_t hi = (l == (int)fl - 1) ? L.S : mid;
-      dev::k_down<R, !DEFER, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-          c.g->gp, BVc, T, FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
+      down(lo, mid, (l == (int)fl - 1) ? L.S : mid);
     }
   }
   if constexpr (std::is_same_v<ST, uint16_t> && !DEFER && R >= 2) {
@@ -1260,7 +1267,7 @@ void noalloc_row_step(chsga_ctx& c, const NoallocBufs& b, const uint16_t* D, uin
     if (!top.h.upg.empty())
       dev::k_pull<1, uint16_t><<<nblocks((uint64_t)top.h.K * G), 256, 0, s>>>(
           b.BV, top.h.K0, L.S, top.upg_off.p, top.upg.p, top.h.K0, b.ctl);
-    dev::k_top<1, uint16_t><<<1, kTopThreads, dev::top_smem_bytes(top.h.K), s>>>(b.BV, top.ptrs,
+    dev::k_top<1, uint16_t><<<1, kTopThreads, dev::top_smem_bytes(top.h.K, top.ptrs.chunk_cap), s>>>(b.BV, top.ptrs,
                                                                                b.word, b.ctl);
   }
   if (fl == 0) {

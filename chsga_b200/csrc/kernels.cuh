@@ -1490,6 +1490,82 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
 }
 
 // ---------------------------------------------------------------------------
+// k_down16: k_down without the row fix-up (score-only steps) for 16-bit rows
+// and R >= 8 slots, 8 slots per lane as four u16x2 words: the downward pull
+// by saturating add and min (exact, as in k_pull_lv16), then the vertex's
+// final first and last scores into FL and the first scores of slots on
+// their last row into the per-slot minimum.
+// ---------------------------------------------------------------------------
+template <int R>
+__global__ void __launch_bounds__(256) k_down16(GraphPtrs g, uint16_t* __restrict__ BV,
+                                                uint16_t* __restrict__ FL, uint32_t lo,
+                                                uint32_t mid, uint32_t hi,
+                                                const uint32_t* __restrict__ slot_word,
+                                                unsigned long long* __restrict__ best,
+                                                const StepCtl* __restrict__ ctl) {
+  static_assert(R >= 8 && R % 8 == 0, "8 slots per lane");
+  constexpr int G = R / 8;
+  __shared__ unsigned long long sm_best[R];
+  const bool ending_any = ctl->any_ending != 0;
+  if (!ctl->any_active) return;
+  if (ending_any) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
+    __syncthreads();
+  }
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  const int lane = (int)(gt % G);
+  if (d < hi) {
+    const size_t so = (size_t)lane * 8;
+    uint4* p = reinterpret_cast<uint4*>(BV + (size_t)(2 * d) * R + so);
+    auto src = [&](uint32_t i) {
+      return __ldg(reinterpret_cast<const uint4*>(BV + (size_t)i * R + so));
+    };
+    const uint4 h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
+    const uint4 m = __ldg(g.fin + d);
+    const uint4 f0 = *p;
+    const uint4 raw = *reinterpret_cast<const uint4*>(BV + (size_t)(2 * d + 1) * R + so);
+    uint4 f = f0;
+    auto relax = [&](const uint4& x, uint32_t w) {
+      const uint32_t ww = min(w, 0xFFFFu) * 0x10001u;
+      f.x = __vminu2(f.x, __vaddus2(x.x, ww));
+      f.y = __vminu2(f.y, __vaddus2(x.y, ww));
+      f.z = __vminu2(f.z, __vaddus2(x.z, ww));
+      f.w = __vminu2(f.w, __vaddus2(x.w, ww));
+    };
+    if (h.y > h.x) {
+      relax(src(h.z), h.w);
+      for (uint32_t k = h.x + 1; k < h.y; ++k) {
+        const int2 ew = __ldg(g.dn_in + k);
+        relax(src((uint32_t)ew.x), (uint32_t)ew.y);
+      }
+      if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
+    }
+    const uint32_t first = m.x, len = m.y, sv = m.z;
+    uint4 lf = f;
+    if (len > 1) {
+      const uint32_t ww = min(len - 1, 0xFFFFu) * 0x10001u;
+      lf.x = __vminu2(raw.x, __vaddus2(f.x, ww));
+      lf.y = __vminu2(raw.y, __vaddus2(f.y, ww));
+      lf.z = __vminu2(raw.z, __vaddus2(f.z, ww));
+      lf.w = __vminu2(raw.w, __vaddus2(f.w, ww));
+    }
+    *reinterpret_cast<uint4*>(FL + (size_t)(2 * sv) * R + so) = f;
+    *reinterpret_cast<uint4*>(FL + (size_t)(2 * sv + 1) * R + so) = lf;
+    if (ending_any) {
+      const uint32_t fw[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {
+        const uint32_t w = __ldg(slot_word + so + v);
+        if ((w & SW_CLOSURE) && (w & SW_ENDING))
+          atomicMin(sm_best + so + v, pack_min((int)((fw[v >> 1] >> (16 * (v & 1))) & 0xFFFFu), first));
+      }
+    }
+  }
+  if (ending_any) flush_min<R>(sm_best, best);
+}
+
+// ---------------------------------------------------------------------------
 // k_top: hierarchy positions [K0, S), one CTA per slot. The first/last
 // scores of the region are staged in shared memory; the region's upward
 // levels (low -> high) and downward levels (high -> low) then run as a
@@ -1503,18 +1579,30 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
 // sources final. Edges from below the region were applied by k_pull
 // before launch.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kTopChunk = 1024;  // edges per chunk (8 KiB)
-constexpr uint32_t kTopBufs = 4;      // chunk buffers (copies in flight + the one in use)
+constexpr uint32_t kTopChunk = 1024;     // edges per chunk (8 KiB): the smallest chunk size
+constexpr uint32_t kTopChunkMax = 4096;  // largest chunk size, for regions that leave room
+constexpr uint32_t kTopBufs = 4;         // chunk buffers (copies in flight + the one in use)
 
 struct TopPtrs {
   uint32_t K0, K, nchunks;
-  const int2* chunk;   // nchunks x {first edge, edge count (even)}
+  const int2* chunk;   // nchunks x {first edge, edge count (even; < 0: warp chunk)}
   const int2* edges;   // chunk edges in schedule order, 16-byte aligned chunks
   const uint32_t* dv_len;  // global, by hierarchy position
+  uint32_t chunk_cap;  // edges per chunk buffer
 };
 
-__host__ __device__ constexpr size_t top_smem_bytes(uint32_t K) {
-  return ((size_t)(2 * K + 2) * 4 + 15) / 16 * 16 + kTopBufs * kTopChunk * 8 + kTopBufs * 8;
+__host__ __device__ constexpr size_t top_smem_bytes(uint32_t K, uint32_t chunk_cap = kTopChunk) {
+  return ((size_t)(2 * K + 2) * 4 + 15) / 16 * 16 + kTopBufs * (size_t)chunk_cap * 8 + kTopBufs * 8;
+}
+
+// Chunk size of a region of K vertices: the largest power of two up to
+// kTopChunkMax whose buffers keep the block within `smem_cap` bytes, so
+// fewer block barriers split the big levels (chunks of one level need none
+// between them but for the buffer ring).
+inline uint32_t top_chunk_for(uint32_t K, size_t smem_cap) {
+  uint32_t c = kTopChunkMax;
+  while (c > kTopChunk && top_smem_bytes(K, c) > smem_cap) c /= 2;
+  return c;
 }
 
 template <int R, typename ST>
@@ -1527,7 +1615,7 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
   if (!(slot_word[r] & SW_CLOSURE)) return;
   int* sm = reinterpret_cast<int*>(top_smem);  // [2j] first, [2j+1] last, [2K] scratch
   int2* ebuf = reinterpret_cast<int2*>(top_smem + ((size_t)(2 * t.K + 2) * 4 + 15) / 16 * 16);
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(ebuf + kTopBufs * kTopChunk);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(ebuf + kTopBufs * t.chunk_cap);
   if (threadIdx.x == 0) {
     for (uint32_t b = 0; b < kTopBufs; ++b) mbar_init(&bar[b], 1);
     fence_async_shared();
@@ -1536,7 +1624,7 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
   if (threadIdx.x == 0) {
     for (uint32_t c = 0; c < kTopBufs && c < t.nchunks; ++c) {
       const int2 ch = t.chunk[c];
-      bulk_load(ebuf + c * kTopChunk, t.edges + ch.x, (uint32_t)abs(ch.y) * 8, &bar[c]);
+      bulk_load(ebuf + c * t.chunk_cap, t.edges + ch.x, (uint32_t)abs(ch.y) * 8, &bar[c]);
     }
   }
   int n_next = t.nchunks ? __ldg(&t.chunk[0].y) : 0;
@@ -1583,7 +1671,7 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
     // reaches the barrier below, so the whole block leaves the loop together
     const bool ok = mbar_wait(&bar[b], (c / kTopBufs) & 1);
     if (!ok) s_fail = 1;
-    const int2* e = ebuf + b * kTopChunk;
+    const int2* e = ebuf + b * t.chunk_cap;
     if (ok && n >= 0) {
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int2 x = e[i];
@@ -1603,7 +1691,7 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
     if (threadIdx.x == 0 && c + kTopBufs < t.nchunks) {
       fence_async_shared();
       const int2 ch = t.chunk[c + kTopBufs];
-      bulk_load(ebuf + b * kTopChunk, t.edges + ch.x, (uint32_t)abs(ch.y) * 8, &bar[b]);
+      bulk_load(ebuf + b * t.chunk_cap, t.edges + ch.x, (uint32_t)abs(ch.y) * 8, &bar[b]);
     }
   }
   if (s_fail) {
