@@ -163,9 +163,9 @@ def algorithmic_row_bytes(st, slots, multi, score_bytes):
 def algorithmic_sweep_bytes(st, lay, slots, score_bytes):
     """Bytes per row-step of the grid-wide sweep kernels below the top
     region (16-byte pull-list heads and vertex words, w bytes per score):
-    up (k_pull_lv): per target its head, first score read and written, one
+    up (k_pull_lv, k_pull_lv16): per target its head, first score read and written, one
     gathered score per edge, 8 bytes per edge after the first;
-    down (k_down): per position its vertex words, first and raw last score
+    down (k_down, k_down16): per position its vertex words, first and raw last score
     read, final first and last written to FL; per target below the top its
     head, first score written, one gathered score per edge, 8 bytes per edge
     after the first."""
@@ -508,7 +508,7 @@ def main():
     opts = dict(slots=args.slots, steps_per_graph=8, row_kernel=0, top_vertices=0)
     tune = None
     if not args.no_tune:
-        tsample = make_reads(g, 2 * args.slots, 60_000 + rank, len_max=2000)
+        tsample = make_reads(g, 4 * args.slots, 60_000 + rank, len_max=2000)
         best, trials = ctx.autotune(tsample, repeats=1)
         opts = {k: best[k] for k in opts}
         tune = {"chosen": opts, "trials": [
@@ -631,11 +631,15 @@ def main():
         up_b, down_b = algorithmic_sweep_bytes(st, lay, R, pr["row_bits"] // 8)
         up_s = pr["sweep_up_ms"] / max(1, pr["row_launches"]) / 1e3
         down_s = pr["sweep_down_ms"] / max(1, pr["row_launches"]) / 1e3
+        # 16-bit rows with R >= 8 run the packed forms of both sweeps
+        packed = pr["row_bits"] == 16 and R >= 8
         line["roofline"]["sweeps"] = {
-            "k_pull_lv": {"algorithmic_bytes_per_step": up_b, "avg_step_ms": up_s * 1e3,
-                          "achieved": up_b / up_s / 1e9, "frac": up_b / up_s / 1e9 / peak},
-            "k_down": {"algorithmic_bytes_per_step": down_b, "avg_step_ms": down_s * 1e3,
-                       "achieved": down_b / down_s / 1e9, "frac": down_b / down_s / 1e9 / peak},
+            "k_pull_lv16" if packed else "k_pull_lv": {
+                "algorithmic_bytes_per_step": up_b, "avg_step_ms": up_s * 1e3,
+                "achieved": up_b / up_s / 1e9, "frac": up_b / up_s / 1e9 / peak},
+            "k_down16" if packed else "k_down": {
+                "algorithmic_bytes_per_step": down_b, "avg_step_ms": down_s * 1e3,
+                "achieved": down_b / down_s / 1e9, "frac": down_b / down_s / 1e9 / peak},
             "top_region": "levels >= %d (%d vertices) run in k_top, latency-bound" % (
                 lay["top_first_level"], lay["top_vertices"]),
         }

@@ -373,7 +373,8 @@ chsga_status chsga_align_traceback_batched(chsga_ctx* ctx, const char* const* re
 uint64_t chsga_ops_to_cigar(const chsga_op* ops, uint64_t n, char* buf, uint64_t cap);
 
 /* Device timing of the last score call. total_ms: CUDA-event time of the
- * whole device sequence (every row-step, reads already resident). With
+ * whole device sequence (every row-step, reads already resident; the batched
+ * engine's CUDA graph is built on the host before the first event). With
  * CHSGA_FLAG_PROFILE (CUDA graphs off, one sync per row-step) the five kernel
  * groups of every row-step are timed with CUDA events: row_ms (k_row),
  * sweep_up_ms (upward level kernels), top_ms (top region), sweep_down_ms
