@@ -77,7 +77,8 @@ class GenGraphCfg(C.Structure):
 class PchOpts(C.Structure):
     _fields_ = [("max_pop_count", C.c_uint32), ("sample_bound", C.c_double),
                 ("weight_bound", C.c_uint64), ("use_label_lengths", C.c_int),
-                ("seed", C.c_uint64), ("threads", C.c_int), ("print_detail", C.c_int)]
+                ("seed", C.c_uint64), ("threads", C.c_int), ("print_detail", C.c_int),
+                ("use_gpu", C.c_int), ("device", C.c_int)]
 
 
 class GenReadsCfg(C.Structure):
@@ -361,9 +362,11 @@ class HostGraph:
         return cls(h)
 
     def build_pch(self, max_pop_count=500, sample_bound=1.0, weight_bound=0, use_label_lengths=True,
-                  seed=0x5EED, threads=0, print_detail=False):
+                  seed=0x5EED, threads=0, print_detail=False, gpu_device=None):
+        """Contraction hierarchy; gpu_device runs the witness searches of each
+        round on that CUDA device (the same hierarchy as the host builder)."""
         o = PchOpts(max_pop_count, sample_bound, weight_bound, int(use_label_lengths), seed, threads,
-                    int(print_detail))
+                    int(print_detail), int(gpu_device is not None), gpu_device or 0)
         _check(_lib.chsga_build_pch(self._h, C.byref(o)))
         return self
 

@@ -4,11 +4,14 @@
 //
 //   build_pch -i string.adj -o string.out [-v string.label_offsets]
 //             [-p max_pop_count] [-s select_fraction] [-k weight_bound] [-d]
+//             [-g cuda_device]
 //
 // Differences from the reference driver: -k only sets the weight bound (the
 // reference's case 'k' falls through into 'v', build_pch.cpp:79-88); -b
 // (degree-bounded contraction, which leaves same-level hierarchy edges) is
-// rejected; -t/-q (query verification counts) are accepted and ignored.
+// rejected; -t/-q (query verification counts) are accepted and ignored; -g
+// (not in the reference) runs each round's witness searches on that CUDA
+// device, with the same resulting hierarchy.
 #include <getopt.h>
 
 #include <chrono>
@@ -32,7 +35,8 @@ int main(int argc, char* argv[]) {
                  "\t-s,\tselect fraction\n"
                  "\t-k,\tshortcut weight bound\n"
                  "\t-v,\tlabel offsets (shortcut weights count the skipped labels)\n"
-                 "\t-d,\tprint per round detail\n",
+                 "\t-d,\tprint per round detail\n"
+                 "\t-g,\tCUDA device for the witness searches\n",
                  argv[0]);
     return 0;
   }
@@ -42,7 +46,7 @@ int main(int argc, char* argv[]) {
   o.sample_bound = 1.0;
   o.seed = 0x5EED;
   int c;
-  while ((c = getopt(argc, argv, "i:o:p:s:t:q:b:dk:v:")) != -1) {
+  while ((c = getopt(argc, argv, "i:o:p:s:t:q:b:dk:v:g:")) != -1) {
     switch (c) {
       case 'i': in = optarg; break;
       case 'o': out = optarg; break;
@@ -68,6 +72,10 @@ int main(int argc, char* argv[]) {
         break;
       }
       case 'v': offs_path = optarg; break;
+      case 'g':
+        o.use_gpu = 1;
+        o.device = std::atoi(optarg);
+        break;
       default: std::fprintf(stderr, "Error: Unknown option %c\n", optopt); return EXIT_FAILURE;
     }
   }

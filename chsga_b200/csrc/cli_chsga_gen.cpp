@@ -72,7 +72,7 @@ int main(int argc, char** argv) {
   if (prefix.empty()) cli::die("usage: chsga_gen -o prefix [options]", "");
   chsga_host_graph* h = nullptr;
   cli::check(chsga_gen_graph(&g, &h), nullptr, "chsga_gen_graph");
-  chsga_pch_opts po{500, 1.0, 0, 1, 0x5EED, 0, 0};
+  chsga_pch_opts po{500, 1.0, 0, 1, 0x5EED, 0, 0, 0, 0};
   cli::check(chsga_build_pch(h, &po), nullptr, "chsga_build_pch");
   cli::check(chsga_graph_write_files(h, prefix.c_str()), nullptr, "chsga_graph_write_files");
   chsga_reads* rd = nullptr;

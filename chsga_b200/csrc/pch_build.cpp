@@ -14,7 +14,10 @@
 //   order            rank by (component, level, id)          build_pch.hpp:1132-1220
 // The upstream builder runs on parlaylib with concurrent hash tables; this
 // one computes the same quantities with per-round snapshots (OpenMP), so
-// selection and contraction within a round see one consistent graph.
+// selection and contraction within a round see one consistent graph. With
+// use_gpu the witness searches of each round run on a CUDA device
+// (pch_gpu.cu) against the same snapshot; a search the device cannot finish
+// within its tables is redone here, so the hierarchy is the same either way.
 #include <omp.h>
 
 #include <algorithm>
@@ -25,6 +28,7 @@
 #include <queue>
 
 #include "host_graph.hpp"
+#include "pch_gpu.hpp"
 
 namespace chsga {
 
@@ -87,6 +91,11 @@ class PchBuilder {
     }
     up_.resize(n_);
     down_.resize(n_);
+    if (opt_.use_gpu) {
+      require(n_ < (1ull << 32) - 1, CHSGA_ERR_UNSUPPORTED, "hierarchy builder: too many vertices");
+      gpu_ = std::make_unique<PchGpu>(opt_.device, pop_limit_);
+      cid_.assign(n_, kNoId);
+    }
     std::vector<uint32_t> remaining(n_);
     std::iota(remaining.begin(), remaining.end(), 0);
     const int nthreads = opt_.threads > 0 ? opt_.threads : omp_get_max_threads();
@@ -98,17 +107,56 @@ class PchBuilder {
       const size_t R = remaining.size();
       std::vector<std::vector<Shortcut>> cuts(R);
       std::vector<std::vector<uint8_t>> in_rel(R);
+      std::vector<uint64_t> toff, masks;
+      if (gpu_) {
+        upload_overlay(remaining, nthreads);
+        // one search per in-arc of every remaining vertex
+        toff.assign(R + 1, 0);
+        for (size_t i = 0; i < R; ++i) toff[i + 1] = toff[i] + in_[remaining[i]].size();
+        std::vector<uint32_t> tu(toff[R]), ts(toff[R]), tw(toff[R]);
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+        for (size_t i = 0; i < R; ++i) {
+          const uint32_t u = remaining[i];
+          for (size_t k = 0; k < in_[u].size(); ++k) {
+            tu[toff[i] + k] = (uint32_t)i;
+            ts[toff[i] + k] = cid_[in_[u][k].v];
+            tw[toff[i] + k] = in_[u][k].w;
+          }
+        }
+        gpu_->run(tu, ts, tw, masks);
+        if (opt_.print_detail) {
+          size_t host = 0;
+          for (uint64_t m : masks) host += (m & kPchOverflow) ? 1 : 0;
+          std::printf("Device witness searches: %zu (redone on the host: %zu)\n", masks.size(), host);
+          std::fflush(stdout);
+        }
+      }
 #pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
       for (size_t i = 0; i < R; ++i)
-        score(remaining[i], cuts[i], in_rel[i], scratch_[omp_get_thread_num()]);
+        score(remaining[i], cuts[i], in_rel[i], scratch_[omp_get_thread_num()],
+              gpu_ ? masks.data() + toff[i] : nullptr);
       double bound = upper_bound(remaining, round);
       std::vector<uint8_t> sel(R, 0);
 #pragma omp parallel for schedule(static) num_threads(nthreads)
       for (size_t i = 0; i < R; ++i) sel[i] = eligible(remaining[i], bound) ? 1 : 0;
       std::vector<std::vector<uint8_t>> out_rel(R);
+      std::vector<uint64_t> rel_of(R, kPchOverflow);
+      if (gpu_) {
+        // one search per selected vertex, same snapshot
+        std::vector<uint32_t> tu, none;
+        std::vector<size_t> at;
+        for (size_t i = 0; i < R; ++i)
+          if (sel[i]) {
+            tu.push_back((uint32_t)i);
+            at.push_back(i);
+          }
+        gpu_->run(tu, none, none, masks);
+        for (size_t k = 0; k < at.size(); ++k) rel_of[at[k]] = masks[k];
+      }
 #pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
       for (size_t i = 0; i < R; ++i)
-        if (sel[i]) out_relevance(remaining[i], out_rel[i], scratch_[omp_get_thread_num()]);
+        if (sel[i])
+          out_relevance(remaining[i], out_rel[i], scratch_[omp_get_thread_num()], rel_of[i]);
       size_t ncontracted = 0;
       for (size_t i = 0; i < R; ++i)
         if (sel[i]) {
@@ -120,6 +168,7 @@ class PchBuilder {
       next.reserve(R - ncontracted);
       for (uint32_t u : remaining)
         if (!contracted_[u]) next.push_back(u);
+        else if (gpu_) cid_[u] = kNoId;
       if (opt_.print_detail)
         std::printf("Round %u\nContract %zu vertices\nOverlay vertices number: %zu\n", round,
                     ncontracted, R);
@@ -191,9 +240,36 @@ class PchBuilder {
     }
   }
 
+  // The overlay snapshot of this round for the device searches: the
+  // remaining vertices renumbered by their index in `remaining` (cid_), as
+  // every arc joins two remaining vertices.
+  void upload_overlay(const std::vector<uint32_t>& remaining, int nthreads) {
+    const size_t R = remaining.size();
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (size_t i = 0; i < R; ++i) cid_[remaining[i]] = (uint32_t)i;
+    std::vector<uint32_t> off(R + 1, 0), thru(R);
+    for (size_t i = 0; i < R; ++i) {
+      require(off[i] + out_[remaining[i]].size() < (1ull << 32), CHSGA_ERR_UNSUPPORTED,
+              "hierarchy builder: overlay above 2^32 arcs");
+      off[i + 1] = off[i] + (uint32_t)out_[remaining[i]].size();
+    }
+    std::vector<uint64_t> arcs(off[R]);
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (size_t i = 0; i < R; ++i) {
+      const uint32_t u = remaining[i];
+      thru[i] = (uint32_t)through(u);
+      for (size_t j = 0; j < out_[u].size(); ++j)
+        arcs[off[i] + j] = cid_[out_[u][j].v] | (uint64_t)out_[u][j].w << 32;
+    }
+    gpu_->set_overlay(off, arcs, thru);
+  }
+
   // Shortcuts contracting u would need, relevance of u's in-arcs, and the
-  // edge-difference score (build_pch.hpp:396-478, 1012-1045).
-  void score(uint32_t u, std::vector<Shortcut>& cuts, std::vector<uint8_t>& in_rel, Scratch& sc) {
+  // edge-difference score (build_pch.hpp:396-478, 1012-1045). masks, when
+  // given, holds the device's answer for each in-arc (pch_gpu.hpp); an
+  // in-arc whose search overflowed there is searched here.
+  void score(uint32_t u, std::vector<Shortcut>& cuts, std::vector<uint8_t>& in_rel, Scratch& sc,
+             const uint64_t* masks) {
     const auto& in = in_[u];
     const auto& out = out_[u];
     in_rel.assign(in.size(), 1);
@@ -202,12 +278,19 @@ class PchBuilder {
     uint64_t added = 0, added_hop = 0;
     for (size_t i = 0; i < in.size(); ++i) {
       const Arc& a = in[i];
-      search(a.v, (uint64_t)a.w + through(u) + max_out, sc);
-      in_rel[i] = sc.get(u) >= a.w ? 1 : 0;
-      for (const Arc& b : out) {
+      const uint64_t m = masks ? masks[i] : kPchOverflow;
+      const bool host = (m & kPchOverflow) != 0;
+      if (host) {
+        search(a.v, (uint64_t)a.w + through(u) + max_out, sc);
+        in_rel[i] = sc.get(u) >= a.w ? 1 : 0;
+      } else {
+        in_rel[i] = (uint8_t)((m >> 62) & 1);
+      }
+      for (size_t j = 0; j < out.size(); ++j) {
+        const Arc& b = out[j];
         if (b.v == a.v) continue;
         uint64_t total = (uint64_t)a.w + b.w + through(u);
-        if (total <= k_ && sc.get(b.v) >= total) {
+        if (total <= k_ && (host ? sc.get(b.v) >= total : ((m >> j) & 1) != 0)) {
           require(total < (1ull << 32), CHSGA_ERR_UNSUPPORTED, "shortcut weight overflow");
           cuts.push_back({a.v, b.v, (uint32_t)total, a.hop + b.hop});
           ++added;
@@ -228,10 +311,15 @@ class PchBuilder {
                      1000.0 * (double)added_hop / removed_hop + 10.0 * removed_arc);
   }
 
-  // Relevance of u's out-arcs: kept unless a strictly shorter u->b path exists.
-  void out_relevance(uint32_t u, std::vector<uint8_t>& rel, Scratch& sc) {
+  // Relevance of u's out-arcs: kept unless a strictly shorter u->b path
+  // exists (the device's mask when it finished the search).
+  void out_relevance(uint32_t u, std::vector<uint8_t>& rel, Scratch& sc, uint64_t mask) {
     const auto& out = out_[u];
     rel.assign(out.size(), 1);
+    if (!(mask & kPchOverflow)) {
+      for (size_t i = 0; i < out.size(); ++i) rel[i] = (uint8_t)((mask >> i) & 1);
+      return;
+    }
     uint64_t max_out = 0;
     for (const Arc& b : out) max_out = std::max<uint64_t>(max_out, b.w);
     search(u, max_out, sc);
@@ -404,6 +492,9 @@ class PchBuilder {
   std::vector<float> ed_;
   std::vector<uint64_t> prio_;
   std::vector<Scratch> scratch_;
+  std::unique_ptr<PchGpu> gpu_;
+  static constexpr uint32_t kNoId = 0xFFFFFFFFu;
+  std::vector<uint32_t> cid_;  // device overlay id of each remaining vertex
   uint32_t max_level_ = 0;
 };
 

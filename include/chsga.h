@@ -152,6 +152,10 @@ typedef struct {
   uint64_t seed;            /* contraction priority permutation */
   int threads;              /* 0 = all */
   int print_detail;         /* -d */
+  int use_gpu;              /* nonzero: each round's witness searches run on CUDA device
+                             * `device` (same hierarchy: a search that outgrows the device's
+                             * per-thread tables is redone on the host) */
+  int device;
 } chsga_pch_opts;
 chsga_status chsga_build_pch(chsga_host_graph* g, const chsga_pch_opts* opts);
 
