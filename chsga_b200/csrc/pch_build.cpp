@@ -21,6 +21,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <parallel/algorithm>
 #include <chrono>
 #include <cstdio>
 #include <limits>
@@ -58,23 +59,50 @@ class PchBuilder {
     }
     k_ = o.weight_bound ? o.weight_bound : kInf;
     pop_limit_ = o.max_pop_count ? o.max_pop_count : 500;
-    // preprocess: sort (u, v, w), drop self loops and repeated (u, v)
-    std::vector<std::tuple<uint32_t, uint32_t, uint32_t>> el;
-    el.reserve(g.m);
-    for (uint64_t u = 0; u < n_; ++u)
+    // preprocess: sort (u, v, w), drop self loops and repeated (u, v). The
+    // sort is by the whole tuple, so any sort gives the same order; every
+    // vertex's out-arcs are a range of it, its in-arcs follow in that order.
+    require(g.offset.size() == n_ + 1 && g.offset[0] == 0 && g.offset[n_] == g.m,
+            CHSGA_ERR_INVALID_ARG, "string graph offsets");
+    const int nthreads = opt_.threads > 0 ? opt_.threads : omp_get_max_threads();
+    std::vector<std::tuple<uint32_t, uint32_t, uint32_t>> el(g.m);
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(nthreads)
+    for (int64_t u = 0; u < (int64_t)n_; ++u)
       for (uint64_t e = g.offset[u]; e < g.offset[u + 1]; ++e)
-        el.emplace_back((uint32_t)u, g.target[e], g.w(e));
-    std::sort(el.begin(), el.end());
+        el[e] = std::make_tuple((uint32_t)u, g.target[e], g.w(e));
+    __gnu_parallel::sort(el.begin(), el.end());
+    const size_t M = el.size();
+    std::vector<uint8_t> keep(M);
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t i = 0; i < (int64_t)M; ++i) {
+      const auto& [u, v, w] = el[i];
+      (void)w;
+      keep[i] = u != v && !(i > 0 && std::get<0>(el[i - 1]) == u && std::get<1>(el[i - 1]) == v);
+    }
+    std::vector<uint64_t> ioff(n_ + 1, 0);
+    for (size_t i = 0; i < M; ++i)
+      if (keep[i]) ++ioff[std::get<1>(el[i]) + 1];
+    for (uint64_t v = 0; v < n_; ++v) ioff[v + 1] += ioff[v];
+    std::vector<Arc> in_flat(ioff[n_]);
+    {
+      std::vector<uint64_t> at(ioff.begin(), ioff.end() - 1);
+      for (size_t i = 0; i < M; ++i)
+        if (keep[i]) in_flat[at[std::get<1>(el[i])]++] = {std::get<0>(el[i]), std::get<2>(el[i]), 1};
+    }
     out_.resize(n_);
     in_.resize(n_);
-    for (size_t i = 0; i < el.size(); ++i) {
-      auto [u, v, w] = el[i];
-      if (u == v) continue;
-      if (i > 0 && std::get<0>(el[i - 1]) == u && std::get<1>(el[i - 1]) == v) continue;
-      out_[u].push_back({v, w, 1});
-      in_[v].push_back({u, w, 1});
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(nthreads)
+    for (int64_t u = 0; u < (int64_t)n_; ++u) {
+      // el[offset[u] .. offset[u+1]) are u's edges: the sort keeps the
+      // per-source counts of the input CSR
+      uint64_t k = 0;
+      for (uint64_t i = g.offset[u]; i < g.offset[u + 1]; ++i) k += keep[i];
+      out_[u].reserve(k);
+      for (uint64_t i = g.offset[u]; i < g.offset[u + 1]; ++i)
+        if (keep[i]) out_[u].push_back({std::get<1>(el[i]), std::get<2>(el[i]), 1});
+      in_[u].assign(in_flat.begin() + ioff[u], in_flat.begin() + ioff[u + 1]);
     }
-    base_edges_ = el;
+    base_edges_ = std::move(el);
   }
 
   HostPch build() {
@@ -100,19 +128,28 @@ class PchBuilder {
     std::iota(remaining.begin(), remaining.end(), 0);
     const int nthreads = opt_.threads > 0 ? opt_.threads : omp_get_max_threads();
     scratch_.resize(nthreads);
-    for (auto& s : scratch_) s.init(n_);
+    tcuts_.resize(nthreads);
+#pragma omp parallel num_threads(nthreads)
+    scratch_[omp_get_thread_num()].init(n_);
+    for (auto& s : scratch_)
+      if (s.dist.size() != n_) s.init(n_);
     uint32_t round = 0;
     while (!remaining.empty()) {
       ++round;
       const size_t R = remaining.size();
-      std::vector<std::vector<Shortcut>> cuts(R);
-      std::vector<std::vector<uint8_t>> in_rel(R);
-      std::vector<uint64_t> toff, masks;
+      // per-vertex results in flat arrays: in-/out-arc relevance by arc
+      // offset, shortcuts in per-thread buffers ({thread, start, count})
+      std::vector<uint64_t> toff(R + 1, 0), ooff(R + 1, 0), masks;
+      for (size_t i = 0; i < R; ++i) {
+        toff[i + 1] = toff[i] + in_[remaining[i]].size();
+        ooff[i + 1] = ooff[i] + out_[remaining[i]].size();
+      }
+      std::vector<uint8_t> in_rel(toff[R]), out_rel(ooff[R]);
+      std::vector<CutRef> cref(R);
+      for (auto& b : tcuts_) b.clear();
       if (gpu_) {
         upload_overlay(remaining, nthreads);
         // one search per in-arc of every remaining vertex
-        toff.assign(R + 1, 0);
-        for (size_t i = 0; i < R; ++i) toff[i + 1] = toff[i] + in_[remaining[i]].size();
         std::vector<uint32_t> tu(toff[R]), ts(toff[R]), tw(toff[R]);
 #pragma omp parallel for schedule(static) num_threads(nthreads)
         for (size_t i = 0; i < R; ++i) {
@@ -132,14 +169,18 @@ class PchBuilder {
         }
       }
 #pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
-      for (size_t i = 0; i < R; ++i)
-        score(remaining[i], cuts[i], in_rel[i], scratch_[omp_get_thread_num()],
+      for (size_t i = 0; i < R; ++i) {
+        const int tid = omp_get_thread_num();
+        std::vector<Shortcut>& buf = tcuts_[tid];
+        const size_t start = buf.size();
+        score(remaining[i], buf, in_rel.data() + toff[i], scratch_[tid],
               gpu_ ? masks.data() + toff[i] : nullptr);
+        cref[i] = {(uint32_t)tid, start, buf.size() - start};
+      }
       double bound = upper_bound(remaining, round);
       std::vector<uint8_t> sel(R, 0);
 #pragma omp parallel for schedule(static) num_threads(nthreads)
       for (size_t i = 0; i < R; ++i) sel[i] = eligible(remaining[i], bound) ? 1 : 0;
-      std::vector<std::vector<uint8_t>> out_rel(R);
       std::vector<uint64_t> rel_of(R, kPchOverflow);
       if (gpu_) {
         // one search per selected vertex, same snapshot
@@ -156,11 +197,13 @@ class PchBuilder {
 #pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
       for (size_t i = 0; i < R; ++i)
         if (sel[i])
-          out_relevance(remaining[i], out_rel[i], scratch_[omp_get_thread_num()], rel_of[i]);
+          out_relevance(remaining[i], out_rel.data() + ooff[i], scratch_[omp_get_thread_num()],
+                        rel_of[i]);
       size_t ncontracted = 0;
       for (size_t i = 0; i < R; ++i)
         if (sel[i]) {
-          contract(remaining[i], cuts[i], in_rel[i], out_rel[i]);
+          contract(remaining[i], tcuts_[cref[i].thread].data() + cref[i].start, cref[i].count,
+                   in_rel.data() + toff[i], out_rel.data() + ooff[i]);
           ++ncontracted;
         }
       require(ncontracted > 0, CHSGA_ERR_INTERNAL, "hierarchy build made no progress");
@@ -174,7 +217,7 @@ class PchBuilder {
                     ncontracted, R);
       remaining.swap(next);
     }
-    HostPch p = order();
+    HostPch p = order(nthreads);
     double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (opt_.print_detail)
       std::printf("G.n: %llu, G.m: %llu, G.rm: %llu, G.layer: %u, total_time: %f\n",
@@ -268,11 +311,10 @@ class PchBuilder {
   // edge-difference score (build_pch.hpp:396-478, 1012-1045). masks, when
   // given, holds the device's answer for each in-arc (pch_gpu.hpp); an
   // in-arc whose search overflowed there is searched here.
-  void score(uint32_t u, std::vector<Shortcut>& cuts, std::vector<uint8_t>& in_rel, Scratch& sc,
+  void score(uint32_t u, std::vector<Shortcut>& cuts, uint8_t* in_rel, Scratch& sc,
              const uint64_t* masks) {
     const auto& in = in_[u];
     const auto& out = out_[u];
-    in_rel.assign(in.size(), 1);
     uint64_t max_out = 0;
     for (const Arc& b : out) max_out = std::max<uint64_t>(max_out, b.w);
     uint64_t added = 0, added_hop = 0;
@@ -313,9 +355,8 @@ class PchBuilder {
 
   // Relevance of u's out-arcs: kept unless a strictly shorter u->b path
   // exists (the device's mask when it finished the search).
-  void out_relevance(uint32_t u, std::vector<uint8_t>& rel, Scratch& sc, uint64_t mask) {
+  void out_relevance(uint32_t u, uint8_t* rel, Scratch& sc, uint64_t mask) {
     const auto& out = out_[u];
-    rel.assign(out.size(), 1);
     if (!(mask & kPchOverflow)) {
       for (size_t i = 0; i < out.size(); ++i) rel[i] = (uint8_t)((mask >> i) & 1);
       return;
@@ -364,8 +405,8 @@ class PchBuilder {
       }
   }
 
-  void contract(uint32_t u, const std::vector<Shortcut>& cuts, const std::vector<uint8_t>& in_rel,
-                const std::vector<uint8_t>& out_rel) {
+  void contract(uint32_t u, const Shortcut* cuts, size_t ncuts, const uint8_t* in_rel,
+                const uint8_t* out_rel) {
     const uint32_t lu = level_[u] + 1;
     for (size_t i = 0; i < out_[u].size(); ++i) {
       const Arc& b = out_[u][i];
@@ -385,7 +426,8 @@ class PchBuilder {
       }
       erase_arc(out_[a.v], u);
     }
-    for (const Shortcut& s : cuts) {
+    for (size_t c = 0; c < ncuts; ++c) {
+      const Shortcut& s = cuts[c];
       bool found = false;
       for (Arc& x : out_[s.a])
         if (x.v == s.b) {
@@ -413,7 +455,7 @@ class PchBuilder {
     contracted_[u] = 1;
   }
 
-  HostPch order() {
+  HostPch order(int nthreads) {
     // connected components of the input graph, ignoring direction
     std::vector<uint32_t> parent(n_);
     std::iota(parent.begin(), parent.end(), 0);
@@ -430,7 +472,8 @@ class PchBuilder {
     for (uint64_t i = 0; i < n_; ++i) cc[i] = find((uint32_t)i);
     std::vector<uint32_t> ord(n_);
     std::iota(ord.begin(), ord.end(), 0);
-    std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+    // a strict total order (ids break every tie): any sort gives one result
+    __gnu_parallel::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
       if (cc[a] != cc[b]) return cc[a] < cc[b];
       if (level_[a] != level_[b]) return level_[a] < level_[b];
       return a < b;
@@ -461,14 +504,18 @@ class PchBuilder {
       for (uint64_t r = 0; r < n_; ++r) off[r + 1] = off[r] + lists[ord[r]].size();
       vv.resize(off[n_]);
       ww.resize(off[n_]);
-      std::vector<std::pair<uint32_t, uint32_t>> tmp;
-      for (uint64_t r = 0; r < n_; ++r) {
-        tmp.clear();
-        for (const Arc& a : lists[ord[r]]) tmp.push_back({p.rank[a.v], a.w});
-        std::sort(tmp.begin(), tmp.end());
-        for (size_t i = 0; i < tmp.size(); ++i) {
-          vv[off[r] + i] = tmp[i].first;
-          ww[off[r] + i] = tmp[i].second;
+#pragma omp parallel num_threads(nthreads)
+      {
+        std::vector<std::pair<uint32_t, uint32_t>> tmp;
+#pragma omp for schedule(dynamic, 4096)
+        for (int64_t r = 0; r < (int64_t)n_; ++r) {
+          tmp.clear();
+          for (const Arc& a : lists[ord[r]]) tmp.push_back({p.rank[a.v], a.w});
+          std::sort(tmp.begin(), tmp.end());
+          for (size_t i = 0; i < tmp.size(); ++i) {
+            vv[off[r] + i] = tmp[i].first;
+            ww[off[r] + i] = tmp[i].second;
+          }
         }
       }
     };
@@ -492,6 +539,11 @@ class PchBuilder {
   std::vector<float> ed_;
   std::vector<uint64_t> prio_;
   std::vector<Scratch> scratch_;
+  struct CutRef {
+    uint32_t thread;
+    size_t start, count;
+  };
+  std::vector<std::vector<Shortcut>> tcuts_;  // per-thread shortcut buffers of a round
   std::unique_ptr<PchGpu> gpu_;
   static constexpr uint32_t kNoId = 0xFFFFFFFFu;
   std::vector<uint32_t> cid_;  // device overlay id of each remaining vertex
