@@ -77,3 +77,35 @@ def gpu_available():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def pch_arrays(g):
+    """Every array of the graph's hierarchy (numpy copies), by name."""
+    import numpy as np
+    p = g.view().pch
+    out = {"n": p.n, "m": p.m, "rm": p.rm}
+    n, L, K = p.n, p.num_layers, p.num_cc
+    sizes = {"rank": n, "level": n, "layer_offset": L + 1, "cc_offset": K + 1,
+             "up_offset": n + 1, "down_offset": n + 1, "up_v": p.m, "up_w": p.m,
+             "down_v": p.rm, "down_w": p.rm}
+    for k, c in sizes.items():
+        out[k] = np.ctypeslib.as_array(getattr(p, k), shape=(int(c),)).copy() if c else np.zeros(0)
+    return out
+
+
+def assert_same(a, b):
+    import numpy as np
+    assert a.keys() == b.keys()
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+def pch_digest(a):
+    """sha256 over the hierarchy arrays of pch_arrays, in name order."""
+    import hashlib
+    h = hashlib.sha256()
+    for k in sorted(a):
+        v = a[k]
+        h.update(k.encode())
+        h.update(v.tobytes() if hasattr(v, "tobytes") else str(v).encode())
+    return h.hexdigest()

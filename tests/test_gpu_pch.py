@@ -15,28 +15,10 @@ import numpy as np
 import pytest
 
 import chsga_b200 as cb
-from conftest import ROOT
+from conftest import ROOT, assert_same, pch_arrays
 
 pytestmark = pytest.mark.gpu
 BIN = os.path.join(ROOT, "chsga_b200", "bin")
-
-
-def pch_arrays(g):
-    p = g.view().pch
-    out = {"n": p.n, "m": p.m, "rm": p.rm}
-    n, L, K = p.n, p.num_layers, p.num_cc
-    sizes = {"rank": n, "level": n, "layer_offset": L + 1, "cc_offset": K + 1,
-             "up_offset": n + 1, "down_offset": n + 1, "up_v": p.m, "up_w": p.m,
-             "down_v": p.rm, "down_w": p.rm}
-    for k, c in sizes.items():
-        out[k] = np.ctypeslib.as_array(getattr(p, k), shape=(int(c),)).copy() if c else np.zeros(0)
-    return out
-
-
-def assert_same(a, b):
-    assert a.keys() == b.keys()
-    for k in a:
-        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
 
 
 def both(cfg, **opts):

@@ -168,3 +168,28 @@ def test_device_layout_preflight(slots, row_bits):
         if st["tiled"]:
             assert st["tiles"] > 0 and st["smem_bytes"] <= 232448
             assert 2 <= st["slots_per_block"] <= 16
+
+
+_PCH_DIGESTS = [
+    (dict(backbone_len=200_000, seed=9), dict(max_pop_count=3),
+     "e578670d7c98789ec0c7aeb7d0b377f4d687bd8bbf35bad64c9d90e8899813f2"),
+    (dict(backbone_len=200_000, seed=10, vlen_max=4), dict(use_label_lengths=False),
+     "1eb43f61965cf588a840781f44ed73c62b59e3e8c1339c4d78700c5acf812b4c"),
+    (dict(backbone_len=200_000, seed=11), dict(weight_bound=40),
+     "d71f94094b09880cc3039dfa8f3ebc6bb0a101dde35283644065fedabb6da788"),
+    (dict(backbone_len=200_000, seed=12), {},
+     "6ac29ab9c2a483e687ee19ae467c6a980a6bbb2fa7e7dd92ddbc7509a4d20356"),
+]
+
+
+@pytest.mark.parametrize("over,opts,digest", _PCH_DIGESTS)
+def test_hierarchy_builder_is_deterministic(over, opts, digest):
+    """The builder's result depends on neither the thread count nor the
+    order its parallel stages finish in; the digests pin the hierarchy of
+    each case (pop limit, no label lengths, weight bound, defaults)."""
+    from conftest import pch_arrays, pch_digest
+    cfg = dict(cb.GRAPH_CONFIGS["cfg2"])
+    cfg.update(over)
+    many = pch_digest(pch_arrays(cb.HostGraph.generate(**cfg).build_pch(**opts)))
+    one = pch_digest(pch_arrays(cb.HostGraph.generate(**cfg).build_pch(threads=1, **opts)))
+    assert many == one == digest
