@@ -68,7 +68,7 @@ struct HostLayout {
 // per slot with the boundary values staged in shared memory. Edges from
 // below the region (upg) are applied by a grid-wide pull first; the region's
 // own edges run as a chunk schedule: upward levels low -> high, then
-// downward levels high -> low, each chunk at most kTopChunk edges of one
+// downward levels high -> low, each chunk at most chunk_edges edges of one
 // level, padded to an even count with a no-op edge into the scratch slot K.
 // Consecutive levels of at most kTopWarpLevelMax edges share one warp chunk
 // instead (count stored negated): each level padded with no-op edges to

@@ -1574,9 +1574,11 @@ __global__ void __launch_bounds__(256) k_down16(GraphPtrs g, uint16_t* __restric
 // kTopBufs shared buffers with a bulk copy, kTopBufs - 1 chunks ahead of
 // the one the block relaxes (atomic min into the target's first score).
 // Every thread reads the next chunk's edge count while the current one
-// runs, so no global load sits between two chunks. A chunk never spans
-// two levels and ends with a block barrier, so every level sees its
-// sources final. Edges from below the region were applied by k_pull
+// runs, so no global load sits between two chunks. A block chunk never
+// spans two levels and ends with a block barrier, so every level sees its
+// sources final; a warp chunk (negative count) holds a run of small levels,
+// each padded to whole 32-edge rounds that warp 0 runs in order, separated
+// by warp barriers. Edges from below the region were applied by k_pull
 // before launch.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kTopChunk = 1024;     // edges per chunk (8 KiB): the smallest chunk size
