@@ -773,6 +773,15 @@ void fill_result(chsga_tb_result* res, std::vector<dev::WalkOp>& path, int32_t s
   res->score = score;
 }
 
+// Rows per sub-segment when a segment of `span` + 1 rows does not fit the
+// device: the longest k2 for which the ceil(span / k2) sub-checkpoint rows
+// plus one sub-segment of k2 + 1 rows fit in `fit` rows; 0 if none does.
+uint64_t sub_segment_rows(uint64_t span, uint64_t fit) {
+  for (uint64_t k2 = std::min<uint64_t>(span, fit); k2 >= 1; --k2)
+    if ((span + k2 - 1) / k2 + k2 + 1 <= fit) return k2;
+  return 0;
+}
+
 void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts* o,
                chsga_tb_result* res) {
   require(len > 0, CHSGA_ERR_INVALID_ARG, "traceback of an empty read");
@@ -877,17 +886,19 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
         forward_rows(c, b, len, seg_start, seg_end, seg.p);
         walk(c, seg.p, seg_start, seg_end, cur_v, len, path, &landing);
       } else {
-        // two levels: sub-checkpoints every k2 rows inside the segment
+        // two levels: sub-segments of k2 rows, as long as the device budget
+        // allows; a first pass keeps the row at the start of each and ends
+        // with the last sub-segment on the device, which is walked at once;
+        // the earlier ones are recomputed from their sub-checkpoints
         const uint64_t span = (uint64_t)(seg_end - seg_start);
-        const uint64_t k2 = std::max<uint64_t>(1, (uint64_t)std::ceil(std::sqrt((double)span)));
-        const uint64_t nsub = span / k2 + 1;
-        require((nsub + k2 + 1) * pitch_bytes <= budget, CHSGA_ERR_OOM,
+        const uint64_t k2 = sub_segment_rows(span, budget / pitch_bytes);
+        require(k2 >= 1, CHSGA_ERR_OOM,
                 "traceback segment does not fit the byte cap even with two-level checkpoints");
+        const uint64_t nsub = (span + k2 - 1) / k2;
         DevArr<int> sub, seg;
         sub.alloc(nsub * N);
         seg.alloc((k2 + 1) * N);
         CK(cudaMemcpyAsync(sub.p, ck, row_bytes, cudaMemcpyHostToDevice, c.st));
-        // forward through the segment keeping rows seg_start + j*k2
         CK(cudaMemcpyAsync(seg.p, ck, row_bytes, cudaMemcpyHostToDevice, c.st));
         int64_t r0 = seg_start;
         for (uint64_t j = 1; j < nsub; ++j) {
@@ -899,10 +910,17 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
                              cudaMemcpyDeviceToDevice, c.st));
           r0 = r1;
         }
-        int64_t row = seg_end;
+        // r0 < seg_end: the last sub-segment holds 1..k2 rows after r0
+        forward_rows(c, b, len, r0, seg_end, seg.p);
         uint32_t v = cur_v;
+        {
+          uint32_t l2 = v;
+          walk(c, seg.p, r0, seg_end, v, len, path, &l2);
+          v = l2;
+        }
+        int64_t row = r0;
         while (row > seg_start) {
-          int64_t s0 = seg_start + (int64_t)(((row - seg_start - 1) / (int64_t)k2) * (int64_t)k2);
+          const int64_t s0 = row - (int64_t)k2;
           CK(cudaMemcpyAsync(seg.p, sub.p + (size_t)((s0 - seg_start) / (int64_t)k2) * N, row_bytes,
                              cudaMemcpyDeviceToDevice, c.st));
           forward_rows(c, b, len, s0, row, seg.p);
@@ -1721,8 +1739,8 @@ uint64_t traceback_device_bytes(const chsga_ctx& c, uint32_t len, const chsga_tb
   uint64_t peak = seg * pb;
   if (!(seg * pb <= budget || seg <= 2)) {
     const uint64_t span = seg - 1;
-    const uint64_t k2 = std::max<uint64_t>(1, (uint64_t)std::ceil(std::sqrt((double)span)));
-    peak = (span / k2 + 1 + k2 + 1) * pb;
+    const uint64_t k2 = std::max<uint64_t>(1, sub_segment_rows(span, budget / pb));
+    peak = ((span + k2 - 1) / k2 + k2 + 1) * pb;
   }
   return std::max<uint64_t>(3 * pb, peak) + read;
 }

@@ -108,14 +108,20 @@ def test_traceback_two_level(small_graph, ctx_small, oracle_small):
     rd = reads[1]
     want = int(oracle_small.scores([rd])[0])
     n = oracle_small.num_chars
-    # a context whose device budget is 40 rows: a segment of 100 rows does
-    # not fit, so the segment is recomputed from sub-checkpoints
-    ctx = cb.Context(0, hbm_cap_bytes=40 * n * 4).load(g)
-    ops, score, ck = ctx.align_traceback(rd, k=100)
-    ctx.close()
-    assert ck and score == want
-    ps, last = orc.rescore(ops, rd, labels)
-    assert ps == want and last == len(rd) - 1
+    full_ops, full_score, full_ck = ctx_small.align_traceback(rd)
+    assert not full_ck and full_score == want
+    # device budgets of 40 and 23 rows: a segment of 100 rows does not fit,
+    # so it runs as sub-segments (a few dozen rows) from sub-checkpoints,
+    # the last one walked straight from the first pass; the path is the
+    # full-matrix one, op for op
+    for rows in (40, 23):
+        ctx = cb.Context(0, hbm_cap_bytes=rows * n * 4).load(g)
+        ops, score, ck = ctx.align_traceback(rd, k=100)
+        ctx.close()
+        assert ck and score == want
+        np.testing.assert_array_equal(ops, full_ops)
+        ps, last = orc.rescore(ops, rd, labels)
+        assert ps == want and last == len(rd) - 1
 
 
 @pytest.mark.parametrize("seed,vmax", [(21, 1), (22, 3), (23, 32)])
