@@ -871,6 +871,16 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
     // like the reference, the cap only decides between the two paths
     // (traceback.hpp:614-645); segment recompute is sized by device memory
     const uint64_t budget = std::max<uint64_t>(c.cap, cap);
+    // segment buffers live across segments (equal segments reuse them; a
+    // buffer whose size changes is released before anything is allocated,
+    // so the device holds one segment's plan at a time)
+    DevArr<int> seg, sub;
+    auto plan = [&](size_t seg_elems, size_t sub_elems) {
+      if (seg.n != seg_elems) seg.release();
+      if (sub.n != sub_elems) sub.release();
+      if (seg_elems) seg.alloc(seg_elems);
+      if (sub_elems) sub.alloc(sub_elems);
+    };
     while (cur_row > 0) {
       int64_t seg_start = (cur_row % k == 0) ? (cur_row - k) : (cur_row / k * k);
       if (seg_start < 0) seg_start = 0;
@@ -880,8 +890,7 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
       uint32_t landing = cur_v;
       const uint64_t pitch_bytes = (uint64_t)N * 4;
       if (rows * pitch_bytes <= budget || rows <= 2) {
-        DevArr<int> seg;
-        seg.alloc(rows * N);
+        plan(rows * N, 0);
         CK(cudaMemcpyAsync(seg.p, ck, row_bytes, cudaMemcpyHostToDevice, c.st));
         forward_rows(c, b, len, seg_start, seg_end, seg.p);
         walk(c, seg.p, seg_start, seg_end, cur_v, len, path, &landing);
@@ -895,9 +904,7 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
         require(k2 >= 1, CHSGA_ERR_OOM,
                 "traceback segment does not fit the byte cap even with two-level checkpoints");
         const uint64_t nsub = (span + k2 - 1) / k2;
-        DevArr<int> sub, seg;
-        sub.alloc(nsub * N);
-        seg.alloc((k2 + 1) * N);
+        plan((k2 + 1) * N, nsub * N);
         CK(cudaMemcpyAsync(sub.p, ck, row_bytes, cudaMemcpyHostToDevice, c.st));
         CK(cudaMemcpyAsync(seg.p, ck, row_bytes, cudaMemcpyHostToDevice, c.st));
         int64_t r0 = seg_start;
