@@ -193,3 +193,19 @@ def test_hierarchy_builder_is_deterministic(over, opts, digest):
     many = pch_digest(pch_arrays(cb.HostGraph.generate(**cfg).build_pch(**opts)))
     one = pch_digest(pch_arrays(cb.HostGraph.generate(**cfg).build_pch(threads=1, **opts)))
     assert many == one == digest
+
+
+def test_gpu_hierarchy_builder_fails_with_a_status_or_matches():
+    """build_pch(gpu_device=0) either builds the host builder's hierarchy or,
+    without a usable CUDA device, returns an error status; the graph stays
+    usable for the host builder."""
+    from conftest import assert_same, pch_arrays
+    cfg = dict(cb.GRAPH_CONFIGS["cfg1"], backbone_len=3000, seed=44)
+    host = pch_arrays(cb.HostGraph.generate(**cfg).build_pch())
+    g = cb.HostGraph.generate(**cfg)
+    try:
+        g.build_pch(gpu_device=0)
+    except cb.ChsgaError as e:
+        assert "hierarchy builder" in str(e)
+        g.build_pch()
+    assert_same(pch_arrays(g), host)
