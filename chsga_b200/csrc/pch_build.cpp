@@ -124,6 +124,8 @@ class PchBuilder {
       gpu_ = std::make_unique<PchGpu>(opt_.device, pop_limit_);
       cid_.assign(n_, kNoId);
     }
+    last_in_.assign(n_, 0);
+    last_out_.assign(n_, 0);
     std::vector<uint32_t> remaining(n_);
     std::iota(remaining.begin(), remaining.end(), 0);
     const int nthreads = opt_.threads > 0 ? opt_.threads : omp_get_max_threads();
@@ -199,14 +201,49 @@ class PchBuilder {
         if (sel[i])
           out_relevance(remaining[i], out_rel.data() + ooff[i], scratch_[omp_get_thread_num()],
                         rel_of[i]);
-      size_t ncontracted = 0;
+      // Contraction in waves. Contracting u changes only out_ of its
+      // in-neighbours and in_ of its out-neighbours (selected vertices are
+      // never adjacent, so no other selected vertex's lists) besides the
+      // commutative level / removed-neighbour updates. A vertex goes to the
+      // first wave after every earlier selected vertex that changes one of
+      // the same lists: within a wave the lists are disjoint and run in
+      // parallel, and every list sees its changes in selection order, as in
+      // one sequential pass.
+      std::vector<uint32_t> chosen;
       for (size_t i = 0; i < R; ++i)
-        if (sel[i]) {
+        if (sel[i]) chosen.push_back((uint32_t)i);
+      const size_t ncontracted = chosen.size();
+      require(ncontracted > 0, CHSGA_ERR_INTERNAL, "hierarchy build made no progress");
+      const uint32_t base = wave_base_ + 1;
+      uint32_t top = base;
+      std::vector<uint32_t> wave(ncontracted);
+      for (size_t k = 0; k < ncontracted; ++k) {
+        const uint32_t u = remaining[chosen[k]];
+        uint32_t w = base;
+        for (const Arc& a : in_[u]) w = std::max(w, last_out_[a.v] + 1);
+        for (const Arc& b : out_[u]) w = std::max(w, last_in_[b.v] + 1);
+        for (const Arc& a : in_[u]) last_out_[a.v] = w;
+        for (const Arc& b : out_[u]) last_in_[b.v] = w;
+        wave[k] = w;
+        top = std::max(top, w);
+      }
+      wave_base_ = top;
+      std::vector<size_t> woff(top - base + 2, 0);
+      for (uint32_t w : wave) ++woff[w - base + 1];
+      for (size_t j = 1; j < woff.size(); ++j) woff[j] += woff[j - 1];
+      std::vector<uint32_t> by_wave(ncontracted);
+      {
+        std::vector<size_t> at(woff.begin(), woff.end() - 1);
+        for (size_t k = 0; k < ncontracted; ++k) by_wave[at[wave[k] - base]++] = chosen[k];
+      }
+      for (size_t j = 0; j + 1 < woff.size(); ++j) {
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+        for (size_t q = woff[j]; q < woff[j + 1]; ++q) {
+          const uint32_t i = by_wave[q];
           contract(remaining[i], tcuts_[cref[i].thread].data() + cref[i].start, cref[i].count,
                    in_rel.data() + toff[i], out_rel.data() + ooff[i]);
-          ++ncontracted;
         }
-      require(ncontracted > 0, CHSGA_ERR_INTERNAL, "hierarchy build made no progress");
+      }
       std::vector<uint32_t> next;
       next.reserve(R - ncontracted);
       for (uint32_t u : remaining)
@@ -407,13 +444,24 @@ class PchBuilder {
 
   void contract(uint32_t u, const Shortcut* cuts, size_t ncuts, const uint8_t* in_rel,
                 const uint8_t* out_rel) {
+    // level_[u] is final here (only neighbours of contracted vertices
+    // change level, and u has none this round); a neighbour may be shared
+    // with a vertex of the same wave, so its level and count are updated
+    // atomically (max and sum do not depend on the order)
     const uint32_t lu = level_[u] + 1;
+    auto raise = [&](uint32_t x) {
+      uint32_t* p = &level_[x];
+      uint32_t cur = __atomic_load_n(p, __ATOMIC_RELAXED);
+      while (cur < lu && !__atomic_compare_exchange_n(p, &cur, lu, true, __ATOMIC_RELAXED,
+                                                      __ATOMIC_RELAXED)) {
+      }
+      __atomic_fetch_add(&removed_nbr_[x], 1u, __ATOMIC_RELAXED);
+    };
     for (size_t i = 0; i < out_[u].size(); ++i) {
       const Arc& b = out_[u][i];
       if (out_rel[i]) {
         up_[u].push_back({b.v, b.w, b.hop});
-        level_[b.v] = std::max(level_[b.v], lu);
-        removed_nbr_[b.v]++;
+        raise(b.v);
       }
       erase_arc(in_[b.v], u);
     }
@@ -421,8 +469,7 @@ class PchBuilder {
       const Arc& a = in_[u][i];
       if (in_rel[i]) {
         down_[u].push_back({a.v, a.w, a.hop});
-        level_[a.v] = std::max(level_[a.v], lu);
-        removed_nbr_[a.v]++;
+        raise(a.v);
       }
       erase_arc(out_[a.v], u);
     }
@@ -544,6 +591,10 @@ class PchBuilder {
     size_t start, count;
   };
   std::vector<std::vector<Shortcut>> tcuts_;  // per-thread shortcut buffers of a round
+  // last contraction wave that changed in_[x] / out_[x] (waves are numbered
+  // on from round to round, so no reset is needed)
+  std::vector<uint32_t> last_in_, last_out_;
+  uint32_t wave_base_ = 0;
   std::unique_ptr<PchGpu> gpu_;
   static constexpr uint32_t kNoId = 0xFFFFFFFFu;
   std::vector<uint32_t> cid_;  // device overlay id of each remaining vertex
