@@ -124,8 +124,8 @@ class PchBuilder {
       gpu_ = std::make_unique<PchGpu>(opt_.device, pop_limit_);
       cid_.assign(n_, kNoId);
     }
-    last_in_.assign(n_, 0);
-    last_out_.assign(n_, 0);
+    claim_in_.assign(n_, kNoClaim);
+    claim_out_.assign(n_, kNoClaim);
     std::vector<uint32_t> remaining(n_);
     std::iota(remaining.begin(), remaining.end(), 0);
     const int nthreads = opt_.threads > 0 ? opt_.threads : omp_get_max_threads();
@@ -204,45 +204,61 @@ class PchBuilder {
       // Contraction in waves. Contracting u changes only out_ of its
       // in-neighbours and in_ of its out-neighbours (selected vertices are
       // never adjacent, so no other selected vertex's lists) besides the
-      // commutative level / removed-neighbour updates. A vertex goes to the
-      // first wave after every earlier selected vertex that changes one of
-      // the same lists: within a wave the lists are disjoint and run in
-      // parallel, and every list sees its changes in selection order, as in
-      // one sequential pass.
-      std::vector<uint32_t> chosen;
+      // commutative level / removed-neighbour updates. Each pending vertex
+      // claims the lists it changes with the smallest selection index; a
+      // vertex holding all its claims runs in this wave, in parallel with
+      // the others (their lists are disjoint), the rest wait for the next.
+      // Every list therefore sees its changes in selection order, as in one
+      // sequential pass, and the smallest pending index always runs.
+      std::vector<uint32_t> pending;
       for (size_t i = 0; i < R; ++i)
-        if (sel[i]) chosen.push_back((uint32_t)i);
-      const size_t ncontracted = chosen.size();
+        if (sel[i]) pending.push_back((uint32_t)i);
+      const size_t ncontracted = pending.size();
       require(ncontracted > 0, CHSGA_ERR_INTERNAL, "hierarchy build made no progress");
-      const uint32_t base = wave_base_ + 1;
-      uint32_t top = base;
-      std::vector<uint32_t> wave(ncontracted);
-      for (size_t k = 0; k < ncontracted; ++k) {
-        const uint32_t u = remaining[chosen[k]];
-        uint32_t w = base;
-        for (const Arc& a : in_[u]) w = std::max(w, last_out_[a.v] + 1);
-        for (const Arc& b : out_[u]) w = std::max(w, last_in_[b.v] + 1);
-        for (const Arc& a : in_[u]) last_out_[a.v] = w;
-        for (const Arc& b : out_[u]) last_in_[b.v] = w;
-        wave[k] = w;
-        top = std::max(top, w);
-      }
-      wave_base_ = top;
-      std::vector<size_t> woff(top - base + 2, 0);
-      for (uint32_t w : wave) ++woff[w - base + 1];
-      for (size_t j = 1; j < woff.size(); ++j) woff[j] += woff[j - 1];
-      std::vector<uint32_t> by_wave(ncontracted);
-      {
-        std::vector<size_t> at(woff.begin(), woff.end() - 1);
-        for (size_t k = 0; k < ncontracted; ++k) by_wave[at[wave[k] - base]++] = chosen[k];
-      }
-      for (size_t j = 0; j + 1 < woff.size(); ++j) {
+      std::vector<uint8_t> runs;
+      while (!pending.empty()) {
+        const int64_t P = (int64_t)pending.size();
+        auto claim = [](uint32_t* p, uint32_t k) {
+          uint32_t cur = __atomic_load_n(p, __ATOMIC_RELAXED);
+          while (k < cur && !__atomic_compare_exchange_n(p, &cur, k, true, __ATOMIC_RELAXED,
+                                                         __ATOMIC_RELAXED)) {
+          }
+        };
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nthreads)
+        for (int64_t q = 0; q < P; ++q) {
+          const uint32_t i = pending[q], u = remaining[i];
+          for (const Arc& a : in_[u]) claim(&claim_out_[a.v], i);
+          for (const Arc& b : out_[u]) claim(&claim_in_[b.v], i);
+        }
+        runs.assign(P, 1);
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nthreads)
+        for (int64_t q = 0; q < P; ++q) {
+          const uint32_t i = pending[q], u = remaining[i];
+          bool own = true;
+          for (const Arc& a : in_[u])
+            own = own && __atomic_load_n(&claim_out_[a.v], __ATOMIC_RELAXED) == i;
+          for (const Arc& b : out_[u])
+            own = own && __atomic_load_n(&claim_in_[b.v], __ATOMIC_RELAXED) == i;
+          runs[q] = own;
+        }
+        // clear the claims while every pending vertex's lists are intact
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nthreads)
+        for (int64_t q = 0; q < P; ++q) {
+          const uint32_t u = remaining[pending[q]];
+          for (const Arc& a : in_[u]) __atomic_store_n(&claim_out_[a.v], kNoClaim, __ATOMIC_RELAXED);
+          for (const Arc& b : out_[u]) __atomic_store_n(&claim_in_[b.v], kNoClaim, __ATOMIC_RELAXED);
+        }
 #pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
-        for (size_t q = woff[j]; q < woff[j + 1]; ++q) {
-          const uint32_t i = by_wave[q];
+        for (int64_t q = 0; q < P; ++q) {
+          if (!runs[q]) continue;
+          const uint32_t i = pending[q];
           contract(remaining[i], tcuts_[cref[i].thread].data() + cref[i].start, cref[i].count,
                    in_rel.data() + toff[i], out_rel.data() + ooff[i]);
         }
+        std::vector<uint32_t> rest;
+        for (int64_t q = 0; q < P; ++q)
+          if (!runs[q]) rest.push_back(pending[q]);
+        pending.swap(rest);
       }
       std::vector<uint32_t> next;
       next.reserve(R - ncontracted);
@@ -591,10 +607,10 @@ class PchBuilder {
     size_t start, count;
   };
   std::vector<std::vector<Shortcut>> tcuts_;  // per-thread shortcut buffers of a round
-  // last contraction wave that changed in_[x] / out_[x] (waves are numbered
-  // on from round to round, so no reset is needed)
-  std::vector<uint32_t> last_in_, last_out_;
-  uint32_t wave_base_ = 0;
+  // smallest selection index of a pending vertex that changes in_[x] /
+  // out_[x] in the current contraction wave (kNoClaim between waves)
+  static constexpr uint32_t kNoClaim = 0xFFFFFFFFu;
+  std::vector<uint32_t> claim_in_, claim_out_;
   std::unique_ptr<PchGpu> gpu_;
   static constexpr uint32_t kNoId = 0xFFFFFFFFu;
   std::vector<uint32_t> cid_;  // device overlay id of each remaining vertex
