@@ -141,10 +141,16 @@ class PchBuilder {
       const size_t R = remaining.size();
       // per-vertex results in flat arrays: in-/out-arc relevance by arc
       // offset, shortcuts in per-thread buffers ({thread, start, count})
-      std::vector<uint64_t> toff(R + 1, 0), ooff(R + 1, 0), masks;
+      std::vector<uint64_t> toff(R + 1), ooff(R + 1), masks;
+      toff[0] = ooff[0] = 0;
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+      for (int64_t i = 0; i < (int64_t)R; ++i) {
+        toff[i + 1] = in_[remaining[i]].size();
+        ooff[i + 1] = out_[remaining[i]].size();
+      }
       for (size_t i = 0; i < R; ++i) {
-        toff[i + 1] = toff[i] + in_[remaining[i]].size();
-        ooff[i + 1] = ooff[i] + out_[remaining[i]].size();
+        toff[i + 1] += toff[i];
+        ooff[i + 1] += ooff[i];
       }
       std::vector<uint8_t> in_rel(toff[R]), out_rel(ooff[R]);
       std::vector<CutRef> cref(R);
@@ -177,7 +183,7 @@ class PchBuilder {
         const size_t start = buf.size();
         score(remaining[i], buf, in_rel.data() + toff[i], scratch_[tid],
               gpu_ ? masks.data() + toff[i] : nullptr);
-        cref[i] = {(uint32_t)tid, start, buf.size() - start};
+        cref[i] = {(uint32_t)tid, (uint32_t)(buf.size() - start), start};
       }
       double bound = upper_bound(remaining, round);
       std::vector<uint8_t> sel(R, 0);
@@ -603,8 +609,8 @@ class PchBuilder {
   std::vector<uint64_t> prio_;
   std::vector<Scratch> scratch_;
   struct CutRef {
-    uint32_t thread;
-    size_t start, count;
+    uint32_t thread, count;
+    uint64_t start;
   };
   std::vector<std::vector<Shortcut>> tcuts_;  // per-thread shortcut buffers of a round
   // smallest selection index of a pending vertex that changes in_[x] /
