@@ -111,8 +111,9 @@ class PchBuilder {
     removed_nbr_.assign(n_, 0);
     contracted_.assign(n_, 0);
     ed_.assign(n_, 0.f);
+    require(n_ < (1ull << 32), CHSGA_ERR_UNSUPPORTED, "hierarchy builder: too many vertices");
     prio_.resize(n_);
-    std::iota(prio_.begin(), prio_.end(), 1);
+    std::iota(prio_.begin(), prio_.end(), 1u);
     {
       Rng rng(opt_.seed ? opt_.seed : 0x5eed);
       for (uint64_t i = n_; i > 1; --i) std::swap(prio_[i - 1], prio_[rng.below(i)]);
@@ -606,7 +607,7 @@ class PchBuilder {
   std::vector<uint32_t> level_, removed_nbr_;
   std::vector<uint8_t> contracted_;
   std::vector<float> ed_;
-  std::vector<uint64_t> prio_;
+  std::vector<uint32_t> prio_;
   std::vector<Scratch> scratch_;
   struct CutRef {
     uint32_t thread, count;
