@@ -438,8 +438,8 @@ HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edg
       }
     }
     if (es.empty()) return;
-    if (es.size() <= kTopWarpLevelMax) {
-      const size_t rounds = (es.size() + 31) / 32;
+    const size_t rounds = (es.size() + 31) / 32;
+    if (es.size() <= kTopWarpLevelMax && 32 * rounds <= chunk_edges) {
       if (warp.size() + 32 * rounds > chunk_edges) flush_warp();
       warp.insert(warp.end(), es.begin(), es.end());
       warp.resize(warp.size() + (32 * rounds - es.size()), pad);
