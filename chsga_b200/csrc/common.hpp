@@ -24,6 +24,13 @@ struct ChsgaError : std::runtime_error {
 inline void require(bool ok, chsga_status s, const std::string& msg) {
   if (!ok) fail(s, msg);
 }
+// A literal message becomes a string only when the check fails (checks run
+// per element of inputs with hundreds of millions of them). Messages built
+// from parts are formed before the call: in such loops, test first and
+// call fail().
+inline void require(bool ok, chsga_status s, const char* msg) {
+  if (!ok) fail(s, msg);
+}
 
 // splitmix64 seeding + xoshiro256** stream. Fixed arithmetic so generated
 // inputs are identical on every machine and library version.

@@ -33,69 +33,117 @@ HostLayout build_layout(const chsga_graph_host& g) {
   const uint32_t N = (uint32_t)N64, S = (uint32_t)S64;
   L.N = N;
   L.S = S;
+  // Every per-element check below keeps the first offending element (a min
+  // over the parallel loop), so errors name what a sequential pass would.
+  constexpr uint64_t kNone = ~0ull;
 
   // --- labels: 2-bit code plus one "special" byte class --------------------
+  // the special byte is the first label byte outside A/C/G/T
+  uint64_t first_sp = kNone;
+#pragma omp parallel for reduction(min : first_sp) schedule(static)
+  for (int64_t c = 0; c < (int64_t)N; ++c)
+    if (base_code((unsigned char)g.labels[c]) < 0) first_sp = std::min(first_sp, (uint64_t)c);
+  if (first_sp != kNone) L.special = (unsigned char)g.labels[first_sp];
   L.lab2.assign((N + 15) / 16, 0);
   L.lab_sp.assign((N + 31) / 32, 0);
   L.lab4.assign((N + 7) / 8 + 2, 0);  // two spare words: the kernels read a word ahead
-  for (uint32_t c = 0; c < N; ++c) {
-    unsigned char ch = (unsigned char)g.labels[c];
-    int code = base_code(ch);
-    if (code < 0) {
-      if (L.special < 0) L.special = ch;
-      require(L.special == ch, CHSGA_ERR_UNSUPPORTED,
-              std::string("labels use more than one byte outside A/C/G/T ('") +
-                  (char)L.special + "' and '" + (char)ch + "')");
-      L.lab_sp[c >> 5] |= 1u << (c & 31);
-      code = 0;
+  uint64_t bad_sp = kNone;
+  const int64_t words = (N + 31) / 32;
+#pragma omp parallel for reduction(min : bad_sp) schedule(static)
+  for (int64_t w = 0; w < words; ++w) {
+    // chars [32w, 32w + 32): one lab_sp word, two lab2 words, four lab4 words
+    const uint32_t c1 = std::min<uint32_t>(N, (uint32_t)(32 * w + 32));
+    for (uint32_t c = (uint32_t)(32 * w); c < c1; ++c) {
+      const unsigned char ch = (unsigned char)g.labels[c];
+      int code = base_code(ch);
+      uint32_t key;
+      if (code < 0) {
+        if ((int)ch != L.special) bad_sp = std::min(bad_sp, (uint64_t)c);
+        L.lab_sp[c >> 5] |= 1u << (c & 31);
+        code = 0;
+        key = 4u;
+      } else {
+        key = (uint32_t)code;
+      }
+      L.lab2[c >> 4] |= (uint32_t)code << ((c & 15) * 2);
+      L.lab4[c >> 3] |= key << ((c & 7) * 4);
     }
-    L.lab2[c >> 4] |= (uint32_t)code << ((c & 15) * 2);
-    const uint32_t key = ((L.lab_sp[c >> 5] >> (c & 31)) & 1u) ? 4u : (uint32_t)code;
-    L.lab4[c >> 3] |= key << ((c & 7) * 4);
   }
+  if (bad_sp != kNone)
+    fail(CHSGA_ERR_UNSUPPORTED, std::string("labels use more than one byte outside A/C/G/T ('") +
+                                    (char)L.special + "' and '" + (char)g.labels[bad_sp] + "')");
 
   // --- string vertices and the char graph -----------------------------------
   L.sv_off.resize(S + 1);
-  for (uint32_t s = 0; s <= S; ++s) L.sv_off[s] = (uint32_t)g.label_offsets[s];
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s <= (int64_t)S; ++s) L.sv_off[s] = (uint32_t)g.label_offsets[s];
   std::vector<uint32_t> vertex_of(N);
-  for (uint32_t s = 0; s < S; ++s) {
-    require(L.sv_off[s] < L.sv_off[s + 1], CHSGA_ERR_UNSUPPORTED,
-            "string vertex " + std::to_string(s) + " has an empty label");
-    require(L.sv_off[s + 1] - L.sv_off[s] < (1u << 29), CHSGA_ERR_UNSUPPORTED,
-            "string vertex labels must be shorter than 2^29 chars");
-    L.max_len = std::max(L.max_len, L.sv_off[s + 1] - L.sv_off[s]);
-    for (uint32_t c = L.sv_off[s]; c < L.sv_off[s + 1]; ++c) vertex_of[c] = s;
-  }
-  const chsga_csr& cg = g.char_graph;
-  // in-CSR with sources in ascending order, as build_in_csr (align.hpp:220-242)
-  std::vector<uint64_t> ioff(N + 1, 0);
-  for (uint64_t u = 0; u < N; ++u)
-    for (uint64_t e = cg.offset[u]; e < cg.offset[u + 1]; ++e) {
-      require(cg.target[e] < N, CHSGA_ERR_FORMAT, "char edge target out of range");
-      ioff[cg.target[e] + 1]++;
+  uint64_t empty_s = kNone;
+  uint32_t max_len = 0;
+#pragma omp parallel for reduction(min : empty_s) reduction(max : max_len) schedule(static)
+  for (int64_t s = 0; s < (int64_t)S; ++s) {
+    if (L.sv_off[s] >= L.sv_off[s + 1]) {
+      empty_s = std::min(empty_s, (uint64_t)s);
+      continue;
     }
+    max_len = std::max(max_len, L.sv_off[s + 1] - L.sv_off[s]);
+    for (uint32_t c = L.sv_off[s]; c < L.sv_off[s + 1]; ++c) vertex_of[c] = (uint32_t)s;
+  }
+  if (empty_s != kNone)
+    fail(CHSGA_ERR_UNSUPPORTED, "string vertex " + std::to_string(empty_s) + " has an empty label");
+  require(max_len < (1u << 29), CHSGA_ERR_UNSUPPORTED, "string vertex labels must be shorter than 2^29 chars");
+  L.max_len = max_len;
+  const chsga_csr& cg = g.char_graph;
+  // in-CSR with sources in ascending order, as build_in_csr (align.hpp:220-242):
+  // counted and placed in parallel, then each target's sources sorted
+  std::vector<uint64_t> ioff(N + 1, 0);
+  uint64_t bad_t = 0;
+#pragma omp parallel for reduction(+ : bad_t) schedule(dynamic, 1 << 14)
+  for (int64_t u = 0; u < (int64_t)N; ++u)
+    for (uint64_t e = cg.offset[u]; e < cg.offset[u + 1]; ++e) {
+      if (cg.target[e] >= N) {
+        ++bad_t;
+        continue;
+      }
+      __atomic_fetch_add(&ioff[cg.target[e] + 1], 1ull, __ATOMIC_RELAXED);
+    }
+  require(bad_t == 0, CHSGA_ERR_FORMAT, "char edge target out of range");
   for (uint32_t v = 0; v < N; ++v) ioff[v + 1] += ioff[v];
   std::vector<uint32_t> isrc(ioff[N]);
   {
     std::vector<uint64_t> cur(ioff.begin(), ioff.end() - 1);
-    for (uint64_t u = 0; u < N; ++u)
-      for (uint64_t e = cg.offset[u]; e < cg.offset[u + 1]; ++e) isrc[cur[cg.target[e]]++] = (uint32_t)u;
+#pragma omp parallel for schedule(dynamic, 1 << 14)
+    for (int64_t u = 0; u < (int64_t)N; ++u)
+      for (uint64_t e = cg.offset[u]; e < cg.offset[u + 1]; ++e)
+        isrc[__atomic_fetch_add(&cur[cg.target[e]], 1ull, __ATOMIC_RELAXED)] = (uint32_t)u;
+#pragma omp parallel for schedule(dynamic, 1 << 14)
+    for (int64_t v = 0; v < (int64_t)N; ++v)
+      if (ioff[v + 1] - ioff[v] > 1) std::sort(isrc.begin() + ioff[v], isrc.begin() + ioff[v + 1]);
   }
   L.char_in_edges = ioff[N];
   L.vin_off.assign(S + 1, 0);
-  for (uint32_t s = 0; s < S; ++s) {
+  uint64_t bad_chain = kNone;
+#pragma omp parallel for reduction(min : bad_chain) schedule(static)
+  for (int64_t s = 0; s < (int64_t)S; ++s) {
     const uint32_t f = L.sv_off[s], e = L.sv_off[s + 1];
     for (uint32_t c = f + 1; c < e; ++c)
-      require(ioff[c + 1] - ioff[c] == 1 && isrc[ioff[c]] == c - 1, CHSGA_ERR_UNSUPPORTED,
-              "char " + std::to_string(c) +
-                  " is not the chain successor of char " + std::to_string(c - 1) +
-                  ": the char graph must be the expansion of the string graph "
-                  "(every char after the first of a string has the single in-edge c-1 -> c)");
-    L.vin_off[s + 1] = L.vin_off[s] + (uint32_t)(ioff[f + 1] - ioff[f]);
+      if (!(ioff[c + 1] - ioff[c] == 1 && isrc[ioff[c]] == c - 1)) {
+        bad_chain = std::min(bad_chain, (uint64_t)c);
+        break;
+      }
+    L.vin_off[s + 1] = (uint32_t)(ioff[f + 1] - ioff[f]);
   }
+  if (bad_chain != kNone)
+    fail(CHSGA_ERR_UNSUPPORTED,
+         "char " + std::to_string(bad_chain) + " is not the chain successor of char " +
+             std::to_string(bad_chain - 1) +
+             ": the char graph must be the expansion of the string graph "
+             "(every char after the first of a string has the single in-edge c-1 -> c)");
+  for (uint32_t s = 0; s < S; ++s) L.vin_off[s + 1] += L.vin_off[s];
   L.vin_src.resize(L.vin_off[S]);
   L.vin_srcv.resize(L.vin_off[S]);
-  for (uint32_t s = 0; s < S; ++s) {
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s < (int64_t)S; ++s) {
     const uint32_t f = L.sv_off[s];
     for (uint64_t k = 0; k < ioff[f + 1] - ioff[f]; ++k) {
       uint32_t u = isrc[ioff[f] + k];
@@ -141,89 +189,107 @@ HostLayout build_layout(const chsga_graph_host& g) {
       }
     }
   }
+  // ranks in (level, rank) order: a stable counting sort by level
   std::vector<uint32_t> order(S);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(),
-                   [&](uint32_t a, uint32_t b) { return p.level[a] < p.level[b]; });
+  {
+    uint32_t max_level = 0;
+    for (uint32_t r = 0; r < S; ++r) max_level = std::max(max_level, p.level[r]);
+    require(max_level < (1u << 24), CHSGA_ERR_UNSUPPORTED, "hierarchy levels above 2^24");
+    std::vector<uint32_t> at((size_t)max_level + 2, 0);
+    for (uint32_t r = 0; r < S; ++r) ++at[p.level[r] + 1];
+    for (size_t l = 1; l < at.size(); ++l) at[l] += at[l - 1];
+    for (uint32_t r = 0; r < S; ++r) order[at[p.level[r]]++] = r;
+  }
   std::vector<uint32_t> dev(S);
   for (uint32_t d = 0; d < S; ++d) dev[order[d]] = d;
   L.dv_first.resize(S);
   L.dv_len.resize(S);
   L.dv_s.resize(S);
-  for (uint32_t d = 0; d < S; ++d) {
+#pragma omp parallel for schedule(static)
+  for (int64_t d = 0; d < (int64_t)S; ++d) {
     uint32_t s = og[order[d]];
     L.dv_first[d] = L.sv_off[s];
     L.dv_len[d] = L.sv_off[s + 1] - L.sv_off[s];
     L.dv_s[d] = s;
   }
   L.sv_dev.resize(S);
-  for (uint32_t s = 0; s < S; ++s) L.sv_dev[s] = dev[p.rank[s]];
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s < (int64_t)S; ++s) L.sv_dev[s] = dev[p.rank[s]];
   // a first char's in-edges come from last chars (the string expansion); the
   // row kernels read those sources' final scores from the per-vertex array
-  for (size_t k = 0; k < L.vin_src.size(); ++k)
-    require(L.vin_src[k] + 1 == L.sv_off[L.vin_srcv[k] + 1], CHSGA_ERR_UNSUPPORTED,
-            "char " + std::to_string(L.vin_src[k]) +
-                " has an edge to the first char of another string but is not the last char of "
-                "its own string: the char graph must be the expansion of the string graph");
+  uint64_t bad_vin = kNone;
+#pragma omp parallel for reduction(min : bad_vin) schedule(static)
+  for (int64_t k = 0; k < (int64_t)L.vin_src.size(); ++k)
+    if (L.vin_src[k] + 1 != L.sv_off[L.vin_srcv[k] + 1]) bad_vin = std::min(bad_vin, (uint64_t)k);
+  if (bad_vin != kNone)
+    fail(CHSGA_ERR_UNSUPPORTED,
+         "char " + std::to_string(L.vin_src[bad_vin]) +
+             " has an edge to the first char of another string but is not the last char of "
+             "its own string: the char graph must be the expansion of the string graph");
   auto bv_last = [&](uint32_t rank) { return 2 * dev[rank] + (L.dv_len[dev[rank]] > 1 ? 1 : 0); };
-  // pull lists
-  std::vector<std::vector<EdgeW>> up(S), dn(S);
+  // pull lists, by target in hierarchy order; each list in the order of its
+  // sources' ranks and of their edges (two passes: count, then fill)
+  L.up_off.assign(S + 1, 0);
+  L.dn_off.assign(S + 1, 0);
   for (uint32_t u = 0; u < S; ++u) {
     for (uint64_t j = p.up_offset[u]; j < p.up_offset[u + 1]; ++j) {
-      uint32_t v = p.up_v[j];
+      const uint32_t v = p.up_v[j];
       require(v < S, CHSGA_ERR_FORMAT, "hierarchy edge out of range");
       require(cc_of[v] == cc_of[u] && layer_of[v] > layer_of[u], CHSGA_ERR_UNSUPPORTED,
               "upward hierarchy edge does not climb to a later layer of its component");
       require(p.up_w[j] >= 1 && p.up_w[j] <= (1u << 30), CHSGA_ERR_UNSUPPORTED,
               "hierarchy weights must be in [1, 2^30]");
-      up[dev[v]].push_back({(int32_t)bv_last(u), (int32_t)p.up_w[j]});
+      ++L.up_off[dev[v] + 1];
     }
     for (uint64_t j = p.down_offset[u]; j < p.down_offset[u + 1]; ++j) {
-      uint32_t v = p.down_v[j];
+      const uint32_t v = p.down_v[j];
       require(v < S, CHSGA_ERR_FORMAT, "hierarchy edge out of range");
       require(cc_of[v] == cc_of[u] && layer_of[v] > layer_of[u], CHSGA_ERR_UNSUPPORTED,
               "downward hierarchy edge does not come from a later layer of its component");
       require(p.down_w[j] >= 1 && p.down_w[j] <= (1u << 30), CHSGA_ERR_UNSUPPORTED,
               "hierarchy weights must be in [1, 2^30]");
-      dn[dev[u]].push_back({(int32_t)bv_last(v), (int32_t)p.down_w[j]});
     }
+    L.dn_off[dev[u] + 1] += (uint32_t)(p.down_offset[u + 1] - p.down_offset[u]);
   }
-  auto flatten = [&](std::vector<std::vector<EdgeW>>& lists, std::vector<uint32_t>& off,
-                     std::vector<EdgeW>& out) {
-    off.assign(S + 1, 0);
-    for (uint32_t d = 0; d < S; ++d) off[d + 1] = off[d] + (uint32_t)lists[d].size();
-    out.reserve(off[S]);
-    for (auto& l : lists) out.insert(out.end(), l.begin(), l.end());
-  };
-  flatten(up, L.up_off, L.up_in);
-  flatten(dn, L.dn_off, L.dn_in);
-  auto heads = [&](const std::vector<uint32_t>& off, const std::vector<EdgeW>& in,
-                   std::vector<uint32_t>& h) {
-    h.assign((size_t)4 * S, 0);
-    for (uint32_t d = 0; d < S; ++d) {
-      h[4 * d] = off[d];
-      h[4 * d + 1] = off[d + 1];
-      if (off[d + 1] > off[d]) {
-        h[4 * d + 2] = (uint32_t)in[off[d]].src;
-        h[4 * d + 3] = (uint32_t)in[off[d]].w;
-      }
-    }
-  };
-  heads(L.dn_off, L.dn_in, L.dn_head);
+  for (uint32_t d = 0; d < S; ++d) {
+    L.up_off[d + 1] += L.up_off[d];
+    L.dn_off[d + 1] += L.dn_off[d];
+  }
+  L.up_in.resize(L.up_off[S]);
+  L.dn_in.resize(L.dn_off[S]);
+  {
+    std::vector<uint32_t> at(L.up_off.begin(), L.up_off.end() - 1);
+    for (uint32_t u = 0; u < S; ++u)
+      for (uint64_t j = p.up_offset[u]; j < p.up_offset[u + 1]; ++j)
+        L.up_in[at[dev[p.up_v[j]]]++] = {(int32_t)bv_last(u), (int32_t)p.up_w[j]};
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t u = 0; u < (int64_t)S; ++u) {
+    uint32_t k = L.dn_off[dev[u]];
+    for (uint64_t j = p.down_offset[u]; j < p.down_offset[u + 1]; ++j)
+      L.dn_in[k++] = {(int32_t)bv_last(p.down_v[j]), (int32_t)p.down_w[j]};
+  }
+  L.dn_head.assign((size_t)4 * S, 0);
   // upward lists average about two edges: their head carries the first two
   // (8 words: begin, end, src0, w0, src1, w1, 0, 0)
   L.up_head.assign((size_t)8 * S, 0);
-  for (uint32_t d = 0; d < S; ++d) {
-    uint32_t* h = &L.up_head[(size_t)8 * d];
-    h[0] = L.up_off[d];
-    h[1] = L.up_off[d + 1];
-    for (uint32_t j = 0; j < 2 && L.up_off[d] + j < L.up_off[d + 1]; ++j) {
-      h[2 + 2 * j] = (uint32_t)L.up_in[L.up_off[d] + j].src;
-      h[3 + 2 * j] = (uint32_t)L.up_in[L.up_off[d] + j].w;
-    }
-  }
   L.fin.assign((size_t)4 * S, 0);
-  for (uint32_t d = 0; d < S; ++d) {
+#pragma omp parallel for schedule(static)
+  for (int64_t d = 0; d < (int64_t)S; ++d) {
+    uint32_t* h = &L.dn_head[(size_t)4 * d];
+    h[0] = L.dn_off[d];
+    h[1] = L.dn_off[d + 1];
+    if (L.dn_off[d + 1] > L.dn_off[d]) {
+      h[2] = (uint32_t)L.dn_in[L.dn_off[d]].src;
+      h[3] = (uint32_t)L.dn_in[L.dn_off[d]].w;
+    }
+    uint32_t* u8 = &L.up_head[(size_t)8 * d];
+    u8[0] = L.up_off[d];
+    u8[1] = L.up_off[d + 1];
+    for (uint32_t j = 0; j < 2 && L.up_off[d] + j < L.up_off[d + 1]; ++j) {
+      u8[2 + 2 * j] = (uint32_t)L.up_in[L.up_off[d] + j].src;
+      u8[3 + 2 * j] = (uint32_t)L.up_in[L.up_off[d] + j].w;
+    }
     L.fin[4 * d] = L.dv_first[d];
     L.fin[4 * d + 1] = L.dv_len[d];
     L.fin[4 * d + 2] = L.dv_s[d];

@@ -12,80 +12,10 @@
 #include <fstream>
 
 #include "host_graph.hpp"
+#include "text_io.hpp"
 
 namespace chsga {
 
-namespace {
-
-std::vector<char> slurp(const std::string& path) {
-  FILE* f = std::fopen(path.c_str(), "rb");
-  require(f != nullptr, CHSGA_ERR_IO, "cannot open " + path + ": " + std::strerror(errno));
-  std::vector<char> buf;
-  std::fseek(f, 0, SEEK_END);
-  long sz = std::ftell(f);
-  std::fseek(f, 0, SEEK_SET);
-  if (sz > 0) {
-    buf.resize((size_t)sz);
-    size_t got = std::fread(buf.data(), 1, buf.size(), f);
-    std::fclose(f);
-    require(got == buf.size(), CHSGA_ERR_IO, "short read of " + path);
-  } else {
-    std::fclose(f);
-  }
-  return buf;
-}
-
-// Whitespace-separated token scanner over an in-memory file.
-struct Tok {
-  const char* p;
-  const char* e;
-  std::string path;
-  explicit Tok(const std::vector<char>& b, std::string pth)
-      : p(b.data()), e(b.data() + b.size()), path(std::move(pth)) {}
-  void skip() {
-    while (p < e && std::isspace((unsigned char)*p)) ++p;
-  }
-  bool more() {
-    skip();
-    return p < e;
-  }
-  bool word(std::string& out) {
-    skip();
-    if (p >= e) return false;
-    const char* s = p;
-    while (p < e && !std::isspace((unsigned char)*p)) ++p;
-    out.assign(s, p);
-    return true;
-  }
-  uint64_t u64(const char* what) {
-    skip();
-    require(p < e && *p >= '0' && *p <= '9', CHSGA_ERR_FORMAT,
-            path + ": expected " + what);
-    uint64_t v = 0;
-    while (p < e && *p >= '0' && *p <= '9') {
-      uint64_t d = (uint64_t)(*p - '0');
-      require(v <= (UINT64_MAX - d) / 10, CHSGA_ERR_FORMAT, path + ": integer overflow");
-      v = v * 10 + d;
-      ++p;
-    }
-    require(p >= e || std::isspace((unsigned char)*p), CHSGA_ERR_FORMAT,
-            path + ": malformed " + what);
-    return v;
-  }
-  double real(const char* what) {
-    skip();
-    require(p < e, CHSGA_ERR_FORMAT, path + ": expected " + what);
-    const char* s = p;
-    while (p < e && !std::isspace((unsigned char)*p)) ++p;
-    std::string t(s, p);
-    char* end = nullptr;
-    double v = std::strtod(t.c_str(), &end);
-    require(end && *end == '\0', CHSGA_ERR_FORMAT, path + ": malformed " + what + " '" + t + "'");
-    return v;
-  }
-};
-
-}  // namespace
 
 HostCsr read_adj(const std::string& path) {
   std::vector<char> buf = slurp(path);
@@ -103,12 +33,12 @@ HostCsr read_adj(const std::string& path) {
   for (uint64_t i = 0; i < g.n; ++i) g.offset[i] = t.u64("offset");
   g.offset[g.n] = g.m;
   for (uint64_t i = 0; i < g.n; ++i)
-    require(g.offset[i] <= g.offset[i + 1], CHSGA_ERR_FORMAT,
-            path + ": offsets not non-decreasing at " + std::to_string(i));
+    if (g.offset[i] > g.offset[i + 1])
+      fail(CHSGA_ERR_FORMAT, path + ": offsets not non-decreasing at " + std::to_string(i));
   g.target.resize(g.m);
   for (uint64_t i = 0; i < g.m; ++i) {
     uint64_t v = t.u64("edge target");
-    require(v < g.n, CHSGA_ERR_FORMAT, path + ": edge target out of range");
+    if (v >= g.n) fail(CHSGA_ERR_FORMAT, path + ": edge target out of range");
     g.target[i] = (uint32_t)v;
   }
   if (t.more()) {
@@ -118,8 +48,8 @@ HostCsr read_adj(const std::string& path) {
     bool all_one = true;
     for (uint64_t i = 0; i < g.m; ++i) {
       double w = t.real("edge weight");
-      require(w >= 0 && w == std::floor(w) && w < 4294967296.0, CHSGA_ERR_UNSUPPORTED,
-              path + ": edge weights must be non-negative integers");
+      if (!(w >= 0 && w == std::floor(w) && w < 4294967296.0))
+        fail(CHSGA_ERR_UNSUPPORTED, path + ": edge weights must be non-negative integers");
       g.weight[i] = (uint32_t)w;
       all_one &= (g.weight[i] == 1);
     }

@@ -46,8 +46,8 @@ void validate_host_graph(const chsga_host_graph& g) {
   require(g.label_offsets[0] == 0 && g.label_offsets[S] == N, CHSGA_ERR_FORMAT,
           "label offsets must run from 0 to the number of labels");
   for (uint64_t s = 0; s < S; ++s)
-    require(g.label_offsets[s] < g.label_offsets[s + 1], CHSGA_ERR_UNSUPPORTED,
-            "string vertex " + std::to_string(s) + " has an empty label");
+    if (g.label_offsets[s] >= g.label_offsets[s + 1])
+      fail(CHSGA_ERR_UNSUPPORTED, "string vertex " + std::to_string(s) + " has an empty label");
   require(g.pch.present, CHSGA_ERR_FORMAT, "no hierarchy attached");
   validate_pch(g.pch, S);
 }

@@ -23,25 +23,29 @@
 // offsets (csr_to_adj.cpp:39-118).
 #include <algorithm>
 #include <cstring>
-#include <fstream>
 #include <memory>
+#include <parallel/algorithm>
 #include <string>
 #include <unordered_map>
 #include <vector>
 
 #include "host_graph.hpp"
+#include "text_io.hpp"
 
 namespace chsga {
 extern thread_local std::string g_last_error;
 
 namespace {
 
-// A string-labeled CSR as handlegraph_to_csr's CSR_container holds it.
+// A string-labeled CSR as handlegraph_to_csr's CSR_container holds it, the
+// labels concatenated: label i is lab[lab_off[i] .. lab_off[i + 1]).
 struct CsrText {
-  std::vector<std::string> labels;
+  std::string lab;
+  std::vector<uint64_t> lab_off{0};
   std::vector<uint64_t> offsets{0};
   std::vector<uint64_t> adj;
-  uint64_t n() const { return labels.size(); }
+  uint64_t n() const { return lab_off.size() - 1; }
+  uint64_t len(uint64_t i) const { return lab_off[i + 1] - lab_off[i]; }
 };
 
 char packed_base(char c) {
@@ -64,153 +68,256 @@ char complement(char c) {
   }
 }
 
-std::vector<std::string> split_tabs(const std::string& line) {
-  std::vector<std::string> f;
-  size_t a = 0;
-  while (true) {
-    size_t b = line.find('\t', a);
-    f.push_back(line.substr(a, b == std::string::npos ? std::string::npos : b - a));
-    if (b == std::string::npos) break;
-    a = b + 1;
+// One tab-separated field of a GFA line, in the file's bytes.
+struct Field {
+  const char* p = nullptr;
+  size_t n = 0;
+  bool is(const char* s) const { return n == std::strlen(s) && std::memcmp(p, s, n) == 0; }
+  std::string str() const { return std::string(p, n); }
+};
+
+// The first `maxf` fields of the line [b, e) (the last one ends at the next
+// tab too); returns how many there are, up to maxf.
+size_t split_tabs(const char* b, const char* e, Field* f, size_t maxf) {
+  size_t k = 0;
+  const char* a = b;
+  while (k < maxf) {
+    const char* t = static_cast<const char*>(std::memchr(a, '\t', (size_t)(e - a)));
+    const char* end = t ? t : e;
+    f[k++] = Field{a, (size_t)(end - a)};
+    if (!t) break;
+    a = t + 1;
   }
-  return f;
+  return k;
 }
 
-uint64_t parse_id(const std::string& s, const std::string& path, uint64_t line) {
-  require(!s.empty() && s.size() < 20 && std::all_of(s.begin(), s.end(), ::isdigit), CHSGA_ERR_FORMAT,
-          path + ":" + std::to_string(line) + ": segment names must be numeric node ids, got '" + s + "'");
-  return std::stoull(s);
+uint64_t parse_id(const Field& s, const std::string& path, uint64_t line) {
+  bool ok = s.n > 0 && s.n < 20;
+  uint64_t v = 0;
+  for (size_t i = 0; ok && i < s.n; ++i) {
+    ok = s.p[i] >= '0' && s.p[i] <= '9';
+    v = v * 10 + (uint64_t)(s.p[i] - '0');
+  }
+  if (!ok)
+    fail(CHSGA_ERR_FORMAT,
+         path + ":" + std::to_string(line) + ": segment names must be numeric node ids, got '" + s.str() + "'");
+  return v;
 }
 
 CsrText gfa_to_string_csr(const std::string& path) {
-  std::ifstream in(path);
-  require(bool(in), CHSGA_ERR_IO, "cannot read " + path);
-  std::vector<std::pair<uint64_t, std::string>> nodes;
+  const std::vector<char> buf = slurp(path);
+  struct Node {
+    uint64_t id, off, len;  // sequence in seqs
+  };
   struct Link {
     uint64_t a, b;
     bool ra, rb;  // reverse orientation
   };
+  std::vector<Node> nodes;
   std::vector<Link> links;
-  std::string line;
+  std::string seqs;
+  const char* p = buf.data();
+  const char* const e = p + buf.size();
   uint64_t ln = 0;
-  while (std::getline(in, line)) {
+  Field f[6];
+  while (p < e) {
+    const char* nl = static_cast<const char*>(std::memchr(p, '\n', (size_t)(e - p)));
+    const char* le = nl ? nl : e;
     ++ln;
-    if (!line.empty() && line.back() == '\r') line.pop_back();
-    if (line.empty()) continue;
-    if (line[0] == 'S') {
-      const auto f = split_tabs(line);
-      require(f.size() >= 3, CHSGA_ERR_FORMAT, path + ":" + std::to_string(ln) + ": S line needs a name and a sequence");
-      require(f[2] != "*" && !f[2].empty(), CHSGA_ERR_FORMAT,
-              path + ":" + std::to_string(ln) + ": segment without a sequence");
-      std::string seq(f[2]);
-      for (char& c : seq) c = packed_base(c);
-      nodes.push_back({parse_id(f[1], path, ln), std::move(seq)});
-    } else if (line[0] == 'L') {
-      const auto f = split_tabs(line);
-      require(f.size() >= 5, CHSGA_ERR_FORMAT, path + ":" + std::to_string(ln) + ": L line needs 5 fields");
-      require((f[2] == "+" || f[2] == "-") && (f[4] == "+" || f[4] == "-"), CHSGA_ERR_FORMAT,
-              path + ":" + std::to_string(ln) + ": link orientations must be + or -");
-      require(f.size() < 6 || f[5] == "*" || f[5] == "0M", CHSGA_ERR_UNSUPPORTED,
-              path + ":" + std::to_string(ln) + ": overlapping links are not supported (blunt graphs only)");
-      links.push_back({parse_id(f[1], path, ln), parse_id(f[3], path, ln), f[2] == "-", f[4] == "-"});
+    if (le > p && le[-1] == '\r') --le;
+    if (le > p && *p == 'S') {
+      const size_t k = split_tabs(p, le, f, 3);
+      if (k < 3)
+        fail(CHSGA_ERR_FORMAT, path + ":" + std::to_string(ln) + ": S line needs a name and a sequence");
+      if (f[2].is("*") || f[2].n == 0)
+        fail(CHSGA_ERR_FORMAT, path + ":" + std::to_string(ln) + ": segment without a sequence");
+      const uint64_t off = seqs.size();
+      seqs.resize(off + f[2].n);
+      for (size_t i = 0; i < f[2].n; ++i) seqs[off + i] = packed_base(f[2].p[i]);
+      nodes.push_back({parse_id(f[1], path, ln), off, f[2].n});
+    } else if (le > p && *p == 'L') {
+      const size_t k = split_tabs(p, le, f, 6);
+      if (k < 5) fail(CHSGA_ERR_FORMAT, path + ":" + std::to_string(ln) + ": L line needs 5 fields");
+      if (!((f[2].is("+") || f[2].is("-")) && (f[4].is("+") || f[4].is("-"))))
+        fail(CHSGA_ERR_FORMAT, path + ":" + std::to_string(ln) + ": link orientations must be + or -");
+      if (!(k < 6 || f[5].is("*") || f[5].is("0M")))
+        fail(CHSGA_ERR_UNSUPPORTED,
+             path + ":" + std::to_string(ln) + ": overlapping links are not supported (blunt graphs only)");
+      links.push_back({parse_id(f[1], path, ln), parse_id(f[3], path, ln), f[2].is("-"), f[4].is("-")});
     }
+    p = nl ? nl + 1 : e;
   }
   require(!nodes.empty(), CHSGA_ERR_FORMAT, path + ": no segments");
-  std::sort(nodes.begin(), nodes.end(),
-            [](const auto& x, const auto& y) { return x.first < y.first; });
+  __gnu_parallel::sort(nodes.begin(), nodes.end(),
+                       [](const Node& x, const Node& y) { return x.id < y.id; });
+  for (uint64_t i = 1; i < nodes.size(); ++i)
+    if (nodes[i].id == nodes[i - 1].id)
+      fail(CHSGA_ERR_FORMAT, path + ": duplicate segment " + std::to_string(nodes[i].id));
+  // node id -> position in id order: a table when the ids are dense enough
+  const uint64_t max_id = nodes.back().id;
+  const bool dense = max_id < 4 * (uint64_t)nodes.size() + 1024;
+  std::vector<uint64_t> table;
   std::unordered_map<uint64_t, uint64_t> index;
-  index.reserve(nodes.size());
-  for (uint64_t i = 0; i < nodes.size(); ++i) {
-    require(index.emplace(nodes[i].first, i).second, CHSGA_ERR_FORMAT,
-            path + ": duplicate segment " + std::to_string(nodes[i].first));
+  if (dense) {
+    table.assign(max_id + 1, ~0ull);
+    for (uint64_t i = 0; i < nodes.size(); ++i) table[nodes[i].id] = i;
+  } else {
+    index.reserve(nodes.size());
+    for (uint64_t i = 0; i < nodes.size(); ++i) index.emplace(nodes[i].id, i);
   }
+  auto handle = [&](uint64_t id, bool rev) {
+    uint64_t i = ~0ull;
+    if (dense) {
+      if (id <= max_id) i = table[id];
+    } else {
+      auto it = index.find(id);
+      if (it != index.end()) i = it->second;
+    }
+    if (i == ~0ull) fail(CHSGA_ERR_FORMAT, path + ": link to unknown segment " + std::to_string(id));
+    return 2 * i + (rev ? 1 : 0);
+  };
   CsrText s;
   const uint64_t V = 2 * nodes.size();
-  s.labels.resize(V);
-  for (uint64_t i = 0; i < nodes.size(); ++i) {
-    const std::string& seq = nodes[i].second;
-    s.labels[2 * i] = seq;
-    std::string rc(seq.rbegin(), seq.rend());
-    for (char& c : rc) c = complement(c);
-    s.labels[2 * i + 1] = std::move(rc);
+  s.lab.reserve(2 * seqs.size());
+  s.lab_off.reserve(V + 1);
+  for (const Node& nd : nodes) {
+    s.lab.append(seqs, nd.off, nd.len);
+    s.lab_off.push_back(s.lab.size());
+    for (uint64_t i = nd.len; i-- > 0;) s.lab.push_back(complement(seqs[nd.off + i]));
+    s.lab_off.push_back(s.lab.size());
   }
-  std::vector<std::vector<uint64_t>> out(V);
-  auto handle = [&](uint64_t id, bool rev) {
-    auto it = index.find(id);
-    require(it != index.end(), CHSGA_ERR_FORMAT, path + ": link to unknown segment " + std::to_string(id));
-    return 2 * it->second + (rev ? 1 : 0);
-  };
+  // every link in both directions, then each handle's targets sorted, once
+  std::vector<std::pair<uint64_t, uint64_t>> arcs;
+  arcs.reserve(2 * links.size());
   for (const Link& l : links) {
-    out[handle(l.a, l.ra)].push_back(handle(l.b, l.rb));
-    out[handle(l.b, !l.rb)].push_back(handle(l.a, !l.ra));
+    arcs.emplace_back(handle(l.a, l.ra), handle(l.b, l.rb));
+    arcs.emplace_back(handle(l.b, !l.rb), handle(l.a, !l.ra));
   }
-  s.offsets.assign(1, 0);
-  for (uint64_t v = 0; v < V; ++v) {
-    auto& o = out[v];
-    std::sort(o.begin(), o.end());
-    o.erase(std::unique(o.begin(), o.end()), o.end());
-    s.adj.insert(s.adj.end(), o.begin(), o.end());
-    s.offsets.push_back(s.adj.size());
+  __gnu_parallel::sort(arcs.begin(), arcs.end());
+  arcs.erase(std::unique(arcs.begin(), arcs.end()), arcs.end());
+  s.offsets.assign(V + 1, 0);
+  s.adj.resize(arcs.size());
+  for (size_t i = 0; i < arcs.size(); ++i) {
+    ++s.offsets[arcs[i].first + 1];
+    s.adj[i] = arcs[i].second;
   }
+  for (uint64_t v = 0; v < V; ++v) s.offsets[v + 1] += s.offsets[v];
   return s;
 }
 
 // handlegraph_to_csr.cpp build(): one vertex per char.
 CsrText expand_chars(const CsrText& s) {
   CsrText c;
-  std::vector<uint64_t> first(s.n() + 1, 0);
-  for (uint64_t i = 0; i < s.n(); ++i) first[i + 1] = first[i] + s.labels[i].size();
-  c.labels.reserve(first.back());
-  c.offsets.assign(1, 0);
+  const uint64_t N = s.lab.size();
+  c.lab = s.lab;
+  c.lab_off.resize(N + 1);
+  for (uint64_t i = 0; i <= N; ++i) c.lab_off[i] = i;
+  c.offsets.resize(N + 1);
+  c.offsets[0] = 0;
+  c.adj.reserve(N + s.adj.size());
+  uint64_t x = 0;
   for (uint64_t i = 0; i < s.n(); ++i) {
-    const std::string& lab = s.labels[i];
-    for (uint64_t j = 0; j < lab.size(); ++j) {
-      c.labels.emplace_back(1, lab[j]);
-      if (j + 1 < lab.size()) {
-        c.adj.push_back(first[i] + j + 1);
+    const uint64_t L = s.len(i), f = s.lab_off[i];
+    for (uint64_t j = 0; j < L; ++j) {
+      if (j + 1 < L) {
+        c.adj.push_back(f + j + 1);
       } else {
-        for (uint64_t e = s.offsets[i]; e < s.offsets[i + 1]; ++e) c.adj.push_back(first[s.adj[e]]);
+        for (uint64_t e = s.offsets[i]; e < s.offsets[i + 1]; ++e) c.adj.push_back(s.lab_off[s.adj[e]]);
       }
-      c.offsets.push_back(c.adj.size());
+      c.offsets[++x] = c.adj.size();
     }
   }
   return c;
 }
 
+// Buffered writer of decimal integers and raw bytes.
+struct TextOut {
+  FILE* f;
+  std::string path;
+  std::vector<char> buf;
+  explicit TextOut(const std::string& p) : f(std::fopen(p.c_str(), "wb")), path(p) {
+    require(f != nullptr, CHSGA_ERR_IO, "cannot write " + path);
+    buf.reserve(1 << 22);
+  }
+  void flush() {
+    if (!buf.empty() && std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) {
+      std::fclose(f);
+      f = nullptr;
+      fail(CHSGA_ERR_IO, "write failed: " + path);
+    }
+    buf.clear();
+  }
+  void room() {
+    if (buf.size() > (1u << 22)) flush();
+  }
+  void num(uint64_t v, char sep) {
+    char t[24];
+    int k = 0;
+    do {
+      t[k++] = (char)('0' + v % 10);
+      v /= 10;
+    } while (v);
+    while (k) buf.push_back(t[--k]);
+    buf.push_back(sep);
+    room();
+  }
+  void bytes(const char* p, size_t n, char sep) {
+    buf.insert(buf.end(), p, p + n);
+    buf.push_back(sep);
+    room();
+  }
+  void put(char c) { buf.push_back(c); }
+  void close() {
+    flush();
+    const bool ok = std::fclose(f) == 0;
+    f = nullptr;
+    require(ok, CHSGA_ERR_IO, "write failed: " + path);
+  }
+  ~TextOut() {
+    if (f) std::fclose(f);
+  }
+};
+
 void write_csr_text(const std::string& path, const CsrText& s) {
-  std::ofstream o(path);
-  require(bool(o), CHSGA_ERR_IO, "cannot write " + path);
+  TextOut o(path);
   // write_csr (handlegraph_to_csr.cpp:130-161): every list ends with " \n"
-  o << s.n() << "\n" << s.adj.size() << "\n";
-  for (const auto& l : s.labels) o << l << " ";
-  o << "\n";
-  for (uint64_t x : s.offsets) o << x << " ";
-  o << "\n";
-  for (uint64_t x : s.adj) o << x << " ";
-  o << "\n";
-  require(bool(o), CHSGA_ERR_IO, "write failed: " + path);
+  o.num(s.n(), '\n');
+  o.num(s.adj.size(), '\n');
+  for (uint64_t i = 0; i < s.n(); ++i) o.bytes(s.lab.data() + s.lab_off[i], s.len(i), ' ');
+  o.put('\n');
+  for (uint64_t x : s.offsets) o.num(x, ' ');
+  o.put('\n');
+  for (uint64_t x : s.adj) o.num(x, ' ');
+  o.put('\n');
+  o.close();
 }
 
 CsrText read_csr_text(const std::string& path) {
-  std::ifstream in(path);
-  require(bool(in), CHSGA_ERR_IO, "cannot read " + path);
-  uint64_t n = 0, m = 0;
-  require(bool(in >> n >> m), CHSGA_ERR_FORMAT, path + ": failed to read header (n m)");
+  const std::vector<char> buf = slurp(path);
+  Tok t(buf, path);
+  const uint64_t n = t.u64("the vertex count (header n m)");
+  const uint64_t m = t.u64("the edge count (header n m)");
   CsrText s;
-  s.labels.resize(n);
-  for (uint64_t i = 0; i < n; ++i)
-    require(bool(in >> s.labels[i]), CHSGA_ERR_FORMAT, path + ": failed to read label " + std::to_string(i));
+  s.lab_off.reserve(n + 1);
+  for (uint64_t i = 0; i < n; ++i) {
+    t.skip();
+    const char* b = t.p;
+    while (t.p < t.e && !std::isspace((unsigned char)*t.p)) ++t.p;
+    if (t.p == b) fail(CHSGA_ERR_FORMAT, path + ": failed to read label " + std::to_string(i));
+    s.lab.append(b, t.p);
+    s.lab_off.push_back(s.lab.size());
+  }
   s.offsets.resize(n + 1);
   for (uint64_t i = 0; i <= n; ++i) {
-    require(bool(in >> s.offsets[i]), CHSGA_ERR_FORMAT, path + ": failed to read offset " + std::to_string(i));
-    require(i == 0 || s.offsets[i] >= s.offsets[i - 1], CHSGA_ERR_FORMAT,
-            path + ": offsets not non-decreasing at index " + std::to_string(i));
+    s.offsets[i] = t.u64("an offset");
+    if (i > 0 && s.offsets[i] < s.offsets[i - 1])
+      fail(CHSGA_ERR_FORMAT, path + ": offsets not non-decreasing at index " + std::to_string(i));
   }
   require(s.offsets[n] == m, CHSGA_ERR_FORMAT, path + ": final offset differs from the edge count");
   s.adj.resize(m);
   for (uint64_t e = 0; e < m; ++e) {
-    require(bool(in >> s.adj[e]), CHSGA_ERR_FORMAT, path + ": failed to read adjacency entry " + std::to_string(e));
-    require(s.adj[e] < n, CHSGA_ERR_FORMAT, path + ": adjacency entry out of range");
+    s.adj[e] = t.u64("an adjacency entry");
+    if (s.adj[e] >= n) fail(CHSGA_ERR_FORMAT, path + ": adjacency entry out of range");
   }
   return s;
 }
@@ -222,7 +329,7 @@ HostCsr to_host_csr(const CsrText& s) {
   g.offset = s.offsets;
   g.target.resize(g.m);
   for (uint64_t e = 0; e < g.m; ++e) {
-    require(s.adj[e] < (1ull << 32), CHSGA_ERR_UNSUPPORTED, "vertex ids above 2^32");
+    if (s.adj[e] >= (1ull << 32)) fail(CHSGA_ERR_UNSUPPORTED, "vertex ids above 2^32");
     g.target[e] = (uint32_t)s.adj[e];
   }
   return g;
@@ -235,16 +342,13 @@ chsga_host_graph* host_graph_from(const CsrText& str, const CsrText& chr) {
   auto g = std::make_unique<chsga_host_graph>();
   g->string_graph = to_host_csr(str);
   g->char_graph = to_host_csr(chr);
-  g->label_offsets.assign(1, 0);
-  for (const auto& l : str.labels) {
-    g->labels.insert(g->labels.end(), l.begin(), l.end());
-    g->label_offsets.push_back(g->labels.size());
-  }
+  g->labels.assign(str.lab.begin(), str.lab.end());
+  g->label_offsets = str.lab_off;
   require(g->labels.size() == chr.n(), CHSGA_ERR_FORMAT,
           "the char CSR does not have one vertex per char of the string CSR");
   for (uint64_t i = 0; i < chr.n(); ++i)
-    require(chr.labels[i].size() == 1 && chr.labels[i][0] == g->labels[i], CHSGA_ERR_FORMAT,
-            "char CSR label " + std::to_string(i) + " differs from the string labels");
+    if (!(chr.len(i) == 1 && chr.lab[chr.lab_off[i]] == g->labels[i]))
+      fail(CHSGA_ERR_FORMAT, "char CSR label " + std::to_string(i) + " differs from the string labels");
   return g.release();
 }
 
@@ -305,14 +409,8 @@ chsga_status chsga_csr_text_to_adj(const char* csr_path, const char* adj_out, co
             "null argument");
     const CsrText s = read_csr_text(csr_path);
     write_adj(adj_out, to_host_csr(s));
-    std::vector<char> labels;
-    std::vector<uint64_t> offs{0};
-    for (const auto& l : s.labels) {
-      labels.insert(labels.end(), l.begin(), l.end());
-      offs.push_back(labels.size());
-    }
-    write_labels(labels_out, labels);
-    write_label_offsets(label_offsets_out, offs);
+    write_labels(labels_out, std::vector<char>(s.lab.begin(), s.lab.end()));
+    write_label_offsets(label_offsets_out, s.lab_off);
   });
 }
 
