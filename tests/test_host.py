@@ -209,3 +209,27 @@ def test_gpu_hierarchy_builder_fails_with_a_status_or_matches():
         assert "hierarchy builder" in str(e)
         g.build_pch()
     assert_same(pch_arrays(g), host)
+
+
+def test_layout_rejects_a_second_special_byte(tmp_path):
+    """The device layout codes A, C, G, T and one other byte: a labels file
+    with 'N' bytes and, later, an 'R' is rejected, naming the two bytes in
+    the order they first occur."""
+    _, files = gen_graph(tmp_path, "sp", backbone_len=20_000, seed=6)
+    lab = bytearray(open(files[3], "rb").read())
+    pos = [i for i, b in enumerate(lab) if b in b"ACGT"]
+    for i in pos[100:200:7]:
+        lab[i] = ord("N")
+    lab[pos[5000]] = ord("R")
+    bad = list(files)
+    bad[3] = str(tmp_path / "two.labels")
+    open(bad[3], "wb").write(bytes(lab))
+    g = cb.HostGraph.read_files(*bad)
+    with pytest.raises(cb.ChsgaError) as e:
+        g.check_layout(64, 16)
+    assert e.value.status == cb.ERR_UNSUPPORTED
+    assert "'N' and 'R'" in str(e.value)
+    # one special byte alone is accepted
+    lab[pos[5000]] = ord("N")
+    open(bad[3], "wb").write(bytes(lab))
+    assert cb.HostGraph.read_files(*bad).check_layout(64, 16)["num_levels"] > 0
