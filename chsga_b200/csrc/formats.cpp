@@ -30,30 +30,60 @@ HostCsr read_adj(const std::string& path) {
   require(g.n < (1ull << 32) && g.m < (1ull << 40), CHSGA_ERR_UNSUPPORTED,
           path + ": graph too large for 32-bit vertex ids");
   g.offset.resize(g.n + 1);
-  for (uint64_t i = 0; i < g.n; ++i) g.offset[i] = t.u64("offset");
+  g.target.resize(g.m);
+  // the n offsets and m targets in one parallel pass; a malformed, missing
+  // or out-of-range number sends the block to the sequential scanner, which
+  // reports it
+  const uint64_t n = g.n;
+  const char* after = nullptr;
+  const bool fast = parse_tokens(t.p, t.e, g.n + g.m, &after, [&](uint64_t k, const char* s, const char* z) {
+    uint64_t v;
+    if (!token_u64(s, z, v)) return false;
+    if (k < n) {
+      g.offset[k] = v;
+      return true;
+    }
+    if (v >= n) return false;
+    g.target[k - n] = (uint32_t)v;
+    return true;
+  });
+  if (fast) {
+    t.p = after;
+  } else {
+    for (uint64_t i = 0; i < g.n; ++i) g.offset[i] = t.u64("offset");
+  }
   g.offset[g.n] = g.m;
   for (uint64_t i = 0; i < g.n; ++i)
     if (g.offset[i] > g.offset[i + 1])
       fail(CHSGA_ERR_FORMAT, path + ": offsets not non-decreasing at " + std::to_string(i));
-  g.target.resize(g.m);
-  for (uint64_t i = 0; i < g.m; ++i) {
-    uint64_t v = t.u64("edge target");
-    if (v >= g.n) fail(CHSGA_ERR_FORMAT, path + ": edge target out of range");
-    g.target[i] = (uint32_t)v;
-  }
+  if (!fast)
+    for (uint64_t i = 0; i < g.m; ++i) {
+      uint64_t v = t.u64("edge target");
+      if (v >= g.n) fail(CHSGA_ERR_FORMAT, path + ": edge target out of range");
+      g.target[i] = (uint32_t)v;
+    }
   if (t.more()) {
     // weights as csr_to_adj writes them ("1.0"); the DP multiplies them by
     // the integer insertion cost, so they must be non-negative integers.
     g.weight.resize(g.m);
-    bool all_one = true;
-    for (uint64_t i = 0; i < g.m; ++i) {
-      double w = t.real("edge weight");
-      if (!(w >= 0 && w == std::floor(w) && w < 4294967296.0))
-        fail(CHSGA_ERR_UNSUPPORTED, path + ": edge weights must be non-negative integers");
-      g.weight[i] = (uint32_t)w;
-      all_one &= (g.weight[i] == 1);
+    uint64_t not_one = 0;
+    const bool wfast = parse_tokens(t.p, t.e, g.m, &after, [&](uint64_t k, const char* s, const char* z) {
+      double w;
+      if (!token_real(s, z, w) || !(w >= 0 && w == std::floor(w) && w < 4294967296.0)) return false;
+      g.weight[k] = (uint32_t)w;
+      return true;
+    });
+    if (!wfast) {
+      for (uint64_t i = 0; i < g.m; ++i) {
+        double w = t.real("edge weight");
+        if (!(w >= 0 && w == std::floor(w) && w < 4294967296.0))
+          fail(CHSGA_ERR_UNSUPPORTED, path + ": edge weights must be non-negative integers");
+        g.weight[i] = (uint32_t)w;
+      }
     }
-    if (all_one) g.weight.clear();
+#pragma omp parallel for reduction(+ : not_one) schedule(static)
+    for (int64_t i = 0; i < (int64_t)g.m; ++i) not_one += g.weight[i] != 1;
+    if (!not_one) g.weight.clear();
   } else {
     require(head == "AdjacencyGraph", CHSGA_ERR_FORMAT, path + ": missing weights");
   }

@@ -233,3 +233,36 @@ def test_layout_rejects_a_second_special_byte(tmp_path):
     lab[pos[5000]] = ord("N")
     open(bad[3], "wb").write(bytes(lab))
     assert cb.HostGraph.read_files(*bad).check_layout(64, 16)["num_levels"] > 0
+
+
+def test_large_adjacency_file_errors(tmp_path):
+    """Adjacency files large enough for the parallel reader still fail with
+    the sequential reader's status and message: a target out of range, a
+    weight that is not an integer, a weight that is not a number."""
+    g, files = gen_graph(tmp_path, "big", backbone_len=600_000, seed=8)
+    text = open(files[0]).read()
+    assert len(text) > (4 << 20)
+    lines = text.split("\n")
+    n, m = int(lines[1]), int(lines[2])
+    first_target, first_weight = 3 + n, 3 + n + m
+    assert lines[first_weight] == "1.0"
+
+    def read_with(line_no, value):
+        bad = list(lines)
+        bad[line_no] = value
+        p = tmp_path / f"bad{line_no}_{value}.adj"
+        p.write_text("\n".join(bad))
+        return cb.HostGraph.read_files(str(p), *files[1:])
+
+    for line_no, value, status, msg in [
+        (first_target + m // 2, str(n), cb.ERR_FORMAT, "edge target out of range"),
+        (first_weight + m // 3, "1.5", cb.ERR_UNSUPPORTED, "non-negative integers"),
+        (first_weight + m // 3, "x1", cb.ERR_FORMAT, "malformed edge weight"),
+    ]:
+        with pytest.raises(cb.ChsgaError) as e:
+            read_with(line_no, value)
+        assert e.value.status == status and msg in str(e.value)
+    # a weight of 2 is kept as a weight, not dropped with the all-one case
+    h = read_with(first_weight + 5, "2")
+    w = np.ctypeslib.as_array(h.view().char_graph.weight, (m,))
+    assert w[5] == 2 and (np.delete(w, 5) == 1).all()
