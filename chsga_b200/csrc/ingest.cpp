@@ -21,6 +21,8 @@
 // labels space-separated, n+1 offsets, m targets), which csr_to_adj turns
 // into an AdjacencyGraph file, the concatenated labels and the label
 // offsets (csr_to_adj.cpp:39-118).
+#include <omp.h>
+
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -278,22 +280,55 @@ struct TextOut {
   }
 };
 
+// Text of items [0, n), each made by put(i, buffer), formatted on every
+// thread in slices and written in order.
+template <typename F>
+void put_parallel(TextOut& o, size_t n, size_t bytes_each, F put) {
+  const int nt = n < (1u << 16) ? 1 : std::max(1, omp_get_max_threads());
+  std::vector<std::vector<char>> part(nt);
+#pragma omp parallel for num_threads(nt) schedule(static, 1)
+  for (int t = 0; t < nt; ++t) {
+    const size_t a = n / nt * t, z = t + 1 == nt ? n : n / nt * (t + 1);
+    part[t].reserve((z - a) * bytes_each);
+    for (size_t i = a; i < z; ++i) put(i, part[t]);
+  }
+  o.flush();
+  for (auto& b : part) {
+    o.buf.swap(b);
+    o.flush();
+  }
+}
+
+void put_number(uint64_t v, char sep, std::vector<char>& b) {
+  char tmp[24];
+  int k = 0;
+  do {
+    tmp[k++] = (char)('0' + v % 10);
+    v /= 10;
+  } while (v);
+  while (k) b.push_back(tmp[--k]);
+  b.push_back(sep);
+}
+
 void write_csr_text(const std::string& path, const CsrText& s) {
   TextOut o(path);
   // write_csr (handlegraph_to_csr.cpp:130-161): every list ends with " \n"
   o.num(s.n(), '\n');
   o.num(s.adj.size(), '\n');
-  for (uint64_t i = 0; i < s.n(); ++i) o.bytes(s.lab.data() + s.lab_off[i], s.len(i), ' ');
+  put_parallel(o, s.n(), 4, [&](size_t i, std::vector<char>& b) {
+    b.insert(b.end(), s.lab.data() + s.lab_off[i], s.lab.data() + s.lab_off[i + 1]);
+    b.push_back(' ');
+  });
   o.put('\n');
-  for (uint64_t x : s.offsets) o.num(x, ' ');
+  put_parallel(o, s.offsets.size(), 10, [&](size_t i, std::vector<char>& b) { put_number(s.offsets[i], ' ', b); });
   o.put('\n');
-  for (uint64_t x : s.adj) o.num(x, ' ');
+  put_parallel(o, s.adj.size(), 10, [&](size_t i, std::vector<char>& b) { put_number(s.adj[i], ' ', b); });
   o.put('\n');
   o.close();
 }
 
-CsrText read_csr_text(const std::string& path) {
-  const std::vector<char> buf = slurp(path);
+// The write_csr layout, sequentially (the checks name what is wrong).
+CsrText read_csr_text_seq(const std::vector<char>& buf, const std::string& path) {
   Tok t(buf, path);
   const uint64_t n = t.u64("the vertex count (header n m)");
   const uint64_t m = t.u64("the edge count (header n m)");
@@ -319,6 +354,51 @@ CsrText read_csr_text(const std::string& path) {
     s.adj[e] = t.u64("an adjacency entry");
     if (s.adj[e] >= n) fail(CHSGA_ERR_FORMAT, path + ": adjacency entry out of range");
   }
+  return s;
+}
+
+// The same, the three lists parsed on every thread; any problem sends the
+// file to the sequential reader, which reports it.
+CsrText read_csr_text(const std::string& path) {
+  const std::vector<char> buf = slurp(path);
+  Tok t(buf, path);
+  uint64_t n = 0, m = 0;
+  t.skip();
+  if (!(t.p < t.e && *t.p >= '0' && *t.p <= '9')) return read_csr_text_seq(buf, path);
+  n = t.u64("the vertex count (header n m)");
+  t.skip();
+  if (!(t.p < t.e && *t.p >= '0' && *t.p <= '9')) return read_csr_text_seq(buf, path);
+  m = t.u64("the edge count (header n m)");
+  CsrText s;
+  std::vector<const char*> lb(n);
+  std::vector<uint32_t> ll(n);
+  const char* after = nullptr;
+  bool ok = parse_tokens(t.p, t.e, n, &after, [&](uint64_t k, const char* a, const char* z) {
+    if (z - a >= (1ll << 32)) return false;
+    lb[k] = a;
+    ll[k] = (uint32_t)(z - a);
+    return true;
+  });
+  if (!ok) return read_csr_text_seq(buf, path);
+  s.lab_off.resize(n + 1);
+  s.lab_off[0] = 0;
+  for (uint64_t i = 0; i < n; ++i) s.lab_off[i + 1] = s.lab_off[i] + ll[i];
+  s.lab.resize(s.lab_off[n]);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; ++i) std::memcpy(&s.lab[s.lab_off[i]], lb[i], ll[i]);
+  s.offsets.resize(n + 1);
+  ok = parse_tokens(after, t.e, n + 1, &after, [&](uint64_t k, const char* a, const char* z) {
+    return token_u64(a, z, s.offsets[k]);
+  });
+  if (!ok) return read_csr_text_seq(buf, path);
+  for (uint64_t i = 1; i <= n; ++i)
+    if (s.offsets[i] < s.offsets[i - 1]) return read_csr_text_seq(buf, path);
+  if (s.offsets[n] != m) return read_csr_text_seq(buf, path);
+  s.adj.resize(m);
+  ok = parse_tokens(after, t.e, m, &after, [&](uint64_t k, const char* a, const char* z) {
+    return token_u64(a, z, s.adj[k]) && s.adj[k] < n;
+  });
+  if (!ok) return read_csr_text_seq(buf, path);
   return s;
 }
 
