@@ -146,3 +146,25 @@ def test_ingested_graph_on_gpu(tmp_path):
     labels = open(files[3], "rb").read().replace(b"\n", b"")
     assert score == want[0] and orc.rescore(ops, reads[0], labels) == (score, len(reads[0]) - 1)
     ctx.close()
+
+
+def test_csr_text_reader_errors(tmp_path):
+    """Malformed CSR text fails with a format status naming the problem."""
+    gfa = tmp_path / "h.gfa"
+    gfa.write_text(HAND_GFA)
+    s, c = str(tmp_path / "s.csr"), str(tmp_path / "c.csr")
+    cb.gfa_to_csr_text(str(gfa), s, c)
+    good = open(s).read()
+    assert cb.HostGraph.from_csr_text(s, c).stats()["num_strings"] == 6
+    cases = [
+        ("6\n", "x6\n", "expected the vertex count"),
+        ("0 2 2 3 4 5 6 \n", "0 2 1 3 4 5 6 \n", "offsets not non-decreasing"),
+        ("2 5 4 1 1 3 \n", "2 5 4 1 1 9 \n", "adjacency entry out of range"),
+    ]
+    for good_line, bad_line, msg in cases:
+        assert good_line in good
+        p = tmp_path / "bad.csr"
+        p.write_text(good.replace(good_line, bad_line, 1))
+        with pytest.raises(cb.ChsgaError) as e:
+            cb.HostGraph.from_csr_text(str(p), c)
+        assert e.value.status == cb.ERR_FORMAT and msg in str(e.value), str(e.value)
