@@ -93,41 +93,26 @@ HostCsr read_adj(const std::string& path) {
 void write_adj(const std::string& path, const HostCsr& g) {
   FILE* f = std::fopen(path.c_str(), "wb");
   require(f != nullptr, CHSGA_ERR_IO, "cannot write " + path);
-  std::vector<char> buf;
-  buf.reserve(1 << 20);
-  auto flush = [&]() {
-    if (!buf.empty()) std::fwrite(buf.data(), 1, buf.size(), f);
-    buf.clear();
-  };
-  auto put = [&](uint64_t v) {
-    char tmp[24];
-    int k = 0;
-    do {
-      tmp[k++] = (char)('0' + v % 10);
-      v /= 10;
-    } while (v);
-    while (k) buf.push_back(tmp[--k]);
-    buf.push_back('\n');
-    if (buf.size() > (1 << 20)) flush();
-  };
-  const char* head = "AdjacencyGraph\n";
-  buf.insert(buf.end(), head, head + std::strlen(head));
-  put(g.n);
-  put(g.m);
-  for (uint64_t i = 0; i < g.n; ++i) put(g.offset[i]);
-  for (uint64_t i = 0; i < g.m; ++i) put(g.target[i]);
-  for (uint64_t i = 0; i < g.m; ++i) {
+  // "AdjacencyGraph", n, m, the offsets, the targets and a weight per edge
+  // ("1.0" for unit weights), one per line, as csr_to_adj writes them
+  std::vector<char> head;
+  const char* h = "AdjacencyGraph\n";
+  head.insert(head.end(), h, h + std::strlen(h));
+  put_decimal(g.n, '\n', head);
+  put_decimal(g.m, '\n', head);
+  bool ok = std::fwrite(head.data(), 1, head.size(), f) == head.size();
+  ok = ok && write_items(f, g.n, 10, [&](size_t i, std::vector<char>& b) { put_decimal(g.offset[i], '\n', b); });
+  ok = ok && write_items(f, g.m, 10, [&](size_t i, std::vector<char>& b) { put_decimal(g.target[i], '\n', b); });
+  ok = ok && write_items(f, g.m, 4, [&](size_t i, std::vector<char>& b) {
     if (g.weight.empty()) {
-      buf.insert(buf.end(), {'1', '.', '0', '\n'});
-      if (buf.size() > (1 << 20)) flush();
+      b.insert(b.end(), {'1', '.', '0', '\n'});
     } else {
-      std::string s = std::to_string(g.weight[i]) + ".0\n";
-      buf.insert(buf.end(), s.begin(), s.end());
-      if (buf.size() > (1 << 20)) flush();
+      put_decimal(g.weight[i], '.', b);
+      b.push_back('0');
+      b.push_back('\n');
     }
-  }
-  flush();
-  bool ok = std::fclose(f) == 0;
+  });
+  ok = (std::fclose(f) == 0) && ok;
   require(ok, CHSGA_ERR_IO, "write failed: " + path);
 }
 

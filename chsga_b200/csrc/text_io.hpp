@@ -192,4 +192,38 @@ inline bool token_real(const char* s, const char* z, double& v) {
   v = std::strtod(tmp, &end);
   return end == tmp + n;
 }
+// Decimal v followed by sep, appended to b.
+inline void put_decimal(uint64_t v, char sep, std::vector<char>& b) {
+  char tmp[24];
+  int k = 0;
+  do {
+    tmp[k++] = (char)('0' + v % 10);
+    v /= 10;
+  } while (v);
+  while (k) b.push_back(tmp[--k]);
+  b.push_back(sep);
+}
+
+// Writes items [0, n) to f, item i formatted by put(i, buffer), on every
+// thread in slices written in order. False on a short write.
+template <typename F>
+inline bool write_items(FILE* f, size_t n, size_t bytes_each, F put) {
+  const int nt = n < (1u << 16) ? 1 : std::max(1, omp_get_max_threads());
+  const size_t per = (n + (size_t)nt * 8 - 1) / ((size_t)nt * 8) + 1;  // slices of at most this many
+  bool ok = true;
+  // rounds of nt slices, so the buffers stay a few MB per thread
+  for (size_t r0 = 0; r0 < n && ok; r0 += per * nt) {
+    std::vector<std::vector<char>> part(nt);
+#pragma omp parallel for num_threads(nt) schedule(static, 1)
+    for (int t = 0; t < nt; ++t) {
+      const size_t a = std::min(n, r0 + per * t), z = std::min(n, a + per);
+      part[t].reserve((z - a) * bytes_each);
+      for (size_t i = a; i < z; ++i) put(i, part[t]);
+    }
+    for (auto& b : part)
+      if (!b.empty() && std::fwrite(b.data(), 1, b.size(), f) != b.size()) ok = false;
+  }
+  return ok;
+}
+
 }  // namespace chsga
