@@ -196,6 +196,28 @@ def ncu_traffic():
         return None
 
 
+def host_threads():
+    """Host threads this process may run on (its CPU affinity)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_harness(oracle, files):
+    """The reference's own code (oracle/_ref) or, without it, the oracle, on
+    every host thread of this process (set explicitly: a launcher such as
+    torchrun sets OMP_NUM_THREADS=1); returns (harness, kind, threads used)."""
+    n = host_threads()
+    if oracle.ref_available():
+        h, kind = oracle.RefHarness(files, threads=n), "reference"
+        used = h.lib.ref_set_threads(0)
+    else:
+        h, kind = oracle.Oracle(files, threads=n), "port"
+        used = h.lib.oracle_set_threads(0)
+    return h, kind, int(used)
+
+
 def cpu_baseline(g, reads, budget_s):
     """The reference's own align_combo (oracle/_ref) on the host cores, on a
     bounded sample of the workload's reads (shortest first, until about
@@ -206,11 +228,7 @@ def cpu_baseline(g, reads, budget_s):
     N = st["num_chars"]
     with tempfile.TemporaryDirectory() as d:
         files = g.write_files(os.path.join(d, "g"))
-        if oracle.ref_available():
-            h, kind = oracle.RefHarness(files), "reference"
-        else:
-            h, kind = oracle.Oracle(files), "port"
-        cores = os.cpu_count()
+        h, kind, cores = cpu_harness(oracle, files)
         sample = sorted(reads, key=len)
         # calibrate on one short read, then size the sample to the budget
         t = time.time()
@@ -319,9 +337,7 @@ def run_reference(args):
     import oracle
     with tempfile.TemporaryDirectory() as d:
         files = g.write_files(os.path.join(d, "g"))
-        kind = "reference" if oracle.ref_available() else "port"
-        h = oracle.RefHarness(files) if kind == "reference" else oracle.Oracle(files)
-        cores = os.cpu_count()
+        h, kind, cores = cpu_harness(oracle, files)
         # each step: the shortest reads of that step's batch until ~budget seconds
         budget = max(2.0, min(20.0, args.cpu_sample_s))
         t = time.time()
