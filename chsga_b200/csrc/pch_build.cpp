@@ -135,7 +135,7 @@ class PchBuilder {
 #pragma omp parallel num_threads(nthreads)
     scratch_[omp_get_thread_num()].init(n_);
     for (auto& s : scratch_)
-      if (s.dist.size() != n_) s.init(n_);
+      if (s.hkey.empty()) s.init(n_);
     uint32_t round = 0;
     while (!remaining.empty()) {
       ++round;
@@ -287,25 +287,78 @@ class PchBuilder {
   }
 
  private:
+  // Tentative distances of one search: a small open-addressing table
+  // (entries of earlier searches told apart by a generation stamp) that
+  // stays in cache, moved to arrays over all vertices when a search
+  // outgrows it (allocated on the first such search).
   struct Scratch {
+    static constexpr uint32_t kBits = 10, kCap = 1u << kBits, kMaxFill = 3 * kCap / 4;
+    uint64_t n = 0;
+    std::vector<uint32_t> hkey, hgen;
+    std::vector<uint64_t> hdist;
+    uint32_t gen = 0, fill = 0;
+    bool big = false;  // this search lives in the arrays
     std::vector<uint64_t> dist;
     std::vector<uint32_t> stamp;
     uint32_t cur = 0;
-    std::vector<uint32_t> touched;
-    void init(uint64_t n) {
-      dist.assign(n, kInf);
-      stamp.assign(n, 0);
+    void init(uint64_t nv) {
+      n = nv;
+      hkey.assign(kCap, 0);
+      hgen.assign(kCap, 0);
+      hdist.assign(kCap, kInf);
     }
     void reset() {
+      if (++gen == 0) {
+        std::fill(hgen.begin(), hgen.end(), 0);
+        gen = 1;
+      }
+      fill = 0;
+      big = false;
+    }
+    uint32_t slot(uint32_t v) const {
+      uint32_t h = (v * 0x9E3779B1u) >> (32 - kBits);
+      while (hgen[h] == gen && hkey[h] != v) h = (h + 1) & (kCap - 1);
+      return h;
+    }
+    uint64_t get(uint32_t v) const {
+      if (big) return stamp[v] == cur ? dist[v] : kInf;
+      const uint32_t h = slot(v);
+      return hgen[h] == gen ? hdist[h] : kInf;
+    }
+    void set(uint32_t v, uint64_t d) {
+      if (!big) {
+        const uint32_t h = slot(v);
+        if (hgen[h] == gen) {
+          hdist[h] = d;
+          return;
+        }
+        if (fill < kMaxFill) {
+          hgen[h] = gen;
+          hkey[h] = v;
+          hdist[h] = d;
+          ++fill;
+          return;
+        }
+        spill();
+      }
+      stamp[v] = cur;
+      dist[v] = d;
+    }
+    void spill() {
+      if (dist.empty()) {
+        dist.assign(n, kInf);
+        stamp.assign(n, 0);
+      }
       if (++cur == 0) {
         std::fill(stamp.begin(), stamp.end(), 0);
         cur = 1;
       }
-    }
-    uint64_t get(uint32_t v) const { return stamp[v] == cur ? dist[v] : kInf; }
-    void set(uint32_t v, uint64_t d) {
-      stamp[v] = cur;
-      dist[v] = d;
+      for (uint32_t h = 0; h < kCap; ++h)
+        if (hgen[h] == gen) {
+          stamp[hkey[h]] = cur;
+          dist[hkey[h]] = hdist[h];
+        }
+      big = true;
     }
   };
 
