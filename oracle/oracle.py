@@ -214,3 +214,31 @@ def rescore(ops: np.ndarray, read: bytes, labels: bytes, match_n: bool = False) 
         else:
             score += 1
     return score, read_pos
+
+def char_edges(files) -> set:
+    """(u, v) pairs of the char graph read from the .char.adj file (files[0])."""
+    toks = open(files[0]).read().split()
+    n, m = int(toks[1]), int(toks[2])
+    off = np.append(np.array(toks[3:3 + n], dtype=np.int64), m)
+    tgt = np.array(toks[3 + n:3 + n + m], dtype=np.int64)
+    return {(u, int(v)) for u in range(n) for v in tgt[off[u]:off[u + 1]]}
+
+
+def check_path(ops: np.ndarray, edges: set) -> list:
+    """Structure of a traceback path (ops in path order, rows ascending), as
+    the reference's walks build it (traceback.hpp:483-586, 945-1011): it
+    starts on row 0; a MATCHSUB step moves one row down along a char edge,
+    a DELETE step one row down on the same char, an INSERT step along a char
+    edge within the row. Returns the offending (previous, step) pairs."""
+    ops = [tuple(int(x) for x in op) for op in ops]
+    bad = [] if ops and ops[0][0] == 0 else [(None, ops[0] if ops else None)]
+    for (pr, pv, _), (r, v, o) in zip(ops[:-1], ops[1:]):
+        if o == 1:
+            ok = r == pr + 1 and (pv, v) in edges
+        elif o == 0:
+            ok = r == pr + 1 and v == pv
+        else:
+            ok = r == pr and (pv, v) in edges
+        if not ok:
+            bad.append(((pr, pv), (r, v, o)))
+    return bad

@@ -76,12 +76,14 @@ def test_traceback_full_matrix(small_graph, ctx_small, oracle_small):
     g, files, reads = small_graph
     labels = open(files[3], "rb").read().replace(b"\n", b"")
     want = oracle_small.scores(reads[:6])
+    edges = orc.char_edges(files)
     for rd, w in zip(reads[:6], want):
         ops, score, ck = ctx_small.align_traceback(rd)
         assert not ck
         assert score == w
         ps, last = orc.rescore(ops, rd, labels)
         assert ps == w and last == len(rd) - 1
+        assert orc.check_path(ops, edges) == []  # every step follows the char graph
 
 
 def test_traceback_checkpointed(small_graph, ctx_small, oracle_small, tmp_path):
@@ -96,6 +98,7 @@ def test_traceback_checkpointed(small_graph, ctx_small, oracle_small, tmp_path):
     assert ck and score == want
     ps, last = orc.rescore(ops, rd, labels)
     assert ps == want and last == len(rd) - 1
+    assert orc.check_path(ops, orc.char_edges(files)) == []
     rows = oracle_small.rows(rd)
     for i in range(0, len(rd), 40):
         got = np.fromfile(str(tmp_path / "ck" / f"row_{i}.bin"), dtype=np.int32)

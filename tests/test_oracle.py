@@ -101,11 +101,22 @@ def test_traceback_paths_rescore(tmp_path):
     labels = open(files[3], "rb").read()
     o, fast, slow = orc.Oracle(files), orc.RefHarness(files), orc.RefHarness(files, True)
     want = o.scores(reads)
+    edges = orc.char_edges(files)
+    kinds = set()
     for i, rd in enumerate(reads):
         for ops in (fast.traceback(rd), slow.traceback(rd, k=25, ckpt_dir=str(tmp_path / f"c{i}")),
                     o.traceback(rd)[0], o.traceback(rd, k=25, fast_cap_bytes=0,
                                                     ckpt_dir=str(tmp_path / f"o{i}"))[0]):
             assert orc.rescore(ops, rd, labels) == (want[i], len(rd) - 1)
+            # every step follows the graph: the reference's paths and the oracle's
+            assert orc.check_path(ops, edges) == []
+            kinds |= {int(op) for op in ops[:, 2]}
+    assert kinds == {0, 1, 2}
+    # a path with one step off the graph is caught
+    ops = o.traceback(reads[0])[0].copy()
+    j = int(np.nonzero(ops[:, 2] == 1)[0][-1])
+    ops[j, 1] = (ops[j, 1] + 7) % len(labels.replace(b"\n", b""))
+    assert orc.check_path(ops, edges) != []
 
 
 @needs_ref
