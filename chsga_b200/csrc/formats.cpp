@@ -3,6 +3,7 @@
 #include <zlib.h>
 
 #include <algorithm>
+#include <array>
 #include <cctype>
 #include <cerrno>
 #include <cmath>
@@ -288,21 +289,40 @@ HostReads read_reads(const std::string& path, uint64_t max_reads) {
   gzFile fp = gzopen(path.c_str(), "r");
   require(fp != nullptr, CHSGA_ERR_IO, "Cannot open reads file: " + path);
   std::vector<char> buf;
-  {
-    char tmp[1 << 16];
+  if (gzdirect(fp) == 0 || gzeof(fp)) {
+    // gzip input (or an empty file): decompress in 1 MB pieces
+    gzbuffer(fp, 1 << 20);
+    size_t used = 0;
+    buf.resize(1 << 20);
     int got;
-    while ((got = gzread(fp, tmp, sizeof(tmp))) > 0) buf.insert(buf.end(), tmp, tmp + got);
+    while ((got = gzread(fp, buf.data() + used, (unsigned)(buf.size() - used))) > 0) {
+      used += (size_t)got;
+      if (used == buf.size()) buf.resize(buf.size() * 2);
+    }
+    buf.resize(used);
     gzclose(fp);
+  } else {
+    // plain text, which gzread would pass through unchanged
+    gzclose(fp);
+    buf = slurp(path);
   }
+  // std::toupper in a program that sets no locale (the reference's): a..z
+  // only, whatever locale the host process runs in
+  static const auto upper = [] {
+    std::array<char, 256> t{};
+    for (int c = 0; c < 256; ++c) t[c] = (char)(c >= 'a' && c <= 'z' ? c - 'a' + 'A' : c);
+    return t;
+  }();
   HostReads r;
+  if (max_reads == 0) r.data.reserve(buf.size());
   size_t i = 0, n = buf.size();
   auto line_end = [&](size_t s) {
-    while (s < n && buf[s] != '\n') ++s;
-    return s;
+    if (s >= n) return n;
+    const void* q = std::memchr(buf.data() + s, '\n', n - s);
+    return q ? (size_t)(static_cast<const char*>(q) - buf.data()) : n;
   };
   auto strip_cr = [&](size_t s, size_t e) { return (e > s && buf[e - 1] == '\r') ? e - 1 : e; };
   int last_char = 0;  // header char already consumed
-  std::string seq;
   while (true) {
     if (last_char == 0) {
       while (i < n && buf[i] != '>' && buf[i] != '@') ++i;
@@ -312,7 +332,8 @@ HostReads read_reads(const std::string& path, uint64_t max_reads) {
     // header line (name + comment)
     i = line_end(i);
     if (i < n) ++i;
-    seq.clear();
+    // the sequence lines, appended to the reads' bytes
+    const size_t start = r.data.size();
     int c = -1;
     while (i < n) {
       c = (unsigned char)buf[i++];
@@ -321,11 +342,12 @@ HostReads read_reads(const std::string& path, uint64_t max_reads) {
         c = -1;
         continue;
       }
-      size_t s = i - 1, e = line_end(i);
-      seq.append(buf.data() + s, strip_cr(s, e) - s);
+      size_t s0 = i - 1, e = line_end(i);
+      r.data.insert(r.data.end(), buf.data() + s0, buf.data() + strip_cr(s0, e));
       i = (e < n) ? e + 1 : e;
       c = -1;
     }
+    const size_t slen = r.data.size() - start;
     if (c == '>' || c == '@') {
       last_char = c;
     } else {
@@ -333,19 +355,25 @@ HostReads read_reads(const std::string& path, uint64_t max_reads) {
     }
     if (c == '+') {
       i = line_end(i);
-      if (i >= n) break;  // no quality string: kseq reports an error
+      if (i >= n) {  // no quality string: kseq reports an error
+        r.data.resize(start);
+        break;
+      }
       ++i;
       size_t ql = 0;
-      while (i < n && ql < seq.size()) {
+      while (i < n && ql < slen) {
         size_t e = line_end(i);
         ql += strip_cr(i, e) - i;
         i = (e < n) ? e + 1 : e;
       }
-      if (ql != seq.size()) break;  // quality length mismatch ends the input
+      if (ql != slen) {  // quality length mismatch ends the input
+        r.data.resize(start);
+        break;
+      }
       last_char = 0;
     }
-    for (char& ch : seq) ch = (char)std::toupper((unsigned char)ch);
-    r.add(seq.data(), seq.size());
+    for (size_t k = start; k < r.data.size(); ++k) r.data[k] = upper[(unsigned char)r.data[k]];
+    r.offsets.push_back(r.data.size());
     if (max_reads != 0 && r.count() >= max_reads) break;
     if (c != '>' && c != '@' && c != '+' && i >= n) break;
   }
