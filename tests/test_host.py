@@ -266,3 +266,25 @@ def test_large_adjacency_file_errors(tmp_path):
     h = read_with(first_weight + 5, "2")
     w = np.ctypeslib.as_array(h.view().char_graph.weight, (m,))
     assert w[5] == 2 and (np.delete(w, 5) == 1).all()
+
+
+def test_packed_u16_relaxation_is_exact():
+    """The packed sweep kernels (k_pull_lv16, k_down16) relax 16-bit scores
+    as min(f, sat16(x + min(w, 65535))) and derive a last score as
+    min(raw, sat16(f + min(len - 1, 65535))). For 16-bit f, x, raw and
+    weights in [1, 2^30] that equals the int form (x + w < f ? x + w : f;
+    min(raw, f + len - 1)), including scores at 65535 and sums past it."""
+    rng = np.random.default_rng(9)
+    n = 200_000
+    edge = np.array([0, 1, 65533, 65534, 65535], dtype=np.int64)
+    f = np.concatenate([rng.integers(0, 65536, n), np.repeat(edge, 5)])
+    x = np.concatenate([rng.integers(0, 65536, n), np.tile(edge, 5)])
+    w = np.concatenate([rng.integers(1, 1 << 30, n // 2), rng.integers(1, 70000, n - n // 2),
+                        np.full(25, 1)])
+    sat = lambda a: np.minimum(a, 65535)
+    packed = np.minimum(f, sat(x + np.minimum(w, 65535)))
+    exact = np.where(x + w < f, x + w, f)
+    np.testing.assert_array_equal(packed, exact)
+    raw, ln = x, rng.integers(1, 1 << 29, f.size)
+    np.testing.assert_array_equal(np.minimum(raw, sat(f + np.minimum(ln - 1, 65535))),
+                                  np.minimum(raw, f + ln - 1))
