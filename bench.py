@@ -61,7 +61,7 @@ def parse():
     p.add_argument("--backbone", type=int, default=0,
                    help="backbone length of the config-2-mix graph (0 = 5 Mbp); for small profiling captures")
     p.add_argument("--scale-cfg4", action="store_true",
-                   help="config-3 scale run instead of the contract line: the 100 Mbp graph, "
+                   help="config-4 run instead of the contract line: the 100 Mbp graph, "
                         "checkpointed tracebacks (-k 500) and batched score-only GCUPS")
     p.add_argument("--traceback-cfg1", action="store_true",
                    help="config-1 run instead of the contract line: tracebacks of 2,000 x 150 bp and "
@@ -72,6 +72,8 @@ def parse():
                    help="time the batched steps only (no server, served run, plain sample, profiled "
                         "pass or CPU baseline): the command profiling captures run under ncu")
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
+    p.add_argument("--plain-reads", type=int, default=64,
+                   help="reads of the first timed batch (drawn at random) run through the plain path")
     return p.parse_args()
 
 
@@ -221,7 +223,8 @@ def cpu_harness(oracle, files):
 def cpu_baseline(g, reads, budget_s):
     """The reference's own align_combo (oracle/_ref) on the host cores, on a
     bounded sample of the workload's reads (shortest first, until about
-    budget_s seconds of CPU work)."""
+    budget_s seconds of CPU work). Returns the baseline record, the indices
+    of the sampled reads in `reads` and the reference's scores for them."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     st = g.stats()
@@ -229,25 +232,30 @@ def cpu_baseline(g, reads, budget_s):
     with tempfile.TemporaryDirectory() as d:
         files = g.write_files(os.path.join(d, "g"))
         h, kind, cores = cpu_harness(oracle, files)
-        sample = sorted(reads, key=len)
+        order = sorted(range(len(reads)), key=lambda i: len(reads[i]))
         # calibrate on one short read, then size the sample to the budget
         t = time.time()
-        h.scores([sample[0]])
-        per_cell = (time.time() - t) / (len(sample[0]) * N)
+        h.scores([reads[order[0]]])
+        per_cell = (time.time() - t) / (len(reads[order[0]]) * N)
         picked, est = [], 0.0
-        for r in sample:
-            c = per_cell * len(r) * N
+        for i in order:
+            c = per_cell * len(reads[i]) * N
             if picked and est + c > budget_s:
                 break
-            picked.append(r)
+            picked.append(i)
             est += c
         t = time.time()
-        h.scores(picked)
+        ref_scores = h.scores([reads[i] for i in picked])
         dt = time.time() - t
-    cells = sum(len(r) for r in picked) * N
-    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": cores, "kind": kind,
-            "sample": f"{len(picked)} reads ({sum(len(r) for r in picked)} bases) of the workload, "
-                      f"shortest first, {dt:.1f} s on {cores} host threads"}
+    bases = sum(len(reads[i]) for i in picked)
+    cells = bases * N
+    what = ("reference code (src/align.hpp align_combo, compiled unchanged) on a project-written "
+            "OpenMP stand-in for parlaylib's scheduler" if kind == "reference" else
+            "the CPU restatement of align_combo (oracle), OpenMP")
+    info = {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": cores, "kind": kind, "what": what,
+            "sample": f"{len(picked)} reads ({bases} bases) of the first timed batch, shortest first, "
+                      f"{dt:.1f} s on {cores} host threads"}
+    return info, picked, ref_scores
 
 
 def served_mix(g, n, seed):
@@ -371,8 +379,11 @@ def run_reference(args):
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "num_chars": N, "batch": "bounded CPU sample per step"},
         "cpu_baseline": {"value": v, "unit": "GCUPS", "cores": cores, "kind": kind,
-                         "sample": f"per step the shortest reads of a 64-read batch up to "
-                                   f"~{budget:.0f} s of CPU work, {cores} host threads"},
+                         "what": ("reference code (src/align.hpp align_combo, compiled unchanged) on a "
+                                  "project-written OpenMP stand-in for parlaylib's scheduler"
+                                  if kind == "reference" else "the CPU restatement of align_combo"),
+                         "sample": f"per step the shortest reads of a 64-read batch (shortest first) "
+                                   f"up to ~{budget:.0f} s of CPU work, {cores} host threads"},
         "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -485,6 +496,72 @@ def ctypes_labels(g):
     return ctypes.string_at(v.labels, v.num_chars)
 
 
+def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits):
+    """A profiled pass (CUDA events around every kernel group of every
+    row-step) with R slots; the row kernel's achieved bandwidth against the
+    algorithmic bytes of one launch, and the sweep kernels' per row-step.
+    R = 1 is the plain one-read-per-launch path (align_scores)."""
+    pctx = cb.Context(device, flags=cb.FLAG_PROFILE)
+    pctx.load(g)
+    if R == 1:
+        sample = make_reads(g, 2, 77_001, len_max=1000)
+        pctx.align_scores(sample)
+    else:
+        sample = make_reads(g, R, 77_777, len_max=1000)
+        pctx.align_scores_batched(sample, **dict(opts, slots=R), row_bits=row_bits)
+    pr = pctx.profile()
+    pctx.close()
+    w = pr["row_bits"] // 8
+    row_avg_s = pr["row_ms"] / max(1, pr["row_launches"]) / 1e3
+    ab = algorithmic_row_bytes(st, R, multi, w)
+    auto16 = "k_row_stream" if R >= 64 else ("k_row_dpx" if R >= 2 else "k_row_direct")
+    kname = {cb.ROW_DIRECT: "k_row_direct", cb.ROW_TILED: "k_row_tiled", cb.ROW_DPX: "k_row_dpx",
+             cb.ROW_STREAM: "k_row_stream"}.get(
+        opts["row_kernel"] if R > 1 else 0, auto16 if pr["row_bits"] == 16 else "k_row_direct")
+    if pr["row_bits"] == 32 and kname in ("k_row_stream", "k_row_dpx"):
+        kname = "k_row_direct"  # the 16-bit kernels do not run 32-bit rows
+    tr = ncu_traffic() if (R > 1 and pr["row_bits"] == 16) else None
+    total = pr["row_ms"] + pr["sweep_up_ms"] + pr["top_ms"] + pr["sweep_down_ms"] + pr["other_ms"]
+    # working set of one row-step: two score rows, BV and FL, graph arrays
+    S = st["num_strings"]
+    work = 2 * w * st["num_chars"] * R + 2 * 2 * w * S * R + 3 * st["num_chars"] / 8 + 40 * S
+    out = {
+        "bound": "hbm", "kernel": f"{kname}<{R}>", "row_bits": int(pr["row_bits"]),
+        "achieved": ab / row_avg_s / 1e9, "peak": peak, "unit": "GB/s",
+        "frac": ab / row_avg_s / 1e9 / peak,
+        "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback 6.65 TB/s",
+        "algorithmic_bytes_per_launch": ab, "avg_launch_ms": row_avg_s * 1e3,
+        "traffic": tr.get("bytes_per_launch_scaled") if tr else None,
+        "traffic_source": tr.get("source") if tr else None,
+        "l2_resident": bool(work < 126e6), "working_set_bytes": work,
+        "row_step_ms": total / max(1, pr["row_launches"]),
+        "kernel_share": {k: pr[k] / total for k in
+                         ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")},
+        "per_row_step_us": {k.replace("_ms", ""): 1e3 * pr[k] / max(1, pr["row_launches"]) for k in
+                            ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")},
+    }
+    # sweep kernels below the top region (the top region the run used)
+    lay = g.check_layout(R, pr["row_bits"], opts["top_vertices"] if R > 1 else 0)
+    up_b, down_b = algorithmic_sweep_bytes(st, lay, R, w)
+    up_s = pr["sweep_up_ms"] / max(1, pr["row_launches"]) / 1e3
+    down_s = pr["sweep_down_ms"] / max(1, pr["row_launches"]) / 1e3
+    # 16-bit rows with R >= 8 run the packed forms of both sweeps
+    packed = pr["row_bits"] == 16 and R >= 8
+    out["sweeps"] = {
+        "k_pull_lv16" if packed else "k_pull_lv": {
+            "algorithmic_bytes_per_step": up_b, "avg_step_ms": up_s * 1e3,
+            "achieved": up_b / up_s / 1e9 if up_s else None,
+            "frac": up_b / up_s / 1e9 / peak if up_s else None},
+        "k_down16" if packed else "k_down": {
+            "algorithmic_bytes_per_step": down_b, "avg_step_ms": down_s * 1e3,
+            "achieved": down_b / down_s / 1e9 if down_s else None,
+            "frac": down_b / down_s / 1e9 / peak if down_s else None},
+        "top_region": "levels >= %d (%d vertices) run in k_top, latency-bound" % (
+            lay["top_first_level"], lay["top_vertices"]),
+    }
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -547,8 +624,9 @@ def main():
     clocks.start()
     dev_ms, lat, launches, steps_work = 0.0, [], 0, 0
     t0 = time.perf_counter()
+    batched_scores = []
     for b in batches:
-        ctx.align_scores_batched(b, **opts)
+        batched_scores.append(ctx.align_scores_batched(b, **opts))
         p = ctx.profile()
         dev_ms += p["total_ms"]
         launches += int(p["launches"])
@@ -564,13 +642,14 @@ def main():
                         order=cb.ORDER_LONGEST)
         barrier()
         t1 = time.perf_counter()
-        for b in batches:
-            for r in b:
-                srv.submit(r)
-        got = 0
-        while got < len(batches) * args.batch:
-            got += len(srv.poll(4096, 100))
+        tickets = [[srv.submit(r) for r in b] for b in batches]
+        served_res = {}
+        while len(served_res) < len(batches) * args.batch:
+            for d in srv.poll(4096, 100):
+                served_res[d["ticket"]] = d
         srv_wall = time.perf_counter() - t1
+        served_bad = sum(int(served_res[t]["status"] != cb.OK or served_res[t]["score"] != w)
+                         for tk, ws_ in zip(tickets, batched_scores) for t, w in zip(tk, ws_))
         sst = srv.stats()
         srv.close()
     barrier()
@@ -584,6 +663,9 @@ def main():
         "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "row_storage": "uint16 rows with u16x2 DPX arithmetic: int32 results exactly, since every "
+                       "row-i value is at most i + 1 (reads of at most 65000 bases; longer reads "
+                       "run int32 rows)",
         "config": {"workload": WORKLOAD, "num_chars": N, "num_strings": st["num_strings"],
                    "hierarchy_levels": st["pch_levels"], "batch_reads": args.batch,
                    "engine": opts, "parallelism": f"replicas x{ws}",
@@ -603,63 +685,36 @@ def main():
     if args.kernels_only:
         line["e2e"]["what"] = "kernels-only run: wall time of the batched calls"
     if rank == 0 and not args.kernels_only:
-        # plain one-read-per-launch path on a sample of the first batch
-        sample = sorted(batches[0], key=len)[: max(2, min(6, len(batches[0])))]
-        ctx.align_scores(sample)
+        # plain one-read-per-launch path on a random sample of the first
+        # timed batch: its GCUPS, and its scores against the batched ones
+        import random
+        idx = sorted(random.Random(5).sample(range(len(batches[0])),
+                                             min(args.plain_reads, len(batches[0]))))
+        sample = [batches[0][i] for i in idx]
+        plain_scores = ctx.align_scores(sample)
         pp = ctx.profile()
         pc = sum(len(r) for r in sample) * N
+        plain_bad = int(np.sum(plain_scores != batched_scores[0][idx]))
         line["plain"] = {"value": pc / (pp["total_ms"] / 1e3) / 1e9, "unit": "GCUPS",
-                         "sample": f"{len(sample)} shortest reads of the first batch"}
+                         "sample": f"{len(sample)} reads drawn at random (seed 5) from the first timed "
+                                   f"batch, {sum(len(r) for r in sample)} bases, device time"}
         line["batched_over_plain"] = value / line["plain"]["value"]
         line["served_over_plain"] = e2e / line["plain"]["value"]
+        line["mismatches"] = {"batched_vs_plain": plain_bad, "batched_vs_plain_reads": len(sample),
+                              "served_vs_batched": served_bad,
+                              "served_vs_batched_reads": len(batches) * args.batch}
         line["served"] = served_run(cb, ctx, g, N, opts, e2e, args.served_s)
     if rank == 0 and not args.no_profile and not args.kernels_only:
-        # profiled pass: CUDA events around every kernel group of every row-step
-        pctx = cb.Context(local, flags=cb.FLAG_PROFILE)
-        pctx.load(g)
-        R = opts["slots"]
-        sample = make_reads(g, R, 77_777, len_max=1000)
-        pctx.align_scores_batched(sample, **opts)
-        pr = pctx.profile()
-        pctx.close()
-        row_avg_s = pr["row_ms"] / max(1, pr["row_launches"]) / 1e3
         peak, src = measured_peak()
-        ab = algorithmic_row_bytes(st, R, multi, pr["row_bits"] // 8)
-        auto16 = "k_row_stream" if R >= 64 else "k_row_dpx"
-        kname = {cb.ROW_DIRECT: "k_row_direct", cb.ROW_TILED: "k_row_tiled", cb.ROW_DPX: "k_row_dpx",
-                 cb.ROW_STREAM: "k_row_stream"}.get(
-            opts["row_kernel"], auto16 if pr["row_bits"] == 16 else "k_row_direct")
-        tr = ncu_traffic()
-        total = pr["row_ms"] + pr["sweep_up_ms"] + pr["top_ms"] + pr["sweep_down_ms"] + pr["other_ms"]
-        line["roofline"] = {
-            "bound": "hbm", "kernel": f"{kname}<{R}>", "row_bits": int(pr["row_bits"]),
-            "achieved": ab / row_avg_s / 1e9, "peak": peak, "unit": "GB/s",
-            "frac": ab / row_avg_s / 1e9 / peak, "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)"
-            if src == "measured" else "fallback 6.65 TB/s",
-            "algorithmic_bytes_per_launch": ab, "avg_launch_ms": row_avg_s * 1e3,
-            "traffic": tr.get("bytes_per_launch_scaled") if tr else None,
-            "traffic_source": tr.get("source") if tr else None,
-            "kernel_share": {k: pr[k] / total for k in
-                             ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")},
-        }
-        # sweep kernels below the top region (default top region of the layout)
-        lay = g.check_layout(R, 16, opts["top_vertices"])
-        up_b, down_b = algorithmic_sweep_bytes(st, lay, R, pr["row_bits"] // 8)
-        up_s = pr["sweep_up_ms"] / max(1, pr["row_launches"]) / 1e3
-        down_s = pr["sweep_down_ms"] / max(1, pr["row_launches"]) / 1e3
-        # 16-bit rows with R >= 8 run the packed forms of both sweeps
-        packed = pr["row_bits"] == 16 and R >= 8
-        line["roofline"]["sweeps"] = {
-            "k_pull_lv16" if packed else "k_pull_lv": {
-                "algorithmic_bytes_per_step": up_b, "avg_step_ms": up_s * 1e3,
-                "achieved": up_b / up_s / 1e9, "frac": up_b / up_s / 1e9 / peak},
-            "k_down16" if packed else "k_down": {
-                "algorithmic_bytes_per_step": down_b, "avg_step_ms": down_s * 1e3,
-                "achieved": down_b / down_s / 1e9, "frac": down_b / down_s / 1e9 / peak},
-            "top_region": "levels >= %d (%d vertices) run in k_top, latency-bound" % (
-                lay["top_first_level"], lay["top_vertices"]),
-        }
-        line["cpu_baseline"] = cpu_baseline(g, batches[0], args.cpu_sample_s)
+        R = opts["slots"]
+        line["roofline"] = profiled_roofline(cb, g, st, multi, local, R, opts, peak, src, 0)
+        line["roofline_plain"] = profiled_roofline(cb, g, st, multi, local, 1, opts, peak, src, 0)
+        line["roofline_int32_rows"] = profiled_roofline(cb, g, st, multi, local, R, opts, peak, src, 32)
+        cb_info, picked, ref_scores = cpu_baseline(g, batches[0], args.cpu_sample_s)
+        line["cpu_baseline"] = cb_info
+        line.setdefault("mismatches", {})
+        line["mismatches"]["vs_reference"] = int(np.sum(batched_scores[0][picked] != ref_scores))
+        line["mismatches"]["vs_reference_reads"] = len(picked)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -1314,6 +1314,10 @@ void noalloc_row_step(chsga_ctx& c, const NoallocBufs& b, const uint16_t* D, uin
   check_launch();
 }
 
+void scores_noalloc_enqueue(chsga_ctx& c, const NoallocBufs& b, const char* const* reads,
+                            const uint32_t* lens, uint32_t n, uint64_t total, uint32_t m,
+                            int32_t* out);
+
 void scores_noalloc(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n,
                     int32_t* out) {
   require(c.device >= 0 && c.device < kNoallocMaxDevices, CHSGA_ERR_UNSUPPORTED,
@@ -1362,6 +1366,20 @@ void scores_noalloc(chsga_ctx& c, const char* const* reads, const uint32_t* lens
   b.res_t0 = reinterpret_cast<unsigned long long*>(base + l.res_t0);
   b.res_t1 = reinterpret_cast<unsigned long long*>(base + l.res_t1);
   b.out = reinterpret_cast<int32_t*>(base + l.out);
+  const cudaStream_t s = c.st;
+  // the lock must not be released while work on the shared array is still
+  // queued: any failure after the first enqueue waits for the stream first
+  try {
+    scores_noalloc_enqueue(c, b, reads, lens, n, total, m, out);
+  } catch (...) {
+    cudaStreamSynchronize(s);
+    throw;
+  }
+}
+
+void scores_noalloc_enqueue(chsga_ctx& c, const NoallocBufs& b, const char* const* reads,
+                            const uint32_t* lens, uint32_t n, uint64_t total, uint32_t m,
+                            int32_t* out) {
   const cudaStream_t s = c.st;
   // copies from pageable caller memory: each returns once its source is read
   CK(cudaMemcpyAsync(b.lens, lens, (size_t)n * 4, cudaMemcpyHostToDevice, s));

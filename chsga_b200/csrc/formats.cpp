@@ -289,9 +289,15 @@ HostReads read_reads(const std::string& path, uint64_t max_reads) {
   gzFile fp = gzopen(path.c_str(), "r");
   require(fp != nullptr, CHSGA_ERR_IO, "Cannot open reads file: " + path);
   std::vector<char> buf;
+  // zlib sizes its buffers when gzdirect first looks at the input, so the
+  // 1 MB decompression buffer is requested before that (a later gzbuffer
+  // call is refused)
+  if (gzbuffer(fp, 1 << 20) != 0) {
+    gzclose(fp);
+    require(false, CHSGA_ERR_IO, "Cannot set the read buffer for: " + path);
+  }
   if (gzdirect(fp) == 0 || gzeof(fp)) {
     // gzip input (or an empty file): decompress in 1 MB pieces
-    gzbuffer(fp, 1 << 20);
     size_t used = 0;
     buf.resize(1 << 20);
     int got;

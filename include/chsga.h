@@ -307,7 +307,10 @@ chsga_status chsga_align_scores_batched(chsga_ctx* ctx, const char* const* reads
  * - The CUDA driver reserves the array on each GPU where it loads the
  *   library's device code, and the GPU keeps it until the process exits.
  * - The first call on a device looks up the array's device address, so
- *   make that first call before any stream capture starts.
+ *   make that first call before any stream capture starts. The library
+ *   keeps that address for the life of the process: resetting the device
+ *   (cudaDeviceReset, or tearing down its primary context) after the first
+ *   call is not supported.
  * - The call fails with CHSGA_ERR_OOM, and runs nothing, when the graph and
  *   the reads need more than the array holds. The need is about
  *   4 N + 8 S + (read bytes) + 52 n bytes, where N = chars and S = string

@@ -29,7 +29,8 @@ REF_CONSGA_TB = os.path.join(HERE, "_ref", "ConSGA_traceback_mismatchN_dag")
 REF_CONSGA_MATCHN = os.path.join(HERE, "_ref", "ConSGA_matchN_dag")
 REF_CONSGA_TB_MATCHN = os.path.join(HERE, "_ref", "ConSGA_traceback_matchN_dag")
 REF_CSR_TO_ADJ = os.path.join(HERE, "_ref", "csr_to_adj")
-REFERENCE_TREE = "/root/reference"
+# the reference source tree (read only); CHSGA_REFERENCE overrides where it lies
+REFERENCE_TREE = os.environ.get("CHSGA_REFERENCE", "/root/reference")
 
 u64p = C.POINTER(C.c_uint64)
 i32p = C.POINTER(C.c_int32)
@@ -43,7 +44,7 @@ def build(with_ref: Optional[bool] = None) -> None:
         with_ref = os.path.isdir(os.path.join(REFERENCE_TREE, "src"))
     if with_ref:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, "-j8"] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "-j8", f"REF={REFERENCE_TREE}"] + targets, check=True)
 
 
 def ref_available(match_n: bool = False) -> bool:
