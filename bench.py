@@ -71,6 +71,10 @@ def parse():
     p.add_argument("--kernels-only", action="store_true",
                    help="time the batched steps only (no server, served run, plain sample, profiled "
                         "pass or CPU baseline): the command profiling captures run under ncu")
+    p.add_argument("--launch-compare", action="store_true",
+                   help="launch-mode comparison instead of the contract line: the same reads at 1, 8 "
+                        "and 128 slots as CUDA-graph chains and as persistent launches, device time, "
+                        "scores compared")
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
     p.add_argument("--plain-reads", type=int, default=64,
                    help="reads of the first timed batch (drawn at random) run through the plain path")
@@ -490,6 +494,59 @@ def run_traceback_cfg1(args):
     return 0
 
 
+def run_launch_compare(args):
+    """Device time of the same reads through the CUDA-graph chain of
+    row-step kernels and through the persistent row-step kernel, at 1, 8 and
+    128 slots, on the config-2-mix graph; the one-slot chain also with the
+    one-thread-per-vertex row kernel (the plain path's row kernel before the
+    tile kernel). Every run's scores must equal the first's. One JSON line."""
+    import numpy as np
+
+    import chsga_b200 as cb
+    g = make_graph(args.backbone)
+    N = g.stats()["num_chars"]
+    ctx = cb.Context(0).load(g)
+    out = {"mode": "launch-compare", "num_chars": N, "shapes": []}
+    shapes = [(1, make_reads(g, 4, 31_000, len_max=1000)),
+              (8, make_reads(g, 32, 31_001, len_max=2000)),
+              (128, make_reads(g, 256, 31_002, len_max=2000))]
+    for R, reads in shapes:
+        cells = sum(len(r) for r in reads) * N
+        runs = [("graphs", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16)),
+                ("persistent", dict(use_graphs=cb.LAUNCH_PERSISTENT, steps_per_graph=16)),
+                ("persistent_64", dict(use_graphs=cb.LAUNCH_PERSISTENT, steps_per_graph=64))]
+        if R == 1:
+            runs.append(("graphs_direct_row", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16,
+                                                   row_kernel=cb.ROW_DIRECT)))
+        rec = {"slots": R, "reads": len(reads), "bases": sum(len(r) for r in reads)}
+        ref = None
+        for name, kw in runs:
+            ctx.align_scores_batched(reads, slots=R, **kw)  # warm-up (graph build, caches)
+            best = None
+            for _ in range(3):
+                sc = ctx.align_scores_batched(reads, slots=R, **kw)
+                p = ctx.profile()
+                best = p["total_ms"] if best is None else min(best, p["total_ms"])
+            if ref is None:
+                ref = sc
+            rec[name] = {"device_ms": best, "gcups": cells / best / 1e6, "launch_mode": int(p["launch_mode"]),
+                         "ms_per_row_step": best / max(1, p["steps"]),
+                         "same_scores": bool(np.array_equal(sc, ref))}
+        out["shapes"].append(rec)
+    # per-kernel-group times at one slot (CUDA events between the groups)
+    pctx = cb.Context(0, flags=cb.FLAG_PROFILE).load(g)
+    for name, rk in (("tile_row", cb.ROW_AUTO), ("direct_row", cb.ROW_DIRECT)):
+        pctx.align_scores_batched(shapes[0][1][:2], slots=1, row_kernel=rk)
+        pr = pctx.profile()
+        st = max(1, pr["row_launches"])
+        out["plain_profile_" + name] = {k.replace("_ms", "_us"): 1e3 * pr[k] / st for k in
+                                        ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")}
+    pctx.close()
+    ctx.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def ctypes_labels(g):
     import ctypes
     v = g.view()
@@ -570,6 +627,8 @@ def main():
         return run_scale_cfg4(args)
     if args.traceback_cfg1:
         return run_traceback_cfg1(args)
+    if args.launch_compare:
+        return run_launch_compare(args)
     ws, rank, local = dist_env()
     if ws > 1:
         import torch

@@ -33,6 +33,7 @@ REQ_SCORE, REQ_TRACEBACK = 0, 1
 FP_PLAN, FP_MODEL, FP_ANALYTIC = 0, 1, 2
 ORDER_FIFO, ORDER_LONGEST = 0, 1
 ROW_AUTO, ROW_DIRECT, ROW_TILED, ROW_DPX, ROW_STREAM = 0, 1, 2, 3, 4
+LAUNCH_STREAM, LAUNCH_GRAPHS, LAUNCH_PERSISTENT = 0, 1, 2
 FLAG_PROFILE = 1
 FLAG_MATCH_N = 2
 NOALLOC_SCRATCH_BYTES = 32 << 20  # CHSGA_NOALLOC_SCRATCH_BYTES
@@ -140,7 +141,7 @@ class ProfileT(C.Structure):
                 ("sweep_down_ms", C.c_double), ("other_ms", C.c_double), ("total_ms", C.c_double),
                 ("row_bits", C.c_uint64), ("rows", C.c_uint64), ("steps", C.c_uint64),
                 ("launches", C.c_uint64),
-                ("row_launches", C.c_uint64)]
+                ("row_launches", C.c_uint64), ("launch_mode", C.c_uint64)]
 
 
 class ServerOpts(C.Structure):
@@ -224,6 +225,7 @@ _sig("chsga_ops_to_cigar", C.c_uint64, C.POINTER(OpT), C.c_uint64, C.c_char_p, C
 _sig("chsga_get_profile", C.c_int32, vp, C.POINTER(ProfileT))
 _sig("chsga_get_read_times", C.c_int32, vp, u64p, u64p, C.c_uint32)
 _sig("chsga_selftest_wait", C.c_int32, vp, C.c_uint32)
+_sig("chsga_selftest_grid_wait", C.c_int32, vp, C.c_uint32)
 f32p = C.POINTER(C.c_float)
 _sig("chsga_cm_create", C.c_int32, C.c_int, C.c_uint64, C.POINTER(vp))
 _sig("chsga_cm_free", None, vp)
@@ -445,8 +447,10 @@ class Context:
         return out
 
     def align_scores_batched(self, reads: Sequence[bytes], slots: int = 64, steps_per_graph: int = 8,
-                             use_graphs: bool = True, row_bits: int = 0, row_kernel: int = 0,
+                             use_graphs: int = LAUNCH_GRAPHS, row_bits: int = 0, row_kernel: int = 0,
                              top_vertices: int = 0) -> np.ndarray:
+        """chsga_align_scores_batched. use_graphs is the launch mode
+        (LAUNCH_STREAM, LAUNCH_GRAPHS or LAUNCH_PERSISTENT; True/False work as 1/0)."""
         arr, lens = _read_ptrs(reads)
         out = np.zeros(len(reads), dtype=np.int32)
         o = BatchOpts(slots, steps_per_graph, int(use_graphs), row_bits, row_kernel, top_vertices)
@@ -523,6 +527,11 @@ class Context:
         d = np.zeros(n, dtype=np.uint64)
         self._ck(_lib.chsga_get_read_times(self._h, a.ctypes.data_as(u64p), d.ctypes.data_as(u64p), n))
         return a, d
+
+    def selftest_grid_wait(self, limit_us: int = 2000) -> None:
+        """Runs the persistent kernel's grid barrier with one block that never
+        arrives (chsga_selftest_grid_wait): raises ChsgaError(ERR_TIMEOUT)."""
+        self._ck(_lib.chsga_selftest_grid_wait(self._h, limit_us))
 
     def selftest_wait(self, polls: int = 4096) -> None:
         """Runs a bounded device wait that cannot succeed (chsga_selftest_wait):

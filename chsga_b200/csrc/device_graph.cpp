@@ -462,6 +462,36 @@ void validate_row_tiles(const HostLayout& L, uint32_t R, uint32_t sz, const Host
   if (next_s != L.S) bad(t.ntiles(), "tiles do not reach the last vertex");
 }
 
+HostT1 build_t1(const HostLayout& L) {
+  HostT1 t;
+  const uint32_t N = L.N, S = L.S;
+  t.heads.assign((size_t)(N + 7) / 8 + 1, 0);
+  t.vrec.assign((size_t)4 * S, 0);
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s < (int64_t)S; ++s) {
+    const uint32_t f = L.sv_off[s], k0 = L.vin_off[s], k1 = L.vin_off[s + 1];
+    uint32_t* r = &t.vrec[4 * (size_t)s];
+    r[0] = f;
+    r[1] = L.sv_dev[s] | (k1 - k0 > 2 ? 0x80000000u : 0u);
+    r[2] = k1 > k0 ? L.vin_srcv[k0] : 0xFFFFFFFFu;
+    r[3] = k1 > k0 + 1 ? L.vin_srcv[k0 + 1] : 0xFFFFFFFFu;
+  }
+  // vertices start in increasing char order, so each head byte has one writer per bit
+  for (uint32_t s = 0; s < S; ++s) t.heads[L.sv_off[s] >> 3] |= (uint8_t)(1u << (L.sv_off[s] & 7));
+  uint32_t s = 0;
+  while (s < S) {
+    const uint32_t cb = L.sv_off[s];
+    uint32_t e = s;
+    while (e < S && e - s < kT1MaxVerts && ((L.sv_off[e + 1] - 1) >> 3) - (cb >> 3) + 1 <= kT1Chunks)
+      ++e;
+    if (e == s) return HostT1{};  // one vertex longer than a tile
+    t.desc.insert(t.desc.end(), {cb, L.sv_off[e], s, e});
+    s = e;
+  }
+  t.ok = true;
+  return t;
+}
+
 HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edges) {
   require(max_vertices < 32768 && chunk_edges >= 32 && chunk_edges % 32 == 0, CHSGA_ERR_INTERNAL,
           "top region limits");

@@ -113,6 +113,28 @@ HostRowTiles build_row_tiles(const HostLayout& L, uint32_t R, uint32_t score_byt
 // Checks every bound and alignment the kernel relies on; throws on violation.
 void validate_row_tiles(const HostLayout& L, uint32_t R, uint32_t score_bytes, const HostRowTiles& t);
 
+// Tiles of the one-read row kernel (k_row_t1, 16-bit rows): runs of whole
+// consecutive string vertices whose chars span at most kT1Chunks aligned
+// chunks of 8 chars and that hold at most kT1MaxVerts vertices; a warp
+// takes one tile, a lane one chunk.
+//   desc   4 words per tile: first char, end char, first vertex, end vertex
+//   heads  1 byte per chunk: bit i set when char 8q + i is the first char of
+//          its string vertex
+//   vrec   4 words per string vertex: first char, hierarchy position (bit 31
+//          set when the first char has more than two in-edges), source
+//          vertex of the first and of the second first-char in-edge
+//          (0xFFFFFFFF when absent)
+// ok is false when some vertex alone spans more than kT1Chunks chunks.
+constexpr uint32_t kT1Chunks = 32, kT1MaxVerts = 64;
+struct HostT1 {
+  bool ok = false;
+  std::vector<uint32_t> desc;
+  std::vector<uint8_t> heads;
+  std::vector<uint32_t> vrec;
+  uint32_t ntiles() const { return (uint32_t)(desc.size() / 4); }
+};
+HostT1 build_t1(const HostLayout& L);
+
 HostLayout build_layout(const chsga_graph_host& g);
 HostTop build_top(const HostLayout& L, uint32_t max_vertices, uint32_t chunk_edges);
 

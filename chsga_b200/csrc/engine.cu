@@ -18,6 +18,7 @@
 #include "engine_api.hpp"
 #include "host_graph.hpp"
 #include "kernels.cuh"
+#include "persist.cuh"
 
 namespace chsga {
 
@@ -94,6 +95,8 @@ struct GraphDev {
   DevArr<uint32_t> dv_s;
   DevArr<int2> up_in, dn_in;
   DevArr<uint4> dn_head, up_head, fin;
+  DevArr<uint4> t1_desc, t1_vrec;  // tiles of the one-read row kernel (k_row_t1)
+  DevArr<uint8_t> t1_heads;
 };
 
 struct TopDev {
@@ -114,6 +117,7 @@ struct SlotBufs {
   DevArr<uint32_t> word;
   DevArr<unsigned long long> best;
   DevArr<dev::StepCtl> ctl;
+  DevArr<dev::GridBar> bar;  // grid barrier of the persistent row-step kernel
 };
 
 // Row kernel choice: the DPX kernel for 16-bit rows (default), the direct
@@ -142,6 +146,7 @@ struct LoadedGraph {
   GraphDev gd;
   dev::GraphPtrs gp{};
   std::unique_ptr<TopDev> top;
+  dev::T1Ptrs t1{};  // ntiles = 0: some vertex is too long for k_row_t1
   size_t pitch = 0;  // traceback matrix row stride (elements), 16-byte aligned rows
   bool nul_label = false;
   bool n_label = false;  // some label byte is 'N'
@@ -163,6 +168,8 @@ struct chsga_ctx {
   const chsga::TopDev* top_sel = nullptr;  // this call's top region (nullptr: the default)
   int num_sms = 148;
   chsga::RowKernel row_kernel = chsga::RowKernel::Auto;
+  // launch mode of the one-read path (chsga_align_scores): CHSGA_LAUNCH_*
+  uint32_t plain_mode = CHSGA_LAUNCH_PERSISTENT;
   chsga::DevArr<unsigned char> reads;
   chsga::DevArr<chsga::dev::ReadDesc> queue;
   uint32_t qmask = 0xFFFFFFFFu;                      // queue ring mask (serving), else linear
@@ -227,6 +234,7 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
   b->word.alloc(R);
   b->best.alloc(R);
   b->ctl.alloc(1);
+  b->bar.alloc(1);
   // the large dynamic shared memory of these kernels, once per device
   once_per_device((const void*)dev::k_top<R, ST>, c.device, [] {
     CK(cudaFuncSetAttribute(dev::k_top<R, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -317,6 +325,7 @@ void reset_slots(chsga_ctx& c, SlotBufs& b, uint32_t q_count) {
   dev::StepCtl ctl{};
   ctl.q_count = q_count;
   CK(cudaMemcpyAsync(b.ctl.p, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, c.st));
+  CK(cudaMemsetAsync(b.bar.p, 0, sizeof(dev::GridBar), c.st));
   CK(cudaStreamSynchronize(c.st));  // host copies above are from stack memory
 }
 
@@ -419,6 +428,14 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   if (ev) CK(cudaEventRecord(ev->e[0], s));
   ST* FL = reinterpret_cast<ST*>(b.FL.p);
   bool done = false;
+  if constexpr (std::is_same_v<ST, uint16_t> && R == 1) {
+    // one read: a warp per tile of whole vertices, a lane per 8 chars
+    if (c.g->t1.ntiles && c.row_kernel == RowKernel::Auto) {
+      dev::k_row_t1<DEFER><<<(c.g->t1.ntiles + dev::kT1Warps - 1) / dev::kT1Warps, dev::kT1Warps * 32, 0,
+                             s>>>(c.g->gp, c.g->t1, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+      done = true;
+    }
+  }
   if constexpr (std::is_same_v<ST, uint16_t> && R >= 2) {
     // packed 16-bit DPX kernels; exact while F + (c - first) stays below 2^16
     if (L.max_len <= 512 && c.row_kernel != RowKernel::Tiled && c.row_kernel != RowKernel::Direct) {
@@ -508,19 +525,110 @@ uint32_t kernels_per_step(const chsga_ctx& c) {
   return k;
 }
 
-// Runs every queued read to completion through R slots. Steps are captured
-// in CUDA graphs of `per_graph` row-steps (even, so the two row buffers
-// alternate identically in every launch).
+constexpr uint32_t kLaunchStream = CHSGA_LAUNCH_STREAM, kLaunchGraphs = CHSGA_LAUNCH_GRAPHS,
+                   kLaunchPersistent = CHSGA_LAUNCH_PERSISTENT;
+
+// Grid of the persistent row-step kernel (k_persist) for this context's
+// configuration, 0 when it does not apply: 32-bit rows, a row kernel other
+// than AUTO, string vertices too long for its row phase, more levels below
+// the top region than its argument block holds, or fewer resident blocks
+// than slots (block r sweeps slot r's top region).
 template <int R, typename ST>
-void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, uint32_t per_graph) {
+uint32_t persist_grid(chsga_ctx& c) {
+  if constexpr (!std::is_same_v<ST, uint16_t>) {
+    return 0;
+  } else {
+    const HostLayout& L = c.g->L;
+    const TopDev& top = cur_top(c);
+    if (c.row_kernel != RowKernel::Auto || top.h.first_level > (uint32_t)dev::kPersistMaxLevels) return 0;
+    if (R == 1 ? c.g->t1.ntiles == 0 : L.max_len > 512) return 0;
+    constexpr int TH = dev::PersistShape<R>::threads;
+    const size_t smem_max = dev::top_smem_bytes(kTopMaxVertices);
+    static_assert(dev::persist_row_smem<R>() <= dev::top_smem_bytes(kTopMaxVertices), "row phase smem");
+    once_per_device((const void*)dev::k_persist<R>, c.device, [&] {
+      CK(cudaFuncSetAttribute(dev::k_persist<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
+    });
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_persist<R>, TH, smem_max));
+    const uint32_t grid = (uint32_t)std::max(per_sm, 0) * (uint32_t)c.num_sms;
+    return grid >= (uint32_t)R ? grid : 0;
+  }
+}
+
+// One cooperative launch of k_persist: `steps` row-steps of every slot
+// (rows[0] holds the previous row at the first step; steps is even).
+template <int R>
+void launch_persist(chsga_ctx& c, SlotBufs& b, uint32_t grid, uint32_t steps, cudaStream_t s) {
+  const HostLayout& L = c.g->L;
+  const TopDev& top = cur_top(c);
+  dev::PersistArgs a{};
+  a.g = c.g->gp;
+  a.t1 = c.g->t1;
+  a.top = top.ptrs;
+  a.upg_off = top.upg_off.p;
+  a.upg = top.upg.p;
+  a.has_upg = top.h.upg.empty() ? 0u : 1u;
+  a.steps = steps;
+  a.rows[0] = reinterpret_cast<uint16_t*>(b.rows[0].p);
+  a.rows[1] = reinterpret_cast<uint16_t*>(b.rows[1].p);
+  a.BV = reinterpret_cast<uint16_t*>(b.BV.p);
+  a.FL = reinterpret_cast<uint16_t*>(b.FL.p);
+  a.word = b.word.p;
+  a.best = b.best.p;
+  a.ctl = b.ctl.p;
+  a.slots = b.slots.p;
+  a.queue = c.queue.p;
+  a.reads = c.reads.p;
+  a.res_score = c.res_score.p;
+  a.res_vertex = c.res_vertex.p;
+  a.res_t0 = c.res_t0.p;
+  a.res_t1 = c.res_t1.p;
+  a.done_ring = c.done_ring.p;
+  a.qmask = c.qmask;
+  a.special = L.special;
+  a.match_n = match_n(c);
+  a.bar = b.bar.p;
+  a.fl = top.h.first_level;
+  for (uint32_t l = 0; l <= a.fl; ++l) a.lvl_off[l] = L.lvl_off[l];
+  for (uint32_t l = 0; l < a.fl; ++l)
+    if (L.lvl_up_edges[l]) a.up_mask |= 1ull << l;
+  const size_t smem = std::max(dev::persist_row_smem<R>(), dev::top_smem_bytes(top.h.K, top.ptrs.chunk_cap));
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(dev::PersistShape<R>::threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, dev::k_persist<R>, a));
+}
+
+// Runs every queued read to completion through R slots, in blocks of
+// `per_graph` row-steps (even, so the two row buffers alternate identically
+// in every block). mode: kLaunchStream = every kernel launched from the
+// host; kLaunchGraphs = each block captured once as a CUDA graph and
+// replayed; kLaunchPersistent = each block one launch of the persistent
+// kernel (the CUDA-graph chain where that kernel does not apply).
+template <int R, typename ST>
+void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, uint32_t mode, uint32_t per_graph) {
   SlotBufs& b = get_bufs<R, ST>(c, true);
   if (c.row_kernel == RowKernel::Tiled) row_tiles<R, ST>(c);  // allocates: never inside a capture
   reset_slots<R>(c, b, n);
   const bool profile = (c.flags & CHSGA_FLAG_PROFILE) != 0;
-  if (profile) use_graphs = false;
+  if (profile) mode = kLaunchStream;
+  uint32_t pgrid = 0;
+  if (mode == kLaunchPersistent) {
+    pgrid = persist_grid<R, ST>(c);
+    if (!pgrid) mode = kLaunchGraphs;
+  }
+  bool use_graphs = mode == kLaunchGraphs;
   std::unique_ptr<StepEvents> sev;
   if (profile) sev = std::make_unique<StepEvents>();
   c.prof = chsga_profile{};
+  c.prof.launch_mode = mode;
   per_graph = std::max<uint32_t>(2, per_graph + (per_graph & 1));
   c.h_ctl.alloc(1);
   cudaEvent_t ev[2];
@@ -550,7 +658,9 @@ void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, u
   CK(cudaEventRecord(t_start, c.st));
   launch_advance<R>(c, b, 0, c.st);  // admit the first reads
   auto launch_block = [&]() {
-    if (use_graphs) {
+    if (mode == kLaunchPersistent) {
+      if constexpr (std::is_same_v<ST, uint16_t>) launch_persist<R>(c, b, pgrid, per_graph, c.st);
+    } else if (use_graphs) {
       CK(cudaGraphLaunch(exec, c.st));
     } else if (profile) {
       for (uint32_t i = 0; i < per_graph; ++i) {
@@ -604,7 +714,8 @@ void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, bool use_graphs, u
   c.prof.rows = total_rows;
   c.prof.steps = fin.steps;
   // every kernel launched, the early-exit ones of steps after the last read included
-  c.prof.launches = 1 + (uint64_t)kernels_per_step(c) * launched * per_graph;
+  c.prof.launches = mode == kLaunchPersistent ? 1 + launched
+                                              : 1 + (uint64_t)kernels_per_step(c) * launched * per_graph;
   c.prof.row_launches = profile ? fin.steps : launched * per_graph;
 }
 
@@ -643,6 +754,16 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   d.up_head.upload(to4(L.up_head), s);
   d.fin.upload(to4(L.fin), s);
   auto top = make_top(L, d, kTopMaxVertices, s);
+  {
+    HostT1 t1 = build_t1(L);
+    if (t1.ok) {
+      d.t1_desc.upload(to4(t1.desc), s);
+      d.t1_vrec.upload(to4(t1.vrec), s);
+      d.t1_heads.upload(t1.heads, s);
+      lg->t1 = dev::T1Ptrs{d.t1_desc.p, d.t1_heads.p, d.t1_vrec.p, t1.ntiles()};
+    }
+    CK(cudaStreamSynchronize(s));  // the host vectors die with this scope
+  }
   lg->gp = dev::GraphPtrs{L.N,          L.S,          L.special,    d.lab2.p,     d.lab_sp.p,
                           d.lab4.p,     d.sv_off.p,   d.sv_dev.p,   d.vin_off.p,  d.vin_src.p,
                           d.vin_srcv.p, d.dv_first.p, d.dv_len.p,   d.dv_s.p,     d.up_off.p,
@@ -666,7 +787,7 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
 
 template <int R>
 void scores_with(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n,
-                 int32_t* out, bool graphs, uint32_t per_graph, uint32_t row_bits) {
+                 int32_t* out, uint32_t mode, uint32_t per_graph, uint32_t row_bits) {
   // length-0 reads never reach the device: the reference scores row 0
   // against read[0] == '\0', i.e. 1 unless a label byte is 0
   std::vector<const char*> rp;
@@ -693,9 +814,9 @@ void scores_with(chsga_ctx& c, const char* const* reads, const uint32_t* lens, u
   require(!(row_bits == 16 && max_len > kRow16Max), CHSGA_ERR_INVALID_ARG,
           "16-bit rows need reads of at most 65000 bases");
   if (narrow) {
-    run_queue<R, uint16_t>(c, (uint32_t)rp.size(), rows, graphs, per_graph);
+    run_queue<R, uint16_t>(c, (uint32_t)rp.size(), rows, mode, per_graph);
   } else {
-    run_queue<R, int>(c, (uint32_t)rp.size(), rows, graphs, per_graph);
+    run_queue<R, int>(c, (uint32_t)rp.size(), rows, mode, per_graph);
   }
   c.prof.row_bits = narrow ? 16 : 32;
   std::vector<int32_t> res(rp.size());
@@ -1433,7 +1554,8 @@ struct CallKnobs {
 void scores_batched(chsga_ctx& c, const char* const* reads, const uint32_t* lens, uint32_t n,
                     const chsga_batch_opts* o, int32_t* out) {
   const uint32_t slots = o && o->slots ? o->slots : 64;
-  const bool graphs = o ? o->use_graphs != 0 : true;
+  const uint32_t graphs = o ? o->use_graphs : kLaunchGraphs;
+  require(graphs <= kLaunchPersistent, CHSGA_ERR_INVALID_ARG, "use_graphs must be CHSGA_LAUNCH_*");
   const uint32_t per = o && o->steps_per_graph ? o->steps_per_graph : 8;
   const uint32_t rb = o ? o->row_bits : 0;
   require(rb == 0 || rb == 16 || rb == 32, CHSGA_ERR_INVALID_ARG, "row_bits must be 0, 16 or 32");
@@ -1744,6 +1866,7 @@ chsga_ctx* fork_context(chsga_ctx& p) {
   c->cap = p.cap;
   c->num_sms = p.num_sms;
   c->row_kernel = p.row_kernel;
+  c->plain_mode = p.plain_mode;
   CK(cudaSetDevice(c->device));
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
@@ -1843,6 +1966,13 @@ chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out) {
       if (std::string(rk) == "dpx") c->row_kernel = RowKernel::Dpx;
       if (std::string(rk) == "stream") c->row_kernel = RowKernel::Stream;
     }
+    // CHSGA_PLAIN_LAUNCH=stream|graphs|persistent: how chsga_align_scores
+    // runs its row-steps (default persistent, where it applies)
+    if (const char* pl = std::getenv("CHSGA_PLAIN_LAUNCH")) {
+      if (std::string(pl) == "stream") c->plain_mode = CHSGA_LAUNCH_STREAM;
+      if (std::string(pl) == "graphs") c->plain_mode = CHSGA_LAUNCH_GRAPHS;
+      if (std::string(pl) == "persistent") c->plain_mode = CHSGA_LAUNCH_PERSISTENT;
+    }
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     size_t free_b = 0, total_b = 0;
@@ -1887,7 +2017,7 @@ chsga_status chsga_align_scores(chsga_ctx* c, const char* const* reads, const ui
   return guarded_ctx(c, [&] {
     require(c && (n == 0 || (reads && lens && scores_out)), CHSGA_ERR_INVALID_ARG, "null argument");
     require(c->loaded, CHSGA_ERR_INVALID_ARG, "no graph loaded");
-    scores_with<1>(*c, reads, lens, n, scores_out, true, 16,
+    scores_with<1>(*c, reads, lens, n, scores_out, c->plain_mode, 16,
                    (uint32_t)std::strtoul(std::getenv("CHSGA_ROW_BITS") ? std::getenv("CHSGA_ROW_BITS") : "0",
                                           nullptr, 10));
   });
@@ -2091,6 +2221,25 @@ chsga_status chsga_selftest_wait(chsga_ctx* c, uint32_t polls) {
     dev::k_wait_selftest<<<1, 32, 0, c->st>>>(b.ctl.p, polls);
     check_launch();
     check_device_error(*c, b);
+  });
+}
+
+chsga_status chsga_selftest_grid_wait(chsga_ctx* c, uint32_t limit_us) {
+  return guarded_ctx(c, [&] {
+    require(c != nullptr, CHSGA_ERR_INVALID_ARG, "null argument");
+    require(limit_us > 0 && limit_us <= 1000000, CHSGA_ERR_INVALID_ARG, "limit_us must be 1 .. 1000000");
+    SlotBufs b;
+    b.ctl.alloc(1);
+    b.bar.alloc(1);
+    CK(cudaMemsetAsync(b.ctl.p, 0, sizeof(dev::StepCtl), c->st));
+    CK(cudaMemsetAsync(b.bar.p, 0, sizeof(dev::GridBar), c->st));
+    dev::k_grid_selftest<<<2, 32, 0, c->st>>>(b.bar.p, b.ctl.p, (unsigned long long)limit_us * 1000ull);
+    check_launch();
+    dev::GridBar gb{};
+    CK(cudaMemcpyAsync(&gb, b.bar.p, sizeof(gb), cudaMemcpyDeviceToHost, c->st));
+    check_device_error(*c, b);  // throws CHSGA_ERR_TIMEOUT when the wait gave up
+    require(false, CHSGA_ERR_INTERNAL,
+            "the grid barrier wait did not give up (abort word " + std::to_string(gb.abort) + ")");
   });
 }
 

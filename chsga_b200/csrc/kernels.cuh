@@ -222,6 +222,16 @@ __device__ __forceinline__ void st(uint16_t* p, const IV<V>& x) {
   }
 }
 
+// Source loads of the sweep and row kernels: the read-only path (__ldg) when
+// the data was written by an earlier launch, plain loads inside the
+// persistent row-step kernel (COH), where other blocks of the same launch
+// wrote it before the last grid barrier.
+template <int V, bool COH, typename ST>
+__device__ __forceinline__ IV<V> ld_src(const ST* p) {
+  if constexpr (COH) return ld<V>(p);
+  else return ld_nc<V>(p);
+}
+
 // Label key of char c: 0..3 for A,C,G,T, 4 for the special byte.
 __device__ __forceinline__ uint32_t label_key(const GraphPtrs& g, uint32_t c) {
   const uint32_t code = (__ldg(g.lab2 + (c >> 4)) >> ((c & 15u) * 2u)) & 3u;
@@ -285,6 +295,10 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
 
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_inval(unsigned long long* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
 __device__ __forceinline__ void fence_async_shared() {
@@ -480,6 +494,23 @@ __device__ __forceinline__ U2<P> ldp_nc(const uint16_t* p) {
   return o;
 }
 
+template <int P, bool COH>
+__device__ __forceinline__ U2<P> ldp_src(const uint16_t* p) {
+  if constexpr (COH) {
+    U2<P> o;
+    if constexpr (P == 1) {
+      o.h[0] = *reinterpret_cast<const uint32_t*>(p);
+    } else {
+      const uint2 t = *reinterpret_cast<const uint2*>(p);
+      o.h[0] = t.x;
+      o.h[1] = t.y;
+    }
+    return o;
+  } else {
+    return ldp_nc<P>(p);
+  }
+}
+
 template <int P>
 __device__ __forceinline__ void stp(uint16_t* p, const U2<P>& x) {
   if constexpr (P == 1) {
@@ -521,7 +552,7 @@ struct KeyWindow {
 
 // The chain chars of one vertex (c = f+1 .. f+len-1); TRACK also keeps the
 // per-slot minimum and its smallest char for slots on their last row.
-template <int R, bool DEFER, bool TRACK, int P>
+template <int R, bool DEFER, bool TRACK, int P, bool COH = false>
 __device__ __forceinline__ void dpx_chain(const uint16_t* __restrict__ dp, uint16_t* __restrict__ tp,
                                           uint32_t len, uint32_t f, KeyWindow& kw, U2<P>& t,
                                           U2<P>& dprev, const U2<P>& F, bool any_fix,
@@ -536,7 +567,7 @@ __device__ __forceinline__ void dpx_chain(const uint16_t* __restrict__ dp, uint1
     U2<P> dq[DEPTH];
 #pragma unroll
     for (int k = 0; k < DEPTH; ++k)
-      if (k < (int)n) dq[k] = ldp_nc<P>(dp + (size_t)k * R);
+      if (k < (int)n) dq[k] = ldp_src<P, COH>(dp + (size_t)k * R);
 #pragma unroll
     for (int k = 0; k < DEPTH; ++k) {
       if (k < (int)n) {
@@ -575,27 +606,14 @@ __device__ __forceinline__ void dpx_chain(const uint16_t* __restrict__ dp, uint1
   }
 }
 
-template <int R, bool DEFER>
-__global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t* __restrict__ D,
-                                                    uint16_t* __restrict__ T,
-                                                    uint16_t* __restrict__ BV,
-                                                    const uint16_t* __restrict__ FL,
-                                                    const uint32_t* __restrict__ slot_word,
-                                                    unsigned long long* __restrict__ best,
-                                                    const StepCtl* __restrict__ ctl) {
-  constexpr int G = Pairs<R>::G, P = Pairs<R>::P;
+// The update of string vertex s for the lane's 2P slots (k_row_dpx's body).
+template <int R, bool DEFER, bool COH>
+__device__ __forceinline__ void dpx_vertex(const GraphPtrs& g, uint32_t s, int lane, const uint16_t* D,
+                                           uint16_t* T, uint16_t* BV, const uint16_t* FL,
+                                           const uint32_t* slot_word, unsigned long long* sm_best,
+                                           bool ending_any) {
+  constexpr int P = Pairs<R>::P;
   constexpr uint32_t ONES = 0x00010001u;
-  __shared__ unsigned long long sm_best[R];
-  const bool ending_any = ctl->any_ending != 0;
-  if (!ctl->any_active) return;
-  if (ending_any) {
-    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
-    __syncthreads();
-  }
-  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t s = (uint32_t)(gt / G);
-  const int lane = (int)(gt % G);
-  if (s < g.S) {
     const size_t so = (size_t)lane * 2 * P;  // first slot of this lane
     // per register pair: delta table over label keys (bit k of each half =
     // mismatch of key k), row-0 mask, deferred-propagation mask
@@ -606,7 +624,7 @@ __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t*
       dtab[p] = imask[p] = fmask[p] = 0;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const uint32_t w = __ldg(slot_word + so + 2 * p + h);
+        const uint32_t w = COH ? slot_word[so + 2 * p + h] : __ldg(slot_word + so + 2 * p + h);
         dtab[p] |= ((w >> SW_MASK_SHIFT) & SW_MASK) << (16 * h);
         if (w & SW_INIT) imask[p] |= 0xFFFFu << (16 * h);
         if (DEFER && (w & SW_FIX)) fmask[p] |= 0xFFFFu << (16 * h);
@@ -621,10 +639,10 @@ __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t*
     U2<P> F;
 #pragma unroll
     for (int p = 0; p < P; ++p) F.h[p] = 0;
-    if (DEFER && any_fix) F = ldp_nc<P>(FL + (size_t)(2 * s) * R + so);
+    if (DEFER && any_fix) F = ldp_src<P, COH>(FL + (size_t)(2 * s) * R + so);
     const uint16_t* dp = D + (size_t)f * R + so;
     uint16_t* tp = T + (size_t)f * R + so;
-    U2<P> dprev = ldp_nc<P>(dp);
+    U2<P> dprev = ldp_src<P, COH>(dp);
     U2<P> t;
     {
       const uint32_t key = kw.next();
@@ -637,7 +655,7 @@ __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t*
       }
       for (uint32_t k = k0; k < k1; ++k) {
         const uint32_t su = __ldg(g.vin_srcv + k);
-        const U2<P> du = ldp_nc<P>(FL + (size_t)(2 * su + 1) * R + so);
+        const U2<P> du = ldp_src<P, COH>(FL + (size_t)(2 * su + 1) * R + so);
 #pragma unroll
         for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(du.h[p], delta[p], t.h[p]);
       }
@@ -656,21 +674,41 @@ __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t*
     }
     const uint32_t len = e - f;
     if (ending_any && any_end) {
-      dpx_chain<R, DEFER, true, P>(dp + R, tp + R, len, f, kw, t, dprev, F, any_fix, dtab, imask,
+      dpx_chain<R, DEFER, true, P, COH>(dp + R, tp + R, len, f, kw, t, dprev, F, any_fix, dtab, imask,
                                    fmask, bmin, barg);
     } else {
-      dpx_chain<R, DEFER, false, P>(dp + R, tp + R, len, f, kw, t, dprev, F, any_fix, dtab, imask,
+      dpx_chain<R, DEFER, false, P, COH>(dp + R, tp + R, len, f, kw, t, dprev, F, any_fix, dtab, imask,
                                     fmask, bmin, barg);
     }
     if (len > 1) stp<P>(BV + (size_t)(2 * d + 1) * R + so, t);
     if (ending_any && any_end) {
 #pragma unroll
       for (int q = 0; q < 2 * P; ++q) {
-        const uint32_t w = __ldg(slot_word + so + q);
+        const uint32_t w = COH ? slot_word[so + q] : __ldg(slot_word + so + q);
         if (w & SW_ENDING) atomicMin(sm_best + so + q, pack_min(bmin[q], barg[q]));
       }
     }
   }
+
+template <int R, bool DEFER>
+__global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t* __restrict__ D,
+                                                    uint16_t* __restrict__ T,
+                                                    uint16_t* __restrict__ BV,
+                                                    const uint16_t* __restrict__ FL,
+                                                    const uint32_t* __restrict__ slot_word,
+                                                    unsigned long long* __restrict__ best,
+                                                    const StepCtl* __restrict__ ctl) {
+  constexpr int G = Pairs<R>::G;
+  __shared__ unsigned long long sm_best[R];
+  const bool ending_any = ctl->any_ending != 0;
+  if (!ctl->any_active) return;
+  if (ending_any) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
+    __syncthreads();
+  }
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t s = (uint32_t)(gt / G);
+  if (s < g.S) dpx_vertex<R, DEFER, false>(g, s, (int)(gt % G), D, T, BV, FL, slot_word, sm_best, ending_any);
   if (ending_any) flush_min<R>(sm_best, best);
 }
 
@@ -741,31 +779,22 @@ __device__ __forceinline__ U2<P> lds_u2(const uint16_t* p) {
   return o;
 }
 
-template <int R, bool DEFER>
-__global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_stream(
-    GraphPtrs g, const uint16_t* __restrict__ D, uint16_t* __restrict__ T, uint16_t* __restrict__ BV,
-    const uint16_t* __restrict__ FL, const uint32_t* __restrict__ slot_word,
-    unsigned long long* __restrict__ best, const StepCtl* __restrict__ ctl) {
-  static_assert(Pairs<R>::G == 32, "one full warp per vertex");
+// One warp's run of 32 string vertices starting at s0 = 32 * run_index (k_row_stream's
+// body); warp_ring = the warp's kStreamRing x R ring in shared memory.
+template <int R, bool DEFER, bool COH>
+__device__ __forceinline__ void stream_run(const GraphPtrs& g, uint32_t run_index, const uint16_t* D, uint16_t* T,
+                                           uint16_t* BV, const uint16_t* FL, const uint32_t* slot_word,
+                                           uint16_t* warp_ring, unsigned long long* sm_best,
+                                           bool ending_any) {
   constexpr int P = Pairs<R>::P;
   constexpr int W = kStreamRing;
   constexpr uint32_t ONES = 0x00010001u;
   constexpr unsigned FULL = 0xFFFFFFFFu;
-  extern __shared__ __align__(16) uint16_t ring_smem[];
-  __shared__ unsigned long long sm_best[R];
-  const bool ending_any = ctl->any_ending != 0;
-  if (!ctl->any_active) return;
-  if (ending_any) {
-    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
-    __syncthreads();
-  }
   const int lane = threadIdx.x & 31;
-  const uint32_t run = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
-  const uint32_t s0 = run * 32;
-  if (s0 < g.S) {
+  const uint32_t s0 = run_index * 32;
     const size_t so = (size_t)lane * 2 * P;
     // this lane's ring: row slot k at ring + k * R (the warp's 32 lanes side by side)
-    uint16_t* ring = ring_smem + (size_t)(threadIdx.x >> 5) * W * R + so;
+    uint16_t* ring = warp_ring + so;
     uint32_t dtab[P], imask[P], fmask[P];
     bool any_fix = false, any_end = false;
 #pragma unroll
@@ -773,7 +802,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
       dtab[p] = imask[p] = fmask[p] = 0;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const uint32_t w = __ldg(slot_word + so + 2 * p + h);
+        const uint32_t w = COH ? slot_word[so + 2 * p + h] : __ldg(slot_word + so + 2 * p + h);
         dtab[p] |= ((w >> SW_MASK_SHIFT) & SW_MASK) << (16 * h);
         if (w & SW_INIT) imask[p] |= 0xFFFFu << (16 * h);
         if (DEFER && (w & SW_FIX)) fmask[p] |= 0xFFFFu << (16 * h);
@@ -820,10 +849,10 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
       v.k1 = __shfl_sync(FULL, mk1, i);
 #pragma unroll
       for (int p = 0; p < P; ++p) v.F.h[p] = v.u[0].h[p] = v.u[1].h[p] = 0;
-      if (DEFER && any_fix) v.F = ldp_nc<P>(FL + (size_t)(2 * (s0 + i)) * R + so);
+      if (DEFER && any_fix) v.F = ldp_src<P, COH>(FL + (size_t)(2 * (s0 + i)) * R + so);
 #pragma unroll
       for (int j = 0; j < 2; ++j)
-        if (v.k0 + j < v.k1) v.u[j] = ldp_nc<P>(FL + (size_t)(2 * src_at(v.k0 + j) + 1) * R + so);
+        if (v.k0 + j < v.k1) v.u[j] = ldp_src<P, COH>(FL + (size_t)(2 * src_at(v.k0 + j) + 1) * R + so);
     };
     // The char stream cb .. ce-1: `slot` is the ring row of the current char
     // (its copy is the oldest of W pending groups), `gnext` the global row
@@ -896,7 +925,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
 #pragma unroll
               for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(cur.u[j].h[p], delta[p], t.h[p]);
           for (uint32_t k = cur.k0 + 2; k < cur.k1; ++k) {
-            const U2<P> du = ldp_nc<P>(FL + (size_t)(2 * src_at(k) + 1) * R + so);
+            const U2<P> du = ldp_src<P, COH>(FL + (size_t)(2 * src_at(k) + 1) * R + so);
 #pragma unroll
             for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(du.h[p], delta[p], t.h[p]);
           }
@@ -939,13 +968,270 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
     if (track) {
 #pragma unroll
       for (int q = 0; q < 2 * P; ++q) {
-        const uint32_t w = __ldg(slot_word + so + q);
+        const uint32_t w = COH ? slot_word[so + q] : __ldg(slot_word + so + q);
         if ((w & SW_ENDING) && bmin[q] != 0x7fffffff)
           atomicMin(sm_best + so + q, pack_min(bmin[q], barg[q]));
       }
     }
   }
+
+template <int R, bool DEFER>
+__global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_stream(
+    GraphPtrs g, const uint16_t* __restrict__ D, uint16_t* __restrict__ T, uint16_t* __restrict__ BV,
+    const uint16_t* __restrict__ FL, const uint32_t* __restrict__ slot_word,
+    unsigned long long* __restrict__ best, const StepCtl* __restrict__ ctl) {
+  static_assert(Pairs<R>::G == 32, "one full warp per vertex");
+  extern __shared__ __align__(16) uint16_t ring_smem[];
+  __shared__ unsigned long long sm_best[R];
+  const bool ending_any = ctl->any_ending != 0;
+  if (!ctl->any_active) return;
+  if (ending_any) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
+    __syncthreads();
+  }
+  const uint32_t run = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+  if (run * 32 < g.S)
+    stream_run<R, DEFER, false>(g, run, D, T, BV, FL, slot_word,
+                                ring_smem + (size_t)(threadIdx.x >> 5) * kStreamRing * R, sm_best,
+                                ending_any);
   if (ending_any) flush_min<R>(sm_best, best);
+}
+
+// ---------------------------------------------------------------------------
+// Loads of data that other blocks of the same launch may have written (the
+// persistent row-step kernel's rows, boundary scores and slot words): L2
+// only (ld.global.cg), never the read-only path, which assumes the data does
+// not change while the kernel runs. COH = false keeps __ldg for kernels that
+// only read what earlier launches wrote.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 ld_cg_v4(const void* p) {
+  uint4 r;
+  asm volatile("ld.global.cg.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(p));
+  return r;
+}
+__device__ __forceinline__ uint32_t ld_cg_u32(const void* p) {
+  uint32_t r;
+  asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(r) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ int ld_cg_u16(const void* p) {
+  unsigned short r;
+  asm volatile("ld.global.cg.u16 %0, [%1];" : "=h"(r) : "l"(p));
+  return (int)r;
+}
+template <bool COH>
+__device__ __forceinline__ uint4 ldv4(const void* p) {
+  if constexpr (COH) return ld_cg_v4(p);
+  else return __ldg(reinterpret_cast<const uint4*>(p));
+}
+template <bool COH>
+__device__ __forceinline__ uint32_t ldu32(const uint32_t* p) {
+  if constexpr (COH) return ld_cg_u32(p);
+  else return __ldg(p);
+}
+template <bool COH>
+__device__ __forceinline__ int ldu16(const uint16_t* p) {
+  if constexpr (COH) return ld_cg_u16(p);
+  else return (int)__ldg(reinterpret_cast<const unsigned short*>(p));
+}
+
+// ---------------------------------------------------------------------------
+// k_row_t1 (R = 1, 16-bit rows): the row update of one read, one warp per
+// tile of whole consecutive string vertices (at most 32 aligned chunks of 8
+// chars and 64 vertices, built on the host). Lane j owns chunk q0 + j: its 8
+// previous-row scores in one 16-byte load, its 8 label keys in one word and
+// its head bits (first chars of vertices) in one byte. Lanes v and v + 32
+// load vertex v's record (first char, hierarchy position, first in-edge
+// sources) and the previous row's final scores it needs; the warp keeps them
+// in shared memory.
+//
+// Within a vertex T[c] = min(X[c], T[c-1] + 1), with X[c] = min(D'[c] + 1,
+// D'[c-1] + delta) for a chain char and X[f] = min(D'[f] + 1, min over
+// in-edges of FL_last(u) + delta) for the first char, D' being the previous
+// row with its deferred propagation applied (as in k_row_direct). A lane
+// runs the recurrence over its 8 chars from no carry. The carry into lane j
+// is the composition of the earlier lanes' maps x -> min(a, x + b) (a = the
+// lane's last value, b = 8, or none when the lane holds a first char), a
+// min-plus scan in 5 shuffle steps; chars before the lane's first head then
+// take min(T, carry + distance). Row 0 takes delta only.
+// ---------------------------------------------------------------------------
+struct T1Ptrs {
+  const uint4* desc;     // per tile {first char, end char, first vertex, end vertex}
+  const uint8_t* heads;  // per 8-char chunk: bit i = char 8q + i starts a vertex
+  const uint4* vrec;     // per vertex {first char, position | many << 31, src0, src1}
+  uint32_t ntiles;
+};
+constexpr int kT1Warps = 8;       // warps per block of k_row_t1
+constexpr int kT1VertMax = 64;    // vertices per tile (kT1MaxVerts on the host)
+
+template <bool DEFER, bool COH>
+__device__ __forceinline__ void row_t1_tile(const GraphPtrs& g, const T1Ptrs& t, uint32_t tile,
+                                            const uint16_t* D, uint16_t* T, uint16_t* BV,
+                                            const uint16_t* FL, uint32_t w, int* s_G, int* s_X,
+                                            uint32_t* s_d, unsigned long long& mn) {
+  constexpr unsigned FULL = 0xFFFFFFFFu;
+  constexpr int BIG = 0x3fffffff;
+  const int lane = threadIdx.x & 31;
+  const uint4 td = __ldg(t.desc + tile);
+  const uint32_t cb = td.x, ce = td.y, sb = td.z, nv = td.w - td.z;
+  const uint32_t q = (cb >> 3) + lane;
+  const bool lv = q <= ((ce - 1) >> 3);
+  const bool init = (w & SW_INIT) != 0;
+  const bool fix = DEFER && (w & SW_FIX) != 0;
+  const bool ending = (w & SW_ENDING) != 0;
+  const uint32_t mask = (w >> SW_MASK_SHIFT) & SW_MASK;
+  uint4 dq = make_uint4(0, 0, 0, 0);
+  uint32_t keys = 0, hb = 0, inm = 0;
+  if (lv) {
+    dq = ldv4<COH>(D + 8 * (size_t)q);
+    keys = __ldg(g.lab4 + q);
+    hb = __ldg(t.heads + q);
+    const uint32_t c0 = 8 * q;
+    const uint32_t lo = cb > c0 ? cb - c0 : 0u;
+    const uint32_t hi = ce - c0 < 8u ? ce - c0 : 8u;
+    inm = (0xFFu >> (8u - hi)) & (0xFFu << lo) & 0xFFu;
+    hb &= inm;
+  }
+  for (uint32_t v = lane; v < nv; v += 32) {
+    const uint32_t sv = sb + v;
+    const uint4 r = __ldg(t.vrec + sv);
+    int G = 0, X = BIG;
+    if (fix) G = ldu16<COH>(FL + 2 * (size_t)sv) - (int)r.x;
+    if (!init) {
+      if (r.z != 0xFFFFFFFFu) X = ldu16<COH>(FL + 2 * (size_t)r.z + 1);
+      if (r.w != 0xFFFFFFFFu) X = min(X, ldu16<COH>(FL + 2 * (size_t)r.w + 1));
+      if (r.y & 0x80000000u) {
+        const uint32_t k1 = __ldg(g.vin_off + sv + 1);
+        for (uint32_t k = __ldg(g.vin_off + sv) + 2; k < k1; ++k)
+          X = min(X, ldu16<COH>(FL + 2 * (size_t)__ldg(g.vin_srcv + k) + 1));
+      }
+    }
+    s_G[v] = G;
+    s_X[v] = X;
+    s_d[v] = r.y & 0x7FFFFFFFu;
+  }
+  __syncwarp();
+  // vertex index (within the tile) of the char before this lane's first head
+  const int nh = __popc(hb);
+  int incl = nh;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int x = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += x;
+  }
+  const int vbase = incl - nh - 1;
+  // previous-row scores, the deferred propagation applied
+  int dp[8];
+  {
+    const uint32_t wv[4] = {dq.x, dq.y, dq.z, dq.w};
+    int vi = vbase;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      dp[i] = (int)((wv[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
+      vi += (hb >> i) & 1;
+      if (fix && ((inm >> i) & 1)) dp[i] = min(dp[i], s_G[vi] + (int)(8 * q + i));
+    }
+  }
+  const int dm1 = __shfl_up_sync(FULL, dp[7], 1);
+  int tl[8];
+  int first_head = 8;
+  {
+    int a = BIG, vi = vbase;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const bool head = (hb >> i) & 1;
+      vi += head;
+      const int delta = (int)((mask >> ((keys >> (4 * i)) & 0xFu)) & 1u);
+      int x;
+      if (init) {
+        x = delta;
+      } else {
+        x = dp[i] + 1;
+        if (head) {
+          x = min(x, s_X[vi] + delta);
+        } else {
+          x = min(x, (i ? dp[i - 1] : dm1) + delta);
+          x = min(x, a + 1);
+        }
+      }
+      if (head && first_head == 8) first_head = i;
+      a = x;
+      tl[i] = x;
+    }
+  }
+  // carry across lanes: inclusive min-plus scan of (last value, distance)
+  int A = tl[7], B = (hb || init) ? BIG : 8;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int Ap = __shfl_up_sync(FULL, A, o), Bp = __shfl_up_sync(FULL, B, o);
+    if (lane >= o) {
+      A = min(A, Ap + B);
+      B = min(BIG, Bp + B);
+    }
+  }
+  const int carry = __shfl_up_sync(FULL, A, 1);
+  if (!init && lane > 0) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      if (i < first_head) tl[i] = min(tl[i], carry + i + 1);
+  }
+  // final scores: the row, the vertex boundary scores, the last-row minimum
+  const uint32_t nb0 = (uint32_t)__shfl_down_sync(FULL, (int)hb, 1) & 1u;
+  if (inm) {
+    uint32_t ow[4] = {0, 0, 0, 0};
+    int vi = vbase;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const bool head = (hb >> i) & 1;
+      vi += head;
+      ow[i >> 1] |= ((uint32_t)tl[i] & 0xFFFFu) << (16 * (i & 1));
+      if ((inm >> i) & 1) {
+        const uint32_t c = 8 * q + i;
+        if (head) BV[2 * (size_t)s_d[vi]] = (uint16_t)tl[i];
+        const bool last = (c + 1 == ce) || (i < 7 ? ((hb >> (i + 1)) & 1u) != 0 : nb0 != 0);
+        if (last && !head) BV[2 * (size_t)s_d[vi] + 1] = (uint16_t)tl[i];
+        if (ending) mn = min(mn, pack_min(tl[i], c));
+        if (inm != 0xFFu) T[8 * (size_t)q + i] = (uint16_t)tl[i];
+      }
+    }
+    if (inm == 0xFFu)
+      *reinterpret_cast<uint4*>(T + 8 * (size_t)q) = make_uint4(ow[0], ow[1], ow[2], ow[3]);
+  }
+  __syncwarp();  // s_G / s_X / s_d are reused by the warp's next tile
+}
+
+template <bool DEFER>
+__global__ void __launch_bounds__(kT1Warps * 32) k_row_t1(GraphPtrs g, T1Ptrs t,
+                                                          const uint16_t* __restrict__ D,
+                                                          uint16_t* __restrict__ T,
+                                                          uint16_t* __restrict__ BV,
+                                                          const uint16_t* __restrict__ FL,
+                                                          const uint32_t* __restrict__ slot_word,
+                                                          unsigned long long* __restrict__ best,
+                                                          const StepCtl* __restrict__ ctl) {
+  __shared__ int s_G[kT1Warps][kT1VertMax], s_X[kT1Warps][kT1VertMax];
+  __shared__ uint32_t s_d[kT1Warps][kT1VertMax];
+  __shared__ unsigned long long sm_best[1];
+  if (!ctl->any_active) return;
+  const bool ending = ctl->any_ending != 0;
+  if (ending) {
+    if (threadIdx.x == 0) sm_best[0] = ~0ull;
+    __syncthreads();
+  }
+  const int wp = threadIdx.x >> 5;
+  const uint32_t tile = blockIdx.x * kT1Warps + wp;
+  unsigned long long mn = ~0ull;
+  if (tile < t.ntiles)
+    row_t1_tile<DEFER, false>(g, t, tile, D, T, BV, FL, __ldg(slot_word), s_G[wp], s_X[wp], s_d[wp],
+                              mn);
+  if (ending) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
+    if ((threadIdx.x & 31) == 0 && mn != ~0ull) atomicMin(sm_best, mn);
+    flush_min<1>(sm_best, best);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1226,17 +1512,10 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_row_tiled(GraphPtrs g, RowTi
 // over the list off[d-base]..off[d-base+1]. Every source lies on another
 // level, finished before this launch, so the gathers use the read-only path.
 // ---------------------------------------------------------------------------
-template <int R, typename ST>
-__global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, uint32_t hi,
-                                              const uint32_t* __restrict__ off,
-                                              const int2* __restrict__ edges, uint32_t base,
-                                              const StepCtl* __restrict__ ctl) {
-  constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
-  if (!ctl->any_active) return;
-  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t d = lo + (uint32_t)(gt / G);
-  const int lane = (int)(gt % G);
-  if (d >= hi) return;
+template <int R, typename ST, bool COH>
+__device__ __forceinline__ void pull_item(ST* BV, uint32_t d, int lane, const uint32_t* __restrict__ off,
+                                          const int2* __restrict__ edges, uint32_t base) {
+  constexpr int V = Lanes<R>::V;
   const size_t so = (size_t)lane * V;
   const uint32_t k0 = __ldg(off + (d - base)), k1 = __ldg(off + (d - base) + 1);
   if (k0 == k1) return;
@@ -1245,7 +1524,7 @@ __global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, 
   bool changed = false;
   for (uint32_t k = k0; k < k1; ++k) {
     const int2 ew = __ldg(edges + k);
-    const IV<V> x = ld_nc<V>(BV + (size_t)ew.x * R + so);
+    const IV<V> x = ld_src<V, COH>(BV + (size_t)ew.x * R + so);
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const int c = x.v[v] + ew.y;
@@ -1258,22 +1537,28 @@ __global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, 
   if (changed) st<V>(p, f);
 }
 
+template <int R, typename ST>
+__global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, uint32_t hi,
+                                              const uint32_t* __restrict__ off,
+                                              const int2* __restrict__ edges, uint32_t base,
+                                              const StepCtl* __restrict__ ctl) {
+  constexpr int G = Lanes<R>::G;
+  if (!ctl->any_active) return;
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  if (d >= hi) return;
+  pull_item<R, ST, false>(BV, d, (int)(gt % G), off, edges, base);
+}
+
 // ---------------------------------------------------------------------------
 // k_pull_lv: one upward level [lo, hi) below the top region, the k_pull
 // update with the list head of each position in two 16-byte loads (the
 // first two sources are gathered without waiting for an edge load).
 // ---------------------------------------------------------------------------
-template <int R, typename ST>
-__global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t lo, uint32_t hi,
-                                                 const uint4* __restrict__ head,
-                                                 const int2* __restrict__ edges,
-                                                 const StepCtl* __restrict__ ctl) {
-  constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
-  if (!ctl->any_active) return;
-  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t d = lo + (uint32_t)(gt / G);
-  const int lane = (int)(gt % G);
-  if (d >= hi) return;
+template <int R, typename ST, bool COH>
+__device__ __forceinline__ void pull_lv_item(ST* BV, uint32_t d, int lane, const uint4* __restrict__ head,
+                                             const int2* __restrict__ edges) {
+  constexpr int V = Lanes<R>::V;
   const uint4 h = __ldg(head + 2 * (size_t)d);
   if (h.x == h.y) return;
   const uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
@@ -1291,9 +1576,9 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
       }
     }
   };
-  const IV<V> x0 = ld_nc<V>(BV + (size_t)h.z * R + so);
+  const IV<V> x0 = ld_src<V, COH>(BV + (size_t)h.z * R + so);
   if (h.y - h.x > 1) {
-    const IV<V> x1 = ld_nc<V>(BV + (size_t)h2.x * R + so);
+    const IV<V> x1 = ld_src<V, COH>(BV + (size_t)h2.x * R + so);
     relax(x0, (int)h.w);
     relax(x1, (int)h2.y);
   } else {
@@ -1301,9 +1586,22 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
   }
   for (uint32_t k = h.x + 2; k < h.y; ++k) {
     const int2 ew = __ldg(edges + k);
-    relax(ld_nc<V>(BV + (size_t)ew.x * R + so), ew.y);
+    relax(ld_src<V, COH>(BV + (size_t)ew.x * R + so), ew.y);
   }
   if (changed) st<V>(p, f);
+}
+
+template <int R, typename ST>
+__global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t lo, uint32_t hi,
+                                                 const uint4* __restrict__ head,
+                                                 const int2* __restrict__ edges,
+                                                 const StepCtl* __restrict__ ctl) {
+  constexpr int G = Lanes<R>::G;
+  if (!ctl->any_active) return;
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  if (d >= hi) return;
+  pull_lv_item<R, ST, false>(BV, d, (int)(gt % G), head, edges);
 }
 
 // ---------------------------------------------------------------------------
@@ -1315,24 +1613,18 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
 // min, as in the int form. Edges beyond the two in the head are fetched four
 // at a time, their sources gathered together.
 // ---------------------------------------------------------------------------
-template <int R>
-__global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, uint32_t lo,
-                                                   uint32_t hi, const uint4* __restrict__ head,
-                                                   const int2* __restrict__ edges,
-                                                   const StepCtl* __restrict__ ctl) {
+template <int R, bool COH>
+__device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lane,
+                                               const uint4* __restrict__ head,
+                                               const int2* __restrict__ edges) {
   static_assert(R >= 8 && R % 8 == 0, "8 slots per lane");
-  constexpr int G = R / 8, B = 4;
-  if (!ctl->any_active) return;
-  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t d = lo + (uint32_t)(gt / G);
-  const int lane = (int)(gt % G);
-  if (d >= hi) return;
+  constexpr int B = 4;
   const uint4 h = __ldg(head + 2 * (size_t)d);
   const uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
   if (h.x == h.y) return;
   const size_t so = (size_t)lane * 8;
   uint4* p = reinterpret_cast<uint4*>(BV + (size_t)(2 * d) * R + so);
-  auto src = [&](uint32_t i) { return __ldg(reinterpret_cast<const uint4*>(BV + (size_t)i * R + so)); };
+  auto src = [&](uint32_t i) { return ldv4<COH>(BV + (size_t)i * R + so); };
   const uint4 f0 = *p;
   uint4 f = f0;
   auto relax = [&](const uint4& x, uint32_t w) {
@@ -1369,6 +1661,19 @@ __global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, ui
   if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
 }
 
+template <int R>
+__global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, uint32_t lo,
+                                                   uint32_t hi, const uint4* __restrict__ head,
+                                                   const int2* __restrict__ edges,
+                                                   const StepCtl* __restrict__ ctl) {
+  constexpr int G = R / 8;
+  if (!ctl->any_active) return;
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  if (d >= hi) return;
+  pull_lv16_item<R, false>(BV, d, (int)(gt % G), head, edges);
+}
+
 // ---------------------------------------------------------------------------
 // k_down: positions [lo, hi). Those below `mid` first pull their downward
 // in-edges (sources on higher levels, final); every position then finalises
@@ -1376,25 +1681,12 @@ __global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, ui
 // and propagate first + (p - first) forward while it improves
 // (align.hpp:381-396). Slots without closure (row 0, idle) are untouched.
 // ---------------------------------------------------------------------------
-template <int R, bool FIXUP, typename ST>
-__global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, ST* __restrict__ T,
-                                              ST* __restrict__ FL, uint32_t lo, uint32_t mid,
-                                              uint32_t hi,
-                                              const uint32_t* __restrict__ slot_word,
-                                              unsigned long long* __restrict__ best,
-                                              const StepCtl* __restrict__ ctl) {
-  constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
-  __shared__ unsigned long long sm_best[R];
-  const bool ending_any = ctl->any_ending != 0;
-  if (!ctl->any_active) return;
-  if (ending_any) {
-    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
-    __syncthreads();
-  }
-  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t d = lo + (uint32_t)(gt / G);
-  const int lane = (int)(gt % G);
-  if (d < hi) {
+template <int R, bool FIXUP, typename ST, bool COH>
+__device__ __forceinline__ void down_item(const GraphPtrs& g, ST* BV, ST* T, ST* FL, uint32_t d, int lane,
+                                          uint32_t mid, const uint32_t* slot_word,
+                                          unsigned long long* sm_best, bool ending_any) {
+  constexpr int V = Lanes<R>::V;
+  {
     const size_t so = (size_t)lane * V;
     ST* p = BV + (size_t)(2 * d) * R + so;
     // independent loads first: the list head, the vertex words, the first
@@ -1416,10 +1708,10 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
           }
         }
       };
-      relax(ld_nc<V>(BV + (size_t)h.z * R + so), (int)h.w);
+      relax(ld_src<V, COH>(BV + (size_t)h.z * R + so), (int)h.w);
       for (uint32_t k = h.x + 1; k < h.y; ++k) {
         const int2 ew = __ldg(g.dn_in + k);
-        relax(ld_nc<V>(BV + (size_t)ew.x * R + so), ew.y);
+        relax(ld_src<V, COH>(BV + (size_t)ew.x * R + so), ew.y);
       }
       if (changed) st<V>(p, f);
     }
@@ -1442,7 +1734,7 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
       if (ending_any) {
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-          const uint32_t w = __ldg(slot_word + so + v);
+          const uint32_t w = COH ? slot_word[so + v] : __ldg(slot_word + so + v);
           if ((w & SW_CLOSURE) && (w & SW_ENDING))
             atomicMin(sm_best + so + v, pack_min(f.v[v], first));
         }
@@ -1453,7 +1745,7 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
     bool any = false;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-      const uint32_t w = __ldg(slot_word + so + v);
+      const uint32_t w = COH ? slot_word[so + v] : __ldg(slot_word + so + v);
       act[v] = (w & SW_CLOSURE) && f.v[v] < tq.v[v];
       endg[v] = act[v] && (w & SW_ENDING);
       if (act[v]) {
@@ -1486,6 +1778,27 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
     }
     }
   }
+}
+
+template <int R, bool FIXUP, typename ST>
+__global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, ST* __restrict__ T,
+                                              ST* __restrict__ FL, uint32_t lo, uint32_t mid,
+                                              uint32_t hi,
+                                              const uint32_t* __restrict__ slot_word,
+                                              unsigned long long* __restrict__ best,
+                                              const StepCtl* __restrict__ ctl) {
+  constexpr int G = Lanes<R>::G;
+  __shared__ unsigned long long sm_best[R];
+  const bool ending_any = ctl->any_ending != 0;
+  if (!ctl->any_active) return;
+  if (ending_any) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
+    __syncthreads();
+  }
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  if (d < hi)
+    down_item<R, FIXUP, ST, false>(g, BV, T, FL, d, (int)(gt % G), mid, slot_word, sm_best, ending_any);
   if (ending_any) flush_min<R>(sm_best, best);
 }
 
@@ -1496,6 +1809,56 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
 // final first and last scores into FL and the first scores of slots on
 // their last row into the per-slot minimum.
 // ---------------------------------------------------------------------------
+template <int R, bool COH>
+__device__ __forceinline__ void down16_item(const GraphPtrs& g, uint16_t* BV, uint16_t* FL, uint32_t d,
+                                            int lane, uint32_t mid, const uint32_t* slot_word,
+                                            unsigned long long* sm_best, bool ending_any) {
+  static_assert(R >= 8 && R % 8 == 0, "8 slots per lane");
+  const size_t so = (size_t)lane * 8;
+  uint4* p = reinterpret_cast<uint4*>(BV + (size_t)(2 * d) * R + so);
+  auto src = [&](uint32_t i) { return ldv4<COH>(BV + (size_t)i * R + so); };
+  const uint4 h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
+  const uint4 m = __ldg(g.fin + d);
+  const uint4 f0 = *p;
+  const uint4 raw = *reinterpret_cast<const uint4*>(BV + (size_t)(2 * d + 1) * R + so);
+  uint4 f = f0;
+  auto relax = [&](const uint4& x, uint32_t w) {
+    const uint32_t ww = min(w, 0xFFFFu) * 0x10001u;
+    f.x = __vminu2(f.x, __vaddus2(x.x, ww));
+    f.y = __vminu2(f.y, __vaddus2(x.y, ww));
+    f.z = __vminu2(f.z, __vaddus2(x.z, ww));
+    f.w = __vminu2(f.w, __vaddus2(x.w, ww));
+  };
+  if (h.y > h.x) {
+    relax(src(h.z), h.w);
+    for (uint32_t k = h.x + 1; k < h.y; ++k) {
+      const int2 ew = __ldg(g.dn_in + k);
+      relax(src((uint32_t)ew.x), (uint32_t)ew.y);
+    }
+    if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
+  }
+  const uint32_t first = m.x, len = m.y, sv = m.z;
+  uint4 lf = f;
+  if (len > 1) {
+    const uint32_t ww = min(len - 1, 0xFFFFu) * 0x10001u;
+    lf.x = __vminu2(raw.x, __vaddus2(f.x, ww));
+    lf.y = __vminu2(raw.y, __vaddus2(f.y, ww));
+    lf.z = __vminu2(raw.z, __vaddus2(f.z, ww));
+    lf.w = __vminu2(raw.w, __vaddus2(f.w, ww));
+  }
+  *reinterpret_cast<uint4*>(FL + (size_t)(2 * sv) * R + so) = f;
+  *reinterpret_cast<uint4*>(FL + (size_t)(2 * sv + 1) * R + so) = lf;
+  if (ending_any) {
+    const uint32_t fw[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      const uint32_t w = COH ? slot_word[so + v] : __ldg(slot_word + so + v);
+      if ((w & SW_CLOSURE) && (w & SW_ENDING))
+        atomicMin(sm_best + so + v, pack_min((int)((fw[v >> 1] >> (16 * (v & 1))) & 0xFFFFu), first));
+    }
+  }
+}
+
 template <int R>
 __global__ void __launch_bounds__(256) k_down16(GraphPtrs g, uint16_t* __restrict__ BV,
                                                 uint16_t* __restrict__ FL, uint32_t lo,
@@ -1503,7 +1866,6 @@ __global__ void __launch_bounds__(256) k_down16(GraphPtrs g, uint16_t* __restric
                                                 const uint32_t* __restrict__ slot_word,
                                                 unsigned long long* __restrict__ best,
                                                 const StepCtl* __restrict__ ctl) {
-  static_assert(R >= 8 && R % 8 == 0, "8 slots per lane");
   constexpr int G = R / 8;
   __shared__ unsigned long long sm_best[R];
   const bool ending_any = ctl->any_ending != 0;
@@ -1514,54 +1876,7 @@ __global__ void __launch_bounds__(256) k_down16(GraphPtrs g, uint16_t* __restric
   }
   const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t d = lo + (uint32_t)(gt / G);
-  const int lane = (int)(gt % G);
-  if (d < hi) {
-    const size_t so = (size_t)lane * 8;
-    uint4* p = reinterpret_cast<uint4*>(BV + (size_t)(2 * d) * R + so);
-    auto src = [&](uint32_t i) {
-      return __ldg(reinterpret_cast<const uint4*>(BV + (size_t)i * R + so));
-    };
-    const uint4 h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
-    const uint4 m = __ldg(g.fin + d);
-    const uint4 f0 = *p;
-    const uint4 raw = *reinterpret_cast<const uint4*>(BV + (size_t)(2 * d + 1) * R + so);
-    uint4 f = f0;
-    auto relax = [&](const uint4& x, uint32_t w) {
-      const uint32_t ww = min(w, 0xFFFFu) * 0x10001u;
-      f.x = __vminu2(f.x, __vaddus2(x.x, ww));
-      f.y = __vminu2(f.y, __vaddus2(x.y, ww));
-      f.z = __vminu2(f.z, __vaddus2(x.z, ww));
-      f.w = __vminu2(f.w, __vaddus2(x.w, ww));
-    };
-    if (h.y > h.x) {
-      relax(src(h.z), h.w);
-      for (uint32_t k = h.x + 1; k < h.y; ++k) {
-        const int2 ew = __ldg(g.dn_in + k);
-        relax(src((uint32_t)ew.x), (uint32_t)ew.y);
-      }
-      if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
-    }
-    const uint32_t first = m.x, len = m.y, sv = m.z;
-    uint4 lf = f;
-    if (len > 1) {
-      const uint32_t ww = min(len - 1, 0xFFFFu) * 0x10001u;
-      lf.x = __vminu2(raw.x, __vaddus2(f.x, ww));
-      lf.y = __vminu2(raw.y, __vaddus2(f.y, ww));
-      lf.z = __vminu2(raw.z, __vaddus2(f.z, ww));
-      lf.w = __vminu2(raw.w, __vaddus2(f.w, ww));
-    }
-    *reinterpret_cast<uint4*>(FL + (size_t)(2 * sv) * R + so) = f;
-    *reinterpret_cast<uint4*>(FL + (size_t)(2 * sv + 1) * R + so) = lf;
-    if (ending_any) {
-      const uint32_t fw[4] = {f.x, f.y, f.z, f.w};
-#pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        const uint32_t w = __ldg(slot_word + so + v);
-        if ((w & SW_CLOSURE) && (w & SW_ENDING))
-          atomicMin(sm_best + so + v, pack_min((int)((fw[v >> 1] >> (16 * (v & 1))) & 0xFFFFu), first));
-      }
-    }
-  }
+  if (d < hi) down16_item<R, false>(g, BV, FL, d, (int)(gt % G), mid, slot_word, sm_best, ending_any);
   if (ending_any) flush_min<R>(sm_best, best);
 }
 
@@ -1607,17 +1922,19 @@ inline uint32_t top_chunk_for(uint32_t K, size_t smem_cap) {
   return c;
 }
 
+// The region's sweeps for slot r by the whole block (top_smem: the block's
+// dynamic shared memory, top_smem_bytes of the region). Returns false when a
+// bounded wait expired (StepCtl::error is set).
 template <int R, typename ST>
-__global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
-                                              const uint32_t* __restrict__ slot_word,
-                                              StepCtl* __restrict__ ctl) {
-  extern __shared__ __align__(16) unsigned char top_smem[];
-  if (!ctl->any_active) return;
-  const int r = blockIdx.x;
-  if (!(slot_word[r] & SW_CLOSURE)) return;
+__device__ __forceinline__ bool top_body(ST* BV, const TopPtrs& t, StepCtl* ctl, int r,
+                                         unsigned char* top_smem) {
   int* sm = reinterpret_cast<int*>(top_smem);  // [2j] first, [2j+1] last, [2K] scratch
   int2* ebuf = reinterpret_cast<int2*>(top_smem + ((size_t)(2 * t.K + 2) * 4 + 15) / 16 * 16);
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(ebuf + kTopBufs * t.chunk_cap);
+  // the buffers may hold what this block last wrote there through the
+  // generic proxy (another phase of the persistent kernel): order those
+  // writes before the bulk copies
+  fence_async_shared();
   if (threadIdx.x == 0) {
     for (uint32_t b = 0; b < kTopBufs; ++b) mbar_init(&bar[b], 1);
     fence_async_shared();
@@ -1705,9 +2022,25 @@ __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
         mbar_wait(&bar[k % kTopBufs], (k / kTopBufs) & 1);
     }
     __syncthreads();
-    return;
+    return false;
   }
   for (uint32_t j = threadIdx.x; j < t.K; j += blockDim.x) BV[(2 * (K0 + j)) * R + r] = (ST)sm[2 * j];
+  // every copy was waited for: the barriers' memory may serve other uses
+  if (threadIdx.x == 0)
+    for (uint32_t b = 0; b < kTopBufs; ++b) mbar_inval(&bar[b]);
+  __syncthreads();
+  return true;
+}
+
+template <int R, typename ST>
+__global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
+                                              const uint32_t* __restrict__ slot_word,
+                                              StepCtl* __restrict__ ctl) {
+  extern __shared__ __align__(16) unsigned char top_smem[];
+  if (!ctl->any_active) return;
+  const int r = blockIdx.x;
+  if (!(slot_word[r] & SW_CLOSURE)) return;
+  top_body<R, ST>(BV, t, ctl, r, top_smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -1786,20 +2119,16 @@ __global__ void k_fl_from_row(GraphPtrs g, const int* __restrict__ row, int* __r
 // refills while the engine runs, ids index the result arrays, and every
 // finished read is also appended to done_ring (entry ctl->done & qmask).
 // ---------------------------------------------------------------------------
+// The body runs on the first 128 threads of a block (R <= 128); the other
+// threads only take part in the block barriers.
 template <int R>
-__global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
-                                                 const ReadDesc* __restrict__ queue,
-                                                 const unsigned char* __restrict__ reads,
-                                                 unsigned long long* __restrict__ best,
-                                                 int32_t* __restrict__ res_score,
-                                                 uint32_t* __restrict__ res_vertex,
-                                                 unsigned long long* __restrict__ res_t0,
-                                                 unsigned long long* __restrict__ res_t1,
-                                                 uint32_t* __restrict__ slot_word,
-                                                 StepCtl* __restrict__ ctl, int special,
-                                                 int prime, uint32_t qmask = 0xFFFFFFFFu,
-                                                 CompletionRec* __restrict__ done_ring = nullptr,
-                                                 int match_n = 0) {
+__device__ __forceinline__ void advance_body(SlotState* slots, const ReadDesc* queue,
+                                             const unsigned char* reads, unsigned long long* best,
+                                             int32_t* res_score, uint32_t* res_vertex,
+                                             unsigned long long* res_t0, unsigned long long* res_t1,
+                                             uint32_t* slot_word, StepCtl* ctl, int special, int prime,
+                                             uint32_t qmask, CompletionRec* done_ring, int match_n) {
+  static_assert(R <= 128, "one thread per slot");
   __shared__ uint32_t s_need[128];
   __shared__ uint32_t s_base, s_take, s_active, s_ending;
   const int r = threadIdx.x;
@@ -1829,7 +2158,7 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
     }
     need = !prime && st.id < 0;
   }
-  s_need[r] = need ? 1u : 0u;
+  if (r < 128) s_need[r] = need ? 1u : 0u;
   __syncthreads();
   if (r == 0) {
     uint32_t total = 0;
@@ -1874,6 +2203,24 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
     ctl->any_ending = s_ending;
     if (s_active) ctl->steps += 1;
   }
+}
+
+template <int R>
+__global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
+                                                 const ReadDesc* __restrict__ queue,
+                                                 const unsigned char* __restrict__ reads,
+                                                 unsigned long long* __restrict__ best,
+                                                 int32_t* __restrict__ res_score,
+                                                 uint32_t* __restrict__ res_vertex,
+                                                 unsigned long long* __restrict__ res_t0,
+                                                 unsigned long long* __restrict__ res_t1,
+                                                 uint32_t* __restrict__ slot_word,
+                                                 StepCtl* __restrict__ ctl, int special,
+                                                 int prime, uint32_t qmask = 0xFFFFFFFFu,
+                                                 CompletionRec* __restrict__ done_ring = nullptr,
+                                                 int match_n = 0) {
+  advance_body<R>(slots, queue, reads, best, res_score, res_vertex, res_t0, res_t1, slot_word, ctl,
+                  special, prime, qmask, done_ring, match_n);
 }
 
 // ---------------------------------------------------------------------------

@@ -261,8 +261,10 @@ chsga_status chsga_align_rows(chsga_ctx* ctx, const char* read, uint32_t len, in
  * reads serially, src/align.hpp:488); results equal chsga_align_scores. */
 typedef struct {
   uint32_t slots;         /* reads advanced together: 1,2,4,8,16,32,64,128; 0 = 64 */
-  uint32_t steps_per_graph; /* row-steps captured per CUDA graph launch; 0 = default */
-  uint32_t use_graphs;    /* 1 = CUDA-graph capture of the row-step sequence */
+  uint32_t steps_per_graph; /* row-steps per CUDA graph or persistent launch; 0 = default */
+  uint32_t use_graphs;    /* launch mode, CHSGA_LAUNCH_*: 0 = every kernel launched from the host,
+                             1 = CUDA-graph capture of the row-step sequence, 2 = the persistent
+                             kernel (where it applies, else 1) */
   uint32_t row_bits;      /* storage of the score rows: 0 = 16 when every read is at most
                              65000 bases (each value of row i is at most i + 1, so this is
                              exact; arithmetic stays int32), else 32; or force 16 / 32 */
@@ -279,6 +281,18 @@ typedef struct {
  * DPX min/add units, one thread group per string vertex; STREAM = DPX with
  * one warp per run of 32 consecutive string vertices, loading the next
  * vertex's inputs while the current one computes (slots >= 64). */
+/* Launch modes of the row-step sequence (chsga_batch_opts::use_graphs).
+ * PERSISTENT runs a block of steps_per_graph row-steps as one cooperative
+ * launch of the persistent row-step kernel: the row update, every hierarchy
+ * level and the slot advance as phases of one kernel, separated by bounded
+ * grid barriers. It applies to 16-bit rows with the AUTO row kernel and
+ * string vertices of at most 512 chars (one slot: at most ~240); otherwise
+ * GRAPHS runs. */
+enum {
+  CHSGA_LAUNCH_STREAM = 0,
+  CHSGA_LAUNCH_GRAPHS = 1,
+  CHSGA_LAUNCH_PERSISTENT = 2
+};
 enum {
   CHSGA_ROW_AUTO = 0,
   CHSGA_ROW_DIRECT = 1,
@@ -392,7 +406,8 @@ typedef struct {
   uint64_t rows;          /* read rows computed */
   uint64_t steps;         /* row-steps that had work */
   uint64_t launches;      /* kernels launched by those steps */
-  uint64_t row_launches;  /* k_row launches */
+  uint64_t row_launches;  /* k_row launches (row phases of the persistent kernel) */
+  uint64_t launch_mode;   /* how the row-steps ran: CHSGA_LAUNCH_* */
 } chsga_profile;
 chsga_status chsga_get_profile(chsga_ctx* ctx, chsga_profile* out);
 
@@ -407,6 +422,14 @@ chsga_status chsga_get_read_times(chsga_ctx* ctx, uint64_t* admit_ns, uint64_t* 
  * block; the call then returns CHSGA_ERR_TIMEOUT exactly as an alignment
  * whose wait expired would, and the context stays usable. */
 chsga_status chsga_selftest_wait(chsga_ctx* ctx, uint32_t polls);
+
+/* Self-test of the persistent kernel's grid barrier, no reference
+ * counterpart: two blocks meet at a barrier that one of them never reaches;
+ * the other gives up after limit_us microseconds of the device's global
+ * timer, sets the abort word every other waiting block watches and flags
+ * the control block. Returns CHSGA_ERR_TIMEOUT as a persistent launch whose
+ * barrier expired would; the context stays usable. */
+chsga_status chsga_selftest_grid_wait(chsga_ctx* ctx, uint32_t limit_us);
 
 /* ------------------------------------------------------------------------- */
 /* Autotuner (no reference counterpart)                                      */

@@ -138,6 +138,9 @@ def test_random_graphs(tmp_path, seed, vmax):
     ctx = cb.Context(0).load(g)
     np.testing.assert_array_equal(ctx.align_scores(reads), want)
     np.testing.assert_array_equal(ctx.align_scores_batched(reads, slots=4), want)
+    for slots in (1, 4, 64):
+        np.testing.assert_array_equal(
+            ctx.align_scores_batched(reads, slots=slots, use_graphs=cb.LAUNCH_PERSISTENT), want)
     ctx.close()
 
 
@@ -157,3 +160,34 @@ def test_traceback_batched_equals_one_by_one(small_graph, ctx_small, oracle_smal
         assert score == w == one[1] and ck == one[2] == (len(rd) > 400)
         np.testing.assert_array_equal(ops, one[0])
         assert orc.rescore(ops, rd, labels) == (w, len(rd) - 1)
+
+
+@pytest.mark.parametrize("slots", [1, 2, 8, 32, 64, 128])
+@pytest.mark.parametrize("top_vertices", [0, 300])
+def test_persistent_kernel_matches_oracle(small_graph, ctx_small, oracle_small, slots, top_vertices):
+    # one cooperative launch per 16 row-steps: row, levels and advance as
+    # phases separated by grid barriers; uneven lengths refill slots mid-launch
+    g, files, reads = small_graph
+    mix = list(reads) + g.gen_reads(20, 19, 1, 400, sub_rate=0.03, indel_rate=0.02,
+                                    n_rate=0.005).to_list()
+    want = oracle_small.scores(mix)
+    got = ctx_small.align_scores_batched(mix, slots=slots, steps_per_graph=16,
+                                         use_graphs=cb.LAUNCH_PERSISTENT, top_vertices=top_vertices)
+    np.testing.assert_array_equal(got, want)
+    p = ctx_small.profile()
+    assert p["launch_mode"] == cb.LAUNCH_PERSISTENT
+    assert p["launches"] == 1 + p["row_launches"] // 16
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_plain_path_every_launch_mode(small_graph, ctx_small, oracle_small, mode):
+    # one slot: the tile row kernel (a warp per tile of whole vertices, a
+    # lane per 8 chars) in launches, in CUDA graphs and in the persistent kernel
+    g, files, reads = small_graph
+    want = oracle_small.scores(reads)
+    got = ctx_small.align_scores_batched(reads, slots=1, use_graphs=mode)
+    np.testing.assert_array_equal(got, want)
+    assert ctx_small.profile()["launch_mode"] == mode
+    # the one-thread-per-vertex row kernel gives the same scores
+    got_d = ctx_small.align_scores_batched(reads, slots=1, use_graphs=mode, row_kernel=cb.ROW_DIRECT)
+    np.testing.assert_array_equal(got_d, want)
