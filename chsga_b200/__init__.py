@@ -241,6 +241,7 @@ _sig("chsga_cm_load", C.c_int32, vp, C.c_char_p)
 _sig("chsga_cm_features", C.c_int32, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int64, C.c_uint64,
      f32p)
 _sig("chsga_server_open", C.c_int32, vp, C.POINTER(ServerOpts), C.POINTER(vp))
+_sig("chsga_server_selftest_fail", C.c_int32, vp)
 _sig("chsga_server_submit", C.c_int32, vp, C.c_char_p, C.c_uint32, C.c_uint32,
      C.POINTER(C.c_uint64))
 _sig("chsga_server_poll", C.c_int32, vp, C.POINTER(ServerResult), C.c_uint32,
@@ -588,6 +589,12 @@ class Server:
         if st != OK:
             msg = _lib.chsga_server_last_error(self._h) or b""
             raise ChsgaError(st, msg.decode(errors="replace"))
+
+    def selftest_fail(self) -> None:
+        """chsga_server_selftest_fail: the score lane runs a bounded device
+        wait that cannot succeed at its next block and fails as after any
+        expired wait."""
+        self._ck(_lib.chsga_server_selftest_fail(self._h))
 
     def submit(self, read: bytes, mode: int = REQ_SCORE) -> int:
         t = C.c_uint64()

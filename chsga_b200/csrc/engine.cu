@@ -1746,6 +1746,11 @@ class ScoreLaneImpl final : public ScoreLane {
   uint64_t blocks() const override { return launched_; }
   uint32_t kernels_per_block() const override { return kernels_per_step(*c_) * per_; }
 
+  void inject_wait_timeout() override {
+    dev::k_wait_selftest<<<1, 32, 0, c_->st>>>(b_->ctl.p, 4096);
+    check_launch();
+  }
+
   void publish(uint64_t lo, uint64_t hi, const LaneRead* reads, uint32_t n) override {
     chsga_ctx& c = *c_;
     require(hi <= arena_ && lo <= hi, CHSGA_ERR_INTERNAL, "arena range");

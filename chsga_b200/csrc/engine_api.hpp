@@ -74,6 +74,10 @@ class ScoreLane {
   virtual void drain(std::vector<LaneDone>& out) = 0;
   virtual uint64_t blocks() const = 0;        // blocks launched
   virtual uint32_t kernels_per_block() const = 0;
+  // Self-test of the failure path: enqueues a bounded device-side wait that
+  // cannot succeed against the lane's control block; the harvest of the
+  // next block then fails with CHSGA_ERR_TIMEOUT, as for an expired wait.
+  virtual void inject_wait_timeout() = 0;
 };
 
 // slots: 2..128 (power of two); capacity: power of two; row_bits 16 or 32.

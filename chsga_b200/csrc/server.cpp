@@ -16,6 +16,7 @@
 // the budget (head-of-line: a large request is never overtaken forever).
 #include <algorithm>
 #include <chrono>
+#include <atomic>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -138,6 +139,7 @@ struct chsga_server {
   std::deque<chsga_server_result> done;
   bool stop = false;
   chsga_status broken = CHSGA_OK;  // the score lane failed: score requests fail with this
+  std::atomic<bool> inject_fail{false};  // chsga_server_selftest_fail: at the next block
   std::string err;
   uint64_t next_ticket = 1;
   uint64_t submitted = 0, finished = 0, failed = 0;
@@ -294,6 +296,7 @@ struct chsga_server {
           busy = lane_running > 0;
         }
         if (busy) {
+          if (inject_fail.exchange(false)) lane->inject_wait_timeout();
           lane->step(d);
           collect(d);
         }
@@ -433,6 +436,15 @@ chsga_status chsga_server_open(chsga_ctx* ctx, const chsga_server_opts* opts, ch
     p->engine = std::thread([p] { p->engine_loop(); });
     for (uint32_t w = 0; w < o.tb_workers; ++w) p->workers.emplace_back([p, w] { p->tb_loop(w); });
     *out = s.release();
+  });
+}
+
+chsga_status chsga_server_selftest_fail(chsga_server* s) {
+  return guarded_srv(s, [&] {
+    require(s != nullptr, CHSGA_ERR_INVALID_ARG, "null argument");
+    s->inject_fail = true;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->cv_engine.notify_all();
   });
 }
 

@@ -541,6 +541,16 @@ chsga_status chsga_server_open(chsga_ctx* ctx, const chsga_server_opts* opts, ch
  * requests already wait; CHSGA_ERR_OOM when a traceback could never fit the
  * budget; CHSGA_ERR_UNSUPPORTED for a score read over 65000 bases with
  * 16-bit rows. */
+/* Self-test of the serving loop's failure path, no reference counterpart:
+ * at its next block of row-steps the score lane also runs a bounded
+ * device-side wait that cannot succeed (as chsga_selftest_wait does)
+ * against its control block. The lane then fails as it would after any
+ * expired device wait: every waiting and running score request completes
+ * with CHSGA_ERR_TIMEOUT, later score submissions are refused with it, and
+ * the context stays usable (a new server on it aligns as before). Nothing
+ * happens until score work is on the lane. */
+chsga_status chsga_server_selftest_fail(chsga_server* srv);
+
 chsga_status chsga_server_submit(chsga_server* s, const char* read, uint32_t len, uint32_t mode,
                                  uint64_t* ticket);
 /* Moves up to `max` finished results to `out`; waits up to wait_ms (-1 =

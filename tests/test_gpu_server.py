@@ -168,3 +168,40 @@ def test_busy_and_rejections(small_graph, ctx):
         srv.submit(b"", cb.REQ_TRACEBACK)
     assert e.value.status == cb.ERR_INVALID_ARG
     srv.close()
+
+
+def test_lane_failure_fails_waiting_and_running_requests(small_graph, ctx):
+    # a bounded device wait that runs out inside the running score lane: every
+    # request not yet finished completes with ERR_TIMEOUT, finished ones keep
+    # their exact scores, later score submissions are refused, and a new
+    # server on the same context aligns exactly
+    g, files, reads = small_graph
+    mix = _mix(g, 61, 160, 300, 1500)
+    want = ctx.align_scores(mix)
+    srv = cb.Server(ctx, slots=8, queue_capacity=64, arena_bytes=1 << 20, steps_per_graph=4)
+    try:
+        tickets = [srv.submit(r) for r in mix]
+        srv.selftest_fail()
+        res = srv.collect()
+        st = srv.stats()
+        failed = [t for t in tickets if res[t]["status"] != cb.OK]
+        assert failed and all(res[t]["status"] == cb.ERR_TIMEOUT for t in failed)
+        for t, w in zip(tickets, want):
+            if res[t]["status"] == cb.OK:
+                assert res[t]["score"] == w
+        assert st["failed"] == len(failed) and st["completed"] == len(mix) - len(failed)
+        # the last submitted reads were still waiting when the lane failed
+        assert res[tickets[-1]]["status"] == cb.ERR_TIMEOUT
+        with pytest.raises(cb.ChsgaError) as e:
+            srv.submit(mix[0])
+        assert e.value.status == cb.ERR_TIMEOUT
+    finally:
+        srv.close()
+    srv2 = cb.Server(ctx, slots=8, queue_capacity=64, arena_bytes=1 << 20, steps_per_graph=4)
+    try:
+        tk = [srv2.submit(r) for r in mix[:40]]
+        res2 = srv2.collect()
+    finally:
+        srv2.close()
+    assert all(res2[t]["status"] == cb.OK for t in tk)
+    np.testing.assert_array_equal([res2[t]["score"] for t in tk], want[:40])
