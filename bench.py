@@ -63,6 +63,8 @@ def parse():
     p.add_argument("--scale-cfg4", action="store_true",
                    help="config-4 run instead of the contract line: the 100 Mbp graph, "
                         "checkpointed tracebacks (-k 500) and batched score-only GCUPS")
+    p.add_argument("--cfg4-reads", type=int, default=4,
+                   help="with --scale-cfg4: how many 10 kbp reads to trace back")
     p.add_argument("--traceback-cfg1", action="store_true",
                    help="config-1 run instead of the contract line: tracebacks of 2,000 x 150 bp and "
                         "200 x 2 kbp reads with full score matrices, batched and one by one")
@@ -395,14 +397,24 @@ def run_reference(args):
 
 
 def run_scale_cfg4(args):
-    """The 100 Mbp config-4 graph (about 139 M chars): checkpointed tracebacks
-    of 10 kbp reads at 5% error with -k 500 (a full int32 matrix would take
-    5.6 TB), each checked by rescoring its path against the score-only
-    result, then batched score-only GCUPS with 128 slots (two 16-bit rows of
-    35.6 GB). Prints one JSON line."""
+    """Config 4: the 100 Mbp graph (about 139 M chars; one int32 row is
+    0.56 GB, so a full 10 kbp matrix would take 5.6 TB) with -k 500.
+      byte-compare  a 1001-base read: the checkpoint files row_0.bin,
+                    row_500.bin and row_1000.bin the GPU writes against the
+                    same rows from the reference's own row functions
+                    (oracle/_ref, two rows held at a time)
+      tracebacks    --cfg4-reads reads of 10 kbp at 5% error, each
+                    checkpointed (16-bit rows; a 501-row recompute segment is
+                    139 GB and fits the device in one level), each path
+                    rescored against the score-only result; GCUPS over the
+                    forward cells (recompute not counted)
+      batched       score-only GCUPS with 128 slots
+    Prints one JSON line."""
     import numpy as np
 
     import chsga_b200 as cb
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
     t0 = time.time()
     g = cb.HostGraph.generate(**cb.GRAPH_CONFIGS["cfg4"])
     g.build_pch()
@@ -411,29 +423,59 @@ def run_scale_cfg4(args):
     prep_s = time.time() - t0
     ctx = cb.Context(0).load(g)
     labels = ctypes_labels(g)
-    reads = g.gen_reads(2, 44, 10000, 10000, sub_rate=0.02, indel_rate=0.03, indel_len_max=3).to_list()
-    want = ctx.align_scores(reads)
+    out = {"mode": "scale-cfg4", "num_chars": N, "num_strings": st["num_strings"],
+           "hierarchy_levels": st["pch_levels"], "graph_prep_s": prep_s}
+    # checkpoint rows against the reference
+    r1 = g.gen_reads(1, 43, 1001, 1001, sub_rate=0.02, indel_rate=0.03, indel_len_max=3).to_list()[0]
+    with tempfile.TemporaryDirectory() as d:
+        ck = os.path.join(d, "ck")
+        t = time.perf_counter()
+        ops, score, ckp = ctx.align_traceback(r1, k=500, ckpt_dir=ck, keep_files=True)
+        gpu_s = time.perf_counter() - t
+        cmp = {"read_len": len(r1), "k": 500, "gpu_seconds": gpu_s, "checkpointed": ckp,
+               "score": score, "rescored": list(path_score(ops, r1, labels))}
+        if oracle.ref_available():
+            files = g.write_files(os.path.join(d, "g"))
+            h, kind, cores = cpu_harness(oracle, files)
+            t = time.time()
+            rows = h.rows_at(r1, N, [0, 500, 1000]) if kind == "reference" else None
+            cmp["reference_seconds"] = time.time() - t
+            cmp["reference_threads"] = cores
+            if rows is not None:
+                same = []
+                for j, i in enumerate((0, 500, 1000)):
+                    got = np.fromfile(os.path.join(ck, f"row_{i}.bin"), dtype=np.int32)
+                    same.append(bool(got.shape == rows[j].shape and np.array_equal(got, rows[j])))
+                cmp["rows"] = [0, 500, 1000]
+                cmp["byte_identical"] = same
+        else:
+            cmp["byte_identical"] = "reference build absent"
+        out["checkpoint_compare"] = cmp
+    # checkpointed tracebacks of 10 kbp reads
+    reads = g.gen_reads(args.cfg4_reads, 44, 10000, 10000, sub_rate=0.02, indel_rate=0.03,
+                        indel_len_max=3).to_list()
+    want = ctx.align_scores_batched(reads, slots=min(128, max(2, 1 << (len(reads) - 1).bit_length())))
     tb = []
     for r, w in zip(reads, want):
         t = time.perf_counter()
-        ops, score, ck = ctx.align_traceback(r, k=500)
+        ops, score, ckp = ctx.align_traceback(r, k=500)
         dt = time.perf_counter() - t
         ps, last = path_score(ops, r, labels)
-        tb.append({"len": len(r), "seconds": dt, "checkpointed": ck, "score": score,
+        tb.append({"len": len(r), "seconds": dt, "checkpointed": ckp, "score": score,
                    "score_only": int(w), "rescored": ps, "last_row": last,
                    "ok": bool(score == w == ps and last == len(r) - 1),
                    "gcups_forward_cells": len(r) * N / dt / 1e9})
+    out["traceback"] = tb
+    out["traceback_summary"] = {"reads": len(tb), "all_ok": all(x["ok"] for x in tb),
+                                "gcups": sum(x["len"] for x in tb) * N / sum(x["seconds"] for x in tb) / 1e9}
     batch = make_reads(g, 256, 4545, len_max=2000)
     ctx.align_scores_batched(batch[:128], slots=128)  # warm-up
     ctx.align_scores_batched(batch, slots=128)
     p = ctx.profile()
     cells = sum(len(r) for r in batch) * N
-    line = {"mode": "scale-cfg4", "num_chars": N, "num_strings": st["num_strings"],
-            "hierarchy_levels": st["pch_levels"], "graph_prep_s": prep_s,
-            "traceback": tb, "batched": {"reads": len(batch), "slots": 128,
-                                         "gcups": cells / p["total_ms"] / 1e6,
-                                         "device_ms": p["total_ms"]}}
-    print(json.dumps(line), flush=True)
+    out["batched"] = {"reads": len(batch), "slots": 128, "gcups": cells / p["total_ms"] / 1e6,
+                      "device_ms": p["total_ms"]}
+    print(json.dumps(out), flush=True)
     ctx.close()
     return 0
 

@@ -179,7 +179,8 @@ struct chsga_ctx {
   chsga::DevArr<unsigned long long> res_t0, res_t1;  // admission / completion, device ns
   std::vector<uint32_t> last_ids;  // caller index of each queued read of the last call
   chsga::PinnedArr<chsga::dev::StepCtl> h_ctl;
-  chsga::PinnedArr<int32_t> h_ckpt;  // checkpoint rows of the checkpointed traceback
+  chsga::PinnedArr<int32_t> h_ckpt;     // checkpoint rows of the checkpointed traceback (int32 rows)
+  chsga::PinnedArr<uint16_t> h_ckpt16;  // the same for 16-bit rows
   chsga_profile prof{};
 };
 
@@ -830,11 +831,12 @@ struct TbState {
   std::vector<dev::WalkOp> path;  // reverse order
 };
 
-// Forward rows [a+1, b] of the single read from `row_a` (row a, on the
-// device), writing row i to out + (i - a) * N if out_rows, else rotating two
-// buffers; sub-checkpoint rows every `sub_k` rows go to sub + j * N.
+// Forward rows [a+1, b] of the single read from row a (on the device at
+// matrix row 0), writing row i to matrix + (i - a) * pitch; rows are final
+// (FIXUP), in ST storage.
+template <typename ST>
 void forward_rows(chsga_ctx& c, SlotBufs& b, uint32_t len, int64_t a, int64_t b_row,
-                  int* matrix /* rows a..b at stride c.g->pitch, row a already present */) {
+                  ST* matrix /* rows a..b at stride c.g->pitch, row a already present */) {
   const size_t N = c.g->pitch;
   // slot 0 at row a+1 of read 0
   dev::SlotState s{0, len, (uint32_t)(a + 1), 0, 0};
@@ -848,22 +850,23 @@ void forward_rows(chsga_ctx& c, SlotBufs& b, uint32_t len, int64_t a, int64_t b_
   launch_advance<1>(c, b, 1, c.st);
   // the row-step reads the previous row's per-vertex first/last scores; row a
   // comes from a checkpoint, so derive them from it
-  dev::k_fl_from_row<<<nblocks(c.g->L.S), 256, 0, c.st>>>(c.g->gp, matrix, reinterpret_cast<int*>(b.FL.p));
+  dev::k_fl_from_row<ST><<<nblocks(c.g->L.S), 256, 0, c.st>>>(c.g->gp, matrix, reinterpret_cast<ST*>(b.FL.p));
   check_launch();
   for (int64_t i = a + 1; i <= b_row; ++i)
-    row_step<1, false, int>(c, b, matrix + (size_t)(i - 1 - a) * N, matrix + (size_t)(i - a) * N, c.st);
+    row_step<1, false, ST>(c, b, matrix + (size_t)(i - 1 - a) * N, matrix + (size_t)(i - a) * N, c.st);
   check_device_error(c, b);
 }
 
-void walk(chsga_ctx& c, const int* M, int64_t lo, int64_t hi, uint32_t start, uint32_t len,
+template <typename MT>
+void walk(chsga_ctx& c, const MT* M, int64_t lo, int64_t hi, uint32_t start, uint32_t len,
           std::vector<dev::WalkOp>& path, uint32_t* landing) {
   const uint32_t max_ops = (uint32_t)(2 * (hi - lo) + 2 * (uint64_t)len + 16);
   DevArr<dev::WalkOp> ops;
   ops.alloc(max_ops);
   DevArr<dev::WalkOut> out;
   out.alloc(1);
-  dev::k_walk<int><<<1, 1, 0, c.st>>>(c.g->gp, M, c.g->pitch, lo, hi, start, c.reads.p, ops.p, max_ops, out.p,
-                                 match_n(c));
+  dev::k_walk<MT><<<1, 1, 0, c.st>>>(c.g->gp, M, c.g->pitch, lo, hi, start, c.reads.p, ops.p, max_ops, out.p,
+                                     match_n(c));
   check_launch();
   dev::WalkOut h{};
   CK(cudaMemcpyAsync(&h, out.p, sizeof(h), cudaMemcpyDeviceToHost, c.st));
@@ -903,8 +906,36 @@ uint64_t sub_segment_rows(uint64_t span, uint64_t fit) {
   return 0;
 }
 
-void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts* o,
-               chsga_tb_result* res) {
+// Pinned host rows of the checkpointed traceback, per row storage.
+template <typename ST>
+PinnedArr<ST>& ckpt_host(chsga_ctx& c);
+template <>
+PinnedArr<int32_t>& ckpt_host<int32_t>(chsga_ctx& c) {
+  return c.h_ckpt;
+}
+template <>
+PinnedArr<uint16_t>& ckpt_host<uint16_t>(chsga_ctx& c) {
+  return c.h_ckpt16;
+}
+
+// Checkpoint files hold raw int32 rows (the reference's format,
+// src/traceback.hpp:215-227) whatever the rows are stored in.
+void write_ckpt(const std::string& dir, int64_t row, const int32_t* d, uint64_t n) {
+  write_ckpt_row(dir, row, d, n);
+}
+void write_ckpt(const std::string& dir, int64_t row, const uint16_t* d, uint64_t n) {
+  std::vector<int32_t> w(n);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)n; ++i) w[i] = d[i];
+  write_ckpt_row(dir, row, w.data(), n);
+}
+
+// One read's traceback with rows stored as ST: int32, or uint16 for reads
+// of at most kRow16Max bases (every value of row i is at most i + 1, so the
+// rows are the same numbers in half the bytes).
+template <typename ST>
+void traceback_rows(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts* o,
+                    chsga_tb_result* res) {
   require(len > 0, CHSGA_ERR_INVALID_ARG, "traceback of an empty read");
   const size_t N = c.g->pitch;   // row stride of every matrix below
   const size_t NC = c.g->L.N;    // chars per row
@@ -914,9 +945,11 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
   const bool keep = o && o->keep_files;
   const char* rp[1] = {read};
   upload_reads(c, rp, &len, 1);
-  SlotBufs& b = get_bufs<1, int>(c, false);
-  const uint64_t row_bytes = (uint64_t)NC * 4;  // one checkpoint row (the reference's file size)
-  const uint64_t store = (uint64_t)len * row_bytes;
+  SlotBufs& b = get_bufs<1, ST>(c, false);
+  // the full-matrix / checkpointed decision counts int32 rows, as the
+  // reference does (src/traceback.hpp:614-645), whatever ST is
+  const uint64_t store = (uint64_t)len * NC * 4;
+  const uint64_t row_bytes = (uint64_t)NC * sizeof(ST);  // one stored row
   std::vector<dev::WalkOp> path;
   uint32_t best_v = 0;
   int32_t best_s = 0;
@@ -930,12 +963,12 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
   if (store <= cap) {
     // one spare row: row 0 reads no previous row, but its input pointer
     // must not alias the row it writes
-    DevArr<int> M;
+    DevArr<ST> M;
     M.alloc((size_t)(len + 1) * N);
     reset_slots<1>(c, b, 1);
     launch_advance<1>(c, b, 0, c.st);
     for (uint32_t i = 0; i < len; ++i)
-      row_step<1, false, int>(c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, c.st);
+      row_step<1, false, ST>(c, b, M.p + (size_t)(i ? i - 1 : len) * N, M.p + (size_t)i * N, c.st);
     harvest();
     uint32_t v = best_v;
     if (len > 1) walk(c, M.p, 0, len - 1, best_v, len, path, &v);
@@ -945,8 +978,9 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
     res->checkpointed = 1;
     const uint64_t nck = (len - 1) / (uint64_t)k + 1;
     res->num_checkpoints = nck;
-    c.h_ckpt.alloc(nck * NC);
-    DevArr<int> ring;
+    PinnedArr<ST>& hck = ckpt_host<ST>(c);
+    hck.alloc(nck * NC);
+    DevArr<ST> ring;
     ring.alloc(3 * N);
     cudaEvent_t done_ev[3];
     for (auto& e : done_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -965,13 +999,13 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
         CK(cudaEventSynchronize(done_ev[cur]));
         busy[cur] = false;
       }
-      row_step<1, false, int>(c, b, ring.p + (size_t)prev * N, ring.p + (size_t)cur * N, c.st);
+      row_step<1, false, ST>(c, b, ring.p + (size_t)prev * N, ring.p + (size_t)cur * N, c.st);
       if (i % k == 0) {
         cudaEvent_t ready;
         CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
         CK(cudaEventRecord(ready, c.st));
         CK(cudaStreamWaitEvent(c.side, ready, 0));
-        CK(cudaMemcpyAsync(c.h_ckpt.p + (size_t)(i / k) * NC, ring.p + (size_t)cur * N, row_bytes,
+        CK(cudaMemcpyAsync(hck.p + (size_t)(i / k) * NC, ring.p + (size_t)cur * N, row_bytes,
                            cudaMemcpyDeviceToHost, c.side));
         CK(cudaEventRecord(done_ev[cur], c.side));
         busy[cur] = true;
@@ -985,7 +1019,7 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
     ring.release();
     if (!dir.empty())
       for (uint64_t j = 0; j < nck; ++j)
-        write_ckpt_row(dir, (int64_t)(j * k), c.h_ckpt.p + (size_t)j * NC, NC);
+        write_ckpt(dir, (int64_t)(j * k), hck.p + (size_t)j * NC, NC);
     // backward, one segment at a time (src/traceback.hpp:945-1011)
     int64_t cur_row = len - 1;
     uint32_t cur_v = best_v;
@@ -995,7 +1029,7 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
     // segment buffers live across segments (equal segments reuse them; a
     // buffer whose size changes is released before anything is allocated,
     // so the device holds one segment's plan at a time)
-    DevArr<int> seg, sub;
+    DevArr<ST> seg, sub;
     auto plan = [&](size_t seg_elems, size_t sub_elems) {
       if (seg.n != seg_elems) seg.release();
       if (sub.n != sub_elems) sub.release();
@@ -1006,10 +1040,10 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
       int64_t seg_start = (cur_row % k == 0) ? (cur_row - k) : (cur_row / k * k);
       if (seg_start < 0) seg_start = 0;
       const int64_t seg_end = cur_row;
-      const int* ck = c.h_ckpt.p + (size_t)(seg_start / k) * NC;
+      const ST* ck = hck.p + (size_t)(seg_start / k) * NC;
       const uint64_t rows = (uint64_t)(seg_end - seg_start + 1);
       uint32_t landing = cur_v;
-      const uint64_t pitch_bytes = (uint64_t)N * 4;
+      const uint64_t pitch_bytes = (uint64_t)N * sizeof(ST);
       if (rows * pitch_bytes <= budget || rows <= 2) {
         plan(rows * N, 0);
         CK(cudaMemcpyAsync(seg.p, ck, row_bytes, cudaMemcpyHostToDevice, c.st));
@@ -1068,6 +1102,14 @@ void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts
     if (!dir.empty() && !keep) std::filesystem::remove(ckpt_row_path(dir, 0));
   }
   fill_result(res, path, best_s);
+}
+
+void traceback(chsga_ctx& c, const char* read, uint32_t len, const chsga_tb_opts* o,
+               chsga_tb_result* res) {
+  if (len <= kRow16Max)
+    traceback_rows<uint16_t>(c, read, len, o, res);
+  else
+    traceback_rows<int32_t>(c, read, len, o, res);
 }
 
 // Publishes queue entries [0, q_count) to k_advance (one thread, stream-ordered).
@@ -1881,7 +1923,8 @@ chsga_ctx* fork_context(chsga_ctx& p) {
 }
 
 uint64_t traceback_device_bytes(const chsga_ctx& c, uint32_t len, const chsga_tb_opts* o) {
-  const uint64_t pb = (uint64_t)c.g->pitch * 4, row_bytes = (uint64_t)c.g->L.N * 4;
+  // rows as traceback_rows stores them; the path choice counts int32 rows
+  const uint64_t pb = (uint64_t)c.g->pitch * (len <= kRow16Max ? 2 : 4), row_bytes = (uint64_t)c.g->L.N * 4;
   const int64_t k = (o && o->k > 0) ? o->k : 500;
   const uint64_t cap = (o && o->cap_bytes) ? o->cap_bytes : c.cap;
   const uint64_t read = (len + 255) / 256 * 256;

@@ -2100,9 +2100,10 @@ __global__ void k_wait_selftest(StepCtl* __restrict__ ctl, uint32_t polls) {
 // ---------------------------------------------------------------------------
 // k_fl_from_row: FL of a final row that was not produced by the preceding
 // row-step (a checkpoint row a segment restarts from): first and last score
-// of every string vertex, read from the row (R = 1, int32 rows).
+// of every string vertex, read from the row (R = 1, int32 or 16-bit rows).
 // ---------------------------------------------------------------------------
-__global__ void k_fl_from_row(GraphPtrs g, const int* __restrict__ row, int* __restrict__ FL) {
+template <typename ST>
+__global__ void k_fl_from_row(GraphPtrs g, const ST* __restrict__ row, ST* __restrict__ FL) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= g.S) return;
   FL[2 * s] = row[g.sv_off[s]];

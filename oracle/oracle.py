@@ -151,6 +151,7 @@ class RefHarness:
         for f in ("ref_align_scores", "ref_exact_scores"):
             getattr(L, f).argtypes = [C.c_void_p, C.c_char_p, u64p, C.c_uint64, i32p]
         L.ref_align_rows.argtypes = [C.c_void_p, C.c_char_p, C.c_uint64, i32p]
+        L.ref_rows_at.argtypes = [C.c_void_p, C.c_char_p, C.c_uint64, u64p, C.c_uint64, i32p]
         L.ref_traceback.argtypes = [C.c_void_p, C.c_char_p, C.c_uint64, C.c_int64, C.c_char_p,
                                     C.c_int, C.c_void_p, C.c_uint64, u64p]
         if threads:
@@ -178,6 +179,15 @@ class RefHarness:
     def rows(self, read: bytes, num_chars: int) -> np.ndarray:
         out = np.zeros((len(read), num_chars), dtype=np.int32)
         self.lib.ref_align_rows(self.h, read, len(read), out.ctypes.data_as(i32p))
+        return out
+
+    def rows_at(self, read: bytes, num_chars: int, want) -> np.ndarray:
+        """Rows `want` (ascending) of the read, two rows held at a time."""
+        w = np.ascontiguousarray(sorted(want), dtype=np.uint64)
+        out = np.zeros((len(w), num_chars), dtype=np.int32)
+        if self.lib.ref_rows_at(self.h, read, len(read), w.ctypes.data_as(u64p), len(w),
+                                out.ctypes.data_as(i32p)):
+            raise RuntimeError("row index beyond the read")
         return out
 
     def traceback(self, read: bytes, k: int = 500, ckpt_dir: str = "/tmp/ref_ckpt",

@@ -105,6 +105,30 @@ int ref_align_rows(void* h, const char* rd, uint64_t len, int32_t* rows) {
   return 0;
 }
 
+// Rows want[0] < want[1] < ... of one read, from the same row functions in
+// the same order as ref_align_rows, keeping two rows in memory instead of
+// len (for graphs whose full matrix does not fit host memory).
+int ref_rows_at(void* h, const char* rd, uint64_t len, const uint64_t* want, uint64_t nwant,
+                int32_t* out) {
+  auto* r = (RefInputs*)h;
+  const size_t N = r->labels.size();
+  std::vector<int32_t> a(N), b(N);
+  int32_t* prev = a.data();
+  int32_t* cur = b.data();
+  uint64_t w = 0;
+  init_func_parallel<int>(prev, r->labels, rd[0], N, 0, 1);
+  if (w < nwant && want[w] == 0) std::copy(prev, prev + N, out + (w++) * N);
+  for (uint64_t i = 1; i < len && w < nwant; ++i) {
+    fused_deletion_substitution<int, VertexLabelMapper<false>>(cur, prev, r->labels, r->in_char, rd[i],
+                                                                0, 1, 1, N);
+    insertion_func_parallel<int, VertexLabelMapper<true>>(cur, r->str_graph, r->to_og, 1, *r->query,
+                                                           *r->mapper);
+    if (want[w] == i) std::copy(cur, cur + N, out + (w++) * N);
+    std::swap(prev, cur);
+  }
+  return w == nwant ? 0 : 1;
+}
+
 // align_read_with_traceback<int> (traceback.hpp:588-1031). ops: 16-byte
 // records {int64 row, uint32 vertex, uint8 op, pad}.
 int ref_traceback(void* h, const char* rd, uint64_t len, int64_t k, const char* dir, int cleanup,

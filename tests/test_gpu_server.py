@@ -73,8 +73,9 @@ def test_server_small_arena_and_waves(small_graph, ctx):
 
 
 def _tb_footprint(n_chars, length):
+    # full matrix of 16-bit rows (reads of at most 65000 bases) plus the read
     pitch = (n_chars + 15) // 16 * 16
-    return (length + 1) * pitch * 4 + (length + 255) // 256 * 256
+    return (length + 1) * pitch * 2 + (length + 255) // 256 * 256
 
 
 def test_same_result_alone_and_in_the_mix(small_graph, ctx):

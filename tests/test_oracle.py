@@ -158,3 +158,15 @@ def test_matchn_oracle_matches_reference_code(tmp_path, seed, vmax):
     for rd, w in zip(reads[:3], want):
         ops, score, _ = o.traceback(rd)
         assert score == w and orc.rescore(ops, rd, labels, match_n=True) == (w, len(rd) - 1)
+
+
+@pytest.mark.skipif(not orc.ref_available(), reason="reference build absent")
+def test_reference_rows_at_equals_every_row(tmp_path):
+    # the two-row harness entry used for the config-4 byte-compare returns
+    # the same rows as the all-rows one
+    g, files = gen_graph(tmp_path, "ra", backbone_len=4000, seed=71)
+    n = g.stats()["num_chars"]
+    rd = g.gen_reads(1, 72, 130, sub_rate=0.03, indel_rate=0.02).to_list()[0]
+    h = orc.RefHarness(files)
+    every = h.rows(rd, n)
+    np.testing.assert_array_equal(h.rows_at(rd, n, [0, 64, 129]), every[[0, 64, 129]])
