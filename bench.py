@@ -65,6 +65,11 @@ def parse():
                         "checkpointed tracebacks (-k 500) and batched score-only GCUPS")
     p.add_argument("--cfg4-reads", type=int, default=4,
                    help="with --scale-cfg4: how many 10 kbp reads to trace back")
+    p.add_argument("--cfg5", action="store_true",
+                   help="config-5 run instead of the contract line: the cost model trained on logs of "
+                        "runs on the config-2 and config-4 graphs, then a Poisson stream of score and "
+                        "traceback requests on the config-4 graph admitted by its footprint")
+    p.add_argument("--cfg5-window-s", type=float, default=30.0, help="with --cfg5: arrival window")
     p.add_argument("--traceback-cfg1", action="store_true",
                    help="config-1 run instead of the contract line: tracebacks of 2,000 x 150 bp and "
                         "200 x 2 kbp reads with full score matrices, batched and one by one")
@@ -589,6 +594,180 @@ def run_launch_compare(args):
     return 0
 
 
+def _served_logs(cb, ctx, g, reads, mode, slots, k=500, cap=0, tb_workers=1):
+    """Runs the reads through a server and returns (features, targets,
+    results): targets are the request's device time in ms (admission to
+    completion) and its device bytes -- the measured peak of a traceback, the
+    slot's share of the engine's 16-bit rows for a score read."""
+    import numpy as np
+    N = g.stats()["num_chars"]
+    srv = cb.Server(ctx, slots=slots, tb_workers=tb_workers, tb_k=k, tb_cap_bytes=cap,
+                    queue_capacity=4096, arena_bytes=64 << 20)
+    tk = [srv.submit(r, mode) for r in reads]
+    res = srv.collect()
+    srv.close()
+    x, y, out = [], [], []
+    for t, r in zip(tk, reads):
+        d = res[t]
+        if d["status"] != cb.OK:
+            raise RuntimeError(f"request failed with status {d['status']}")
+        x.append(cb.cm_features(ctx, len(r), mode, slots if mode == cb.REQ_SCORE else 1, k, cap))
+        ms = max(1e-3, (d["done_ns"] - d["start_ns"]) / 1e6)
+        by = d["peak_bytes"] if mode == cb.REQ_TRACEBACK else 4.0 * (N + 32) + len(r)
+        y.append([ms, by])
+        out.append(d)
+    return np.array(x, np.float32), np.array(y, np.float32), out
+
+
+def run_cfg5(args):
+    """Config 5: served mode plus the learned cost model on the config-4
+    graph resident in HBM.
+      logs     the library's own runs on the config-2 graph (5 Mbp) and the
+               config-4 graph (100 Mbp): score requests through the serving
+               loop, full-matrix and checkpointed tracebacks; per request the
+               8 features, device time and device bytes
+      model    the FP32 MLP trained on the GPU on 3/4 of the logs; mean
+               absolute log error on the held-out 1/4 for time and bytes,
+               against the analytic |V| x |read| model (time = a |V| |read|
+               with a fitted on the training logs, bytes = 4 |V| |read|)
+      stream   Poisson arrivals on the config-4 graph for --cfg5-window-s
+               seconds at ~80% of the score capacity measured in the logs:
+               80% 150 bp at 1% error and 16% log-uniform 1-10 kbp at 5%
+               error as score requests, 4% 150-1000 bp traceback requests,
+               tracebacks admitted by the model's predicted footprint
+               (CHSGA_FP_MODEL); p50/p99 per kind, GCUPS, the model's error on
+               the stream. The 50,000-read stream of the configuration would
+               take hours on one GPU; the window is a sample of it.
+    Prints one JSON line."""
+    import numpy as np
+
+    import chsga_b200 as cb
+    t0 = time.time()
+    g2 = make_graph(args.backbone)
+    g4 = cb.HostGraph.generate(**cb.GRAPH_CONFIGS["cfg4"])
+    g4.build_pch()
+    prep_s = time.time() - t0
+    N2, N4 = g2.stats()["num_chars"], g4.stats()["num_chars"]
+    ctx2 = cb.Context(0).load(g2)
+    X, Y, src = [], [], []
+
+    def add(x, y, tag):
+        X.append(x)
+        Y.append(y)
+        src.extend([tag] * len(x))
+
+    t = time.time()
+    # config-2 graph: score reads (log-uniform 150-10k), tracebacks full-matrix and checkpointed
+    add(*_served_logs(cb, ctx2, g2, make_reads(g2, 256, 5001), cb.REQ_SCORE, 128)[:2], "cfg2-score")
+    add(*_served_logs(cb, ctx2, g2, make_reads(g2, 24, 5002, len_max=2000), cb.REQ_TRACEBACK, 1)[:2],
+        "cfg2-tb-full")
+    for k in (100, 250):
+        add(*_served_logs(cb, ctx2, g2, make_reads(g2, 8, 5003 + k, len_max=2000), cb.REQ_TRACEBACK, 1,
+                          k=k, cap=12 * N2 * 4)[:2], f"cfg2-tb-ckpt-k{k}")
+    ctx2.close()
+    ctx4 = cb.Context(0).load(g4)
+    add(*_served_logs(cb, ctx4, g4, make_reads(g4, 64, 5101, len_max=2000), cb.REQ_SCORE, 64)[:2],
+        "cfg4-score")
+    add(*_served_logs(cb, ctx4, g4, make_reads(g4, 8, 5102, len_max=1000), cb.REQ_TRACEBACK, 1)[:2],
+        "cfg4-tb-full")
+    add(*_served_logs(cb, ctx4, g4, g4.gen_reads(4, 5103, 1500, 3000, sub_rate=0.02, indel_rate=0.03)
+                      .to_list(), cb.REQ_TRACEBACK, 1, k=500)[:2], "cfg4-tb-ckpt")
+    log_s = time.time() - t
+    X, Y = np.concatenate(X), np.concatenate(Y)
+    rng = np.random.default_rng(0)
+    order = rng.permutation(len(X))
+    tr, te = order[: len(X) * 3 // 4], order[len(X) * 3 // 4:]
+    m = cb.CostModel(0, seed=9)
+    t = time.time()
+    m.train(X[tr], Y[tr], epochs=1500, batch=64, lr=2e-3, seed=4)
+    train_s = time.time() - t
+    pred = m.predict(X[te])
+    cells = (2 ** X[:, 1]) * (2 ** X[:, 0] - 1)
+    a = np.exp(np.mean(np.log(Y[tr, 0] / cells[tr])))
+    ana = np.stack([a * cells[te], 4 * cells[te]], 1)
+    err_mlp = np.mean(np.abs(np.log(pred / Y[te])), 0)
+    err_ana = np.mean(np.abs(np.log(ana / Y[te])), 0)
+    out = {"mode": "cfg5", "num_chars_cfg2": N2, "num_chars_cfg4": N4, "graph_prep_s": prep_s,
+           "logs": {"requests": len(X), "by_kind": {k: src.count(k) for k in sorted(set(src))},
+                    "seconds": log_s},
+           "cost_model": {"train": len(tr), "held_out": len(te), "train_seconds": train_s,
+                          "mlp_mean_abs_log_err": {"time": float(err_mlp[0]), "bytes": float(err_mlp[1])},
+                          "analytic_mean_abs_log_err": {"time": float(err_ana[0]),
+                                                        "bytes": float(err_ana[1])}}}
+    # stream on the config-4 graph
+    short = g4.gen_reads(4000, 6001, 150, 150, sub_rate=0.006, indel_rate=0.003, n_rate=0.001).to_list()
+    longr = [r for r in make_reads(g4, 3000, 6002, len_max=10000) if len(r) >= 1000]
+    tbr = g4.gen_reads(400, 6003, 150, 1000, sub_rate=0.01, indel_rate=0.005).to_list()
+    mix = []
+    pick = np.random.default_rng(6).random(8000)
+    si = li = ti = 0
+    for u in pick:
+        if u < 0.80:
+            mix.append((short[si % len(short)], cb.REQ_SCORE)); si += 1
+        elif u < 0.96:
+            mix.append((longr[li % len(longr)], cb.REQ_SCORE)); li += 1
+        else:
+            mix.append((tbr[ti % len(tbr)], cb.REQ_TRACEBACK)); ti += 1
+    mean_len = float(np.mean([len(r) for r, _ in mix]))
+    # capacity: the 64-slot lane advances 64 reads a row-step; its row-step
+    # time from the score logs (a read of L bases spends L row-steps)
+    y_sc = Y[[i for i, k in enumerate(src) if k == "cfg4-score"]]
+    x_sc = X[[i for i, k in enumerate(src) if k == "cfg4-score"]]
+    ms_per_row = float(np.median(y_sc[:, 0] / (2 ** x_sc[:, 0] - 1)))
+    lane_gcups = 64 * N4 / (ms_per_row * 1e6)
+    rate = 0.8 * lane_gcups * 1e9 / (mean_len * N4)
+    n = max(16, min(len(mix), int(rate * args.cfg5_window_s)))
+    mix = mix[:n]
+    arrivals = np.cumsum(np.random.default_rng(7).exponential(1.0 / rate, n))
+    srv = cb.Server(ctx4, cost_model=m, slots=64, tb_workers=2, footprint=cb.FP_MODEL,
+                    queue_capacity=4096, arena_bytes=64 << 20)
+    tickets = [None] * n
+    res = {}
+
+    def producer():
+        t1 = time.perf_counter()
+        for i, ((r, mode), at) in enumerate(zip(mix, arrivals)):
+            d = at - (time.perf_counter() - t1)
+            if d > 0:
+                time.sleep(d)
+            tickets[i] = srv.submit(r, mode)
+
+    t = time.time()
+    th = threading.Thread(target=producer)
+    th.start()
+    while th.is_alive() or len(res) < n:
+        for d in srv.poll(1024, 50):
+            res[d["ticket"]] = d
+    th.join()
+    stream_s = time.time() - t
+    st = srv.stats()
+    srv.close()
+    ok = all(res[t]["status"] == cb.OK for t in tickets)
+    lat = {}
+    for mode, name in ((cb.REQ_SCORE, "score"), (cb.REQ_TRACEBACK, "traceback")):
+        v = np.array([(res[t]["done_ns"] - res[t]["submit_ns"]) / 1e6 for t, (r, md) in zip(tickets, mix)
+                      if md == mode])
+        lat[name] = {"n": int(len(v)), "p50_ms": float(np.percentile(v, 50)) if len(v) else None,
+                     "p99_ms": float(np.percentile(v, 99)) if len(v) else None}
+    # the model's error on the stream's own requests
+    xs = np.array([cb.cm_features(ctx4, len(r), md, 64 if md == cb.REQ_SCORE else 1, 500, 0)
+                   for r, md in mix], np.float32)
+    ys = np.array([max(1e-3, (res[t]["done_ns"] - res[t]["start_ns"]) / 1e6) for t in tickets])
+    ps = m.predict(xs)[:, 0]
+    cs = N4 * np.array([len(r) for r, _ in mix], np.float64)
+    m.close()
+    ctx4.close()
+    out["stream"] = {"arrivals": "Poisson", "window_s": args.cfg5_window_s, "requests": n,
+                     "rate_per_s": rate, "load": 0.8, "lane_capacity_gcups": lane_gcups,
+                     "mix": "80% 150 bp @1% score, 16% 1-10 kbp @5% score, 4% 150-1000 bp traceback",
+                     "admission": "traceback footprint predicted by the cost model (CHSGA_FP_MODEL)",
+                     "all_ok": ok, "seconds": stream_s, "gcups": st["gcups"], "latency": lat,
+                     "model_time_mean_abs_log_err": float(np.mean(np.abs(np.log(ps / ys)))),
+                     "analytic_time_mean_abs_log_err": float(np.mean(np.abs(np.log(a * cs / ys))))}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def ctypes_labels(g):
     import ctypes
     v = g.view()
@@ -671,6 +850,8 @@ def main():
         return run_traceback_cfg1(args)
     if args.launch_compare:
         return run_launch_compare(args)
+    if args.cfg5:
+        return run_cfg5(args)
     ws, rank, local = dist_env()
     if ws > 1:
         import torch

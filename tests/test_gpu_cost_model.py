@@ -113,3 +113,60 @@ def test_trained_model_beats_analytic_fallback(small_graph):
         np.testing.assert_array_equal(res[t]["ops"], ops)
         assert res[t]["peak_bytes"] <= budget and res[t]["predicted_ms"] > 0
     ctx.close()
+
+
+def _server_logs(ctx, g, n_chars, reads, mode, slots, k=500, cap=0):
+    srv = cb.Server(ctx, slots=slots, tb_workers=1, tb_k=k, tb_cap_bytes=cap)
+    tk = [srv.submit(r, mode) for r in reads]
+    res = srv.collect()
+    srv.close()
+    x, y = [], []
+    for t, r in zip(tk, reads):
+        d = res[t]
+        assert d["status"] == cb.OK
+        x.append(cb.cm_features(ctx, len(r), mode, slots if mode == cb.REQ_SCORE else 1, k, cap))
+        by = d["peak_bytes"] if mode == cb.REQ_TRACEBACK else 4.0 * (n_chars + 32) + len(r)
+        y.append([max(1e-3, (d["done_ns"] - d["start_ns"]) / 1e6), by])
+    return x, y
+
+
+def test_gain_on_config2_size_graph_logs():
+    # logs of the library's own runs on the 5 Mbp config-2 graph: score
+    # requests at two slot counts, full-matrix and checkpointed tracebacks;
+    # the network trained on 3/4 of them predicts the held-out quarter's
+    # device time and bytes better than the analytic |V| x |read| model
+    g = cb.HostGraph.generate(**cb.GRAPH_CONFIGS["cfg2"])
+    g.build_pch()
+    n = g.stats()["num_chars"]
+    ctx = cb.Context(0).load(g)
+    try:
+        def mk(count, seed, lo, hi):
+            return g.gen_reads(count, seed, lo, hi, sub_rate=0.02, indel_rate=0.03).to_list()
+        x, y = [], []
+        for slots, seed in ((16, 1), (64, 2)):
+            a, b = _server_logs(ctx, g, n, mk(48, seed, 150, 3000), cb.REQ_SCORE, slots)
+            x += a
+            y += b
+        a, b = _server_logs(ctx, g, n, mk(24, 3, 100, 1500), cb.REQ_TRACEBACK, 1)
+        x += a
+        y += b
+        for k, seed in ((64, 4), (200, 5)):
+            a, b = _server_logs(ctx, g, n, mk(8, seed, 300, 1500), cb.REQ_TRACEBACK, 1, k=k,
+                                cap=12 * n * 4)
+            x += a
+            y += b
+    finally:
+        ctx.close()
+    x, y = np.array(x, np.float32), np.array(y, np.float32)
+    order = np.random.default_rng(1).permutation(len(x))
+    tr, te = order[: len(x) * 3 // 4], order[len(x) * 3 // 4:]
+    m = cb.CostModel(0, seed=9)
+    m.train(x[tr], y[tr], epochs=1500, batch=32, lr=2e-3, seed=4)
+    pred = m.predict(x[te])
+    m.close()
+    cells = n * (2 ** x[:, 0] - 1)
+    a = np.exp(np.mean(np.log(y[tr, 0] / cells[tr])))
+    ana = np.stack([a * cells[te], 4 * cells[te]], 1)
+    err_mlp = np.mean(np.abs(np.log(pred / y[te])), 0)
+    err_ana = np.mean(np.abs(np.log(ana / y[te])), 0)
+    assert err_mlp[0] < err_ana[0] and err_mlp[1] < err_ana[1], (err_mlp, err_ana)
