@@ -82,6 +82,7 @@ def parse():
                    help="launch-mode comparison instead of the contract line: the same reads at 1, 8 "
                         "and 128 slots as CUDA-graph chains and as persistent launches, device time, "
                         "scores compared")
+    p.add_argument("--shapes", default="1,8,128", help="with --launch-compare: slot counts to compare")
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
     p.add_argument("--plain-reads", type=int, default=64,
                    help="reads of the first timed batch (drawn at random) run through the plain path")
@@ -554,9 +555,9 @@ def run_launch_compare(args):
     N = g.stats()["num_chars"]
     ctx = cb.Context(0).load(g)
     out = {"mode": "launch-compare", "num_chars": N, "shapes": []}
-    shapes = [(1, make_reads(g, 4, 31_000, len_max=1000)),
-              (8, make_reads(g, 32, 31_001, len_max=2000)),
-              (128, make_reads(g, 256, 31_002, len_max=2000))]
+    want = [int(x) for x in args.shapes.split(",")]
+    shapes = [(R, make_reads(g, n, seed, len_max=lm)) for R, n, seed, lm in
+              ((1, 4, 31_000, 1000), (8, 32, 31_001, 2000), (128, 256, 31_002, 2000)) if R in want]
     for R, reads in shapes:
         cells = sum(len(r) for r in reads) * N
         runs = [("graphs", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16)),
@@ -582,8 +583,9 @@ def run_launch_compare(args):
         out["shapes"].append(rec)
     # per-kernel-group times at one slot (CUDA events between the groups)
     pctx = cb.Context(0, flags=cb.FLAG_PROFILE).load(g)
+    one = make_reads(g, 4, 31_000, len_max=1000)
     for name, rk in (("tile_row", cb.ROW_AUTO), ("direct_row", cb.ROW_DIRECT)):
-        pctx.align_scores_batched(shapes[0][1][:2], slots=1, row_kernel=rk)
+        pctx.align_scores_batched(one[:2], slots=1, row_kernel=rk)
         pr = pctx.profile()
         st = max(1, pr["row_launches"])
         out["plain_profile_" + name] = {k.replace("_ms", "_us"): 1e3 * pr[k] / st for k in
@@ -792,7 +794,7 @@ def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits):
     w = pr["row_bits"] // 8
     row_avg_s = pr["row_ms"] / max(1, pr["row_launches"]) / 1e3
     ab = algorithmic_row_bytes(st, R, multi, w)
-    auto16 = "k_row_stream" if R >= 64 else ("k_row_dpx" if R >= 2 else "k_row_direct")
+    auto16 = "k_row_stream" if R >= 64 else ("k_row_dpx" if R >= 2 else "k_row_t1")
     kname = {cb.ROW_DIRECT: "k_row_direct", cb.ROW_TILED: "k_row_tiled", cb.ROW_DPX: "k_row_dpx",
              cb.ROW_STREAM: "k_row_stream"}.get(
         opts["row_kernel"] if R > 1 else 0, auto16 if pr["row_bits"] == 16 else "k_row_direct")

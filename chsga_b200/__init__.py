@@ -16,7 +16,9 @@ from typing import Dict, List, Optional, Sequence, Tuple
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libchsga.so")
+# CHSGA_LIBRARY: another build of the library (the checked build,
+# chsga_b200/lib_checked/libchsga.so)
+LIB_PATH = os.environ.get("CHSGA_LIBRARY") or os.path.join(_HERE, "lib", "libchsga.so")
 BIN_DIR = os.path.join(_HERE, "bin")
 
 if not os.path.exists(LIB_PATH):

@@ -168,8 +168,9 @@ struct chsga_ctx {
   const chsga::TopDev* top_sel = nullptr;  // this call's top region (nullptr: the default)
   int num_sms = 148;
   chsga::RowKernel row_kernel = chsga::RowKernel::Auto;
-  // launch mode of the one-read path (chsga_align_scores): CHSGA_LAUNCH_*
-  uint32_t plain_mode = CHSGA_LAUNCH_PERSISTENT;
+  // launch mode of the one-read path (chsga_align_scores): CHSGA_LAUNCH_*;
+  // CUDA graphs, measured faster than the persistent kernel at one slot
+  uint32_t plain_mode = CHSGA_LAUNCH_GRAPHS;
   chsga::DevArr<unsigned char> reads;
   chsga::DevArr<chsga::dev::ReadDesc> queue;
   uint32_t qmask = 0xFFFFFFFFu;                      // queue ring mask (serving), else linear
@@ -369,6 +370,28 @@ const dev::RowTiles* row_tiles(chsga_ctx& c) {
   }
 }
 
+// The checked build (CHSGA_CHECKED): fails with CHSGA_ERR_INTERNAL, naming
+// the check site and the index, when a kernel met a graph-derived index out
+// of range (kernels.cuh, CHSGA_CHK), and clears the record. Every entry
+// point that takes a context runs it after its own work, which has finished
+// on the device by then. The regular build has no record and no check.
+void check_indices() {
+#ifdef CHSGA_CHECKED
+  CK(cudaDeviceSynchronize());
+  unsigned int flag = 0;
+  unsigned long long first = 0;
+  CK(cudaMemcpyFromSymbol(&flag, dev::g_chk_fail, sizeof(flag)));
+  if (!flag) return;
+  CK(cudaMemcpyFromSymbol(&first, dev::g_chk_first, sizeof(first)));
+  const unsigned int zero = 0;
+  const unsigned long long zero64 = 0;
+  CK(cudaMemcpyToSymbol(dev::g_chk_fail, &zero, sizeof(zero)));
+  CK(cudaMemcpyToSymbol(dev::g_chk_first, &zero64, sizeof(zero64)));
+  fail(CHSGA_ERR_INTERNAL, "device index check failed at check site " + std::to_string(first >> 40) +
+                               ", index " + std::to_string(first & 0xFFFFFFFFFFull));
+#endif
+}
+
 // Fails with CHSGA_ERR_TIMEOUT if a kernel's bounded wait expired.
 void check_device_error(chsga_ctx& c, SlotBufs& b) {
   dev::StepCtl fin{};
@@ -476,10 +499,10 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
     if constexpr (std::is_same_v<ST, uint16_t> && R >= 8)
       dev::k_pull_lv16<R><<<nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s>>>(
-          BVc, lo, hi, c.g->gd.up_head.p, c.g->gd.up_in.p, b.ctl.p);
+          BVc, lo, hi, c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
     else
       dev::k_pull_lv<R, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-          BVc, lo, hi, c.g->gd.up_head.p, c.g->gd.up_in.p, b.ctl.p);
+          BVc, lo, hi, c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[2], s));
   if (top.h.K) {
@@ -769,7 +792,8 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
                           d.lab4.p,     d.sv_off.p,   d.sv_dev.p,   d.vin_off.p,  d.vin_src.p,
                           d.vin_srcv.p, d.dv_first.p, d.dv_len.p,   d.dv_s.p,     d.up_off.p,
                           d.up_in.p,    d.dn_off.p,   d.dn_in.p,    d.istr_off.p, d.istr_src.p,
-                          d.dn_head.p,  d.up_head.p,  d.fin.p};
+                          d.dn_head.p,  d.up_head.p,  d.fin.p,
+                          (uint32_t)L.vin_srcv.size(), (uint32_t)L.up_in.size(), (uint32_t)L.dn_in.size()};
   lg->nul_label = false;
   for (uint32_t i = 0; i < g.num_chars; ++i) {
     lg->nul_label |= g.labels[i] == '\0';
@@ -1713,6 +1737,7 @@ chsga_status guarded_ctx(chsga_ctx* c, F&& f) {
   try {
     if (c) set_device(*c);
     f();
+    check_indices();
     return CHSGA_OK;
   } catch (const ChsgaError& e) {
     if (c) c->err = e.what();
@@ -2015,7 +2040,7 @@ chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out) {
       if (std::string(rk) == "stream") c->row_kernel = RowKernel::Stream;
     }
     // CHSGA_PLAIN_LAUNCH=stream|graphs|persistent: how chsga_align_scores
-    // runs its row-steps (default persistent, where it applies)
+    // runs its row-steps (default graphs)
     if (const char* pl = std::getenv("CHSGA_PLAIN_LAUNCH")) {
       if (std::string(pl) == "stream") c->plain_mode = CHSGA_LAUNCH_STREAM;
       if (std::string(pl) == "graphs") c->plain_mode = CHSGA_LAUNCH_GRAPHS;

@@ -63,7 +63,59 @@ struct GraphPtrs {
   const uint4* dn_head;
   const uint4* up_head;
   const uint4* fin;
+  uint32_t n_vin, n_up, n_dn;  // entries of vin_srcv, up_in, dn_in (index checks)
 };
+
+// ---------------------------------------------------------------------------
+// Index checks of the CHSGA_CHECKED build (make CHECKED=1): every index a
+// kernel reads from a graph array before using it as an address is checked
+// against the size of what it indexes. An index out of range records the
+// check site and the index (the first failure wins) and is replaced by 0, so
+// the access stays inside the array; the host turns the record into
+// CHSGA_ERR_INTERNAL after the call. No trap, no fault. Without
+// CHSGA_CHECKED the checks compile to the index itself.
+// ---------------------------------------------------------------------------
+#ifdef CHSGA_CHECKED
+static __device__ unsigned int g_chk_fail;
+static __device__ unsigned long long g_chk_first;  // site << 40 | index
+__device__ __forceinline__ void chk_fail(uint64_t i, uint32_t site) {
+  if (atomicCAS(&g_chk_fail, 0u, 1u) == 0u)
+    atomicExch(&g_chk_first, ((unsigned long long)site << 40) | (i & 0xFFFFFFFFFFull));
+}
+__device__ __forceinline__ uint32_t chk_index(uint64_t i, uint64_t n, uint32_t site) {
+  if (i < n) return (uint32_t)i;
+  chk_fail(i, site);
+  return 0;
+}
+// an index below n, else 0
+#define CHSGA_CHK(i, n, site) (::chsga::dev::chk_index((uint64_t)(i), (uint64_t)(n), (site)))
+// lo <= hi <= n, else the empty range 0..0
+#define CHSGA_CHK_RANGE(lo, hi, n, site)                                                  \
+  do {                                                                                    \
+    if (!((uint64_t)(lo) <= (uint64_t)(hi) && (uint64_t)(hi) <= (uint64_t)(n))) {         \
+      ::chsga::dev::chk_fail((uint64_t)(hi), (site));                                     \
+      (lo) = 0;                                                                           \
+      (hi) = 0;                                                                           \
+    }                                                                                     \
+  } while (0)
+// the chars f .. e-1 of one vertex: f < e <= n, else the one char 0
+#define CHSGA_CHK_CHARS(f, e, n, site)                                                    \
+  do {                                                                                    \
+    if (!((uint64_t)(f) < (uint64_t)(e) && (uint64_t)(e) <= (uint64_t)(n))) {            \
+      ::chsga::dev::chk_fail((uint64_t)(e), (site));                                      \
+      (f) = 0;                                                                            \
+      (e) = 1;                                                                            \
+    }                                                                                     \
+  } while (0)
+#else
+#define CHSGA_CHK(i, n, site) (i)
+#define CHSGA_CHK_RANGE(lo, hi, n, site) \
+  do {                                   \
+  } while (0)
+#define CHSGA_CHK_CHARS(f, e, n, site) \
+  do {                                 \
+  } while (0)
+#endif
 
 // Per-slot word for the current row-step, written by k_advance.
 constexpr uint32_t SW_CODE = 0xFFu;         // read base code: 0..3 A,C,G,T, 4 special, 5 none
@@ -378,8 +430,9 @@ __global__ void __launch_bounds__(256, 3) k_row_direct(GraphPtrs g, const ST* __
       fix[v] = DEFER && (w & SW_FIX) != 0;
       any_fix |= fix[v];
     }
-    const uint32_t f = __ldg(g.sv_off + s), e = __ldg(g.sv_off + s + 1);
-    const uint32_t d = __ldg(g.sv_dev + s);
+    uint32_t f = __ldg(g.sv_off + s), e = __ldg(g.sv_off + s + 1);
+    CHSGA_CHK_CHARS(f, e, g.N, 1);
+    const uint32_t d = CHSGA_CHK(__ldg(g.sv_dev + s), g.S, 3);
     const size_t so = (size_t)lane * V;
     constexpr int kBig = 0x3fffffff;
     IV<V> F;
@@ -404,9 +457,10 @@ __global__ void __launch_bounds__(256, 3) k_row_direct(GraphPtrs g, const ST* __
         delta[v] = (int)((code[v] >> key) & 1u);
         t.v[v] = dprev.v[v] + 1;
       }
-      const uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
+      uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
+      CHSGA_CHK_RANGE(k0, k1, g.n_vin, 4);
       for (uint32_t k = k0; k < k1; ++k) {
-        const uint32_t su = __ldg(g.vin_srcv + k);
+        const uint32_t su = CHSGA_CHK(__ldg(g.vin_srcv + k), g.S, 5);
         const IV<V> du = ld_nc<V>(FL + (size_t)(2 * su + 1) * R + so);
 #pragma unroll
         for (int v = 0; v < V; ++v) t.v[v] = min(t.v[v], du.v[v] + delta[v]);
@@ -632,9 +686,11 @@ __device__ __forceinline__ void dpx_vertex(const GraphPtrs& g, uint32_t s, int l
       }
       any_fix |= fmask[p] != 0;
     }
-    const uint32_t f = __ldg(g.sv_off + s), e = __ldg(g.sv_off + s + 1);
-    const uint32_t d = __ldg(g.sv_dev + s);
-    const uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
+    uint32_t f = __ldg(g.sv_off + s), e = __ldg(g.sv_off + s + 1);
+    CHSGA_CHK_CHARS(f, e, g.N, 1);
+    const uint32_t d = CHSGA_CHK(__ldg(g.sv_dev + s), g.S, 3);
+    uint32_t k0 = __ldg(g.vin_off + s), k1 = __ldg(g.vin_off + s + 1);
+    CHSGA_CHK_RANGE(k0, k1, g.n_vin, 4);
     KeyWindow kw(g.lab4, f);
     U2<P> F;
 #pragma unroll
@@ -654,7 +710,7 @@ __device__ __forceinline__ void dpx_vertex(const GraphPtrs& g, uint32_t s, int l
         t.h[p] = dprev.h[p] + ONES;
       }
       for (uint32_t k = k0; k < k1; ++k) {
-        const uint32_t su = __ldg(g.vin_srcv + k);
+        const uint32_t su = CHSGA_CHK(__ldg(g.vin_srcv + k), g.S, 5);
         const U2<P> du = ldp_src<P, COH>(FL + (size_t)(2 * su + 1) * R + so);
 #pragma unroll
         for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(du.h[p], delta[p], t.h[p]);
@@ -819,9 +875,11 @@ __device__ __forceinline__ void stream_run(const GraphPtrs& g, uint32_t run_inde
       const uint32_t s = s0 + lane;
       mf = __ldg(g.sv_off + s);
       me = __ldg(g.sv_off + s + 1);
-      md = __ldg(g.sv_dev + s);
+      md = CHSGA_CHK(__ldg(g.sv_dev + s), g.S, 3);
       mk0 = __ldg(g.vin_off + s);
       mk1 = __ldg(g.vin_off + s + 1);
+      CHSGA_CHK_CHARS(mf, me, g.N, 1);
+      CHSGA_CHK_RANGE(mk0, mk1, g.n_vin, 4);
     }
     const uint32_t cb = __shfl_sync(FULL, mf, 0), ce = __shfl_sync(FULL, me, nv - 1);
     // previous-row scores of the run's chars cb .. ce-1: row c goes to slot
@@ -833,13 +891,13 @@ __device__ __forceinline__ void stream_run(const GraphPtrs& g, uint32_t run_inde
       cp_async_commit();
     }
     const uint32_t kb = __shfl_sync(FULL, mk0, 0), ke = __shfl_sync(FULL, mk1, nv - 1);
-    const uint32_t src_a = kb + lane < ke ? __ldg(g.vin_srcv + kb + lane) : 0u;
-    const uint32_t src_b = kb + 32 + lane < ke ? __ldg(g.vin_srcv + kb + 32 + lane) : 0u;
+    const uint32_t src_a = kb + lane < ke ? CHSGA_CHK(__ldg(g.vin_srcv + kb + lane), g.S, 5) : 0u;
+    const uint32_t src_b = kb + 32 + lane < ke ? CHSGA_CHK(__ldg(g.vin_srcv + kb + 32 + lane), g.S, 5) : 0u;
     // source vertex of in-edge k (k warp-uniform)
     auto src_at = [&](uint32_t k) -> uint32_t {
       const uint32_t i = k - kb;
       const uint32_t a = __shfl_sync(FULL, src_a, i & 31), b = __shfl_sync(FULL, src_b, i & 31);
-      return i < 32 ? a : i < 64 ? b : __ldg(g.vin_srcv + k);
+      return i < 32 ? a : i < 64 ? b : CHSGA_CHK(__ldg(g.vin_srcv + k), g.S, 5);
     };
     auto prefetch = [&](uint32_t i, StreamVertex<P>& v) {
       v.f = __shfl_sync(FULL, mf, i);
@@ -1075,6 +1133,15 @@ __device__ __forceinline__ void row_t1_tile(const GraphPtrs& g, const T1Ptrs& t,
   constexpr int BIG = 0x3fffffff;
   const int lane = threadIdx.x & 31;
   const uint4 td = __ldg(t.desc + tile);
+#ifdef CHSGA_CHECKED
+  // a tile outside the graph, or larger than a warp's lanes and vertex slots,
+  // is skipped whole (every lane reads the same descriptor)
+  if (!(td.x < td.y && td.y <= g.N && td.z < td.w && td.w <= g.S && td.w - td.z <= (uint32_t)kT1VertMax &&
+        ((td.y - 1) >> 3) - (td.x >> 3) < 32u)) {
+    if ((threadIdx.x & 31) == 0) chk_fail(tile, 6);
+    return;
+  }
+#endif
   const uint32_t cb = td.x, ce = td.y, sb = td.z, nv = td.w - td.z;
   const uint32_t q = (cb >> 3) + lane;
   const bool lv = q <= ((ce - 1) >> 3);
@@ -1100,17 +1167,18 @@ __device__ __forceinline__ void row_t1_tile(const GraphPtrs& g, const T1Ptrs& t,
     int G = 0, X = BIG;
     if (fix) G = ldu16<COH>(FL + 2 * (size_t)sv) - (int)r.x;
     if (!init) {
-      if (r.z != 0xFFFFFFFFu) X = ldu16<COH>(FL + 2 * (size_t)r.z + 1);
-      if (r.w != 0xFFFFFFFFu) X = min(X, ldu16<COH>(FL + 2 * (size_t)r.w + 1));
+      if (r.z != 0xFFFFFFFFu) X = ldu16<COH>(FL + 2 * (size_t)CHSGA_CHK(r.z, g.S, 10) + 1);
+      if (r.w != 0xFFFFFFFFu) X = min(X, ldu16<COH>(FL + 2 * (size_t)CHSGA_CHK(r.w, g.S, 10) + 1));
       if (r.y & 0x80000000u) {
-        const uint32_t k1 = __ldg(g.vin_off + sv + 1);
-        for (uint32_t k = __ldg(g.vin_off + sv) + 2; k < k1; ++k)
-          X = min(X, ldu16<COH>(FL + 2 * (size_t)__ldg(g.vin_srcv + k) + 1));
+        uint32_t k0 = __ldg(g.vin_off + sv) + 2, k1 = __ldg(g.vin_off + sv + 1);
+        CHSGA_CHK_RANGE(k0, k1, g.n_vin, 4);
+        for (uint32_t k = k0; k < k1; ++k)
+          X = min(X, ldu16<COH>(FL + 2 * (size_t)CHSGA_CHK(__ldg(g.vin_srcv + k), g.S, 5) + 1));
       }
     }
     s_G[v] = G;
     s_X[v] = X;
-    s_d[v] = r.y & 0x7FFFFFFFu;
+    s_d[v] = CHSGA_CHK(r.y & 0x7FFFFFFFu, g.S, 9);
   }
   __syncwarp();
   // vertex index (within the tile) of the char before this lane's first head
@@ -1524,7 +1592,7 @@ __device__ __forceinline__ void pull_item(ST* BV, uint32_t d, int lane, const ui
   bool changed = false;
   for (uint32_t k = k0; k < k1; ++k) {
     const int2 ew = __ldg(edges + k);
-    const IV<V> x = ld_src<V, COH>(BV + (size_t)ew.x * R + so);
+    const IV<V> x = ld_src<V, COH>(BV + (size_t)CHSGA_CHK(ew.x, 2 * (uint64_t)d, 12) * R + so);
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const int c = x.v[v] + ew.y;
@@ -1557,11 +1625,15 @@ __global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, 
 // ---------------------------------------------------------------------------
 template <int R, typename ST, bool COH>
 __device__ __forceinline__ void pull_lv_item(ST* BV, uint32_t d, int lane, const uint4* __restrict__ head,
-                                             const int2* __restrict__ edges) {
+                                             const int2* __restrict__ edges, uint32_t n_edges) {
   constexpr int V = Lanes<R>::V;
-  const uint4 h = __ldg(head + 2 * (size_t)d);
+  uint4 h = __ldg(head + 2 * (size_t)d);
   if (h.x == h.y) return;
-  const uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
+  uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
+  CHSGA_CHK_RANGE(h.x, h.y, n_edges, 11);
+  if (h.x == h.y) return;
+  h.z = CHSGA_CHK(h.z, 2 * (uint64_t)d, 12);
+  h2.x = CHSGA_CHK(h2.x, 2 * (uint64_t)d, 12);
   const size_t so = (size_t)lane * V;
   ST* p = BV + (size_t)(2 * d) * R + so;
   IV<V> f = ld<V>(p);
@@ -1586,7 +1658,7 @@ __device__ __forceinline__ void pull_lv_item(ST* BV, uint32_t d, int lane, const
   }
   for (uint32_t k = h.x + 2; k < h.y; ++k) {
     const int2 ew = __ldg(edges + k);
-    relax(ld_src<V, COH>(BV + (size_t)ew.x * R + so), ew.y);
+    relax(ld_src<V, COH>(BV + (size_t)CHSGA_CHK(ew.x, 2 * (uint64_t)d, 12) * R + so), ew.y);
   }
   if (changed) st<V>(p, f);
 }
@@ -1594,14 +1666,14 @@ __device__ __forceinline__ void pull_lv_item(ST* BV, uint32_t d, int lane, const
 template <int R, typename ST>
 __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t lo, uint32_t hi,
                                                  const uint4* __restrict__ head,
-                                                 const int2* __restrict__ edges,
+                                                 const int2* __restrict__ edges, uint32_t n_edges,
                                                  const StepCtl* __restrict__ ctl) {
   constexpr int G = Lanes<R>::G;
   if (!ctl->any_active) return;
   const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t d = lo + (uint32_t)(gt / G);
   if (d >= hi) return;
-  pull_lv_item<R, ST, false>(BV, d, (int)(gt % G), head, edges);
+  pull_lv_item<R, ST, false>(BV, d, (int)(gt % G), head, edges, n_edges);
 }
 
 // ---------------------------------------------------------------------------
@@ -1616,12 +1688,16 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
 template <int R, bool COH>
 __device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lane,
                                                const uint4* __restrict__ head,
-                                               const int2* __restrict__ edges) {
+                                               const int2* __restrict__ edges, uint32_t n_edges) {
   static_assert(R >= 8 && R % 8 == 0, "8 slots per lane");
   constexpr int B = 4;
-  const uint4 h = __ldg(head + 2 * (size_t)d);
-  const uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
+  uint4 h = __ldg(head + 2 * (size_t)d);
+  uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
   if (h.x == h.y) return;
+  CHSGA_CHK_RANGE(h.x, h.y, n_edges, 11);
+  if (h.x == h.y) return;
+  h.z = CHSGA_CHK(h.z, 2 * (uint64_t)d, 12);
+  h2.x = CHSGA_CHK(h2.x, 2 * (uint64_t)d, 12);
   const size_t so = (size_t)lane * 8;
   uint4* p = reinterpret_cast<uint4*>(BV + (size_t)(2 * d) * R + so);
   auto src = [&](uint32_t i) { return ldv4<COH>(BV + (size_t)i * R + so); };
@@ -1648,7 +1724,7 @@ __device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lan
     uint4 x[B];
 #pragma unroll
     for (int q = 0; q < B; ++q)
-      if (k + q < h.y) x[q] = src((uint32_t)e[q].x);
+      if (k + q < h.y) x[q] = src(CHSGA_CHK((uint32_t)e[q].x, 2 * (uint64_t)d, 12));
 #pragma unroll
     for (int q = 0; q < B; ++q)
       if (k + q < h.y) relax(x[q], (uint32_t)e[q].y);
@@ -1664,14 +1740,14 @@ __device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lan
 template <int R>
 __global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, uint32_t lo,
                                                    uint32_t hi, const uint4* __restrict__ head,
-                                                   const int2* __restrict__ edges,
+                                                   const int2* __restrict__ edges, uint32_t n_edges,
                                                    const StepCtl* __restrict__ ctl) {
   constexpr int G = R / 8;
   if (!ctl->any_active) return;
   const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t d = lo + (uint32_t)(gt / G);
   if (d >= hi) return;
-  pull_lv16_item<R, false>(BV, d, (int)(gt % G), head, edges);
+  pull_lv16_item<R, false>(BV, d, (int)(gt % G), head, edges, n_edges);
 }
 
 // ---------------------------------------------------------------------------
@@ -1692,8 +1768,19 @@ __device__ __forceinline__ void down_item(const GraphPtrs& g, ST* BV, ST* T, ST*
     // independent loads first: the list head, the vertex words, the first
     // score and the raw last score (the last entry is never written here;
     // for a one-char vertex it is unused)
-    const uint4 h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
-    const uint4 m = __ldg(g.fin + d);
+    uint4 h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
+    uint4 m = __ldg(g.fin + d);
+    CHSGA_CHK_RANGE(h.x, h.y, g.n_dn, 13);
+    h.z = CHSGA_CHK(h.z, 2 * (uint64_t)g.S, 14);
+    m.z = CHSGA_CHK(m.z, g.S, 15);
+#ifdef CHSGA_CHECKED
+    // the vertex's chars first .. first + len - 1 (the fix-up writes them)
+    if (!(m.y >= 1 && m.x < g.N && m.y <= g.N - m.x)) {
+      chk_fail(m.x, 16);
+      m.x = 0;
+      m.y = 1;
+    }
+#endif
     IV<V> f = ld<V>(p);
     const IV<V> raw = ld<V>(BV + (size_t)(2 * d + 1) * R + so);
     if (h.y > h.x) {
@@ -1711,7 +1798,7 @@ __device__ __forceinline__ void down_item(const GraphPtrs& g, ST* BV, ST* T, ST*
       relax(ld_src<V, COH>(BV + (size_t)h.z * R + so), (int)h.w);
       for (uint32_t k = h.x + 1; k < h.y; ++k) {
         const int2 ew = __ldg(g.dn_in + k);
-        relax(ld_src<V, COH>(BV + (size_t)ew.x * R + so), ew.y);
+        relax(ld_src<V, COH>(BV + (size_t)CHSGA_CHK(ew.x, 2 * (uint64_t)g.S, 14) * R + so), ew.y);
       }
       if (changed) st<V>(p, f);
     }
@@ -1817,8 +1904,11 @@ __device__ __forceinline__ void down16_item(const GraphPtrs& g, uint16_t* BV, ui
   const size_t so = (size_t)lane * 8;
   uint4* p = reinterpret_cast<uint4*>(BV + (size_t)(2 * d) * R + so);
   auto src = [&](uint32_t i) { return ldv4<COH>(BV + (size_t)i * R + so); };
-  const uint4 h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
-  const uint4 m = __ldg(g.fin + d);
+  uint4 h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
+  uint4 m = __ldg(g.fin + d);
+  CHSGA_CHK_RANGE(h.x, h.y, g.n_dn, 13);
+  h.z = CHSGA_CHK(h.z, 2 * (uint64_t)g.S, 14);
+  m.z = CHSGA_CHK(m.z, g.S, 15);
   const uint4 f0 = *p;
   const uint4 raw = *reinterpret_cast<const uint4*>(BV + (size_t)(2 * d + 1) * R + so);
   uint4 f = f0;
@@ -1833,7 +1923,7 @@ __device__ __forceinline__ void down16_item(const GraphPtrs& g, uint16_t* BV, ui
     relax(src(h.z), h.w);
     for (uint32_t k = h.x + 1; k < h.y; ++k) {
       const int2 ew = __ldg(g.dn_in + k);
-      relax(src((uint32_t)ew.x), (uint32_t)ew.y);
+      relax(src(CHSGA_CHK((uint32_t)ew.x, 2 * (uint64_t)g.S, 14)), (uint32_t)ew.y);
     }
     if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
   }
@@ -1922,6 +2012,18 @@ inline uint32_t top_chunk_for(uint32_t K, size_t smem_cap) {
   return c;
 }
 
+// Edge count of a chunk of the top-region schedule (negative: warp chunk);
+// the checked build clamps it to the chunk buffer.
+__device__ __forceinline__ int top_chunk_count(int y, uint32_t cap) {
+#ifdef CHSGA_CHECKED
+  if ((uint32_t)abs(y) > cap) {
+    chk_fail((uint32_t)abs(y), 19);
+    return y < 0 ? -(int)cap : (int)cap;
+  }
+#endif
+  return y;
+}
+
 // The region's sweeps for slot r by the whole block (top_smem: the block's
 // dynamic shared memory, top_smem_bytes of the region). Returns false when a
 // bounded wait expired (StepCtl::error is set).
@@ -1943,7 +2045,8 @@ __device__ __forceinline__ bool top_body(ST* BV, const TopPtrs& t, StepCtl* ctl,
   if (threadIdx.x == 0) {
     for (uint32_t c = 0; c < kTopBufs && c < t.nchunks; ++c) {
       const int2 ch = t.chunk[c];
-      bulk_load(ebuf + c * t.chunk_cap, t.edges + ch.x, (uint32_t)abs(ch.y) * 8, &bar[c]);
+      bulk_load(ebuf + c * t.chunk_cap, t.edges + ch.x, (uint32_t)abs(top_chunk_count(ch.y, t.chunk_cap)) * 8,
+                &bar[c]);
     }
   }
   int n_next = t.nchunks ? __ldg(&t.chunk[0].y) : 0;
@@ -1984,7 +2087,7 @@ __device__ __forceinline__ bool top_body(ST* BV, const TopPtrs& t, StepCtl* ctl,
   uint32_t c = 0;
   for (; c < t.nchunks; ++c) {
     const uint32_t b = c % kTopBufs;
-    const int n = n_next;
+    const int n = top_chunk_count(n_next, t.chunk_cap);
     if (c + 1 < t.nchunks) n_next = __ldg(&t.chunk[c + 1].y);
     // a thread whose wait expires flags it, skips the chunk and still
     // reaches the barrier below, so the whole block leaves the loop together
@@ -1994,14 +2097,14 @@ __device__ __forceinline__ bool top_body(ST* BV, const TopPtrs& t, StepCtl* ctl,
     if (ok && n >= 0) {
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int2 x = e[i];
-        atomicMin(&sm[2 * (x.x >> 16)], sm[x.x & 0xFFFF] + x.y);
+        atomicMin(&sm[2 * CHSGA_CHK(x.x >> 16, t.K + 1, 17)], sm[CHSGA_CHK(x.x & 0xFFFF, 2 * t.K + 2, 18)] + x.y);
       }
     } else if (ok && threadIdx.x < 32) {
       // warp chunk: a run of small levels in rounds of 32 edges, each level
       // whole rounds, the rounds ordered by the warp barrier
       for (int i = threadIdx.x; i < -n; i += 32) {
         const int2 x = e[i];
-        atomicMin(&sm[2 * (x.x >> 16)], sm[x.x & 0xFFFF] + x.y);
+        atomicMin(&sm[2 * CHSGA_CHK(x.x >> 16, t.K + 1, 17)], sm[CHSGA_CHK(x.x & 0xFFFF, 2 * t.K + 2, 18)] + x.y);
         __syncwarp();
       }
     }
@@ -2010,7 +2113,8 @@ __device__ __forceinline__ bool top_body(ST* BV, const TopPtrs& t, StepCtl* ctl,
     if (threadIdx.x == 0 && c + kTopBufs < t.nchunks) {
       fence_async_shared();
       const int2 ch = t.chunk[c + kTopBufs];
-      bulk_load(ebuf + b * t.chunk_cap, t.edges + ch.x, (uint32_t)abs(ch.y) * 8, &bar[b]);
+      bulk_load(ebuf + b * t.chunk_cap, t.edges + ch.x, (uint32_t)abs(top_chunk_count(ch.y, t.chunk_cap)) * 8,
+                &bar[b]);
     }
   }
   if (s_fail) {

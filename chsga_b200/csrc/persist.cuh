@@ -26,11 +26,16 @@
 namespace chsga {
 namespace dev {
 
+// The arrival counter, the generation word and the abort word sit on
+// separate 128-byte lines, so the blocks spinning on the generation do not
+// slow the arrivals down.
 struct GridBar {
   unsigned int count;  // arrivals at the current barrier
+  unsigned int pad0[31];
   unsigned int gen;    // barriers completed (only grows)
+  unsigned int pad1[31];
   unsigned int abort;  // nonzero: some block gave up waiting
-  unsigned int pad;
+  unsigned int pad2[31];
 };
 
 constexpr uint32_t ERR_GRID_WAIT = 4;
@@ -41,9 +46,19 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ unsigned int atom_add_acq_rel(unsigned int* p, unsigned int v) {
+  unsigned int old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void red_add_release(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 // Every block of the grid meets here. False when this block's wait gave up
-// or another block's did (the caller returns at once).
+// or another block's did (the caller returns at once). The block barrier
+// orders every thread's writes before thread 0's release-acquire arrival;
+// the acquire load that sees the new generation orders the reads after it.
 __device__ __forceinline__ bool grid_sync(GridBar* gb, unsigned int& gen, StepCtl* ctl,
                                           unsigned long long limit_ns = kGridWaitNs) {
   __shared__ int s_ok;
@@ -51,11 +66,9 @@ __device__ __forceinline__ bool grid_sync(GridBar* gb, unsigned int& gen, StepCt
   if (threadIdx.x == 0) {
     int ok = 1;
     const unsigned int g0 = gen;
-    __threadfence();
-    if (atomicAdd(&gb->count, 1u) == gridDim.x - 1) {
-      atomicExch(&gb->count, 0u);
-      __threadfence();
-      atomicAdd(&gb->gen, 1u);
+    if (atom_add_acq_rel(&gb->count, 1u) == gridDim.x - 1) {
+      gb->count = 0;  // nobody arrives again before the generation moves
+      red_add_release(&gb->gen, 1u);
     } else {
       const unsigned long long t0 = global_ns();
       unsigned int polls = 0;
@@ -74,7 +87,6 @@ __device__ __forceinline__ bool grid_sync(GridBar* gb, unsigned int& gen, StepCt
       atomicExch(&gb->abort, 1u);
       atomicOr(&ctl->error, ERR_GRID_WAIT);
     }
-    __threadfence();
     gen = g0 + 1;
     s_ok = ok;
   }
@@ -203,12 +215,13 @@ __global__ void __launch_bounds__(PersistShape<R>::threads, 1) k_persist(Persist
         if constexpr (R >= 8) {
           constexpr int G = R / 8;
           for (uint64_t it = gtid; it < (uint64_t)(hi - lo) * G; it += nthreads)
-            pull_lv16_item<R, true>(a.BV, lo + (uint32_t)(it / G), (int)(it % G), g.up_head, g.up_in);
+            pull_lv16_item<R, true>(a.BV, lo + (uint32_t)(it / G), (int)(it % G), g.up_head, g.up_in,
+                                    g.n_up);
         } else {
           constexpr int G = Lanes<R>::G;
           for (uint64_t it = gtid; it < (uint64_t)(hi - lo) * G; it += nthreads)
             pull_lv_item<R, uint16_t, true>(a.BV, lo + (uint32_t)(it / G), (int)(it % G), g.up_head,
-                                            g.up_in);
+                                            g.up_in, g.n_up);
         }
         if (!grid_sync(a.bar, gen, a.ctl)) return;
       }
