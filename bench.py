@@ -544,7 +544,8 @@ def run_traceback_cfg1(args):
 
 def run_launch_compare(args):
     """Device time of the same reads through the CUDA-graph chain of
-    row-step kernels and through the persistent row-step kernel, at 1, 8 and
+    row-step kernels (with and without programmatic dependent launch between
+    its kernels) and through the persistent row-step kernel, at 1, 8 and
     128 slots, on the config-2-mix graph; the one-slot chain also with the
     one-thread-per-vertex row kernel (the plain path's row kernel before the
     tile kernel). Every run's scores must equal the first's. One JSON line."""
@@ -554,6 +555,9 @@ def run_launch_compare(args):
     g = make_graph(args.backbone)
     N = g.stats()["num_chars"]
     ctx = cb.Context(0).load(g)
+    os.environ["CHSGA_PDL"] = "1"  # read when a context opens
+    ctx_pdl = cb.Context(0).load(g)
+    del os.environ["CHSGA_PDL"]
     out = {"mode": "launch-compare", "num_chars": N, "shapes": []}
     want = [int(x) for x in args.shapes.split(",")]
     shapes = [(R, make_reads(g, n, seed, len_max=lm)) for R, n, seed, lm in
@@ -561,6 +565,7 @@ def run_launch_compare(args):
     for R, reads in shapes:
         cells = sum(len(r) for r in reads) * N
         runs = [("graphs", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16)),
+                ("graphs_pdl", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16, ctx=ctx_pdl)),
                 ("persistent", dict(use_graphs=cb.LAUNCH_PERSISTENT, steps_per_graph=16)),
                 ("persistent_64", dict(use_graphs=cb.LAUNCH_PERSISTENT, steps_per_graph=64))]
         if R == 1:
@@ -569,11 +574,13 @@ def run_launch_compare(args):
         rec = {"slots": R, "reads": len(reads), "bases": sum(len(r) for r in reads)}
         ref = None
         for name, kw in runs:
-            ctx.align_scores_batched(reads, slots=R, **kw)  # warm-up (graph build, caches)
+            kw = dict(kw)
+            cx = kw.pop("ctx", ctx)
+            cx.align_scores_batched(reads, slots=R, **kw)  # warm-up (graph build, caches)
             best = None
             for _ in range(3):
-                sc = ctx.align_scores_batched(reads, slots=R, **kw)
-                p = ctx.profile()
+                sc = cx.align_scores_batched(reads, slots=R, **kw)
+                p = cx.profile()
                 best = p["total_ms"] if best is None else min(best, p["total_ms"])
             if ref is None:
                 ref = sc
@@ -591,6 +598,7 @@ def run_launch_compare(args):
         out["plain_profile_" + name] = {k.replace("_ms", "_us"): 1e3 * pr[k] / st for k in
                                         ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")}
     pctx.close()
+    ctx_pdl.close()
     ctx.close()
     print(json.dumps(out), flush=True)
     return 0

@@ -171,6 +171,8 @@ struct chsga_ctx {
   // launch mode of the one-read path (chsga_align_scores): CHSGA_LAUNCH_*;
   // CUDA graphs, measured faster than the persistent kernel at one slot
   uint32_t plain_mode = CHSGA_LAUNCH_GRAPHS;
+  // programmatic dependent launch between the kernels of a row-step (CHSGA_PDL)
+  bool pdl = false;
   chsga::DevArr<unsigned char> reads;
   chsga::DevArr<chsga::dev::ReadDesc> queue;
   uint32_t qmask = 0xFFFFFFFFu;                      // queue ring mask (serving), else linear
@@ -401,12 +403,34 @@ void check_device_error(chsga_ctx& c, SlotBufs& b) {
           "a bounded device-side wait expired (code " + std::to_string(fin.error) + ")");
 }
 
+// Launches a kernel of the row-step chain. With programmatic dependent launch
+// (chsga_ctx::pdl, CHSGA_PDL=1) the launch may begin while the kernel before
+// it on the stream drains; every chain kernel starts with
+// griddepcontrol.wait (dev::pdl_wait), which holds it until that kernel has
+// finished and its writes are visible, so results are the same either way.
+template <typename... KArgs, typename... Args>
+void chain_launch(const chsga_ctx& c, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                  cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  if (c.pdl) {
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+  }
+  CK(cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...));
+}
+
 template <int R>
 void launch_advance(chsga_ctx& c, SlotBufs& b, int prime, cudaStream_t s) {
-  dev::k_advance<R><<<1, 128, 0, s>>>(b.slots.p, c.queue.p, c.reads.p, b.best.p, c.res_score.p,
-                                      c.res_vertex.p, c.res_t0.p, c.res_t1.p, b.word.p, b.ctl.p,
-                                      c.g->L.special, prime, c.qmask, c.done_ring.p, match_n(c));
-  check_launch();
+  chain_launch(c, dev::k_advance<R>, 1, 128, 0, s, b.slots.p, c.queue.p, c.reads.p, b.best.p, c.res_score.p,
+               c.res_vertex.p, c.res_t0.p, c.res_t1.p, b.word.p, b.ctl.p, c.g->L.special, prime, c.qmask,
+               c.done_ring.p, match_n(c));
 }
 
 // CUDA events between the kernel groups of one row-step (profiling mode).
@@ -455,8 +479,8 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   if constexpr (std::is_same_v<ST, uint16_t> && R == 1) {
     // one read: a warp per tile of whole vertices, a lane per 8 chars
     if (c.g->t1.ntiles && c.row_kernel == RowKernel::Auto) {
-      dev::k_row_t1<DEFER><<<(c.g->t1.ntiles + dev::kT1Warps - 1) / dev::kT1Warps, dev::kT1Warps * 32, 0,
-                             s>>>(c.g->gp, c.g->t1, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+      chain_launch(c, dev::k_row_t1<DEFER>, (c.g->t1.ntiles + dev::kT1Warps - 1) / dev::kT1Warps,
+                   dev::kT1Warps * 32, 0, s, c.g->gp, c.g->t1, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
       done = true;
     }
   }
@@ -467,14 +491,14 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
         if (c.row_kernel != RowKernel::Dpx) {
           const uint64_t runs = ((uint64_t)L.S + 31) / 32;
           constexpr unsigned tpb = dev::kStreamWarps * 32;
-          dev::k_row_stream<R, DEFER><<<nblocks(runs * 32, tpb), tpb, dev::stream_smem_bytes(R), s>>>(
-              c.g->gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+          chain_launch(c, dev::k_row_stream<R, DEFER>, nblocks(runs * 32, tpb), tpb, dev::stream_smem_bytes(R), s,
+                       c.g->gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
           done = true;
         }
       }
       if (!done) {
-        dev::k_row_dpx<R, DEFER><<<nblocks((uint64_t)L.S * dev::Pairs<R>::G), 256, 0, s>>>(
-            c.g->gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+        chain_launch(c, dev::k_row_dpx<R, DEFER>, nblocks((uint64_t)L.S * dev::Pairs<R>::G), 256, 0, s,
+                     c.g->gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
         done = true;
       }
     }
@@ -482,44 +506,44 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   if constexpr (R >= 32) {
     if (!done && c.row_kernel == RowKernel::Tiled) {
       if (const dev::RowTiles* rt = row_tiles<R, ST>(c)) {
-        dev::k_row_tiled<R, DEFER, ST>
-            <<<c.num_sms, dev::kRowThreads, dev::row_smem_bytes(dev::row_slot_bytes(*rt), rt->nslots, R),
-               s>>>(c.g->gp, *rt, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+        chain_launch(c, dev::k_row_tiled<R, DEFER, ST>, c.num_sms, dev::kRowThreads,
+                     dev::row_smem_bytes(dev::row_slot_bytes(*rt), rt->nslots, R), s, c.g->gp, *rt, D, T, BVc,
+                     FL, b.word.p, b.best.p, b.ctl.p);
         done = true;
       }
     }
   }
   if (!done)
-    dev::k_row_direct<R, DEFER, ST><<<nblocks((uint64_t)L.S * G), 256, 0, s>>>(
-        c.g->gp, D, T, BVc, FL, b.word.p, b.best.p, b.ctl.p);
+    chain_launch(c, dev::k_row_direct<R, DEFER, ST>, nblocks((uint64_t)L.S * G), 256, 0, s, c.g->gp, D, T,
+                 BVc, FL, b.word.p, b.best.p, b.ctl.p);
   if (ev) CK(cudaEventRecord(ev->e[1], s));
   const uint32_t fl = top.h.first_level;
   for (uint32_t l = 0; l < fl; ++l) {
     if (L.lvl_up_edges[l] == 0) continue;
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
     if constexpr (std::is_same_v<ST, uint16_t> && R >= 8)
-      dev::k_pull_lv16<R><<<nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s>>>(
-          BVc, lo, hi, c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
+      chain_launch(c, dev::k_pull_lv16<R>, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, BVc, lo, hi,
+                   c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
     else
-      dev::k_pull_lv<R, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-          BVc, lo, hi, c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
+      chain_launch(c, dev::k_pull_lv<R, ST>, nblocks((uint64_t)(hi - lo) * G), 256, 0, s, BVc, lo, hi,
+                   c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[2], s));
   if (top.h.K) {
     if (!top.h.upg.empty())
-      dev::k_pull<R, ST><<<nblocks((uint64_t)top.h.K * G), 256, 0, s>>>(
-          BVc, top.h.K0, L.S, top.upg_off.p, top.upg.p, top.h.K0, b.ctl.p);
-    dev::k_top<R, ST><<<R, kTopThreads, dev::top_smem_bytes(top.h.K, top.ptrs.chunk_cap), s>>>(BVc, top.ptrs, b.word.p,
-                                                                       b.ctl.p);
+      chain_launch(c, dev::k_pull<R, ST>, nblocks((uint64_t)top.h.K * G), 256, 0, s, BVc, top.h.K0, L.S,
+                   top.upg_off.p, top.upg.p, top.h.K0, b.ctl.p);
+    chain_launch(c, dev::k_top<R, ST>, R, kTopThreads, dev::top_smem_bytes(top.h.K, top.ptrs.chunk_cap), s, BVc,
+                 top.ptrs, b.word.p, b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[3], s));
   auto down = [&](uint32_t lo, uint32_t mid, uint32_t hi) {
     if constexpr (std::is_same_v<ST, uint16_t> && DEFER && R >= 8)
-      dev::k_down16<R><<<nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s>>>(
-          c.g->gp, BVc, FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
+      chain_launch(c, dev::k_down16<R>, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, c.g->gp, BVc, FL, lo,
+                   mid, hi, b.word.p, b.best.p, b.ctl.p);
     else
-      dev::k_down<R, !DEFER, ST><<<nblocks((uint64_t)(hi - lo) * G), 256, 0, s>>>(
-          c.g->gp, BVc, T, FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
+      chain_launch(c, dev::k_down<R, !DEFER, ST>, nblocks((uint64_t)(hi - lo) * G), 256, 0, s, c.g->gp, BVc, T,
+                   FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
   };
   if (fl == 0) {
     down(0, 0, L.S);
@@ -531,8 +555,8 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   }
   if constexpr (std::is_same_v<ST, uint16_t> && !DEFER && R >= 2) {
     if (sink)
-      dev::k_store_rows<R><<<(L.N + 63) / 64, 256, 0, s>>>(T, b.slots.p, sink->mats, sink->pitch, L.N,
-                                                          b.ctl.p);
+      chain_launch(c, dev::k_store_rows<R>, (L.N + 63) / 64, 256, 0, s, T, b.slots.p, sink->mats, sink->pitch,
+                   L.N, b.ctl.p);
   }
   if (ev) CK(cudaEventRecord(ev->e[4], s));
   launch_advance<R>(c, b, 0, s);
@@ -1939,6 +1963,7 @@ chsga_ctx* fork_context(chsga_ctx& p) {
   c->num_sms = p.num_sms;
   c->row_kernel = p.row_kernel;
   c->plain_mode = p.plain_mode;
+  c->pdl = p.pdl;
   CK(cudaSetDevice(c->device));
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
@@ -2046,6 +2071,7 @@ chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out) {
       if (std::string(pl) == "graphs") c->plain_mode = CHSGA_LAUNCH_GRAPHS;
       if (std::string(pl) == "persistent") c->plain_mode = CHSGA_LAUNCH_PERSISTENT;
     }
+    if (const char* pd = std::getenv("CHSGA_PDL")) c->pdl = std::string(pd) == "1";
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     size_t free_b = 0, total_b = 0;

@@ -314,6 +314,11 @@ __device__ __forceinline__ uint32_t mismatch_mask(int b, int special, int match_
   return m;
 }
 
+// Programmatic dependent launch: a row-step kernel launched while the kernel
+// before it on the stream drains waits here until that kernel has finished
+// and its writes are visible (a no-op for a kernel launched the usual way).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -406,6 +411,7 @@ __global__ void __launch_bounds__(256, 3) k_row_direct(GraphPtrs g, const ST* __
                                                        const uint32_t* __restrict__ slot_word,
                                                        unsigned long long* __restrict__ best,
                                                        const StepCtl* __restrict__ ctl) {
+  pdl_wait();
   constexpr int G = Lanes<R>::G, V = Lanes<R>::V;
   __shared__ unsigned long long sm_best[R];
   const bool ending_any = ctl->any_ending != 0;
@@ -754,6 +760,7 @@ __global__ void __launch_bounds__(256, 4) k_row_dpx(GraphPtrs g, const uint16_t*
                                                     const uint32_t* __restrict__ slot_word,
                                                     unsigned long long* __restrict__ best,
                                                     const StepCtl* __restrict__ ctl) {
+  pdl_wait();
   constexpr int G = Pairs<R>::G;
   __shared__ unsigned long long sm_best[R];
   const bool ending_any = ctl->any_ending != 0;
@@ -1038,6 +1045,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
     GraphPtrs g, const uint16_t* __restrict__ D, uint16_t* __restrict__ T, uint16_t* __restrict__ BV,
     const uint16_t* __restrict__ FL, const uint32_t* __restrict__ slot_word,
     unsigned long long* __restrict__ best, const StepCtl* __restrict__ ctl) {
+  pdl_wait();
   static_assert(Pairs<R>::G == 32, "one full warp per vertex");
   extern __shared__ __align__(16) uint16_t ring_smem[];
   __shared__ unsigned long long sm_best[R];
@@ -1279,6 +1287,7 @@ __global__ void __launch_bounds__(kT1Warps * 32) k_row_t1(GraphPtrs g, T1Ptrs t,
                                                           const uint32_t* __restrict__ slot_word,
                                                           unsigned long long* __restrict__ best,
                                                           const StepCtl* __restrict__ ctl) {
+  pdl_wait();
   __shared__ int s_G[kT1Warps][kT1VertMax], s_X[kT1Warps][kT1VertMax];
   __shared__ uint32_t s_d[kT1Warps][kT1VertMax];
   __shared__ unsigned long long sm_best[1];
@@ -1369,6 +1378,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_row_tiled(GraphPtrs g, RowTi
                                                              const uint32_t* __restrict__ slot_word,
                                                              unsigned long long* __restrict__ best,
                                                              StepCtl* __restrict__ ctl) {
+  pdl_wait();
   static_assert(R >= 32, "one warp per vertex");
   constexpr int V = Lanes<R>::V;
   constexpr uint32_t PC = R * sizeof(ST);  // bytes per char (and per FL entry)
@@ -1610,6 +1620,7 @@ __global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, 
                                               const uint32_t* __restrict__ off,
                                               const int2* __restrict__ edges, uint32_t base,
                                               const StepCtl* __restrict__ ctl) {
+  pdl_wait();
   constexpr int G = Lanes<R>::G;
   if (!ctl->any_active) return;
   const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1668,6 +1679,7 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
                                                  const uint4* __restrict__ head,
                                                  const int2* __restrict__ edges, uint32_t n_edges,
                                                  const StepCtl* __restrict__ ctl) {
+  pdl_wait();
   constexpr int G = Lanes<R>::G;
   if (!ctl->any_active) return;
   const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1742,6 +1754,7 @@ __global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, ui
                                                    uint32_t hi, const uint4* __restrict__ head,
                                                    const int2* __restrict__ edges, uint32_t n_edges,
                                                    const StepCtl* __restrict__ ctl) {
+  pdl_wait();
   constexpr int G = R / 8;
   if (!ctl->any_active) return;
   const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1874,6 +1887,7 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
                                               const uint32_t* __restrict__ slot_word,
                                               unsigned long long* __restrict__ best,
                                               const StepCtl* __restrict__ ctl) {
+  pdl_wait();
   constexpr int G = Lanes<R>::G;
   __shared__ unsigned long long sm_best[R];
   const bool ending_any = ctl->any_ending != 0;
@@ -1956,6 +1970,7 @@ __global__ void __launch_bounds__(256) k_down16(GraphPtrs g, uint16_t* __restric
                                                 const uint32_t* __restrict__ slot_word,
                                                 unsigned long long* __restrict__ best,
                                                 const StepCtl* __restrict__ ctl) {
+  pdl_wait();
   constexpr int G = R / 8;
   __shared__ unsigned long long sm_best[R];
   const bool ending_any = ctl->any_ending != 0;
@@ -2140,6 +2155,7 @@ template <int R, typename ST>
 __global__ void __launch_bounds__(1024) k_top(ST* __restrict__ BV, TopPtrs t,
                                               const uint32_t* __restrict__ slot_word,
                                               StepCtl* __restrict__ ctl) {
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char top_smem[];
   if (!ctl->any_active) return;
   const int r = blockIdx.x;
@@ -2161,6 +2177,7 @@ __global__ void __launch_bounds__(256) k_store_rows(const uint16_t* __restrict__
                                                     uint16_t* const* __restrict__ mats,
                                                     size_t pitch, uint32_t N,
                                                     const StepCtl* __restrict__ ctl) {
+  pdl_wait();
   constexpr int C = 64;
   __shared__ uint16_t tile[C][R + 2];
   __shared__ uint16_t* dst[R];
@@ -2324,6 +2341,7 @@ __global__ void __launch_bounds__(128) k_advance(SlotState* __restrict__ slots,
                                                  int prime, uint32_t qmask = 0xFFFFFFFFu,
                                                  CompletionRec* __restrict__ done_ring = nullptr,
                                                  int match_n = 0) {
+  pdl_wait();
   advance_body<R>(slots, queue, reads, best, res_score, res_vertex, res_t0, res_t1, slot_word, ctl,
                   special, prime, qmask, done_ring, match_n);
 }

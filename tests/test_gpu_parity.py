@@ -191,3 +191,21 @@ def test_plain_path_every_launch_mode(small_graph, ctx_small, oracle_small, mode
     # the one-thread-per-vertex row kernel gives the same scores
     got_d = ctx_small.align_scores_batched(reads, slots=1, use_graphs=mode, row_kernel=cb.ROW_DIRECT)
     np.testing.assert_array_equal(got_d, want)
+
+
+def test_programmatic_dependent_launch_matches_oracle(small_graph, oracle_small, monkeypatch):
+    # CHSGA_PDL=1: each row-step kernel may launch while the one before it
+    # drains and waits on griddepcontrol.wait before reading its results
+    g, files, reads = small_graph
+    monkeypatch.setenv("CHSGA_PDL", "1")
+    ctx = cb.Context(0).load(g)
+    try:
+        want = oracle_small.scores(reads)
+        np.testing.assert_array_equal(ctx.align_scores(reads), want)
+        for slots in (8, 64, 128):
+            np.testing.assert_array_equal(ctx.align_scores_batched(reads, slots=slots), want)
+        labels = open(files[3], "rb").read().replace(b"\n", b"")
+        ops, score, _ = ctx.align_traceback(reads[0])
+        assert score == want[0] and orc.rescore(ops, reads[0], labels) == (want[0], len(reads[0]) - 1)
+    finally:
+        ctx.close()
