@@ -611,7 +611,8 @@ def _served_logs(cb, ctx, g, reads, mode, slots, k=500, cap=0, tb_workers=1):
     slot's share of the engine's 16-bit rows for a score read."""
     import numpy as np
     N = g.stats()["num_chars"]
-    srv = cb.Server(ctx, slots=slots, tb_workers=tb_workers, tb_k=k, tb_cap_bytes=cap,
+    # the score lane has at least 2 slots; tracebacks run one read at a time
+    srv = cb.Server(ctx, slots=max(2, slots), tb_workers=tb_workers, tb_k=k, tb_cap_bytes=cap,
                     queue_capacity=4096, arena_bytes=64 << 20)
     tk = [srv.submit(r, mode) for r in reads]
     res = srv.collect()

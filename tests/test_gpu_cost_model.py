@@ -116,7 +116,9 @@ def test_trained_model_beats_analytic_fallback(small_graph):
 
 
 def _server_logs(ctx, g, n_chars, reads, mode, slots, k=500, cap=0):
-    srv = cb.Server(ctx, slots=slots, tb_workers=1, tb_k=k, tb_cap_bytes=cap)
+    # a server's score lane has at least 2 slots; traceback requests run one
+    # read at a time whatever it has
+    srv = cb.Server(ctx, slots=max(2, slots), tb_workers=1, tb_k=k, tb_cap_bytes=cap)
     tk = [srv.submit(r, mode) for r in reads]
     res = srv.collect()
     srv.close()
