@@ -558,6 +558,10 @@ def run_launch_compare(args):
     os.environ["CHSGA_PDL"] = "1"  # read when a context opens
     ctx_pdl = cb.Context(0).load(g)
     del os.environ["CHSGA_PDL"]
+    os.environ["CHSGA_PULL_COOP"] = "1"
+    ctx_coop = cb.Context(0).load(g)
+    pctx_coop = cb.Context(0, flags=cb.FLAG_PROFILE).load(g)
+    del os.environ["CHSGA_PULL_COOP"]
     out = {"mode": "launch-compare", "num_chars": N, "shapes": []}
     want = [int(x) for x in args.shapes.split(",")]
     shapes = [(R, make_reads(g, n, seed, len_max=lm)) for R, n, seed, lm in
@@ -571,6 +575,9 @@ def run_launch_compare(args):
         if R == 1:
             runs.append(("graphs_direct_row", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16,
                                                    row_kernel=cb.ROW_DIRECT)))
+        if R >= 64:
+            runs.append(("graphs_pull_coop", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16,
+                                                  ctx=ctx_coop)))
         rec = {"slots": R, "reads": len(reads), "bases": sum(len(r) for r in reads)}
         ref = None
         for name, kw in runs:
@@ -597,7 +604,18 @@ def run_launch_compare(args):
         st = max(1, pr["row_launches"])
         out["plain_profile_" + name] = {k.replace("_ms", "_us"): 1e3 * pr[k] / st for k in
                                         ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")}
+    # per-kernel-group times at 128 slots, upward levels as k_pull_lv16 and as k_pull_lv16c
+    if 128 in want:
+        reads128 = make_reads(g, 128, 31_003, len_max=1000)
+        for name, cx in (("pull16", pctx), ("pull16c", pctx_coop)):
+            cx.align_scores_batched(reads128, slots=128)
+            pr = cx.profile()
+            st = max(1, pr["row_launches"])
+            out["batched_profile_" + name] = {k.replace("_ms", "_us"): 1e3 * pr[k] / st for k in
+                                              ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")}
     pctx.close()
+    pctx_coop.close()
+    ctx_coop.close()
     ctx_pdl.close()
     ctx.close()
     print(json.dumps(out), flush=True)

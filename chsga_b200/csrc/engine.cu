@@ -173,6 +173,8 @@ struct chsga_ctx {
   uint32_t plain_mode = CHSGA_LAUNCH_GRAPHS;
   // programmatic dependent launch between the kernels of a row-step (CHSGA_PDL)
   bool pdl = false;
+  // upward levels with the lane group's cooperative edge loads, 64+ slots (CHSGA_PULL_COOP)
+  bool pull_coop = false;
   chsga::DevArr<unsigned char> reads;
   chsga::DevArr<chsga::dev::ReadDesc> queue;
   uint32_t qmask = 0xFFFFFFFFu;                      // queue ring mask (serving), else linear
@@ -521,7 +523,14 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   for (uint32_t l = 0; l < fl; ++l) {
     if (L.lvl_up_edges[l] == 0) continue;
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
-    if constexpr (std::is_same_v<ST, uint16_t> && R >= 8)
+    if constexpr (std::is_same_v<ST, uint16_t> && R >= 64) {
+      if (c.pull_coop)
+        chain_launch(c, dev::k_pull_lv16c<R>, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, BVc, lo, hi,
+                     c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
+      else
+        chain_launch(c, dev::k_pull_lv16<R>, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, BVc, lo, hi,
+                     c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
+    } else if constexpr (std::is_same_v<ST, uint16_t> && R >= 8)
       chain_launch(c, dev::k_pull_lv16<R>, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, BVc, lo, hi,
                    c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
     else
@@ -1964,6 +1973,7 @@ chsga_ctx* fork_context(chsga_ctx& p) {
   c->row_kernel = p.row_kernel;
   c->plain_mode = p.plain_mode;
   c->pdl = p.pdl;
+  c->pull_coop = p.pull_coop;
   CK(cudaSetDevice(c->device));
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
@@ -2072,6 +2082,7 @@ chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out) {
       if (std::string(pl) == "persistent") c->plain_mode = CHSGA_LAUNCH_PERSISTENT;
     }
     if (const char* pd = std::getenv("CHSGA_PDL")) c->pdl = std::string(pd) == "1";
+    if (const char* pc = std::getenv("CHSGA_PULL_COOP")) c->pull_coop = std::string(pc) == "1";
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     size_t free_b = 0, total_b = 0;

@@ -1278,8 +1278,11 @@ __device__ __forceinline__ void row_t1_tile(const GraphPtrs& g, const T1Ptrs& t,
   __syncwarp();  // s_G / s_X / s_d are reused by the warp's next tile
 }
 
+#ifndef CHSGA_T1_BLOCKS
+#define CHSGA_T1_BLOCKS 6  // blocks per SM the register budget is sized for (build-time tuning)
+#endif
 template <bool DEFER>
-__global__ void __launch_bounds__(kT1Warps * 32) k_row_t1(GraphPtrs g, T1Ptrs t,
+__global__ void __launch_bounds__(kT1Warps * 32, CHSGA_T1_BLOCKS) k_row_t1(GraphPtrs g, T1Ptrs t,
                                                           const uint16_t* __restrict__ D,
                                                           uint16_t* __restrict__ T,
                                                           uint16_t* __restrict__ BV,
@@ -1761,6 +1764,93 @@ __global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, ui
   const uint32_t d = lo + (uint32_t)(gt / G);
   if (d >= hi) return;
   pull_lv16_item<R, false>(BV, d, (int)(gt % G), head, edges, n_edges);
+}
+
+// ---------------------------------------------------------------------------
+// k_pull_lv16c: k_pull_lv16 with the target's edge list loaded by its lane
+// group at once. A target's G = R / 8 lanes (G >= 8) each load one edge of
+// the list after the two in the head, shuffles hand every edge to every lane,
+// and each lane then issues the gathers of up to kPullBatch edges before it
+// uses any of them. The chain of dependent loads per target is head ->
+// edges -> gathers (the first two gathers start from the head), instead of
+// one round trip per batch of four edges.
+// ---------------------------------------------------------------------------
+constexpr int kPullBatch = 8;
+
+template <int R, bool COH>
+__device__ __forceinline__ void pull_lv16c_item(uint16_t* BV, uint32_t d, int lane,
+                                                const uint4* __restrict__ head,
+                                                const int2* __restrict__ edges, uint32_t n_edges) {
+  constexpr int G = R / 8;
+  static_assert(G >= 8 && G <= 32 && (G & (G - 1)) == 0, "a lane group of 8 to 32 lanes per target");
+  uint4 h = __ldg(head + 2 * (size_t)d);
+  uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
+  if (h.x == h.y) return;
+  CHSGA_CHK_RANGE(h.x, h.y, n_edges, 11);
+  if (h.x == h.y) return;
+  h.z = CHSGA_CHK(h.z, 2 * (uint64_t)d, 12);
+  h2.x = CHSGA_CHK(h2.x, 2 * (uint64_t)d, 12);
+  // every lane of the group has this target: the group's lanes are G
+  // consecutive lanes of the warp
+  const int wl = threadIdx.x & 31;
+  const unsigned gmask = G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (wl & ~(G - 1)));
+  const size_t so = (size_t)lane * 8;
+  uint4* p = reinterpret_cast<uint4*>(BV + (size_t)(2 * d) * R + so);
+  auto src = [&](uint32_t i) { return ldv4<COH>(BV + (size_t)i * R + so); };
+  const uint4 f0 = *p;
+  uint4 f = f0;
+  auto relax = [&](const uint4& x, uint32_t w) {
+    const uint32_t ww = min(w, 0xFFFFu) * 0x10001u;
+    f.x = __vminu2(f.x, __vaddus2(x.x, ww));
+    f.y = __vminu2(f.y, __vaddus2(x.y, ww));
+    f.z = __vminu2(f.z, __vaddus2(x.z, ww));
+    f.w = __vminu2(f.w, __vaddus2(x.w, ww));
+  };
+  const bool two = h.y - h.x > 1;
+  const uint32_t base0 = h.x + 2;
+  // this lane's edge of the first group-sized window after the head's two
+  const int2 mine = base0 + (uint32_t)lane < h.y ? __ldg(edges + base0 + lane) : make_int2(0, 0);
+  const uint4 x0 = src(h.z);
+  uint4 x1 = x0;
+  if (two) x1 = src(h2.x);
+  relax(x0, h.w);
+  if (two) relax(x1, h2.y);
+  int2 win = mine;
+  for (uint32_t base = base0; base < h.y; base += G) {
+    if (base != base0)
+      win = base + (uint32_t)lane < h.y ? __ldg(edges + base + lane) : make_int2(0, 0);
+    const uint32_t cnt = min((uint32_t)G, h.y - base);
+    for (uint32_t q = 0; q < cnt; q += kPullBatch) {
+      uint4 x[kPullBatch];
+      uint32_t w[kPullBatch];
+#pragma unroll
+      for (int b = 0; b < kPullBatch; ++b) {
+        if (q + b < cnt) {
+          const uint32_t sidx = (uint32_t)__shfl_sync(gmask, win.x, (int)(q + b), G);
+          w[b] = (uint32_t)__shfl_sync(gmask, win.y, (int)(q + b), G);
+          x[b] = src(CHSGA_CHK(sidx, 2 * (uint64_t)d, 12));
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < kPullBatch; ++b)
+        if (q + b < cnt) relax(x[b], w[b]);
+    }
+  }
+  if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) k_pull_lv16c(uint16_t* __restrict__ BV, uint32_t lo,
+                                                    uint32_t hi, const uint4* __restrict__ head,
+                                                    const int2* __restrict__ edges, uint32_t n_edges,
+                                                    const StepCtl* __restrict__ ctl) {
+  pdl_wait();
+  constexpr int G = R / 8;
+  if (!ctl->any_active) return;
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  if (d >= hi) return;  // whole lane groups: 256 threads hold whole groups
+  pull_lv16c_item<R, false>(BV, d, (int)(gt % G), head, edges, n_edges);
 }
 
 // ---------------------------------------------------------------------------
