@@ -209,3 +209,20 @@ def test_programmatic_dependent_launch_matches_oracle(small_graph, oracle_small,
         assert score == want[0] and orc.rescore(ops, reads[0], labels) == (want[0], len(reads[0]) - 1)
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("top_vertices", [0, 300])
+def test_cooperative_pull_matches_oracle(small_graph, oracle_small, monkeypatch, top_vertices):
+    # CHSGA_PULL_COOP=1: upward levels load each target's edge list across its
+    # lane group and shuffle it to every lane (64 and 128 slots)
+    g, files, reads = small_graph
+    monkeypatch.setenv("CHSGA_PULL_COOP", "1")
+    ctx = cb.Context(0).load(g)
+    try:
+        mix = list(reads) + g.gen_reads(30, 23, 1, 500, sub_rate=0.03, indel_rate=0.02).to_list()
+        want = oracle_small.scores(mix)
+        for slots in (64, 128):
+            got = ctx.align_scores_batched(mix, slots=slots, top_vertices=top_vertices)
+            np.testing.assert_array_equal(got, want)
+    finally:
+        ctx.close()
