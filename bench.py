@@ -662,7 +662,8 @@ def run_cfg5(args):
       stream   Poisson arrivals on the config-4 graph for --cfg5-window-s
                seconds at ~80% of the score capacity measured in the logs:
                80% 150 bp at 1% error and 16% log-uniform 1-10 kbp at 5%
-               error as score requests, 4% 150-1000 bp traceback requests,
+               error as score requests, 4% 150-600 bp traceback requests
+               (k = 100, full matrices up to 200 bases),
                tracebacks admitted by the model's predicted footprint
                (CHSGA_FP_MODEL); p50/p99 per kind, GCUPS, the model's error on
                the stream. The 50,000-read stream of the configuration would
@@ -697,10 +698,13 @@ def run_cfg5(args):
     ctx4 = cb.Context(0).load(g4)
     add(*_served_logs(cb, ctx4, g4, make_reads(g4, 64, 5101, len_max=2000), cb.REQ_SCORE, 64)[:2],
         "cfg4-score")
-    add(*_served_logs(cb, ctx4, g4, make_reads(g4, 8, 5102, len_max=1000), cb.REQ_TRACEBACK, 1)[:2],
-        "cfg4-tb-full")
-    add(*_served_logs(cb, ctx4, g4, g4.gen_reads(4, 5103, 1500, 3000, sub_rate=0.02, indel_rate=0.03)
-                      .to_list(), cb.REQ_TRACEBACK, 1, k=500)[:2], "cfg4-tb-ckpt")
+    # on the 139 M-char graph a 16-bit row is 278 MB: full matrices up to 200
+    # bases, checkpointed above that with k = 100 (101-row segments, 28 GB)
+    cap4 = 200 * N4 * 4
+    add(*_served_logs(cb, ctx4, g4, g4.gen_reads(8, 5102, 100, 200, sub_rate=0.01, indel_rate=0.005)
+                      .to_list(), cb.REQ_TRACEBACK, 1, k=100, cap=cap4)[:2], "cfg4-tb-full")
+    add(*_served_logs(cb, ctx4, g4, g4.gen_reads(4, 5103, 400, 1500, sub_rate=0.02, indel_rate=0.03)
+                      .to_list(), cb.REQ_TRACEBACK, 1, k=100, cap=cap4)[:2], "cfg4-tb-ckpt")
     log_s = time.time() - t
     X, Y = np.concatenate(X), np.concatenate(Y)
     rng = np.random.default_rng(0)
@@ -726,7 +730,7 @@ def run_cfg5(args):
     # stream on the config-4 graph
     short = g4.gen_reads(4000, 6001, 150, 150, sub_rate=0.006, indel_rate=0.003, n_rate=0.001).to_list()
     longr = [r for r in make_reads(g4, 3000, 6002, len_max=10000) if len(r) >= 1000]
-    tbr = g4.gen_reads(400, 6003, 150, 1000, sub_rate=0.01, indel_rate=0.005).to_list()
+    tbr = g4.gen_reads(400, 6003, 150, 600, sub_rate=0.01, indel_rate=0.005).to_list()
     mix = []
     pick = np.random.default_rng(6).random(8000)
     si = li = ti = 0
@@ -748,8 +752,8 @@ def run_cfg5(args):
     n = max(16, min(len(mix), int(rate * args.cfg5_window_s)))
     mix = mix[:n]
     arrivals = np.cumsum(np.random.default_rng(7).exponential(1.0 / rate, n))
-    srv = cb.Server(ctx4, cost_model=m, slots=64, tb_workers=2, footprint=cb.FP_MODEL,
-                    queue_capacity=4096, arena_bytes=64 << 20)
+    srv = cb.Server(ctx4, cost_model=m, slots=64, tb_workers=2, footprint=cb.FP_MODEL, tb_k=100,
+                    tb_cap_bytes=cap4, queue_capacity=4096, arena_bytes=64 << 20)
     tickets = [None] * n
     res = {}
 
@@ -779,8 +783,8 @@ def run_cfg5(args):
         lat[name] = {"n": int(len(v)), "p50_ms": float(np.percentile(v, 50)) if len(v) else None,
                      "p99_ms": float(np.percentile(v, 99)) if len(v) else None}
     # the model's error on the stream's own requests
-    xs = np.array([cb.cm_features(ctx4, len(r), md, 64 if md == cb.REQ_SCORE else 1, 500, 0)
-                   for r, md in mix], np.float32)
+    xs = np.array([cb.cm_features(ctx4, len(r), md, 64 if md == cb.REQ_SCORE else 1, 100,
+                                  cap4 if md == cb.REQ_TRACEBACK else 0) for r, md in mix], np.float32)
     ys = np.array([max(1e-3, (res[t]["done_ns"] - res[t]["start_ns"]) / 1e6) for t in tickets])
     ps = m.predict(xs)[:, 0]
     cs = N4 * np.array([len(r) for r, _ in mix], np.float64)
@@ -788,7 +792,7 @@ def run_cfg5(args):
     ctx4.close()
     out["stream"] = {"arrivals": "Poisson", "window_s": args.cfg5_window_s, "requests": n,
                      "rate_per_s": rate, "load": 0.8, "lane_capacity_gcups": lane_gcups,
-                     "mix": "80% 150 bp @1% score, 16% 1-10 kbp @5% score, 4% 150-1000 bp traceback",
+                     "mix": "80% 150 bp @1% score, 16% 1-10 kbp @5% score, 4% 150-600 bp traceback (k 100)",
                      "admission": "traceback footprint predicted by the cost model (CHSGA_FP_MODEL)",
                      "all_ok": ok, "seconds": stream_s, "gcups": st["gcups"], "latency": lat,
                      "model_time_mean_abs_log_err": float(np.mean(np.abs(np.log(ps / ys)))),
