@@ -174,6 +174,19 @@ def algorithmic_row_bytes(st, slots, multi, score_bytes):
             + 3 * N / 8 + 12 * S + 4 * e_first)
 
 
+def algorithmic_delta_row_bytes(st, slots, multi):
+    """Bytes one k_row_delta launch must move (128 slots, 2-bit delta rows):
+    the previous and the new row's per-char deltas (2 bits per slot each,
+    N R / 4 bytes per row), the previous and the new raw first score of every
+    vertex (2 R S bytes each), and the boundary, in-edge and graph terms of
+    algorithmic_row_bytes."""
+    N, S = st["num_chars"], st["num_strings"]
+    e_first = st["num_char_edges"] - (N - S)
+    w = 2
+    return (2 * N * slots / 4 + 2 * w * slots * S + w * slots * (S + multi) + w * slots * (S + e_first)
+            + 3 * N / 8 + 12 * S + 4 * e_first)
+
+
 def algorithmic_sweep_bytes(st, lay, slots, score_bytes):
     """Bytes per row-step of the grid-wide sweep kernels below the top
     region (16-byte pull-list heads and vertex words, w bytes per score):
@@ -824,14 +837,15 @@ def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits):
     pctx.close()
     w = pr["row_bits"] // 8
     row_avg_s = pr["row_ms"] / max(1, pr["row_launches"]) / 1e3
-    ab = algorithmic_row_bytes(st, R, multi, w)
-    auto16 = "k_row_stream" if R >= 64 else ("k_row_dpx" if R >= 2 else "k_row_t1")
+    auto16 = "k_row_delta" if R == 128 else ("k_row_stream" if R >= 64 else ("k_row_dpx" if R >= 2 else "k_row_t1"))
     kname = {cb.ROW_DIRECT: "k_row_direct", cb.ROW_TILED: "k_row_tiled", cb.ROW_DPX: "k_row_dpx",
-             cb.ROW_STREAM: "k_row_stream"}.get(
+             cb.ROW_STREAM: "k_row_stream", cb.ROW_DELTA: "k_row_delta"}.get(
         opts["row_kernel"] if R > 1 else 0, auto16 if pr["row_bits"] == 16 else "k_row_direct")
-    if pr["row_bits"] == 32 and kname in ("k_row_stream", "k_row_dpx"):
+    if pr["row_bits"] == 32 and kname in ("k_row_stream", "k_row_dpx", "k_row_delta"):
         kname = "k_row_direct"  # the 16-bit kernels do not run 32-bit rows
-    tr = ncu_traffic() if (R > 1 and pr["row_bits"] == 16) else None
+    ab = algorithmic_delta_row_bytes(st, R, multi) if kname == "k_row_delta" else \
+        algorithmic_row_bytes(st, R, multi, w)
+    tr = ncu_traffic() if kname == "k_row_stream" else None
     total = pr["row_ms"] + pr["sweep_up_ms"] + pr["top_ms"] + pr["sweep_down_ms"] + pr["other_ms"]
     # working set of one row-step: two score rows, BV and FL, graph arrays
     S = st["num_strings"]

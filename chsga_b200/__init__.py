@@ -34,7 +34,7 @@ OP_DELETE, OP_MATCHSUB, OP_INSERT = 0, 1, 2
 REQ_SCORE, REQ_TRACEBACK = 0, 1
 FP_PLAN, FP_MODEL, FP_ANALYTIC = 0, 1, 2
 ORDER_FIFO, ORDER_LONGEST = 0, 1
-ROW_AUTO, ROW_DIRECT, ROW_TILED, ROW_DPX, ROW_STREAM = 0, 1, 2, 3, 4
+ROW_AUTO, ROW_DIRECT, ROW_TILED, ROW_DPX, ROW_STREAM, ROW_DELTA = 0, 1, 2, 3, 4, 5
 LAUNCH_STREAM, LAUNCH_GRAPHS, LAUNCH_PERSISTENT = 0, 1, 2
 FLAG_PROFILE = 1
 FLAG_MATCH_N = 2

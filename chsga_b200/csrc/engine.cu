@@ -123,7 +123,7 @@ struct SlotBufs {
 // Row kernel choice: the DPX kernel for 16-bit rows (default), the direct
 // kernel, or the shared-memory tile-staged kernel (CHSGA_ROW_KERNEL=direct |
 // tiled, for comparisons).
-enum class RowKernel { Auto, Direct, Tiled, Dpx, Stream };
+enum class RowKernel { Auto, Direct, Tiled, Dpx, Stream, Delta };
 
 struct RowTileDev {
   DevArr<int4> rec;
@@ -231,9 +231,12 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
   b->R = R;
   const size_t N = c.g->L.N, S = c.g->L.S;
   if (need_rows) {
-    // bulk tile copies may read up to 16 bytes past the last char
-    b->rows[0].alloc((N + 32) * R * sizeof(ST));
-    b->rows[1].alloc((N + 32) * R * sizeof(ST));
+    // bulk tile copies may read up to 16 bytes past the last char; 128
+    // 16-bit slots may hold delta rows instead (k_row_delta)
+    size_t rb = (N + 32) * R * sizeof(ST);
+    if (std::is_same_v<ST, uint16_t> && R == 128) rb = std::max(rb, dev::delta_row_bytes(N, S));
+    b->rows[0].alloc(rb);
+    b->rows[1].alloc(rb);
   }
   b->BV.alloc(2 * S * R * sizeof(ST));
   b->FL.alloc(2 * (S + 16) * R * sizeof(ST));
@@ -247,6 +250,12 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
     CK(cudaFuncSetAttribute(dev::k_top<R, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)dev::top_smem_bytes(kTopMaxVertices)));
   });
+  if constexpr (std::is_same_v<ST, uint16_t> && R == 128) {
+    once_per_device((const void*)dev::k_row_delta, c.device, [] {
+      CK(cudaFuncSetAttribute(dev::k_row_delta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)dev::delta_smem_bytes()));
+    });
+  }
   if constexpr (std::is_same_v<ST, uint16_t> && R >= 64) {
     once_per_device((const void*)dev::k_row_stream<R, true>, c.device, [] {
       for (auto k : {dev::k_row_stream<R, true>, dev::k_row_stream<R, false>})
@@ -398,12 +407,18 @@ void check_indices() {
 }
 
 // Fails with CHSGA_ERR_TIMEOUT if a kernel's bounded wait expired.
+void require_step_ok(uint32_t error) {
+  require(!(error & dev::ERR_ROW_DELTA), CHSGA_ERR_INTERNAL,
+          "a 2-bit row delta fell outside -1..1 (code " + std::to_string(error) + ")");
+  require(error == 0, CHSGA_ERR_TIMEOUT,
+          "a bounded device-side wait expired (code " + std::to_string(error) + ")");
+}
+
 void check_device_error(chsga_ctx& c, SlotBufs& b) {
   dev::StepCtl fin{};
   CK(cudaMemcpyAsync(&fin, b.ctl.p, sizeof(fin), cudaMemcpyDeviceToHost, c.st));
   CK(cudaStreamSynchronize(c.st));
-  require(fin.error == 0, CHSGA_ERR_TIMEOUT,
-          "a bounded device-side wait expired (code " + std::to_string(fin.error) + ")");
+  require_step_ok(fin.error);
 }
 
 // Launches a kernel of the row-step chain. With programmatic dependent launch
@@ -487,9 +502,20 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
       done = true;
     }
   }
+  if constexpr (std::is_same_v<ST, uint16_t> && DEFER && R == 128) {
+    // 2-bit delta rows (score-only): every step of a run uses this kernel,
+    // so the rows stay in its format from the first admission on
+    if (L.max_len <= 512 && (c.row_kernel == RowKernel::Auto || c.row_kernel == RowKernel::Delta)) {
+      const uint64_t runs = ((uint64_t)L.S + 31) / 32;
+      constexpr unsigned tpb = dev::kStreamWarps * 32;
+      chain_launch(c, dev::k_row_delta, nblocks(runs * 32, tpb), tpb, dev::delta_smem_bytes(), s, c.g->gp, D, T,
+                   BVc, FL, b.word.p, b.best.p, b.ctl.p);
+      done = true;
+    }
+  }
   if constexpr (std::is_same_v<ST, uint16_t> && R >= 2) {
     // packed 16-bit DPX kernels; exact while F + (c - first) stays below 2^16
-    if (L.max_len <= 512 && c.row_kernel != RowKernel::Tiled && c.row_kernel != RowKernel::Direct) {
+    if (!done && L.max_len <= 512 && c.row_kernel != RowKernel::Tiled && c.row_kernel != RowKernel::Direct) {
       if constexpr (R >= 64) {
         if (c.row_kernel != RowKernel::Dpx) {
           const uint64_t runs = ((uint64_t)L.S + 31) / 32;
@@ -766,8 +792,7 @@ void run_queue(chsga_ctx& c, uint32_t n, uint64_t total_rows, uint32_t mode, uin
   cudaEventDestroy(ev[1]);
   dev::StepCtl fin{};
   CK(cudaMemcpy(&fin, b.ctl.p, sizeof(fin), cudaMemcpyDeviceToHost));
-  require(fin.error == 0, CHSGA_ERR_TIMEOUT,
-          "a bounded device-side wait expired (code " + std::to_string(fin.error) + ")");
+  require_step_ok(fin.error);
   c.prof.total_ms = dev_ms;
   c.prof.rows = total_rows;
   c.prof.steps = fin.steps;
@@ -1638,11 +1663,12 @@ struct CallKnobs {
   const TopDev* ts;
   CallKnobs(chsga_ctx& cx, uint32_t row_kernel, uint32_t top_vertices)
       : c(cx), rk(cx.row_kernel), ts(cx.top_sel) {
-    require(row_kernel <= CHSGA_ROW_STREAM, CHSGA_ERR_INVALID_ARG, "row_kernel must be CHSGA_ROW_*");
+    require(row_kernel <= CHSGA_ROW_DELTA, CHSGA_ERR_INVALID_ARG, "row_kernel must be CHSGA_ROW_*");
     if (row_kernel == CHSGA_ROW_DIRECT) c.row_kernel = RowKernel::Direct;
     if (row_kernel == CHSGA_ROW_TILED) c.row_kernel = RowKernel::Tiled;
     if (row_kernel == CHSGA_ROW_DPX) c.row_kernel = RowKernel::Dpx;
     if (row_kernel == CHSGA_ROW_STREAM) c.row_kernel = RowKernel::Stream;
+    if (row_kernel == CHSGA_ROW_DELTA) c.row_kernel = RowKernel::Delta;
     c.top_sel = top_for(c, top_vertices);
   }
   ~CallKnobs() {
@@ -1747,9 +1773,11 @@ chsga_batch_opts autotune(chsga_ctx& c, const char* const* reads, const uint32_t
   }
   // row kernel
   cur = best;
-  for (uint32_t rk : {(uint32_t)CHSGA_ROW_DPX, (uint32_t)CHSGA_ROW_DIRECT, (uint32_t)CHSGA_ROW_TILED}) {
+  for (uint32_t rk : {(uint32_t)CHSGA_ROW_STREAM, (uint32_t)CHSGA_ROW_DPX, (uint32_t)CHSGA_ROW_DIRECT,
+                      (uint32_t)CHSGA_ROW_TILED}) {
     if (rk == CHSGA_ROW_TILED && cur.slots < 32) continue;
-    if (rk == CHSGA_ROW_DPX && cur.slots < 64) continue;  // AUTO already is DPX there
+    if (rk == CHSGA_ROW_DPX && cur.slots < 64) continue;        // AUTO already is DPX there
+    if (rk == CHSGA_ROW_STREAM && cur.slots != 128) continue;   // AUTO is STREAM at 64
     chsga_batch_opts b = cur;
     b.row_kernel = rk;
     const double g = run(b, 0);
@@ -1898,8 +1926,7 @@ class ScoreLaneImpl final : public ScoreLane {
   void harvest(int k, std::vector<LaneDone>& out) {
     CK(cudaEventSynchronize(ev_[k]));
     const dev::StepCtl& s = hctl_.p[k];
-    require(s.error == 0, CHSGA_ERR_TIMEOUT,
-            "a bounded device-side wait expired (code " + std::to_string(s.error) + ")");
+    require_step_ok(s.error);
     const uint32_t mask = cap_ - 1;
     for (uint32_t i = hdone_; i != s.done; ++i) {
       const dev::CompletionRec& r = hring_.p[(size_t)k * cap_ + (i & mask)];
@@ -2074,6 +2101,7 @@ chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out) {
       if (std::string(rk) == "tiled") c->row_kernel = RowKernel::Tiled;
       if (std::string(rk) == "dpx") c->row_kernel = RowKernel::Dpx;
       if (std::string(rk) == "stream") c->row_kernel = RowKernel::Stream;
+      if (std::string(rk) == "delta") c->row_kernel = RowKernel::Delta;
     }
     // CHSGA_PLAIN_LAUNCH=stream|graphs|persistent: how chsga_align_scores
     // runs its row-steps (default graphs)

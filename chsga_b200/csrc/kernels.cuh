@@ -1064,6 +1064,281 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
 }
 
 // ---------------------------------------------------------------------------
+// Delta rows (128 slots, score-only). Within a string vertex two consecutive
+// chars' scores differ by at most 1 in every row: row 0 holds 0/1; a row's
+// raw update keeps the bound when the previous final row has it (a chain
+// char takes min(D[c] + 1, D[c-1] + delta, T[c-1] + 1) and D is 1-Lipschitz
+// along the chain), and the closure only lowers a vertex's chars to
+// min(T[c], F + (c - first)), a line of slope 1. So a row is stored as the
+// raw first score of every vertex (16 bits per slot, "H") and, for every
+// char, T[c] - T[c-1] + 1 in {0, 1, 2} (2 bits per slot, "Z"): 0.26 bytes
+// per cell instead of 2. Z: chars in groups of 4; group q, lane L (slots
+// 4L .. 4L+3) is the 32-bit word q * 32 + L, byte c & 3 for char c, slot
+// 4L + j at bits 2j .. 2j+1 (a first char's byte is unused). H[s * 128 + r]
+// follows Z at a 256-byte boundary. A delta outside {0, 1, 2} for an active
+// slot would mean the bound failed: the kernel sets ERR_ROW_DELTA and the
+// call fails instead of returning a wrong score.
+// ---------------------------------------------------------------------------
+constexpr uint32_t ERR_ROW_DELTA = 8;
+constexpr int kDeltaRing = 16;  // Z words in flight per lane (64 chars)
+
+__host__ __device__ constexpr size_t delta_z_bytes(size_t N) { return ((N + 3) / 4 + 1) * 32 * 4; }
+__host__ __device__ constexpr size_t delta_h_offset(size_t N) { return (delta_z_bytes(N) + 255) / 256 * 256; }
+__host__ __device__ constexpr size_t delta_row_bytes(size_t N, size_t S) {
+  return delta_h_offset(N) + S * 128 * 2 + 256;
+}
+__host__ __device__ constexpr size_t delta_smem_bytes() { return (size_t)kStreamWarps * kDeltaRing * 32 * 4; }
+
+__device__ __forceinline__ void cp_async_word(uint32_t* dst, const uint32_t* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+
+// the four 2-bit deltas of a lane's byte as two u16x2 words (slots 0,1 / 2,3)
+__device__ __forceinline__ void delta_expand(uint32_t b, uint32_t& e0, uint32_t& e1) {
+  e0 = (b & 3u) | ((b & 0xCu) << 14);
+  e1 = ((b >> 4) & 3u) | ((b & 0xC0u) << 10);
+}
+
+template <bool COH>
+__device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index, const uint32_t* DZ,
+                                          const uint16_t* DH, uint32_t* TZ, uint16_t* TH, uint16_t* BV,
+                                          const uint16_t* FL, const uint32_t* slot_word, uint32_t* warp_ring,
+                                          unsigned long long* sm_best, bool ending_any, StepCtl* ctl) {
+  constexpr int R = 128, P = 2, W = kDeltaRing;
+  constexpr uint32_t ONES = 0x00010001u;
+  constexpr unsigned FULL = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  const uint32_t s0 = run_index * 32;
+  const size_t so = (size_t)lane * 4;
+  uint32_t* ring = warp_ring + lane;  // word k of this lane at ring[k * 32]
+  uint32_t dtab[P], imask[P], fmask[P], amask[P];
+  bool any_fix = false, any_end = false;
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    dtab[p] = imask[p] = fmask[p] = amask[p] = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t w = COH ? slot_word[so + 2 * p + h] : __ldg(slot_word + so + 2 * p + h);
+      dtab[p] |= ((w >> SW_MASK_SHIFT) & SW_MASK) << (16 * h);
+      if (w & SW_INIT) imask[p] |= 0xFFFFu << (16 * h);
+      if (w & SW_FIX) fmask[p] |= 0xFFFFu << (16 * h);
+      if (w & SW_ACTIVE) amask[p] |= 0xFFFFu << (16 * h);
+      any_end |= (w & SW_ENDING) != 0;
+    }
+    any_fix |= fmask[p] != 0;
+  }
+  any_fix = __any_sync(FULL, any_fix);
+  const bool track = ending_any && __any_sync(FULL, any_end);
+  const uint32_t nv = min(32u, g.S - s0);
+  uint32_t mf = 0, me = 0, md = 0, mk0 = 0, mk1 = 0;
+  if ((uint32_t)lane < nv) {
+    const uint32_t s = s0 + lane;
+    mf = __ldg(g.sv_off + s);
+    me = __ldg(g.sv_off + s + 1);
+    md = CHSGA_CHK(__ldg(g.sv_dev + s), g.S, 3);
+    mk0 = __ldg(g.vin_off + s);
+    mk1 = __ldg(g.vin_off + s + 1);
+    CHSGA_CHK_CHARS(mf, me, g.N, 1);
+    CHSGA_CHK_RANGE(mk0, mk1, g.n_vin, 4);
+  }
+  const uint32_t cb = __shfl_sync(FULL, mf, 0), ce = __shfl_sync(FULL, me, nv - 1);
+  // previous-row Z words of the run's char groups q0 .. q1, W in flight
+  const uint32_t q0 = cb >> 2, q1 = (ce - 1) >> 2;
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    if (q0 + k <= q1) cp_async_word(ring + k * 32, DZ + (size_t)(q0 + k) * 32 + lane);
+    cp_async_commit();
+  }
+  uint32_t rslot = 0;                 // ring word of the current group
+  uint32_t qnext = q0 + W;            // next group to fetch
+  auto take_word = [&]() -> uint32_t {
+    cp_async_wait<W - 1>();
+    const uint32_t w = ring[rslot * 32];
+    if (qnext <= q1) cp_async_word(ring + rslot * 32, DZ + (size_t)qnext * 32 + lane);
+    cp_async_commit();
+    ++qnext;
+    rslot = (rslot + 1) % W;
+    return w;
+  };
+  const uint32_t kb = __shfl_sync(FULL, mk0, 0), ke = __shfl_sync(FULL, mk1, nv - 1);
+  const uint32_t src_a = kb + lane < ke ? CHSGA_CHK(__ldg(g.vin_srcv + kb + lane), g.S, 5) : 0u;
+  const uint32_t src_b = kb + 32 + lane < ke ? CHSGA_CHK(__ldg(g.vin_srcv + kb + 32 + lane), g.S, 5) : 0u;
+  auto src_at = [&](uint32_t k) -> uint32_t {
+    const uint32_t i = k - kb;
+    const uint32_t a = __shfl_sync(FULL, src_a, i & 31), b = __shfl_sync(FULL, src_b, i & 31);
+    return i < 32 ? a : i < 64 ? b : CHSGA_CHK(__ldg(g.vin_srcv + k), g.S, 5);
+  };
+  struct DV {
+    uint32_t f, len, d, k0, k1;
+    U2<P> F, H, u[2];
+  };
+  auto prefetch = [&](uint32_t i, DV& v) {
+    v.f = __shfl_sync(FULL, mf, i);
+    v.len = __shfl_sync(FULL, me, i) - v.f;
+    v.d = __shfl_sync(FULL, md, i);
+    v.k0 = __shfl_sync(FULL, mk0, i);
+    v.k1 = __shfl_sync(FULL, mk1, i);
+#pragma unroll
+    for (int p = 0; p < P; ++p) v.F.h[p] = v.u[0].h[p] = v.u[1].h[p] = 0;
+    v.H = ldp_src<P, COH>(DH + (size_t)(s0 + i) * R + so);
+    if (any_fix) v.F = ldp_src<P, COH>(FL + (size_t)(2 * (s0 + i)) * R + so);
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      if (v.k0 + j < v.k1) v.u[j] = ldp_src<P, COH>(FL + (size_t)(2 * src_at(v.k0 + j) + 1) * R + so);
+  };
+  int bmin[2 * P];
+  uint32_t barg[2 * P];
+#pragma unroll
+  for (int q = 0; q < 2 * P; ++q) {
+    bmin[q] = 0x7fffffff;
+    barg[q] = 0;
+  }
+  auto track_char = [&](const U2<P>& t, uint32_t c) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const int lo = (int)(t.h[p] & 0xFFFFu), hi = (int)(t.h[p] >> 16);
+      if (lo < bmin[2 * p]) {
+        bmin[2 * p] = lo;
+        barg[2 * p] = c;
+      }
+      if (hi < bmin[2 * p + 1]) {
+        bmin[2 * p + 1] = hi;
+        barg[2 * p + 1] = c;
+      }
+    }
+  };
+  // output: the current group's word and the chars of it this run owns
+  uint32_t zin = 0, zout = 0, own = 0, bad = 0;
+  auto put = [&](uint32_t c, uint32_t byte) {
+    const uint32_t sh = 8 * (c & 3u);
+    zout |= byte << sh;
+    own |= 0xFFu << sh;
+    if ((c & 3u) == 3u || c + 1 == ce) {
+      uint32_t* dst = TZ + (size_t)(c >> 2) * 32 + lane;
+      if (own == 0xFFFFFFFFu) {
+        *dst = zout;
+      } else {
+        unsigned char* db = reinterpret_cast<unsigned char*>(dst);
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          if ((own >> (8 * b)) & 0xFFu) db[b] = (unsigned char)(zout >> (8 * b));
+      }
+      zout = own = 0;
+    }
+  };
+  KeyWindow kw(g.lab4, cb);
+  DV cur, nxt;
+  prefetch(0, cur);
+  if (cb & 3u) zin = take_word();  // the run starts inside a group
+  auto run = [&](auto track_tag) {
+    constexpr bool TRACK = decltype(track_tag)::value;
+    for (uint32_t i = 0; i < nv; ++i) {
+      if (i + 1 < nv) prefetch(i + 1, nxt);
+      const uint32_t f = cur.f, len = cur.len;
+      const U2<P> F = cur.F;
+      U2<P> t, draw = cur.H, dprev = cur.H;
+      // first char: its byte of the group is unused
+      if ((f & 3u) == 0) zin = take_word();
+      {
+        const uint32_t key = kw.next();
+        uint32_t delta[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          delta[p] = (dtab[p] >> key) & ONES;
+          if (any_fix) dprev.h[p] = sel(__vminu2(dprev.h[p], F.h[p]), dprev.h[p], fmask[p]);
+          t.h[p] = __vadd2(dprev.h[p], ONES);
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+          if (cur.k0 + j < cur.k1)
+#pragma unroll
+            for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(cur.u[j].h[p], delta[p], t.h[p]);
+        for (uint32_t k = cur.k0 + 2; k < cur.k1; ++k) {
+          const U2<P> du = ldp_src<P, COH>(FL + (size_t)(2 * src_at(k) + 1) * R + so);
+#pragma unroll
+          for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(du.h[p], delta[p], t.h[p]);
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) t.h[p] = sel(delta[p], t.h[p], imask[p]);
+      }
+      stp<P>(TH + (size_t)(s0 + i) * R + so, t);
+      stp<P>(BV + (size_t)(2 * cur.d) * R + so, t);
+      put(f, 0u);
+      if (TRACK) track_char(t, f);
+      uint32_t off2 = 0;
+      for (uint32_t q = 1; q < len; ++q) {
+        const uint32_t c = f + q;
+        if ((c & 3u) == 0) zin = take_word();
+        uint32_t e0, e1;
+        delta_expand((zin >> (8 * (c & 3u))) & 0xFFu, e0, e1);
+        // per-halfword arithmetic: an idle slot's arbitrary values never
+        // carry into its neighbour
+        draw.h[0] = __vsub2(__vadd2(draw.h[0], e0), ONES);
+        draw.h[1] = __vsub2(__vadd2(draw.h[1], e1), ONES);
+        U2<P> dq = draw;
+        const uint32_t key = kw.next();
+        off2 += ONES;
+        const U2<P> tp = t;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const uint32_t delta = (dtab[p] >> key) & ONES;
+          if (any_fix) dq.h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq.h[p]), dq.h[p], fmask[p]);
+          uint32_t x = __viaddmin_u16x2(t.h[p], ONES, __vadd2(dq.h[p], ONES));
+          x = __viaddmin_u16x2(dprev.h[p], delta, x);
+          t.h[p] = sel(delta, x, imask[p]);
+        }
+        dprev = dq;
+        // T[c] - T[c-1] + 1 per slot, 2 bits each
+        const uint32_t d0 = __vsub2(__vadd2(t.h[0], ONES), tp.h[0]);
+        const uint32_t d1 = __vsub2(__vadd2(t.h[1], ONES), tp.h[1]);
+        bad |= ((d0 & amask[0]) | (d1 & amask[1])) & 0xFFFCFFFCu;
+        put(c, (d0 & 3u) | ((d0 >> 14) & 0xCu) | ((d1 & 3u) << 4) | ((d1 >> 10) & 0xC0u));
+        if (TRACK) track_char(t, c);
+      }
+      if (len > 1) stp<P>(BV + (size_t)(2 * cur.d + 1) * R + so, t);
+      cur = nxt;
+    }
+  };
+  if (track)
+    run(std::true_type{});
+  else
+    run(std::false_type{});
+  cp_async_wait<0>();
+  if (bad) atomicOr(&ctl->error, ERR_ROW_DELTA);
+  if (track) {
+#pragma unroll
+    for (int q = 0; q < 2 * P; ++q) {
+      const uint32_t w = COH ? slot_word[so + q] : __ldg(slot_word + so + q);
+      if ((w & SW_ENDING) && bmin[q] != 0x7fffffff) atomicMin(sm_best + so + q, pack_min(bmin[q], barg[q]));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_delta(
+    GraphPtrs g, const uint16_t* __restrict__ D, uint16_t* __restrict__ T, uint16_t* __restrict__ BV,
+    const uint16_t* __restrict__ FL, const uint32_t* __restrict__ slot_word,
+    unsigned long long* __restrict__ best, StepCtl* __restrict__ ctl) {
+  pdl_wait();
+  extern __shared__ __align__(16) uint32_t dring_smem[];
+  __shared__ unsigned long long sm_best[128];
+  const bool ending_any = ctl->any_ending != 0;
+  if (!ctl->any_active) return;
+  if (ending_any) {
+    for (int r = threadIdx.x; r < 128; r += blockDim.x) sm_best[r] = ~0ull;
+    __syncthreads();
+  }
+  const uint32_t run = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+  const size_t hoff = delta_h_offset(g.N);
+  if (run * 32 < g.S)
+    delta_run<false>(g, run, reinterpret_cast<const uint32_t*>(D),
+                     reinterpret_cast<const uint16_t*>(reinterpret_cast<const unsigned char*>(D) + hoff),
+                     reinterpret_cast<uint32_t*>(T),
+                     reinterpret_cast<uint16_t*>(reinterpret_cast<unsigned char*>(T) + hoff), BV, FL, slot_word,
+                     dring_smem + (size_t)(threadIdx.x >> 5) * kDeltaRing * 32, sm_best, ending_any, ctl);
+  if (ending_any) flush_min<128>(sm_best, best);
+}
+
+// ---------------------------------------------------------------------------
 // Loads of data that other blocks of the same launch may have written (the
 // persistent row-step kernel's rows, boundary scores and slot words): L2
 // only (ld.global.cg), never the read-only path, which assumes the data does

@@ -170,3 +170,21 @@ def test_reference_rows_at_equals_every_row(tmp_path):
     h = orc.RefHarness(files)
     every = h.rows(rd, n)
     np.testing.assert_array_equal(h.rows_at(rd, n, [0, 64, 129]), every[[0, 64, 129]])
+
+
+@pytest.mark.parametrize("seed,vmax,gap", [(61, 32, 20.0), (62, 3, 6.0), (63, 32, 6.0)])
+def test_rows_change_by_at_most_one_within_a_vertex(tmp_path, seed, vmax, gap):
+    # the premise of the 2-bit delta rows (k_row_delta): in every DP row two
+    # consecutive chars of one string vertex differ by at most 1
+    g, files = gen_graph(tmp_path, f"d{seed}", backbone_len=3000, seed=seed, vlen_max=vmax,
+                         bubble_gap_mean=gap, p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=2, alt_max=60)
+    o = orc.Oracle(files)
+    off = np.array(open(files[4]).read().split(), dtype=np.int64)
+    heads = np.zeros(o.num_chars, dtype=bool)
+    heads[off[:-1]] = True
+    reads = g.gen_reads(6, seed, 40, 300, sub_rate=0.08, indel_rate=0.06, n_rate=0.02).to_list()
+    for rd in reads:
+        rows = o.rows(rd)
+        diff = np.diff(rows, axis=1)
+        chain = ~heads[1:]  # char c (c >= 1) continues the vertex of c - 1
+        assert np.abs(diff[:, chain]).max() <= 1
