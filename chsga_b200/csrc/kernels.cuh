@@ -1093,10 +1093,12 @@ __device__ __forceinline__ void cp_async_word(uint32_t* dst, const uint32_t* src
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 
-// the four 2-bit deltas of a lane's byte as two u16x2 words (slots 0,1 / 2,3)
+// the four 2-bit deltas in the low byte of b as two u16x2 words (slots 0,1
+// and 2,3): b | b << 14 puts bits 2-3 at 16-17 and bits 6-7 at 20-21
 __device__ __forceinline__ void delta_expand(uint32_t b, uint32_t& e0, uint32_t& e1) {
-  e0 = (b & 3u) | ((b & 0xCu) << 14);
-  e1 = ((b >> 4) & 3u) | ((b & 0xC0u) << 10);
+  const uint32_t t = b | (b << 14);
+  e0 = t & 0x00030003u;
+  e1 = (t >> 4) & 0x00030003u;
 }
 
 template <bool COH>
@@ -1207,23 +1209,20 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
       }
     }
   };
-  // output: the current group's word and the chars of it this run owns
-  uint32_t zin = 0, zout = 0, own = 0, bad = 0;
+  // output: the bytes of the current group shift in from the top of zout;
+  // a whole group is one word store, the run's first and last groups (shared
+  // with the neighbouring runs) are stored byte by byte
+  uint32_t zin = 0, zout = 0, bad = 0;
   auto put = [&](uint32_t c, uint32_t byte) {
-    const uint32_t sh = 8 * (c & 3u);
-    zout |= byte << sh;
-    own |= 0xFFu << sh;
-    if ((c & 3u) == 3u || c + 1 == ce) {
+    zout = (zout >> 8) | (byte << 24);
+    if ((c & 3u) == 3u) {
       uint32_t* dst = TZ + (size_t)(c >> 2) * 32 + lane;
-      if (own == 0xFFFFFFFFu) {
+      if (c >= cb + 3) {
         *dst = zout;
       } else {
         unsigned char* db = reinterpret_cast<unsigned char*>(dst);
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if ((own >> (8 * b)) & 0xFFu) db[b] = (unsigned char)(zout >> (8 * b));
+        for (uint32_t b = cb & 3u; b < 4; ++b) db[b] = (unsigned char)(zout >> (8 * b));
       }
-      zout = own = 0;
     }
   };
   KeyWindow kw(g.lab4, cb);
@@ -1270,7 +1269,7 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
         const uint32_t c = f + q;
         if ((c & 3u) == 0) zin = take_word();
         uint32_t e0, e1;
-        delta_expand((zin >> (8 * (c & 3u))) & 0xFFu, e0, e1);
+        delta_expand(zin >> (8 * (c & 3u)), e0, e1);
         // per-halfword arithmetic: an idle slot's arbitrary values never
         // carry into its neighbour
         draw.h[0] = __vsub2(__vadd2(draw.h[0], e0), ONES);
@@ -1291,8 +1290,9 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
         // T[c] - T[c-1] + 1 per slot, 2 bits each
         const uint32_t d0 = __vsub2(__vadd2(t.h[0], ONES), tp.h[0]);
         const uint32_t d1 = __vsub2(__vadd2(t.h[1], ONES), tp.h[1]);
-        bad |= ((d0 & amask[0]) | (d1 & amask[1])) & 0xFFFCFFFCu;
-        put(c, (d0 & 3u) | ((d0 >> 14) & 0xCu) | ((d1 & 3u) << 4) | ((d1 >> 10) & 0xC0u));
+        bad |= (d0 & amask[0]) | (d1 & amask[1]);
+        const uint32_t dd = d0 | (d1 << 4);  // slot pairs' low halves at bits 0, 4, high halves at 16, 20
+        put(c, (dd | (dd >> 14)) & 0xFFu);
         if (TRACK) track_char(t, c);
       }
       if (len > 1) stp<P>(BV + (size_t)(2 * cur.d + 1) * R + so, t);
@@ -1303,8 +1303,15 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
     run(std::true_type{});
   else
     run(std::false_type{});
+  // the run's last group when it ends inside a group
+  if (((ce - 1) & 3u) != 3u) {
+    const uint32_t g0 = (ce - 1) & ~3u, k = ce - g0;  // bytes of the group this run holds
+    unsigned char* db = reinterpret_cast<unsigned char*>(TZ + (size_t)(g0 >> 2) * 32 + lane);
+    const uint32_t first = cb > g0 ? cb - g0 : 0u;
+    for (uint32_t b = first; b < k; ++b) db[b] = (unsigned char)(zout >> (8 * (4 - k + b)));
+  }
   cp_async_wait<0>();
-  if (bad) atomicOr(&ctl->error, ERR_ROW_DELTA);
+  if (bad & 0xFFFCFFFCu) atomicOr(&ctl->error, ERR_ROW_DELTA);
   if (track) {
 #pragma unroll
     for (int q = 0; q < 2 * P; ++q) {

@@ -274,13 +274,13 @@ typedef struct {
                              launch each; 0 = 23000 (the most shared memory holds) */
 } chsga_batch_opts;
 /* Row kernels. With 16-bit rows, slots >= 2 and no string vertex label over
- * 512 chars, AUTO runs DELTA for 128 slots, STREAM for 64 and DPX below,
- * else DIRECT; one slot runs the tile kernel (one warp per tile of whole
- * vertices, one lane per 8 chars). DELTA = STREAM over rows stored as the
- * raw first score of every vertex (16 bits per slot) and, per char, the
- * difference to the char before in 2 bits per slot (consecutive chars of a
- * vertex differ by at most 1 in every row), 0.26 bytes per cell instead of 2
- * (128 slots, score-only).
+ * 512 chars, AUTO runs STREAM for slots >= 64 and DPX below, else DIRECT;
+ * one slot runs the tile kernel (one warp per tile of whole vertices, one
+ * lane per 8 chars). DELTA (128 slots, score-only) = STREAM over rows stored
+ * as the raw first score of every vertex (16 bits per slot) and, per char,
+ * the difference to the char before in 2 bits per slot (consecutive chars of
+ * a vertex differ by at most 1 in every row): 0.26 bytes per cell instead of
+ * 2, bound by instruction issue rather than memory.
  * DIRECT = one thread group per string vertex, 16- or 32-bit rows;
  * TILED = shared-memory tiles of consecutive string vertices staged by TMA
  * bulk copies (slots >= 32); DPX = two 16-bit scores per register on the

@@ -30,7 +30,7 @@ def main(workdir):
     ctx = cb.Context(0).load(g)
     np.testing.assert_array_equal(ctx.align_scores(reads), want)
     for slots in (1, 2, 8, 32, 64, 128):
-        for rk in (cb.ROW_AUTO, cb.ROW_DIRECT, cb.ROW_DPX, cb.ROW_STREAM, cb.ROW_TILED):
+        for rk in (cb.ROW_AUTO, cb.ROW_DIRECT, cb.ROW_DPX, cb.ROW_STREAM, cb.ROW_TILED, cb.ROW_DELTA):
             got = ctx.align_scores_batched(reads, slots=slots, row_kernel=rk)
             np.testing.assert_array_equal(got, want, err_msg=f"slots {slots} row kernel {rk}")
         got = ctx.align_scores_batched(reads, slots=slots, use_graphs=cb.LAUNCH_PERSISTENT)

@@ -230,15 +230,15 @@ def test_cooperative_pull_matches_oracle(small_graph, oracle_small, monkeypatch,
 
 @pytest.mark.parametrize("top_vertices", [0, 300])
 def test_delta_rows_equal_oracle_and_16bit_rows(small_graph, ctx_small, oracle_small, top_vertices):
-    # 128 slots store rows as 2-bit within-vertex deltas (k_row_delta, AUTO);
-    # uneven lengths refill slots while others run, so a slot's new read
-    # starts on rows another read left behind
+    # ROW_DELTA: 128 slots store rows as 2-bit within-vertex deltas
+    # (k_row_delta); uneven lengths refill slots while others run, so a
+    # slot's new read starts on rows another read left behind
     g, files, reads = small_graph
     mix = list(reads) + g.gen_reads(150, 29, 1, 2500, sub_rate=0.04, indel_rate=0.03,
                                     n_rate=0.01).to_list()
     want = oracle_small.scores(mix)
-    got = ctx_small.align_scores_batched(mix, slots=128, top_vertices=top_vertices)
+    got = ctx_small.align_scores_batched(mix, slots=128, top_vertices=top_vertices,
+                                         row_kernel=cb.ROW_DELTA)
     np.testing.assert_array_equal(got, want)
-    got16 = ctx_small.align_scores_batched(mix, slots=128, top_vertices=top_vertices,
-                                           row_kernel=cb.ROW_STREAM)
+    got16 = ctx_small.align_scores_batched(mix, slots=128, top_vertices=top_vertices)
     np.testing.assert_array_equal(got16, want)
