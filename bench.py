@@ -57,6 +57,8 @@ def parse():
                    help="reads per warm-up step (lengths capped at 1 kbp)")
     p.add_argument("--no-profile", action="store_true")
     p.add_argument("--no-tune", action="store_true", help="skip the autotuner (use --slots)")
+    p.add_argument("--row-kernel", default="auto", choices=["auto", "direct", "tiled", "dpx", "stream", "delta"],
+                   help="with --no-tune: the row kernel")
     p.add_argument("--served-s", type=float, default=12.0, help="Poisson arrival window, seconds")
     p.add_argument("--backbone", type=int, default=0,
                    help="backbone length of the config-2-mix graph (0 = 5 Mbp); for small profiling captures")
@@ -930,7 +932,9 @@ def main():
         return replicas.max_over_ranks(x, ws, device=f"cuda:{local}")
 
     # autotuner on a sample of the distribution (reads capped at 2 kbp)
-    opts = dict(slots=args.slots, steps_per_graph=8, row_kernel=0, top_vertices=0)
+    opts = dict(slots=args.slots, steps_per_graph=8,
+                row_kernel=["auto", "direct", "tiled", "dpx", "stream", "delta"].index(args.row_kernel),
+                top_vertices=0)
     tune = None
     if not args.no_tune:
         tsample = make_reads(g, 4 * args.slots, 60_000 + rank, len_max=2000)
