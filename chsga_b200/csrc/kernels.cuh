@@ -1096,6 +1096,7 @@ __device__ __forceinline__ void cp_async_word(uint32_t* dst, const uint32_t* src
 // the four 2-bit deltas in the low byte of b as two u16x2 words (slots 0,1
 // and 2,3): b | b << 14 puts bits 2-3 at 16-17 and bits 6-7 at 20-21
 __device__ __forceinline__ void delta_expand(uint32_t b, uint32_t& e0, uint32_t& e1) {
+  b &= 0xFFu;  // the other bytes of the word would reach bits 16-21
   const uint32_t t = b | (b << 14);
   e0 = t & 0x00030003u;
   e1 = (t >> 4) & 0x00030003u;
@@ -1128,6 +1129,10 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
       any_end |= (w & SW_ENDING) != 0;
     }
     any_fix |= fmask[p] != 0;
+    // an idle slot computes a row-0 row of a read that matches everywhere
+    // (its mismatch mask is empty): all 0, so every slot's scores stay in
+    // 0..65535 and the pair arithmetic below never carries between halves
+    imask[p] |= ~amask[p];
   }
   any_fix = __any_sync(FULL, any_fix);
   const bool track = ending_any && __any_sync(FULL, any_end);
@@ -1245,7 +1250,7 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
         for (int p = 0; p < P; ++p) {
           delta[p] = (dtab[p] >> key) & ONES;
           if (any_fix) dprev.h[p] = sel(__vminu2(dprev.h[p], F.h[p]), dprev.h[p], fmask[p]);
-          t.h[p] = __vadd2(dprev.h[p], ONES);
+          t.h[p] = dprev.h[p] + ONES;
         }
 #pragma unroll
         for (int j = 0; j < 2; ++j)
@@ -1270,10 +1275,10 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
         if ((c & 3u) == 0) zin = take_word();
         uint32_t e0, e1;
         delta_expand(zin >> (8 * (c & 3u)), e0, e1);
-        // per-halfword arithmetic: an idle slot's arbitrary values never
-        // carry into its neighbour
-        draw.h[0] = __vsub2(__vadd2(draw.h[0], e0), ONES);
-        draw.h[1] = __vsub2(__vadd2(draw.h[1], e1), ONES);
+        // no half carries or borrows: every stored score is in 0..65001 and
+        // consecutive chars differ by at most 1
+        draw.h[0] = draw.h[0] + e0 - ONES;
+        draw.h[1] = draw.h[1] + e1 - ONES;
         U2<P> dq = draw;
         const uint32_t key = kw.next();
         off2 += ONES;
@@ -1282,16 +1287,19 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
         for (int p = 0; p < P; ++p) {
           const uint32_t delta = (dtab[p] >> key) & ONES;
           if (any_fix) dq.h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq.h[p]), dq.h[p], fmask[p]);
-          uint32_t x = __viaddmin_u16x2(t.h[p], ONES, __vadd2(dq.h[p], ONES));
+          uint32_t x = __viaddmin_u16x2(t.h[p], ONES, dq.h[p] + ONES);
           x = __viaddmin_u16x2(dprev.h[p], delta, x);
           t.h[p] = sel(delta, x, imask[p]);
         }
         dprev = dq;
         // T[c] - T[c-1] + 1 per slot, 2 bits each
-        const uint32_t d0 = __vsub2(__vadd2(t.h[0], ONES), tp.h[0]);
-        const uint32_t d1 = __vsub2(__vadd2(t.h[1], ONES), tp.h[1]);
-        bad |= (d0 & amask[0]) | (d1 & amask[1]);
-        const uint32_t dd = d0 | (d1 << 4);  // slot pairs' low halves at bits 0, 4, high halves at 16, 20
+        const uint32_t d0 = t.h[0] + ONES - tp.h[0];
+        const uint32_t d1 = t.h[1] + ONES - tp.h[1];
+        bad |= d0 | d1;
+        // two bits per slot (an idle slot's arbitrary difference must not
+        // reach its neighbour's bits); low halves at bits 0 and 4, high
+        // halves at 16 and 20, folded into one byte
+        const uint32_t dd = (d0 & 0x00030003u) | ((d1 & 0x00030003u) << 4);
         put(c, (dd | (dd >> 14)) & 0xFFu);
         if (TRACK) track_char(t, c);
       }
