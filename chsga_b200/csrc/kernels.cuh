@@ -1106,7 +1106,8 @@ template <bool COH>
 __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index, const uint32_t* DZ,
                                           const uint16_t* DH, uint32_t* TZ, uint16_t* TH, uint16_t* BV,
                                           const uint16_t* FL, const uint32_t* slot_word, uint32_t* warp_ring,
-                                          unsigned long long* sm_best, bool ending_any, StepCtl* ctl) {
+                                          const uint2* lut, unsigned long long* sm_best, bool ending_any,
+                                          StepCtl* ctl) {
   constexpr int R = 128, P = 2, W = kDeltaRing;
   constexpr uint32_t ONES = 0x00010001u;
   constexpr unsigned FULL = 0xFFFFFFFFu;
@@ -1217,9 +1218,11 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
   // output: the bytes of the current group shift in from the top of zout;
   // a whole group is one word store, the run's first and last groups (shared
   // with the neighbouring runs) are stored byte by byte
+  // the group's input word is fetched where its output word is stored, so a
+  // char takes one branch
   uint32_t zin = 0, zout = 0, bad = 0;
   auto put = [&](uint32_t c, uint32_t byte) {
-    zout = (zout >> 8) | (byte << 24);
+    zout = __funnelshift_r(zout, byte, 8);
     if ((c & 3u) == 3u) {
       uint32_t* dst = TZ + (size_t)(c >> 2) * 32 + lane;
       if (c >= cb + 3) {
@@ -1228,12 +1231,13 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
         unsigned char* db = reinterpret_cast<unsigned char*>(dst);
         for (uint32_t b = cb & 3u; b < 4; ++b) db[b] = (unsigned char)(zout >> (8 * b));
       }
+      if (c + 1 < ce) zin = take_word();
     }
   };
   KeyWindow kw(g.lab4, cb);
   DV cur, nxt;
   prefetch(0, cur);
-  if (cb & 3u) zin = take_word();  // the run starts inside a group
+  zin = take_word();  // the run's first group
   auto run = [&](auto track_tag) {
     constexpr bool TRACK = decltype(track_tag)::value;
     for (uint32_t i = 0; i < nv; ++i) {
@@ -1242,7 +1246,6 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
       const U2<P> F = cur.F;
       U2<P> t, draw = cur.H, dprev = cur.H;
       // first char: its byte of the group is unused
-      if ((f & 3u) == 0) zin = take_word();
       {
         const uint32_t key = kw.next();
         uint32_t delta[P];
@@ -1272,13 +1275,14 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
       uint32_t off2 = 0;
       for (uint32_t q = 1; q < len; ++q) {
         const uint32_t c = f + q;
-        if ((c & 3u) == 0) zin = take_word();
-        uint32_t e0, e1;
-        delta_expand(zin >> (8 * (c & 3u)), e0, e1);
-        // no half carries or borrows: every stored score is in 0..65001 and
-        // consecutive chars differ by at most 1
-        draw.h[0] = draw.h[0] + e0 - ONES;
-        draw.h[1] = draw.h[1] + e1 - ONES;
+        // the pair increments of this char's byte, -1..1 per half: a 32-bit
+        // add is exact since no half leaves 0..65535 (scores stay in
+        // 0..65001, consecutive chars differ by at most 1)
+        // selector: byte c & 3 of zin, then three zero bytes of the second
+        // operand (an index below 256)
+        const uint2 e = lut[__byte_perm(zin, 0u, (c & 3u) | 0x4440u)];
+        draw.h[0] += e.x;
+        draw.h[1] += e.y;
         U2<P> dq = draw;
         const uint32_t key = kw.next();
         off2 += ONES;
@@ -1296,10 +1300,9 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
         const uint32_t d0 = t.h[0] + ONES - tp.h[0];
         const uint32_t d1 = t.h[1] + ONES - tp.h[1];
         bad |= d0 | d1;
-        // two bits per slot (an idle slot's arbitrary difference must not
-        // reach its neighbour's bits); low halves at bits 0 and 4, high
-        // halves at 16 and 20, folded into one byte
-        const uint32_t dd = (d0 & 0x00030003u) | ((d1 & 0x00030003u) << 4);
+        // 0..2 in every half (idle slots included): low halves at bits 0
+        // and 4, high halves at 16 and 20, folded into one byte
+        const uint32_t dd = d0 | (d1 << 4);
         put(c, (dd | (dd >> 14)) & 0xFFu);
         if (TRACK) track_char(t, c);
       }
@@ -1342,6 +1345,14 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
     for (int r = threadIdx.x; r < 128; r += blockDim.x) sm_best[r] = ~0ull;
     __syncthreads();
   }
+  // byte -> increments of the two slot pairs (the 2-bit fields minus 1)
+  __shared__ uint2 s_lut[256];
+  for (int v = threadIdx.x; v < 256; v += blockDim.x) {
+    uint32_t e0, e1;
+    delta_expand((uint32_t)v, e0, e1);
+    s_lut[v] = make_uint2(e0 - 0x00010001u, e1 - 0x00010001u);
+  }
+  __syncthreads();
   const uint32_t run = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
   const size_t hoff = delta_h_offset(g.N);
   if (run * 32 < g.S)
@@ -1349,7 +1360,8 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
                      reinterpret_cast<const uint16_t*>(reinterpret_cast<const unsigned char*>(D) + hoff),
                      reinterpret_cast<uint32_t*>(T),
                      reinterpret_cast<uint16_t*>(reinterpret_cast<unsigned char*>(T) + hoff), BV, FL, slot_word,
-                     dring_smem + (size_t)(threadIdx.x >> 5) * kDeltaRing * 32, sm_best, ending_any, ctl);
+                     dring_smem + (size_t)(threadIdx.x >> 5) * kDeltaRing * 32, s_lut, sm_best, ending_any,
+                     ctl);
   if (ending_any) flush_min<128>(sm_best, best);
 }
 
