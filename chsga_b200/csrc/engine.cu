@@ -1298,8 +1298,7 @@ void traceback_batched(chsga_ctx& parent, const char* const* reads, const uint32
   auto harvest = [&](int k) {
     CK(cudaEventSynchronize(ev[k]));
     const dev::StepCtl& st = hctl.p[k];
-    require(st.error == 0, CHSGA_ERR_TIMEOUT,
-            "a bounded device-side wait expired (code " + std::to_string(st.error) + ")");
+    require_step_ok(st.error);
     for (uint32_t i0 = hdone; i0 < st.done; i0 += wcap) {
       const uint32_t i1 = std::min<uint32_t>(st.done, i0 + wcap);
       for (uint32_t i = i0; i < i1; ++i) {
