@@ -6,6 +6,7 @@ import os
 import socket
 
 import numpy as np
+import pytest
 import torch.multiprocessing as mp
 
 from conftest import ROOT
@@ -71,3 +72,39 @@ def test_shard_indices_cover_everything():
             parts = [replicas.shard_indices(n, w, r) for r in range(w)]
             allv = np.sort(np.concatenate(parts)) if parts else np.array([])
             assert allv.tolist() == list(range(n))
+
+
+def _nccl_worker(port, q):
+    import sys
+    sys.path.insert(0, ROOT)
+    import torch
+    import torch.distributed as dist
+    from chsga_b200 import replicas
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        dev = replicas.collective_device()
+        buf = torch.arange(4, dtype=torch.int32, device=dev)
+        out = [torch.empty_like(buf)]
+        dist.all_gather(out, buf)
+        t = torch.tensor([3.5], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        q.put((dev.type, out[0].cpu().tolist(), float(t.item())))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_nccl_group_gathers_on_the_device():
+    """Under NCCL the gather and max buffers go to the current CUDA device
+    (one rank: this run has one GPU)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_worker, args=(_free_port(), q))
+    p.start()
+    res = q.get(timeout=180)
+    p.join(timeout=60)
+    assert p.exitcode == 0
+    assert res == ("cuda", [0, 1, 2, 3], 3.5)
