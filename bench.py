@@ -570,8 +570,8 @@ def run_launch_compare(args):
     g = make_graph(args.backbone)
     N = g.stats()["num_chars"]
     ctx = cb.Context(0).load(g)
-    os.environ["CHSGA_PDL"] = "1"  # read when a context opens
-    ctx_pdl = cb.Context(0).load(g)
+    os.environ["CHSGA_PDL"] = "0"  # read when a context opens (on by default)
+    ctx_nopdl = cb.Context(0).load(g)
     del os.environ["CHSGA_PDL"]
     os.environ["CHSGA_PULL_COOP"] = "1"
     ctx_coop = cb.Context(0).load(g)
@@ -584,7 +584,7 @@ def run_launch_compare(args):
     for R, reads in shapes:
         cells = sum(len(r) for r in reads) * N
         runs = [("graphs", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16)),
-                ("graphs_pdl", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16, ctx=ctx_pdl)),
+                ("graphs_no_pdl", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16, ctx=ctx_nopdl)),
                 ("persistent", dict(use_graphs=cb.LAUNCH_PERSISTENT, steps_per_graph=16)),
                 ("persistent_64", dict(use_graphs=cb.LAUNCH_PERSISTENT, steps_per_graph=64))]
         if R == 1:
@@ -634,7 +634,7 @@ def run_launch_compare(args):
     pctx.close()
     pctx_coop.close()
     ctx_coop.close()
-    ctx_pdl.close()
+    ctx_nopdl.close()
     ctx.close()
     print(json.dumps(out), flush=True)
     return 0

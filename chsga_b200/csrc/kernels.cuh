@@ -317,7 +317,15 @@ __device__ __forceinline__ uint32_t mismatch_mask(int b, int special, int match_
 // Programmatic dependent launch: a row-step kernel launched while the kernel
 // before it on the stream drains waits here until that kernel has finished
 // and its writes are visible (a no-op for a kernel launched the usual way).
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Once every block of this kernel has passed the wait, the next kernel of the
+// chain may launch into the SMs this one frees and load its graph constants
+// before its own wait. Every block of a chain kernel calls this before it
+// reads anything a kernel writes, and before it exits, so a kernel completes
+// only after the one before it.
+__device__ __forceinline__ void pdl_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -842,13 +850,36 @@ __device__ __forceinline__ U2<P> lds_u2(const uint16_t* p) {
   return o;
 }
 
+// The graph constants of lane j of a k_row_stream run: vertex s0 + j's char
+// range, hierarchy position and first-char in-edge range (zeros past the
+// graph). Loaded before the kernel's pdl_wait.
+struct RunHead {
+  uint32_t mf, me, md, mk0, mk1;
+};
+
+__device__ __forceinline__ RunHead run_head(const GraphPtrs& g, uint32_t run_index) {
+  RunHead r{0, 0, 0, 0, 0};
+  const uint32_t s0 = run_index * 32, lane = threadIdx.x & 31;
+  if (lane < min(32u, g.S - s0)) {
+    const uint32_t s = s0 + lane;
+    r.mf = __ldg(g.sv_off + s);
+    r.me = __ldg(g.sv_off + s + 1);
+    r.md = CHSGA_CHK(__ldg(g.sv_dev + s), g.S, 3);
+    r.mk0 = __ldg(g.vin_off + s);
+    r.mk1 = __ldg(g.vin_off + s + 1);
+    CHSGA_CHK_CHARS(r.mf, r.me, g.N, 1);
+    CHSGA_CHK_RANGE(r.mk0, r.mk1, g.n_vin, 4);
+  }
+  return r;
+}
+
 // One warp's run of 32 string vertices starting at s0 = 32 * run_index (k_row_stream's
 // body); warp_ring = the warp's kStreamRing x R ring in shared memory.
 template <int R, bool DEFER, bool COH>
-__device__ __forceinline__ void stream_run(const GraphPtrs& g, uint32_t run_index, const uint16_t* D, uint16_t* T,
-                                           uint16_t* BV, const uint16_t* FL, const uint32_t* slot_word,
-                                           uint16_t* warp_ring, unsigned long long* sm_best,
-                                           bool ending_any) {
+__device__ __forceinline__ void stream_run(const GraphPtrs& g, uint32_t run_index, const RunHead& rh,
+                                           const uint16_t* D, uint16_t* T, uint16_t* BV, const uint16_t* FL,
+                                           const uint32_t* slot_word, uint16_t* warp_ring,
+                                           unsigned long long* sm_best, bool ending_any) {
   constexpr int P = Pairs<R>::P;
   constexpr int W = kStreamRing;
   constexpr uint32_t ONES = 0x00010001u;
@@ -877,17 +908,7 @@ __device__ __forceinline__ void stream_run(const GraphPtrs& g, uint32_t run_inde
     const bool track = ending_any && __any_sync(FULL, any_end);
     // the run's vertex words, vertex s0 + lane on each lane
     const uint32_t nv = min(32u, g.S - s0);
-    uint32_t mf = 0, me = 0, md = 0, mk0 = 0, mk1 = 0;
-    if ((uint32_t)lane < nv) {
-      const uint32_t s = s0 + lane;
-      mf = __ldg(g.sv_off + s);
-      me = __ldg(g.sv_off + s + 1);
-      md = CHSGA_CHK(__ldg(g.sv_dev + s), g.S, 3);
-      mk0 = __ldg(g.vin_off + s);
-      mk1 = __ldg(g.vin_off + s + 1);
-      CHSGA_CHK_CHARS(mf, me, g.N, 1);
-      CHSGA_CHK_RANGE(mk0, mk1, g.n_vin, 4);
-    }
+    const uint32_t mf = rh.mf, me = rh.me, md = rh.md, mk0 = rh.mk0, mk1 = rh.mk1;
     const uint32_t cb = __shfl_sync(FULL, mf, 0), ce = __shfl_sync(FULL, me, nv - 1);
     // previous-row scores of the run's chars cb .. ce-1: row c goes to slot
     // (c - cb) % W; one commit group per row, empty past the run
@@ -1045,19 +1066,21 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
     GraphPtrs g, const uint16_t* __restrict__ D, uint16_t* __restrict__ T, uint16_t* __restrict__ BV,
     const uint16_t* __restrict__ FL, const uint32_t* __restrict__ slot_word,
     unsigned long long* __restrict__ best, const StepCtl* __restrict__ ctl) {
-  pdl_wait();
   static_assert(Pairs<R>::G == 32, "one full warp per vertex");
   extern __shared__ __align__(16) uint16_t ring_smem[];
   __shared__ unsigned long long sm_best[R];
+  const uint32_t run = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+  RunHead rh{0, 0, 0, 0, 0};
+  if (run * 32 < g.S) rh = run_head(g, run);
+  pdl_wait();
   const bool ending_any = ctl->any_ending != 0;
   if (!ctl->any_active) return;
   if (ending_any) {
     for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
     __syncthreads();
   }
-  const uint32_t run = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
   if (run * 32 < g.S)
-    stream_run<R, DEFER, false>(g, run, D, T, BV, FL, slot_word,
+    stream_run<R, DEFER, false>(g, run, rh, D, T, BV, FL, slot_word,
                                 ring_smem + (size_t)(threadIdx.x >> 5) * kStreamRing * R, sm_best,
                                 ending_any);
   if (ending_any) flush_min<R>(sm_best, best);
@@ -1434,23 +1457,50 @@ struct T1Ptrs {
 constexpr int kT1Warps = 8;       // warps per block of k_row_t1
 constexpr int kT1VertMax = 64;    // vertices per tile (kT1MaxVerts on the host)
 
+// The graph constants of one lane of a k_row_t1 tile: the tile descriptor,
+// the lane's chunk of label keys and head bits, and the record of vertex
+// `lane` of the tile. Loaded before the kernel's pdl_wait. In the checked
+// build a descriptor outside the graph, or larger than a warp's lanes and
+// vertex slots, comes back as the empty tile {0, 0, 0, 0} and is skipped
+// whole (every lane reads the same descriptor).
+struct T1Head {
+  uint4 td, r0;
+  uint32_t keys, hb;
+};
+
+__device__ __forceinline__ T1Head t1_head(const GraphPtrs& g, const T1Ptrs& t, uint32_t tile) {
+  const int lane = threadIdx.x & 31;
+  T1Head r{};
+  r.td = __ldg(t.desc + tile);
+#ifdef CHSGA_CHECKED
+  const uint4 td = r.td;
+  if (!(td.x < td.y && td.y <= g.N && td.z < td.w && td.w <= g.S && td.w - td.z <= (uint32_t)kT1VertMax &&
+        ((td.y - 1) >> 3) - (td.x >> 3) < 32u)) {
+    if (lane == 0) chk_fail(tile, 6);
+    r.td = make_uint4(0, 0, 0, 0);
+    return r;
+  }
+#endif
+  const uint32_t q = (r.td.x >> 3) + lane;
+  if (q <= ((r.td.y - 1) >> 3)) {
+    r.keys = __ldg(g.lab4 + q);
+    r.hb = __ldg(t.heads + q);
+  }
+  if ((uint32_t)lane < r.td.w - r.td.z) r.r0 = __ldg(t.vrec + r.td.z + lane);
+  return r;
+}
+
 template <bool DEFER, bool COH>
-__device__ __forceinline__ void row_t1_tile(const GraphPtrs& g, const T1Ptrs& t, uint32_t tile,
+__device__ __forceinline__ void row_t1_tile(const GraphPtrs& g, const T1Ptrs& t, const T1Head& th,
                                             const uint16_t* D, uint16_t* T, uint16_t* BV,
                                             const uint16_t* FL, uint32_t w, int* s_G, int* s_X,
                                             uint32_t* s_d, unsigned long long& mn) {
   constexpr unsigned FULL = 0xFFFFFFFFu;
   constexpr int BIG = 0x3fffffff;
   const int lane = threadIdx.x & 31;
-  const uint4 td = __ldg(t.desc + tile);
+  const uint4 td = th.td;
 #ifdef CHSGA_CHECKED
-  // a tile outside the graph, or larger than a warp's lanes and vertex slots,
-  // is skipped whole (every lane reads the same descriptor)
-  if (!(td.x < td.y && td.y <= g.N && td.z < td.w && td.w <= g.S && td.w - td.z <= (uint32_t)kT1VertMax &&
-        ((td.y - 1) >> 3) - (td.x >> 3) < 32u)) {
-    if ((threadIdx.x & 31) == 0) chk_fail(tile, 6);
-    return;
-  }
+  if (td.y == 0) return;
 #endif
   const uint32_t cb = td.x, ce = td.y, sb = td.z, nv = td.w - td.z;
   const uint32_t q = (cb >> 3) + lane;
@@ -1463,8 +1513,8 @@ __device__ __forceinline__ void row_t1_tile(const GraphPtrs& g, const T1Ptrs& t,
   uint32_t keys = 0, hb = 0, inm = 0;
   if (lv) {
     dq = ldv4<COH>(D + 8 * (size_t)q);
-    keys = __ldg(g.lab4 + q);
-    hb = __ldg(t.heads + q);
+    keys = th.keys;
+    hb = th.hb;
     const uint32_t c0 = 8 * q;
     const uint32_t lo = cb > c0 ? cb - c0 : 0u;
     const uint32_t hi = ce - c0 < 8u ? ce - c0 : 8u;
@@ -1473,7 +1523,7 @@ __device__ __forceinline__ void row_t1_tile(const GraphPtrs& g, const T1Ptrs& t,
   }
   for (uint32_t v = lane; v < nv; v += 32) {
     const uint32_t sv = sb + v;
-    const uint4 r = __ldg(t.vrec + sv);
+    const uint4 r = v == (uint32_t)lane ? th.r0 : __ldg(t.vrec + sv);
     int G = 0, X = BIG;
     if (fix) G = ldu16<COH>(FL + 2 * (size_t)sv) - (int)r.x;
     if (!init) {
@@ -1592,22 +1642,23 @@ __global__ void __launch_bounds__(kT1Warps * 32, CHSGA_T1_BLOCKS) k_row_t1(Graph
                                                           const uint32_t* __restrict__ slot_word,
                                                           unsigned long long* __restrict__ best,
                                                           const StepCtl* __restrict__ ctl) {
-  pdl_wait();
   __shared__ int s_G[kT1Warps][kT1VertMax], s_X[kT1Warps][kT1VertMax];
   __shared__ uint32_t s_d[kT1Warps][kT1VertMax];
   __shared__ unsigned long long sm_best[1];
+  const int wp = threadIdx.x >> 5;
+  const uint32_t tile = blockIdx.x * kT1Warps + wp;
+  T1Head th{};
+  if (tile < t.ntiles) th = t1_head(g, t, tile);
+  pdl_wait();
   if (!ctl->any_active) return;
   const bool ending = ctl->any_ending != 0;
   if (ending) {
     if (threadIdx.x == 0) sm_best[0] = ~0ull;
     __syncthreads();
   }
-  const int wp = threadIdx.x >> 5;
-  const uint32_t tile = blockIdx.x * kT1Warps + wp;
   unsigned long long mn = ~0ull;
   if (tile < t.ntiles)
-    row_t1_tile<DEFER, false>(g, t, tile, D, T, BV, FL, __ldg(slot_word), s_G[wp], s_X[wp], s_d[wp],
-                              mn);
+    row_t1_tile<DEFER, false>(g, t, th, D, T, BV, FL, __ldg(slot_word), s_G[wp], s_X[wp], s_d[wp], mn);
   if (ending) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
@@ -1934,19 +1985,38 @@ __global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, 
   pull_item<R, ST, false>(BV, d, (int)(gt % G), off, edges, base);
 }
 
+// The graph constants of one k_pull_lv / k_pull_lv16 target: its list head
+// (edge range, first two sources and weights) and the four edges after those
+// two. Nothing here is written during a run, so the kernel loads it before
+// its pdl_wait, while the kernel before it drains.
+constexpr int kPullHeadEdges = 4;
+struct PullHead {
+  uint4 h, h2;
+  int2 e[kPullHeadEdges];
+};
+
+__device__ __forceinline__ PullHead pull_head(uint32_t d, const uint4* __restrict__ head,
+                                              const int2* __restrict__ edges, uint32_t n_edges) {
+  PullHead r;
+  r.h = __ldg(head + 2 * (size_t)d);
+  r.h2 = __ldg(head + 2 * (size_t)d + 1);
+  CHSGA_CHK_RANGE(r.h.x, r.h.y, n_edges, 11);
+  const uint32_t k = r.h.x + 2;
+#pragma unroll
+  for (int q = 0; q < kPullHeadEdges; ++q) r.e[q] = k + q < r.h.y ? __ldg(edges + k + q) : make_int2(0, 0);
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // k_pull_lv: one upward level [lo, hi) below the top region, the k_pull
 // update with the list head of each position in two 16-byte loads (the
 // first two sources are gathered without waiting for an edge load).
 // ---------------------------------------------------------------------------
 template <int R, typename ST, bool COH>
-__device__ __forceinline__ void pull_lv_item(ST* BV, uint32_t d, int lane, const uint4* __restrict__ head,
-                                             const int2* __restrict__ edges, uint32_t n_edges) {
+__device__ __forceinline__ void pull_lv_item(ST* BV, uint32_t d, int lane, const PullHead& hd,
+                                             const int2* __restrict__ edges) {
   constexpr int V = Lanes<R>::V;
-  uint4 h = __ldg(head + 2 * (size_t)d);
-  if (h.x == h.y) return;
-  uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
-  CHSGA_CHK_RANGE(h.x, h.y, n_edges, 11);
+  uint4 h = hd.h, h2 = hd.h2;
   if (h.x == h.y) return;
   h.z = CHSGA_CHK(h.z, 2 * (uint64_t)d, 12);
   h2.x = CHSGA_CHK(h2.x, 2 * (uint64_t)d, 12);
@@ -1972,7 +2042,14 @@ __device__ __forceinline__ void pull_lv_item(ST* BV, uint32_t d, int lane, const
   } else {
     relax(x0, (int)h.w);
   }
-  for (uint32_t k = h.x + 2; k < h.y; ++k) {
+  IV<V> xe[kPullHeadEdges];
+#pragma unroll
+  for (int q = 0; q < kPullHeadEdges; ++q)
+    if (h.x + 2 + q < h.y) xe[q] = ld_src<V, COH>(BV + (size_t)CHSGA_CHK(hd.e[q].x, 2 * (uint64_t)d, 12) * R + so);
+#pragma unroll
+  for (int q = 0; q < kPullHeadEdges; ++q)
+    if (h.x + 2 + q < h.y) relax(xe[q], hd.e[q].y);
+  for (uint32_t k = h.x + 2 + kPullHeadEdges; k < h.y; ++k) {
     const int2 ew = __ldg(edges + k);
     relax(ld_src<V, COH>(BV + (size_t)CHSGA_CHK(ew.x, 2 * (uint64_t)d, 12) * R + so), ew.y);
   }
@@ -1984,13 +2061,14 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
                                                  const uint4* __restrict__ head,
                                                  const int2* __restrict__ edges, uint32_t n_edges,
                                                  const StepCtl* __restrict__ ctl) {
-  pdl_wait();
   constexpr int G = Lanes<R>::G;
-  if (!ctl->any_active) return;
   const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t d = lo + (uint32_t)(gt / G);
-  if (d >= hi) return;
-  pull_lv_item<R, ST, false>(BV, d, (int)(gt % G), head, edges, n_edges);
+  PullHead hd{};
+  if (d < hi) hd = pull_head(d, head, edges, n_edges);
+  pdl_wait();
+  if (!ctl->any_active || d >= hi) return;
+  pull_lv_item<R, ST, false>(BV, d, (int)(gt % G), hd, edges);
 }
 
 // ---------------------------------------------------------------------------
@@ -2003,15 +2081,11 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
 // at a time, their sources gathered together.
 // ---------------------------------------------------------------------------
 template <int R, bool COH>
-__device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lane,
-                                               const uint4* __restrict__ head,
-                                               const int2* __restrict__ edges, uint32_t n_edges) {
+__device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lane, const PullHead& hd,
+                                               const int2* __restrict__ edges) {
   static_assert(R >= 8 && R % 8 == 0, "8 slots per lane");
-  constexpr int B = 4;
-  uint4 h = __ldg(head + 2 * (size_t)d);
-  uint4 h2 = __ldg(head + 2 * (size_t)d + 1);
-  if (h.x == h.y) return;
-  CHSGA_CHK_RANGE(h.x, h.y, n_edges, 11);
+  constexpr int B = kPullHeadEdges;
+  uint4 h = hd.h, h2 = hd.h2;
   if (h.x == h.y) return;
   h.z = CHSGA_CHK(h.z, 2 * (uint64_t)d, 12);
   h2.x = CHSGA_CHK(h2.x, 2 * (uint64_t)d, 12);
@@ -2034,7 +2108,7 @@ __device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lan
   uint32_t k = h.x + 2;
   int2 e[B];
 #pragma unroll
-  for (int q = 0; q < B; ++q) e[q] = k + q < h.y ? __ldg(edges + k + q) : make_int2(0, 0);
+  for (int q = 0; q < B; ++q) e[q] = hd.e[q];
   relax(x0, h.w);
   if (two) relax(x1, h2.y);
   for (; k < h.y; k += B) {
@@ -2059,13 +2133,14 @@ __global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, ui
                                                    uint32_t hi, const uint4* __restrict__ head,
                                                    const int2* __restrict__ edges, uint32_t n_edges,
                                                    const StepCtl* __restrict__ ctl) {
-  pdl_wait();
   constexpr int G = R / 8;
-  if (!ctl->any_active) return;
   const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t d = lo + (uint32_t)(gt / G);
-  if (d >= hi) return;
-  pull_lv16_item<R, false>(BV, d, (int)(gt % G), head, edges, n_edges);
+  PullHead hd{};
+  if (d < hi) hd = pull_head(d, head, edges, n_edges);
+  pdl_wait();
+  if (!ctl->any_active || d >= hi) return;
+  pull_lv16_item<R, false>(BV, d, (int)(gt % G), hd, edges);
 }
 
 // ---------------------------------------------------------------------------
@@ -2155,6 +2230,24 @@ __global__ void __launch_bounds__(256) k_pull_lv16c(uint16_t* __restrict__ BV, u
   pull_lv16c_item<R, false>(BV, d, (int)(gt % G), head, edges, n_edges);
 }
 
+// The graph constants of one k_down / k_down16 position: its downward list
+// head (edge range, first source and weight; none at or above `mid`), its
+// vertex (first char, length, string vertex) and its second in-edge. Loaded
+// before the kernel's pdl_wait, like PullHead.
+struct DownHead {
+  uint4 h, m;
+  int2 e1;
+};
+
+__device__ __forceinline__ DownHead down_head(const GraphPtrs& g, uint32_t d, uint32_t mid) {
+  DownHead r;
+  r.h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
+  r.m = __ldg(g.fin + d);
+  CHSGA_CHK_RANGE(r.h.x, r.h.y, g.n_dn, 13);
+  r.e1 = r.h.x + 1 < r.h.y ? __ldg(g.dn_in + r.h.x + 1) : make_int2(0, 0);
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // k_down: positions [lo, hi). Those below `mid` first pull their downward
 // in-edges (sources on higher levels, final); every position then finalises
@@ -2164,18 +2257,17 @@ __global__ void __launch_bounds__(256) k_pull_lv16c(uint16_t* __restrict__ BV, u
 // ---------------------------------------------------------------------------
 template <int R, bool FIXUP, typename ST, bool COH>
 __device__ __forceinline__ void down_item(const GraphPtrs& g, ST* BV, ST* T, ST* FL, uint32_t d, int lane,
-                                          uint32_t mid, const uint32_t* slot_word,
+                                          const DownHead& hd, const uint32_t* slot_word,
                                           unsigned long long* sm_best, bool ending_any) {
   constexpr int V = Lanes<R>::V;
   {
     const size_t so = (size_t)lane * V;
     ST* p = BV + (size_t)(2 * d) * R + so;
-    // independent loads first: the list head, the vertex words, the first
-    // score and the raw last score (the last entry is never written here;
-    // for a one-char vertex it is unused)
-    uint4 h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
-    uint4 m = __ldg(g.fin + d);
-    CHSGA_CHK_RANGE(h.x, h.y, g.n_dn, 13);
+    // the list head and vertex words came with the head; the first score and
+    // the raw last score load together (the last entry is never written
+    // here; for a one-char vertex it is unused)
+    uint4 h = hd.h;
+    uint4 m = hd.m;
     h.z = CHSGA_CHK(h.z, 2 * (uint64_t)g.S, 14);
     m.z = CHSGA_CHK(m.z, g.S, 15);
 #ifdef CHSGA_CHECKED
@@ -2200,8 +2292,15 @@ __device__ __forceinline__ void down_item(const GraphPtrs& g, ST* BV, ST* T, ST*
           }
         }
       };
-      relax(ld_src<V, COH>(BV + (size_t)h.z * R + so), (int)h.w);
-      for (uint32_t k = h.x + 1; k < h.y; ++k) {
+      const IV<V> x0 = ld_src<V, COH>(BV + (size_t)h.z * R + so);
+      if (h.y > h.x + 1) {
+        const IV<V> x1 = ld_src<V, COH>(BV + (size_t)CHSGA_CHK(hd.e1.x, 2 * (uint64_t)g.S, 14) * R + so);
+        relax(x0, (int)h.w);
+        relax(x1, hd.e1.y);
+      } else {
+        relax(x0, (int)h.w);
+      }
+      for (uint32_t k = h.x + 2; k < h.y; ++k) {
         const int2 ew = __ldg(g.dn_in + k);
         relax(ld_src<V, COH>(BV + (size_t)CHSGA_CHK(ew.x, 2 * (uint64_t)g.S, 14) * R + so), ew.y);
       }
@@ -2279,19 +2378,21 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
                                               const uint32_t* __restrict__ slot_word,
                                               unsigned long long* __restrict__ best,
                                               const StepCtl* __restrict__ ctl) {
-  pdl_wait();
   constexpr int G = Lanes<R>::G;
   __shared__ unsigned long long sm_best[R];
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  DownHead hd{};
+  if (d < hi) hd = down_head(g, d, mid);
+  pdl_wait();
   const bool ending_any = ctl->any_ending != 0;
   if (!ctl->any_active) return;
   if (ending_any) {
     for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
     __syncthreads();
   }
-  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t d = lo + (uint32_t)(gt / G);
   if (d < hi)
-    down_item<R, FIXUP, ST, false>(g, BV, T, FL, d, (int)(gt % G), mid, slot_word, sm_best, ending_any);
+    down_item<R, FIXUP, ST, false>(g, BV, T, FL, d, (int)(gt % G), hd, slot_word, sm_best, ending_any);
   if (ending_any) flush_min<R>(sm_best, best);
 }
 
@@ -2304,15 +2405,14 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
 // ---------------------------------------------------------------------------
 template <int R, bool COH>
 __device__ __forceinline__ void down16_item(const GraphPtrs& g, uint16_t* BV, uint16_t* FL, uint32_t d,
-                                            int lane, uint32_t mid, const uint32_t* slot_word,
+                                            int lane, const DownHead& hd, const uint32_t* slot_word,
                                             unsigned long long* sm_best, bool ending_any) {
   static_assert(R >= 8 && R % 8 == 0, "8 slots per lane");
   const size_t so = (size_t)lane * 8;
   uint4* p = reinterpret_cast<uint4*>(BV + (size_t)(2 * d) * R + so);
   auto src = [&](uint32_t i) { return ldv4<COH>(BV + (size_t)i * R + so); };
-  uint4 h = d < mid ? __ldg(g.dn_head + d) : make_uint4(0, 0, 0, 0);
-  uint4 m = __ldg(g.fin + d);
-  CHSGA_CHK_RANGE(h.x, h.y, g.n_dn, 13);
+  uint4 h = hd.h;
+  uint4 m = hd.m;
   h.z = CHSGA_CHK(h.z, 2 * (uint64_t)g.S, 14);
   m.z = CHSGA_CHK(m.z, g.S, 15);
   const uint4 f0 = *p;
@@ -2326,8 +2426,15 @@ __device__ __forceinline__ void down16_item(const GraphPtrs& g, uint16_t* BV, ui
     f.w = __vminu2(f.w, __vaddus2(x.w, ww));
   };
   if (h.y > h.x) {
-    relax(src(h.z), h.w);
-    for (uint32_t k = h.x + 1; k < h.y; ++k) {
+    const uint4 x0 = src(h.z);
+    if (h.y > h.x + 1) {
+      const uint4 x1 = src(CHSGA_CHK((uint32_t)hd.e1.x, 2 * (uint64_t)g.S, 14));
+      relax(x0, h.w);
+      relax(x1, (uint32_t)hd.e1.y);
+    } else {
+      relax(x0, h.w);
+    }
+    for (uint32_t k = h.x + 2; k < h.y; ++k) {
       const int2 ew = __ldg(g.dn_in + k);
       relax(src(CHSGA_CHK((uint32_t)ew.x, 2 * (uint64_t)g.S, 14)), (uint32_t)ew.y);
     }
@@ -2362,18 +2469,20 @@ __global__ void __launch_bounds__(256) k_down16(GraphPtrs g, uint16_t* __restric
                                                 const uint32_t* __restrict__ slot_word,
                                                 unsigned long long* __restrict__ best,
                                                 const StepCtl* __restrict__ ctl) {
-  pdl_wait();
   constexpr int G = R / 8;
   __shared__ unsigned long long sm_best[R];
+  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t d = lo + (uint32_t)(gt / G);
+  DownHead hd{};
+  if (d < hi) hd = down_head(g, d, mid);
+  pdl_wait();
   const bool ending_any = ctl->any_ending != 0;
   if (!ctl->any_active) return;
   if (ending_any) {
     for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
     __syncthreads();
   }
-  const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t d = lo + (uint32_t)(gt / G);
-  if (d < hi) down16_item<R, false>(g, BV, FL, d, (int)(gt % G), mid, slot_word, sm_best, ending_any);
+  if (d < hi) down16_item<R, false>(g, BV, FL, d, (int)(gt % G), hd, slot_word, sm_best, ending_any);
   if (ending_any) flush_min<R>(sm_best, best);
 }
 

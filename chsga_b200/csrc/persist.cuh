@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(PersistShape<R>::threads, 1) k_persist(Persist
         const uint32_t w = ld_cg_u32(a.word);
         unsigned long long mn = ~0ull;
         for (uint32_t tile = gwarp; tile < a.t1.ntiles; tile += nwarps)
-          row_t1_tile<true, true>(g, a.t1, tile, D, T, a.BV, a.FL, w, s_G, s_X, s_d, mn);
+          row_t1_tile<true, true>(g, a.t1, t1_head(g, a.t1, tile), D, T, a.BV, a.FL, w, s_G, s_X, s_d, mn);
         if (ending_any) {
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
@@ -197,7 +197,8 @@ __global__ void __launch_bounds__(PersistShape<R>::threads, 1) k_persist(Persist
       } else if constexpr (R >= 64) {
         uint16_t* ring = reinterpret_cast<uint16_t*>(psm) + (size_t)warp * kStreamRing * R;
         for (uint32_t run = gwarp; run * 32 < S; run += nwarps)
-          stream_run<R, true, true>(g, run, D, T, a.BV, a.FL, a.word, ring, sm_best, ending_any);
+          stream_run<R, true, true>(g, run, run_head(g, run), D, T, a.BV, a.FL, a.word, ring, sm_best,
+                                    ending_any);
       } else {
         constexpr int G = Pairs<R>::G;
         for (uint64_t it = gtid; it < (uint64_t)S * G; it += nthreads)
@@ -214,14 +215,18 @@ __global__ void __launch_bounds__(PersistShape<R>::threads, 1) k_persist(Persist
         const uint32_t lo = a.lvl_off[l], hi = a.lvl_off[l + 1];
         if constexpr (R >= 8) {
           constexpr int G = R / 8;
-          for (uint64_t it = gtid; it < (uint64_t)(hi - lo) * G; it += nthreads)
-            pull_lv16_item<R, true>(a.BV, lo + (uint32_t)(it / G), (int)(it % G), g.up_head, g.up_in,
-                                    g.n_up);
+          for (uint64_t it = gtid; it < (uint64_t)(hi - lo) * G; it += nthreads) {
+            const uint32_t d = lo + (uint32_t)(it / G);
+            pull_lv16_item<R, true>(a.BV, d, (int)(it % G), pull_head(d, g.up_head, g.up_in, g.n_up),
+                                    g.up_in);
+          }
         } else {
           constexpr int G = Lanes<R>::G;
-          for (uint64_t it = gtid; it < (uint64_t)(hi - lo) * G; it += nthreads)
-            pull_lv_item<R, uint16_t, true>(a.BV, lo + (uint32_t)(it / G), (int)(it % G), g.up_head,
-                                            g.up_in, g.n_up);
+          for (uint64_t it = gtid; it < (uint64_t)(hi - lo) * G; it += nthreads) {
+            const uint32_t d = lo + (uint32_t)(it / G);
+            pull_lv_item<R, uint16_t, true>(a.BV, d, (int)(it % G), pull_head(d, g.up_head, g.up_in, g.n_up),
+                                            g.up_in);
+          }
         }
         if (!grid_sync(a.bar, gen, a.ctl)) return;
       }
@@ -244,14 +249,18 @@ __global__ void __launch_bounds__(PersistShape<R>::threads, 1) k_persist(Persist
       auto down = [&](uint32_t lo, uint32_t mid, uint32_t hi) {
         if constexpr (R >= 8) {
           constexpr int G = R / 8;
-          for (uint64_t it = gtid; it < (uint64_t)(hi - lo) * G; it += nthreads)
-            down16_item<R, true>(g, a.BV, a.FL, lo + (uint32_t)(it / G), (int)(it % G), mid, a.word,
-                                 sm_best, ending_any);
+          for (uint64_t it = gtid; it < (uint64_t)(hi - lo) * G; it += nthreads) {
+            const uint32_t d = lo + (uint32_t)(it / G);
+            down16_item<R, true>(g, a.BV, a.FL, d, (int)(it % G), down_head(g, d, mid), a.word, sm_best,
+                                 ending_any);
+          }
         } else {
           constexpr int G = Lanes<R>::G;
-          for (uint64_t it = gtid; it < (uint64_t)(hi - lo) * G; it += nthreads)
-            down_item<R, false, uint16_t, true>(g, a.BV, T, a.FL, lo + (uint32_t)(it / G), (int)(it % G),
-                                                mid, a.word, sm_best, ending_any);
+          for (uint64_t it = gtid; it < (uint64_t)(hi - lo) * G; it += nthreads) {
+            const uint32_t d = lo + (uint32_t)(it / G);
+            down_item<R, false, uint16_t, true>(g, a.BV, T, a.FL, d, (int)(it % G), down_head(g, d, mid), a.word,
+                                                sm_best, ending_any);
+          }
         }
       };
       if (a.fl == 0) {
