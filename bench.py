@@ -842,7 +842,7 @@ def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits):
     pctx.close()
     w = pr["row_bits"] // 8
     row_avg_s = pr["row_ms"] / max(1, pr["row_launches"]) / 1e3
-    auto16 = "k_row_delta" if R == 128 else ("k_row_stream" if R >= 64 else ("k_row_dpx" if R >= 2 else "k_row_t1"))
+    auto16 = "k_row_stream" if R >= 64 else ("k_row_dpx" if R >= 2 else "k_row_t1")
     kname = {cb.ROW_DIRECT: "k_row_direct", cb.ROW_TILED: "k_row_tiled", cb.ROW_DPX: "k_row_dpx",
              cb.ROW_STREAM: "k_row_stream", cb.ROW_DELTA: "k_row_delta"}.get(
         opts["row_kernel"] if R > 1 else 0, auto16 if pr["row_bits"] == 16 else "k_row_direct")

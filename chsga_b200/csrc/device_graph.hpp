@@ -74,6 +74,13 @@ struct HostLayout {
 // instead (count stored negated): each level padded with no-op edges to
 // whole rounds of 32, the rounds run in order by one warp.
 constexpr uint32_t kTopWarpLevelMax = 64;
+// Region size limits in hierarchy vertices: the most a region's scores and
+// chunk buffers leave room for in one CTA's shared memory, and the default.
+// A region that holds the big levels (6 and 7 on the config-2 graph) sweeps
+// them on one SM per slot; in grid launches they cost less, and 8000
+// vertices measured fastest or within 1 % of it at every slot count.
+constexpr uint32_t kTopMaxVertices = 23000;
+constexpr uint32_t kTopDefaultVertices = 8000;
 struct HostTop {
   uint32_t first_level = 0;  // level index where the top region starts
   uint32_t K0 = 0, K = 0;    // hierarchy positions [K0, K0+K)

@@ -132,7 +132,6 @@ struct RowTileDev {
   bool ok = false;
 };
 
-constexpr uint32_t kTopMaxVertices = 23000;
 constexpr uint32_t kRow16Max = 65000;  // longest read whose rows fit uint16  // 2 x int32 per vertex in shared memory
 constexpr int kTopThreads = 1024;
 
@@ -296,7 +295,7 @@ std::unique_ptr<TopDev> make_top(const HostLayout& L, const GraphDev& d, uint32_
 // The top region for a vertex limit (0 = the graph's default), built once
 // per context and limit.
 const TopDev* top_for(chsga_ctx& c, uint32_t K) {
-  if (K == 0 || K == kTopMaxVertices) return nullptr;
+  if (K == 0 || K == kTopDefaultVertices) return nullptr;
   require(K <= kTopMaxVertices, CHSGA_ERR_INVALID_ARG,
           "top_vertices above " + std::to_string(kTopMaxVertices) + " do not fit shared memory");
   auto& t = c.tops[K];
@@ -836,7 +835,7 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   d.dn_head.upload(to4(L.dn_head), s);
   d.up_head.upload(to4(L.up_head), s);
   d.fin.upload(to4(L.fin), s);
-  auto top = make_top(L, d, kTopMaxVertices, s);
+  auto top = make_top(L, d, kTopDefaultVertices, s);
   {
     HostT1 t1 = build_t1(L);
     if (t1.ok) {
@@ -1784,7 +1783,7 @@ chsga_batch_opts autotune(chsga_ctx& c, const char* const* reads, const uint32_t
   }
   // level grouping
   cur = best;
-  for (uint32_t K : {8000u, 2000u}) {
+  for (uint32_t K : {kTopMaxVertices, 3000u}) {
     chsga_batch_opts b = cur;
     b.top_vertices = K;
     const double g = run(b, 0);

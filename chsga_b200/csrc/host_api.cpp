@@ -208,8 +208,9 @@ chsga_status chsga_check_layout(const chsga_host_graph* g, uint32_t slots, uint3
     HostLayout L = build_layout(v);
     std::memset(out, 0, sizeof(*out));
     out->num_levels = L.levels;
-    require(top_vertices <= 23000, CHSGA_ERR_INVALID_ARG, "top_vertices above 23000");
-    HostTop top = build_top(L, top_vertices ? top_vertices : 23000, 1024);
+    require(top_vertices <= kTopMaxVertices, CHSGA_ERR_INVALID_ARG,
+            "top_vertices above " + std::to_string(kTopMaxVertices));
+    HostTop top = build_top(L, top_vertices ? top_vertices : kTopDefaultVertices, 1024);
     out->top_first_level = top.first_level;
     out->top_vertices = top.K;
     for (uint32_t d = 0; d < top.K0; ++d) {

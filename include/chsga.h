@@ -207,7 +207,7 @@ typedef struct {
   uint64_t sweep_up_targets, sweep_up_edges, sweep_down_targets, sweep_down_edges;
 } chsga_layout_stats;
 chsga_status chsga_check_layout(const chsga_host_graph* g, uint32_t slots, uint32_t row_bits,
-                                uint32_t top_vertices /* 0 = 23000, as chsga_batch_opts */,
+                                uint32_t top_vertices /* 0 = 8000, as chsga_batch_opts */,
                                 chsga_layout_stats* out);
 
 const char* chsga_last_error_global(void);
@@ -271,7 +271,8 @@ typedef struct {
   uint32_t row_kernel;    /* CHSGA_ROW_*: which row kernel runs; 0 = AUTO */
   uint32_t top_vertices;  /* level grouping: hierarchy vertices (highest levels first) swept
                              by the one-CTA-per-slot top kernel, the levels below one grid
-                             launch each; 0 = 23000 (the most shared memory holds) */
+                             launch each; 0 = 8000; at most 23000 (the most shared memory
+                             holds) */
 } chsga_batch_opts;
 /* Row kernels. With 16-bit rows, slots >= 2 and no string vertex label over
  * 512 chars, AUTO runs STREAM for slots >= 64 and DPX below, else DIRECT;
