@@ -577,6 +577,10 @@ def run_launch_compare(args):
     ctx_coop = cb.Context(0).load(g)
     pctx_coop = cb.Context(0, flags=cb.FLAG_PROFILE).load(g)
     del os.environ["CHSGA_PULL_COOP"]
+    os.environ["CHSGA_PULL_LEAN"] = "0"  # the unbounded upward form on every level
+    ctx_gen = cb.Context(0).load(g)
+    pctx_gen = cb.Context(0, flags=cb.FLAG_PROFILE).load(g)
+    del os.environ["CHSGA_PULL_LEAN"]
     out = {"mode": "launch-compare", "num_chars": N, "shapes": []}
     want = [int(x) for x in args.shapes.split(",")]
     shapes = [(R, make_reads(g, n, seed, len_max=lm)) for R, n, seed, lm in
@@ -590,6 +594,9 @@ def run_launch_compare(args):
         if R == 1:
             runs.append(("graphs_direct_row", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16,
                                                    row_kernel=cb.ROW_DIRECT)))
+        if R >= 8:
+            runs.append(("graphs_pull_unbounded", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16,
+                                                       ctx=ctx_gen)))
         if R >= 64:
             runs.append(("graphs_pull_coop", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16,
                                                   ctx=ctx_coop)))
@@ -622,10 +629,11 @@ def run_launch_compare(args):
         st = max(1, pr["row_launches"])
         out["plain_profile_" + name] = {k.replace("_ms", "_us"): 1e3 * pr[k] / st for k in
                                         ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")}
-    # per-kernel-group times at 128 slots, upward levels as k_pull_lv16 and as k_pull_lv16c
+    # per-kernel-group times at 128 slots, upward levels as k_pull_lv16 (two-edge form where it
+    # applies), as the unbounded k_pull_lv16 and as k_pull_lv16c
     if 128 in want:
         reads128 = make_reads(g, 128, 31_003, len_max=1000)
-        for name, cx in (("pull16", pctx), ("pull16c", pctx_coop)):
+        for name, cx in (("pull16", pctx), ("pull16_unbounded", pctx_gen), ("pull16c", pctx_coop)):
             cx.align_scores_batched(reads128, slots=128)
             pr = cx.profile()
             st = max(1, pr["row_launches"])
@@ -634,6 +642,8 @@ def run_launch_compare(args):
     pctx.close()
     pctx_coop.close()
     ctx_coop.close()
+    pctx_gen.close()
+    ctx_gen.close()
     ctx_nopdl.close()
     ctx.close()
     print(json.dumps(out), flush=True)

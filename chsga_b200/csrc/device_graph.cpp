@@ -46,7 +46,7 @@ HostLayout build_layout(const chsga_graph_host& g) {
   if (first_sp != kNone) L.special = (unsigned char)g.labels[first_sp];
   L.lab2.assign((N + 15) / 16, 0);
   L.lab_sp.assign((N + 31) / 32, 0);
-  L.lab4.assign((N + 7) / 8 + 2, 0);  // two spare words: the kernels read a word ahead
+  L.lab4.assign((N + 7) / 8 + 3, 0);  // three spare words: the key window reads two words ahead
   uint64_t bad_sp = kNone;
   const int64_t words = (N + 31) / 32;
 #pragma omp parallel for reduction(min : bad_sp) schedule(static)
@@ -301,8 +301,12 @@ HostLayout build_layout(const chsga_graph_host& g) {
   L.lvl_off.push_back(S);
   L.levels = (uint32_t)L.lvl_off.size() - 1;
   L.lvl_up_edges.resize(L.levels);
-  for (uint32_t l = 0; l < L.levels; ++l)
+  L.lvl_up_maxdeg.assign(L.levels, 0);
+  for (uint32_t l = 0; l < L.levels; ++l) {
     L.lvl_up_edges[l] = L.up_off[L.lvl_off[l + 1]] - L.up_off[L.lvl_off[l]];
+    for (uint32_t d = L.lvl_off[l]; d < L.lvl_off[l + 1]; ++d)
+      L.lvl_up_maxdeg[l] = std::max(L.lvl_up_maxdeg[l], L.up_off[d + 1] - L.up_off[d]);
+  }
 
   // --- string-graph in-CSR for the traceback walk (traceback.hpp:716) -------
   const chsga_csr& sg = g.string_graph;

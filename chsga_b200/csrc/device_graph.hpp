@@ -60,6 +60,7 @@ struct HostLayout {
   std::vector<uint32_t> fin;               // 4 words per position: first char, length, string vertex, 0
   std::vector<uint32_t> lvl_off;           // levels+1
   std::vector<uint32_t> lvl_up_edges;      // per level: number of up_in entries
+  std::vector<uint32_t> lvl_up_maxdeg;     // per level: most up_in entries of one position
   std::vector<uint32_t> istr_off, istr_src;  // string-graph in-CSR (ascending source)
   uint64_t char_in_edges = 0;
 };

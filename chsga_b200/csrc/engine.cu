@@ -175,6 +175,9 @@ struct chsga_ctx {
   bool pdl = true;
   // upward levels with the lane group's cooperative edge loads, 64+ slots (CHSGA_PULL_COOP)
   bool pull_coop = false;
+  // upward levels in the form bounded by the level's largest edge list
+  // (CHSGA_PULL_LEAN=0 runs the unbounded form everywhere)
+  bool pull_lean = true;
   chsga::DevArr<unsigned char> reads;
   chsga::DevArr<chsga::dev::ReadDesc> queue;
   uint32_t qmask = 0xFFFFFFFFu;                      // queue ring mask (serving), else linear
@@ -549,17 +552,15 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   for (uint32_t l = 0; l < fl; ++l) {
     if (L.lvl_up_edges[l] == 0) continue;
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
-    if constexpr (std::is_same_v<ST, uint16_t> && R >= 64) {
-      if (c.pull_coop)
-        chain_launch(c, dev::k_pull_lv16c<R>, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, BVc, lo, hi,
-                     c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
-      else
-        chain_launch(c, dev::k_pull_lv16<R>, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, BVc, lo, hi,
-                     c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
-    } else if constexpr (std::is_same_v<ST, uint16_t> && R >= 8)
-      chain_launch(c, dev::k_pull_lv16<R>, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, BVc, lo, hi,
-                   c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
-    else
+    if constexpr (std::is_same_v<ST, uint16_t> && R >= 8) {
+      // the two-edge form where no target of the level has more
+      auto k = c.pull_lean && L.lvl_up_maxdeg[l] <= 2 ? dev::k_pull_lv16<R, 2> : dev::k_pull_lv16<R, 0>;
+      if constexpr (R >= 64) {
+        if (c.pull_coop) k = dev::k_pull_lv16c<R>;
+      }
+      chain_launch(c, k, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, BVc, lo, hi, c.g->gd.up_head.p,
+                   c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
+    } else
       chain_launch(c, dev::k_pull_lv<R, ST>, nblocks((uint64_t)(hi - lo) * G), 256, 0, s, BVc, lo, hi,
                    c.g->gd.up_head.p, c.g->gd.up_in.p, c.g->gp.n_up, b.ctl.p);
   }
@@ -2000,6 +2001,7 @@ chsga_ctx* fork_context(chsga_ctx& p) {
   c->plain_mode = p.plain_mode;
   c->pdl = p.pdl;
   c->pull_coop = p.pull_coop;
+  c->pull_lean = p.pull_lean;
   CK(cudaSetDevice(c->device));
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
@@ -2110,6 +2112,7 @@ chsga_status chsga_open(const chsga_opts* opts, chsga_ctx** out) {
     }
     if (const char* pd = std::getenv("CHSGA_PDL")) c->pdl = std::string(pd) != "0";
     if (const char* pc = std::getenv("CHSGA_PULL_COOP")) c->pull_coop = std::string(pc) == "1";
+    if (const char* pn = std::getenv("CHSGA_PULL_LEAN")) c->pull_lean = std::string(pn) != "0";
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     size_t free_b = 0, total_b = 0;

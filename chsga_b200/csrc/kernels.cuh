@@ -599,11 +599,13 @@ __device__ __forceinline__ uint32_t sel(uint32_t a, uint32_t b, uint32_t m) {
 struct KeyWindow {
   const uint32_t* w;
   uint64_t win;
+  uint32_t nx;  // the word after the window, loaded a word (8 chars) before it is needed
   uint32_t sh;
   KeyWindow() = default;
   __device__ __forceinline__ KeyWindow(const uint32_t* lab4, uint32_t c) {
     w = lab4 + (c >> 3);
     win = (uint64_t)__ldg(w) | ((uint64_t)__ldg(w + 1) << 32);
+    nx = __ldg(w + 2);
     sh = (c & 7u) * 4u;
   }
   __device__ __forceinline__ uint32_t next() {
@@ -611,7 +613,8 @@ struct KeyWindow {
     sh += 4;
     if (sh == 32) {
       ++w;
-      win = (win >> 32) | ((uint64_t)__ldg(w + 1) << 32);
+      win = (win >> 32) | ((uint64_t)nx << 32);
+      nx = __ldg(w + 2);
       sh = 0;
     }
     return k;
@@ -1990,20 +1993,24 @@ __global__ void __launch_bounds__(256) k_pull(ST* __restrict__ BV, uint32_t lo, 
 // two. Nothing here is written during a run, so the kernel loads it before
 // its pdl_wait, while the kernel before it drains.
 constexpr int kPullHeadEdges = 4;
-struct PullHead {
+template <int NE>
+struct PullHeadT {
   uint4 h, h2;
-  int2 e[kPullHeadEdges];
+  int2 e[NE > 0 ? NE : 1];  // unused when NE = 0
 };
+using PullHead = PullHeadT<kPullHeadEdges>;
 
-__device__ __forceinline__ PullHead pull_head(uint32_t d, const uint4* __restrict__ head,
-                                              const int2* __restrict__ edges, uint32_t n_edges) {
-  PullHead r;
+// NE = the edges after the head's two that come with it (0 or kPullHeadEdges)
+template <int NE = kPullHeadEdges>
+__device__ __forceinline__ PullHeadT<NE> pull_head(uint32_t d, const uint4* __restrict__ head,
+                                                   const int2* __restrict__ edges, uint32_t n_edges) {
+  PullHeadT<NE> r;
   r.h = __ldg(head + 2 * (size_t)d);
   r.h2 = __ldg(head + 2 * (size_t)d + 1);
   CHSGA_CHK_RANGE(r.h.x, r.h.y, n_edges, 11);
   const uint32_t k = r.h.x + 2;
 #pragma unroll
-  for (int q = 0; q < kPullHeadEdges; ++q) r.e[q] = k + q < r.h.y ? __ldg(edges + k + q) : make_int2(0, 0);
+  for (int q = 0; q < NE; ++q) r.e[q] = k + q < r.h.y ? __ldg(edges + k + q) : make_int2(0, 0);
   return r;
 }
 
@@ -2080,10 +2087,16 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
 // min, as in the int form. Edges beyond the two in the head are fetched four
 // at a time, their sources gathered together.
 // ---------------------------------------------------------------------------
-template <int R, bool COH>
-__device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lane, const PullHead& hd,
+// MAXE = 2: every target of the level has at most the head's two edges (the
+// host knows each level's largest list), so the form has no edge loop and
+// needs about half the registers (26 against 48 at 128 slots): eight blocks
+// per SM instead of five. MAXE = 0: any number of edges.
+template <int R, bool COH, int MAXE = 0, int NE = kPullHeadEdges>
+__device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lane, const PullHeadT<NE>& hd,
                                                const int2* __restrict__ edges) {
   static_assert(R >= 8 && R % 8 == 0, "8 slots per lane");
+  static_assert(MAXE == 0 || MAXE == 2, "edge bound");
+  static_assert(MAXE == 2 || NE == kPullHeadEdges, "the prefetched edges");
   constexpr int B = kPullHeadEdges;
   uint4 h = hd.h, h2 = hd.h2;
   if (h.x == h.y) return;
@@ -2105,6 +2118,12 @@ __device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lan
   const uint4 x0 = src(h.z);
   uint4 x1 = x0;
   if (two) x1 = src(h2.x);
+  if constexpr (MAXE == 2) {
+    relax(x0, h.w);
+    if (two) relax(x1, h2.y);
+    if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
+    return;
+  }
   uint32_t k = h.x + 2;
   int2 e[B];
 #pragma unroll
@@ -2128,19 +2147,20 @@ __device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lan
   if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
 }
 
-template <int R>
+template <int R, int MAXE = 0>
 __global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, uint32_t lo,
                                                    uint32_t hi, const uint4* __restrict__ head,
                                                    const int2* __restrict__ edges, uint32_t n_edges,
                                                    const StepCtl* __restrict__ ctl) {
   constexpr int G = R / 8;
+  constexpr int NE = MAXE == 2 ? 0 : kPullHeadEdges;
   const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t d = lo + (uint32_t)(gt / G);
-  PullHead hd{};
-  if (d < hi) hd = pull_head(d, head, edges, n_edges);
+  PullHeadT<NE> hd{};
+  if (d < hi) hd = pull_head<NE>(d, head, edges, n_edges);
   pdl_wait();
   if (!ctl->any_active || d >= hi) return;
-  pull_lv16_item<R, false>(BV, d, (int)(gt % G), hd, edges);
+  pull_lv16_item<R, false, MAXE, NE>(BV, d, (int)(gt % G), hd, edges);
 }
 
 // ---------------------------------------------------------------------------
