@@ -619,6 +619,19 @@ struct KeyWindow {
     }
     return k;
   }
+  // the keys of the next four chars, 4 bits each; the window must be at a
+  // char c with c % 4 == 0
+  __device__ __forceinline__ uint32_t next4() {
+    const uint32_t k = (uint32_t)(win >> sh) & 0xFFFFu;
+    sh += 16;
+    if (sh == 32) {
+      ++w;
+      win = (win >> 32) | ((uint64_t)nx << 32);
+      nx = __ldg(w + 2);
+      sh = 0;
+    }
+    return k;
+  }
 };
 
 // The chain chars of one vertex (c = f+1 .. f+len-1); TRACK also keeps the
@@ -1264,8 +1277,9 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
   DV cur, nxt;
   prefetch(0, cur);
   zin = take_word();  // the run's first group
-  auto run = [&](auto track_tag) {
+  auto run = [&](auto track_tag, auto fix_tag) {
     constexpr bool TRACK = decltype(track_tag)::value;
+    constexpr bool FIX = decltype(fix_tag)::value;  // some slot of the warp applies a deferred closure
     for (uint32_t i = 0; i < nv; ++i) {
       if (i + 1 < nv) prefetch(i + 1, nxt);
       const uint32_t f = cur.f, len = cur.len;
@@ -1278,7 +1292,7 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
 #pragma unroll
         for (int p = 0; p < P; ++p) {
           delta[p] = (dtab[p] >> key) & ONES;
-          if (any_fix) dprev.h[p] = sel(__vminu2(dprev.h[p], F.h[p]), dprev.h[p], fmask[p]);
+          if (FIX) dprev.h[p] = sel(__vminu2(dprev.h[p], F.h[p]), dprev.h[p], fmask[p]);
           t.h[p] = dprev.h[p] + ONES;
         }
 #pragma unroll
@@ -1299,24 +1313,23 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
       put(f, 0u);
       if (TRACK) track_char(t, f);
       uint32_t off2 = 0;
-      for (uint32_t q = 1; q < len; ++q) {
-        const uint32_t c = f + q;
-        // the pair increments of this char's byte, -1..1 per half: a 32-bit
-        // add is exact since no half leaves 0..65535 (scores stay in
-        // 0..65001, consecutive chars differ by at most 1)
-        // selector: byte c & 3 of zin, then three zero bytes of the second
-        // operand (an index below 256)
-        const uint2 e = lut[__byte_perm(zin, 0u, (c & 3u) | 0x4440u)];
+      // one chain char from its input byte (its four slots' 2-bit fields)
+      // and its label key; returns its output byte in bits 0-7 (bits 16-21
+      // hold leftovers that the caller drops)
+      auto step = [&](uint32_t byte_in, uint32_t key) -> uint32_t {
+        // the pair increments of the byte, -1..1 per half: a 32-bit add is
+        // exact since no half leaves 0..65535 (scores stay in 0..65001,
+        // consecutive chars differ by at most 1)
+        const uint2 e = lut[byte_in];
         draw.h[0] += e.x;
         draw.h[1] += e.y;
         U2<P> dq = draw;
-        const uint32_t key = kw.next();
         off2 += ONES;
         const U2<P> tp = t;
 #pragma unroll
         for (int p = 0; p < P; ++p) {
           const uint32_t delta = (dtab[p] >> key) & ONES;
-          if (any_fix) dq.h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq.h[p]), dq.h[p], fmask[p]);
+          if (FIX) dq.h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq.h[p]), dq.h[p], fmask[p]);
           uint32_t x = __viaddmin_u16x2(t.h[p], ONES, dq.h[p] + ONES);
           x = __viaddmin_u16x2(dprev.h[p], delta, x);
           t.h[p] = sel(delta, x, imask[p]);
@@ -1329,17 +1342,50 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
         // 0..2 in every half (idle slots included): low halves at bits 0
         // and 4, high halves at 16 and 20, folded into one byte
         const uint32_t dd = d0 | (d1 << 4);
-        put(c, (dd | (dd >> 14)) & 0xFFu);
+        return dd | (dd >> 14);
+      };
+      // one char at a time up to a group boundary: selector = byte c & 3 of
+      // zin, then three zero bytes of the second operand (an index below 256)
+      auto one = [&](uint32_t c) {
+        put(c, step(__byte_perm(zin, 0u, (c & 3u) | 0x4440u), kw.next()) & 0xFFu);
         if (TRACK) track_char(t, c);
+      };
+      uint32_t c = f + 1;
+      const uint32_t cend = f + len;
+      for (; c < cend && (c & 3u); ++c) one(c);
+      // whole groups inside the vertex: constant byte positions, the four
+      // keys from one window read, one word store (a group that starts
+      // after cb lies wholly in this run)
+      for (; c + 4 <= cend; c += 4) {
+        const uint32_t k4 = kw.next4();
+        uint32_t word = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint32_t o = step(__byte_perm(zin, 0u, 0x4440u | (uint32_t)j), (k4 >> (4 * j)) & 0xFu);
+          // byte j of word := byte 0 of o
+          word = __byte_perm(word, o, j == 0 ? 0x3214u : j == 1 ? 0x3240u : j == 2 ? 0x3410u : 0x4210u);
+          if (TRACK) track_char(t, c + j);
+        }
+        TZ[(size_t)(c >> 2) * 32 + lane] = word;
+        zout = word;
+        if (c + 4 < ce) zin = take_word();
       }
+      for (; c < cend; ++c) one(c);
       if (len > 1) stp<P>(BV + (size_t)(2 * cur.d + 1) * R + so, t);
       cur = nxt;
     }
   };
-  if (track)
-    run(std::true_type{});
-  else
-    run(std::false_type{});
+  if (track) {
+    if (any_fix)
+      run(std::true_type{}, std::true_type{});
+    else
+      run(std::true_type{}, std::false_type{});
+  } else {
+    if (any_fix)
+      run(std::false_type{}, std::true_type{});
+    else
+      run(std::false_type{}, std::false_type{});
+  }
   // the run's last group when it ends inside a group
   if (((ce - 1) & 3u) != 3u) {
     const uint32_t g0 = (ce - 1) & ~3u, k = ce - g0;  // bytes of the group this run holds
