@@ -216,8 +216,14 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    p = os.path.join(ROOT, "profiles", "k_row_traffic.json")
+def ncu_traffic(kname="k_row_stream"):
+    """The ncu DRAM bytes of one row-kernel launch, scaled to the bench graph
+    (profiles/k_row_traffic.json for k_row_stream, k_row_delta_traffic.json
+    for k_row_delta)."""
+    name = {"k_row_stream": "k_row_traffic.json", "k_row_delta": "k_row_delta_traffic.json"}.get(kname)
+    if name is None:
+        return None
+    p = os.path.join(ROOT, "profiles", name)
     try:
         with open(p) as f:
             return json.load(f)
@@ -852,7 +858,8 @@ def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits):
     pctx.close()
     w = pr["row_bits"] // 8
     row_avg_s = pr["row_ms"] / max(1, pr["row_launches"]) / 1e3
-    auto16 = "k_row_stream" if R >= 64 else ("k_row_dpx" if R >= 2 else "k_row_t1")
+    # AUTO: delta rows for score-only steps at 128 slots (this pass is score-only)
+    auto16 = "k_row_delta" if R == 128 else ("k_row_stream" if R >= 64 else ("k_row_dpx" if R >= 2 else "k_row_t1"))
     kname = {cb.ROW_DIRECT: "k_row_direct", cb.ROW_TILED: "k_row_tiled", cb.ROW_DPX: "k_row_dpx",
              cb.ROW_STREAM: "k_row_stream", cb.ROW_DELTA: "k_row_delta"}.get(
         opts["row_kernel"] if R > 1 else 0, auto16 if pr["row_bits"] == 16 else "k_row_direct")
@@ -860,7 +867,7 @@ def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits):
         kname = "k_row_direct"  # the 16-bit kernels do not run 32-bit rows
     ab = algorithmic_delta_row_bytes(st, R, multi) if kname == "k_row_delta" else \
         algorithmic_row_bytes(st, R, multi, w)
-    tr = ncu_traffic() if kname == "k_row_stream" else None
+    tr = ncu_traffic(kname)
     total = pr["row_ms"] + pr["sweep_up_ms"] + pr["top_ms"] + pr["sweep_down_ms"] + pr["other_ms"]
     # working set of one row-step: two score rows, BV and FL, graph arrays
     S = st["num_strings"]
@@ -880,6 +887,22 @@ def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits):
         "per_row_step_us": {k.replace("_ms", ""): 1e3 * pr[k] / max(1, pr["row_launches"]) for k in
                             ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")},
     }
+    if kname == "k_row_delta":
+        # delta rows move about a quarter of the 16-bit rows' bytes and are bound by
+        # instruction issue; the 16-bit stream kernel on the same reads, for context
+        out["limiter"] = "instruction issue (2-bit rows: a quarter of the 16-bit rows' bytes)"
+        q = cb.Context(device, flags=cb.FLAG_PROFILE)
+        q.load(g)
+        q.align_scores_batched(sample, **dict(opts, slots=R, row_kernel=cb.ROW_STREAM), row_bits=16)
+        qs = q.profile()
+        q.close()
+        s_avg = qs["row_ms"] / max(1, qs["row_launches"]) / 1e3
+        s_ab = algorithmic_row_bytes(st, R, multi, 2)
+        out["stream_rows"] = {"kernel": f"k_row_stream<{R}>", "avg_launch_ms": s_avg * 1e3,
+                              "algorithmic_bytes_per_launch": s_ab, "achieved": s_ab / s_avg / 1e9,
+                              "frac": s_ab / s_avg / 1e9 / peak,
+                              "row_step_ms": sum(qs[k] for k in ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms",
+                                                                 "other_ms")) / max(1, qs["row_launches"])}
     # sweep kernels below the top region (the top region the run used)
     lay = g.check_layout(R, pr["row_bits"], opts["top_vertices"] if R > 1 else 0)
     up_b, down_b = algorithmic_sweep_bytes(st, lay, R, w)

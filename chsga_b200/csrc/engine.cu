@@ -505,9 +505,10 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
     }
   }
   if constexpr (std::is_same_v<ST, uint16_t> && DEFER && R == 128) {
-    // 2-bit delta rows (score-only): every step of a run uses this kernel,
-    // so the rows stay in its format from the first admission on
-    if (L.max_len <= 512 && c.row_kernel == RowKernel::Delta) {
+    // 2-bit delta rows (score-only; AUTO at 128 slots): every step of a run
+    // uses this kernel, so the rows stay in its format from the first
+    // admission on
+    if (L.max_len <= 512 && (c.row_kernel == RowKernel::Delta || c.row_kernel == RowKernel::Auto)) {
       const uint64_t runs = ((uint64_t)L.S + 31) / 32;
       constexpr unsigned tpb = dev::kStreamWarps * 32;
       chain_launch(c, dev::k_row_delta, nblocks(runs * 32, tpb), tpb, dev::delta_smem_bytes(), s, c.g->gp, D, T,
@@ -1772,11 +1773,11 @@ chsga_batch_opts autotune(chsga_ctx& c, const char* const* reads, const uint32_t
   }
   // row kernel
   cur = best;
-  for (uint32_t rk : {(uint32_t)CHSGA_ROW_DELTA, (uint32_t)CHSGA_ROW_DPX, (uint32_t)CHSGA_ROW_DIRECT,
+  for (uint32_t rk : {(uint32_t)CHSGA_ROW_STREAM, (uint32_t)CHSGA_ROW_DPX, (uint32_t)CHSGA_ROW_DIRECT,
                       (uint32_t)CHSGA_ROW_TILED}) {
     if (rk == CHSGA_ROW_TILED && cur.slots < 32) continue;
     if (rk == CHSGA_ROW_DPX && cur.slots < 64) continue;        // AUTO already is DPX there
-    if (rk == CHSGA_ROW_DELTA && cur.slots != 128) continue;    // 128 slots only
+    if (rk == CHSGA_ROW_STREAM && cur.slots != 128) continue;   // AUTO is STREAM at 64, DELTA at 128
     chsga_batch_opts b = cur;
     b.row_kernel = rk;
     const double g = run(b, 0);

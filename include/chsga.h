@@ -275,9 +275,10 @@ typedef struct {
                              holds) */
 } chsga_batch_opts;
 /* Row kernels. With 16-bit rows, slots >= 2 and no string vertex label over
- * 512 chars, AUTO runs STREAM for slots >= 64 and DPX below, else DIRECT;
- * one slot runs the tile kernel (one warp per tile of whole vertices, one
- * lane per 8 chars). DELTA (128 slots, score-only) = STREAM over rows stored
+ * 512 chars, AUTO runs DELTA for score-only steps at 128 slots, STREAM for
+ * other steps at 64 slots and up, DPX below, else DIRECT; one slot runs the
+ * tile kernel (one warp per tile of whole vertices, one lane per 8 chars).
+ * DELTA (128 slots, score-only) = STREAM over rows stored
  * as the raw first score of every vertex (16 bits per slot) and, per char,
  * the difference to the char before in 2 bits per slot (consecutive chars of
  * a vertex differ by at most 1 in every row): 0.26 bytes per cell instead of
