@@ -85,6 +85,8 @@ def parse():
                         "and 128 slots as CUDA-graph chains and as persistent launches, device time, "
                         "scores compared")
     p.add_argument("--shapes", default="1,8,128", help="with --launch-compare: slot counts to compare")
+    p.add_argument("--top-compare", action="store_true",
+                   help="device time per row-step for several top-region sizes at 1-128 slots, one JSON line")
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
     p.add_argument("--plain-reads", type=int, default=64,
                    help="reads of the first timed batch (drawn at random) run through the plain path")
@@ -563,6 +565,49 @@ def run_traceback_cfg1(args):
     return 0
 
 
+def run_top_compare(args):
+    """Device time per row-step of the same reads with top regions of
+    23000, 12000, 8000 (the default), 5000 and 3000 hierarchy vertices, at
+    1, 8, 16, 32, 64 and 128 slots on the config-2-mix graph, and the
+    per-kernel-group split (CUDA events between the groups) at 1, 8 and 128
+    slots. Every run's scores must equal the first's. One JSON line."""
+    import numpy as np
+
+    import chsga_b200 as cb
+    g = make_graph(args.backbone)
+    ctx = cb.Context(0).load(g)
+    pctx = cb.Context(0, flags=cb.FLAG_PROFILE).load(g)
+    out = {"mode": "top-compare", "num_chars": g.stats()["num_chars"], "shapes": []}
+    for R, n, seed, lm in ((1, 4, 31_000, 1000), (8, 32, 31_001, 2000), (16, 64, 31_004, 2000),
+                           (32, 96, 31_005, 2000), (64, 160, 31_006, 2000), (128, 256, 31_002, 2000)):
+        reads = make_reads(g, n, seed, len_max=lm)
+        rec, ref = {"slots": R, "reads": n}, None
+        for K in (23000, 12000, 8000, 5000, 3000):
+            lay = g.check_layout(R, 16, K)
+            ctx.align_scores_batched(reads, slots=R, steps_per_graph=16, top_vertices=K)
+            best = None
+            for _ in range(3):
+                sc = ctx.align_scores_batched(reads, slots=R, steps_per_graph=16, top_vertices=K)
+                p = ctx.profile()
+                t = p["total_ms"] / max(1, p["steps"])
+                best = t if best is None else min(best, t)
+            ref = sc if ref is None else ref
+            e = {"first_level": lay["top_first_level"], "top_vertices": lay["top_vertices"],
+                 "us_per_row_step": best * 1e3, "same_scores": bool(np.array_equal(sc, ref))}
+            if R in (1, 8, 128):
+                pctx.align_scores_batched(reads[:max(2, R)], slots=R, steps_per_graph=16, top_vertices=K)
+                pr = pctx.profile()
+                st = max(1, pr["row_launches"])
+                e["split_us"] = {k.replace("_ms", ""): 1e3 * pr[k] / st for k in
+                                 ("row_ms", "sweep_up_ms", "top_ms", "sweep_down_ms", "other_ms")}
+            rec[str(K)] = e
+        out["shapes"].append(rec)
+    pctx.close()
+    ctx.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_launch_compare(args):
     """Device time of the same reads through the CUDA-graph chain of
     row-step kernels (with and without programmatic dependent launch between
@@ -935,6 +980,8 @@ def main():
         return run_traceback_cfg1(args)
     if args.launch_compare:
         return run_launch_compare(args)
+    if args.top_compare:
+        return run_top_compare(args)
     if args.cfg5:
         return run_cfg5(args)
     ws, rank, local = dist_env()

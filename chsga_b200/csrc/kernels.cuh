@@ -1404,7 +1404,10 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
   }
 }
 
-__global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_delta(
+#ifndef CHSGA_DELTA_BLOCKS
+#define CHSGA_DELTA_BLOCKS CHSGA_STREAM_BLOCKS  // blocks per SM the register budget is sized for
+#endif
+__global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_DELTA_BLOCKS) k_row_delta(
     GraphPtrs g, const uint16_t* __restrict__ D, uint16_t* __restrict__ T, uint16_t* __restrict__ BV,
     const uint16_t* __restrict__ FL, const uint32_t* __restrict__ slot_word,
     unsigned long long* __restrict__ best, StepCtl* __restrict__ ctl) {
