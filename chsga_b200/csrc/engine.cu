@@ -97,6 +97,7 @@ struct GraphDev {
   DevArr<uint4> dn_head, up_head, fin;
   DevArr<uint4> t1_desc, t1_vrec;  // tiles of the one-read row kernel (k_row_t1)
   DevArr<uint8_t> t1_heads;
+  DevArr<uint32_t> delta_order;    // k_row_delta: runs of 32 string vertices by decreasing char count
 };
 
 struct TopDev {
@@ -178,6 +179,8 @@ struct chsga_ctx {
   // upward levels in the form bounded by the level's largest edge list
   // (CHSGA_PULL_LEAN=0 runs the unbounded form everywhere)
   bool pull_lean = true;
+  // resident blocks of k_row_delta on this device (0 until the first 128-slot buffers)
+  uint32_t delta_grid = 0;
   chsga::DevArr<unsigned char> reads;
   chsga::DevArr<chsga::dev::ReadDesc> queue;
   uint32_t qmask = 0xFFFFFFFFu;                      // queue ring mask (serving), else linear
@@ -257,6 +260,12 @@ SlotBufs& get_bufs(chsga_ctx& c, bool need_rows) {
       CK(cudaFuncSetAttribute(dev::k_row_delta, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)dev::delta_smem_bytes()));
     });
+    if (!c.delta_grid) {
+      int per_sm = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_row_delta, dev::kStreamWarps * 32,
+                                                       dev::delta_smem_bytes()));
+      c.delta_grid = (uint32_t)std::max(per_sm, 1) * (uint32_t)c.num_sms;
+    }
   }
   if constexpr (std::is_same_v<ST, uint16_t> && R >= 64) {
     once_per_device((const void*)dev::k_row_stream<R, true>, c.device, [] {
@@ -509,10 +518,13 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
     // uses this kernel, so the rows stay in its format from the first
     // admission on
     if (L.max_len <= 512 && (c.row_kernel == RowKernel::Delta || c.row_kernel == RowKernel::Auto)) {
-      const uint64_t runs = ((uint64_t)L.S + 31) / 32;
+      const uint32_t runs = (L.S + 31) / 32;
       constexpr unsigned tpb = dev::kStreamWarps * 32;
-      chain_launch(c, dev::k_row_delta, nblocks(runs * 32, tpb), tpb, dev::delta_smem_bytes(), s, c.g->gp, D, T,
-                   BVc, FL, b.word.p, b.best.p, b.ctl.p);
+      // at most the resident blocks: every warp after its first run takes the next from the list
+      const uint32_t all = (uint32_t)nblocks((uint64_t)runs * 32, tpb);
+      const uint32_t grid = c.delta_grid ? std::min(all, c.delta_grid) : all;
+      chain_launch(c, dev::k_row_delta, grid, tpb, dev::delta_smem_bytes(), s, c.g->gp, D, T, BVc, FL, b.word.p,
+                   b.best.p, b.ctl.p, (const uint32_t*)c.g->gd.delta_order.p, runs);
       done = true;
     }
   }
@@ -837,6 +849,19 @@ void upload_graph(chsga_ctx& c, const chsga_graph_host& g) {
   d.dn_head.upload(to4(L.dn_head), s);
   d.up_head.upload(to4(L.up_head), s);
   d.fin.upload(to4(L.fin), s);
+  {
+    // runs of 32 consecutive string vertices, longest (in chars) first; ties by index
+    const uint32_t nruns = (L.S + 31) / 32;
+    std::vector<uint32_t> order(nruns);
+    std::vector<uint32_t> len(nruns);
+    for (uint32_t r = 0; r < nruns; ++r) {
+      order[r] = r;
+      len[r] = L.sv_off[std::min<uint64_t>((uint64_t)32 * r + 32, L.S)] - L.sv_off[(uint64_t)32 * r];
+    }
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return len[a] > len[b]; });
+    d.delta_order.upload(order, s);
+    CK(cudaStreamSynchronize(s));  // the host vectors die with this scope
+  }
   auto top = make_top(L, d, kTopDefaultVertices, s);
   {
     HostT1 t1 = build_t1(L);

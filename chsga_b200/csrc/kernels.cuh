@@ -158,7 +158,7 @@ struct StepCtl {        // device-resident control block
   uint32_t done;        // reads finished
   uint32_t steps;       // row-steps with work
   uint32_t error;       // nonzero: a bounded device-side wait gave up
-  uint32_t pad;
+  uint32_t run_next;    // k_row_delta: runs handed out after each warp's first (k_advance resets it)
 };
 
 template <int R>
@@ -1142,7 +1142,8 @@ __device__ __forceinline__ void delta_expand(uint32_t b, uint32_t& e0, uint32_t&
 }
 
 template <bool COH>
-__device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index, const uint32_t* DZ,
+__device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index, const RunHead& rh,
+                                          const uint32_t* DZ,
                                           const uint16_t* DH, uint32_t* TZ, uint16_t* TH, uint16_t* BV,
                                           const uint16_t* FL, const uint32_t* slot_word, uint32_t* warp_ring,
                                           const uint2* lut, unsigned long long* sm_best, bool ending_any,
@@ -1175,19 +1176,10 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
     imask[p] |= ~amask[p];
   }
   any_fix = __any_sync(FULL, any_fix);
+  const bool any_init = __any_sync(FULL, (imask[0] | imask[1]) != 0);
   const bool track = ending_any && __any_sync(FULL, any_end);
   const uint32_t nv = min(32u, g.S - s0);
-  uint32_t mf = 0, me = 0, md = 0, mk0 = 0, mk1 = 0;
-  if ((uint32_t)lane < nv) {
-    const uint32_t s = s0 + lane;
-    mf = __ldg(g.sv_off + s);
-    me = __ldg(g.sv_off + s + 1);
-    md = CHSGA_CHK(__ldg(g.sv_dev + s), g.S, 3);
-    mk0 = __ldg(g.vin_off + s);
-    mk1 = __ldg(g.vin_off + s + 1);
-    CHSGA_CHK_CHARS(mf, me, g.N, 1);
-    CHSGA_CHK_RANGE(mk0, mk1, g.n_vin, 4);
-  }
+  const uint32_t mf = rh.mf, me = rh.me, md = rh.md, mk0 = rh.mk0, mk1 = rh.mk1;
   const uint32_t cb = __shfl_sync(FULL, mf, 0), ce = __shfl_sync(FULL, me, nv - 1);
   // previous-row Z words of the run's char groups q0 .. q1, W in flight
   const uint32_t q0 = cb >> 2, q1 = (ce - 1) >> 2;
@@ -1277,9 +1269,10 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
   DV cur, nxt;
   prefetch(0, cur);
   zin = take_word();  // the run's first group
-  auto run = [&](auto track_tag, auto fix_tag) {
+  auto run = [&](auto track_tag, auto fix_tag, auto init_tag) {
     constexpr bool TRACK = decltype(track_tag)::value;
-    constexpr bool FIX = decltype(fix_tag)::value;  // some slot of the warp applies a deferred closure
+    constexpr bool FIX = decltype(fix_tag)::value;    // some slot of the warp applies a deferred closure
+    constexpr bool INIT = decltype(init_tag)::value;  // some slot of the warp is on row 0 (or idle)
     for (uint32_t i = 0; i < nv; ++i) {
       if (i + 1 < nv) prefetch(i + 1, nxt);
       const uint32_t f = cur.f, len = cur.len;
@@ -1306,7 +1299,8 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
           for (int p = 0; p < P; ++p) t.h[p] = __viaddmin_u16x2(du.h[p], delta[p], t.h[p]);
         }
 #pragma unroll
-        for (int p = 0; p < P; ++p) t.h[p] = sel(delta[p], t.h[p], imask[p]);
+        for (int p = 0; p < P; ++p)
+          if (INIT) t.h[p] = sel(delta[p], t.h[p], imask[p]);
       }
       stp<P>(TH + (size_t)(s0 + i) * R + so, t);
       stp<P>(BV + (size_t)(2 * cur.d) * R + so, t);
@@ -1332,7 +1326,7 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
           if (FIX) dq.h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq.h[p]), dq.h[p], fmask[p]);
           uint32_t x = __viaddmin_u16x2(t.h[p], ONES, dq.h[p] + ONES);
           x = __viaddmin_u16x2(dprev.h[p], delta, x);
-          t.h[p] = sel(delta, x, imask[p]);
+          t.h[p] = INIT ? sel(delta, x, imask[p]) : x;
         }
         dprev = dq;
         // T[c] - T[c-1] + 1 per slot, 2 bits each
@@ -1375,16 +1369,22 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
       cur = nxt;
     }
   };
+  auto with_init = [&](auto track_tag, auto fix_tag) {
+    if (any_init)
+      run(track_tag, fix_tag, std::true_type{});
+    else
+      run(track_tag, fix_tag, std::false_type{});
+  };
   if (track) {
     if (any_fix)
-      run(std::true_type{}, std::true_type{});
+      with_init(std::true_type{}, std::true_type{});
     else
-      run(std::true_type{}, std::false_type{});
+      with_init(std::true_type{}, std::false_type{});
   } else {
     if (any_fix)
-      run(std::false_type{}, std::true_type{});
+      with_init(std::false_type{}, std::true_type{});
     else
-      run(std::false_type{}, std::false_type{});
+      with_init(std::false_type{}, std::false_type{});
   }
   // the run's last group when it ends inside a group
   if (((ce - 1) & 3u) != 3u) {
@@ -1407,10 +1407,22 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
 #ifndef CHSGA_DELTA_BLOCKS
 #define CHSGA_DELTA_BLOCKS CHSGA_STREAM_BLOCKS  // blocks per SM the register budget is sized for
 #endif
+// Runs are taken longest first: run_order lists the run indices by
+// decreasing char count (built on the host). Warp w of the grid takes entry
+// w, then entries from the launch's counter (StepCtl::run_next, reset by
+// k_advance) until the list is done, so the last runs to finish are the
+// short ones. The grid is at most the resident blocks.
 __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_DELTA_BLOCKS) k_row_delta(
     GraphPtrs g, const uint16_t* __restrict__ D, uint16_t* __restrict__ T, uint16_t* __restrict__ BV,
     const uint16_t* __restrict__ FL, const uint32_t* __restrict__ slot_word,
-    unsigned long long* __restrict__ best, StepCtl* __restrict__ ctl) {
+    unsigned long long* __restrict__ best, StepCtl* __restrict__ ctl, const uint32_t* __restrict__ run_order,
+    uint32_t nruns) {
+  constexpr unsigned FULL = 0xFFFFFFFFu;
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  uint32_t k = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+  uint32_t run = k < nruns ? CHSGA_CHK(__ldg(run_order + k), nruns, 7) : 0u;
+  RunHead rh{0, 0, 0, 0, 0};
+  if (k < nruns) rh = run_head(g, run);
   pdl_wait();
   extern __shared__ __align__(16) uint32_t dring_smem[];
   __shared__ unsigned long long sm_best[128];
@@ -1428,15 +1440,22 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_DELTA_BLOCKS) k_row_d
     s_lut[v] = make_uint2(e0 - 0x00010001u, e1 - 0x00010001u);
   }
   __syncthreads();
-  const uint32_t run = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
   const size_t hoff = delta_h_offset(g.N);
-  if (run * 32 < g.S)
-    delta_run<false>(g, run, reinterpret_cast<const uint32_t*>(D),
+  while (k < nruns) {
+    delta_run<false>(g, run, rh, reinterpret_cast<const uint32_t*>(D),
                      reinterpret_cast<const uint16_t*>(reinterpret_cast<const unsigned char*>(D) + hoff),
                      reinterpret_cast<uint32_t*>(T),
                      reinterpret_cast<uint16_t*>(reinterpret_cast<unsigned char*>(T) + hoff), BV, FL, slot_word,
                      dring_smem + (size_t)(threadIdx.x >> 5) * kDeltaRing * 32, s_lut, sm_best, ending_any,
                      ctl);
+    uint32_t nk = 0;
+    if ((threadIdx.x & 31) == 0) nk = nwarps + atomicAdd(&ctl->run_next, 1u);
+    k = __shfl_sync(FULL, nk, 0);
+    if (k < nruns) {
+      run = CHSGA_CHK(__ldg(run_order + k), nruns, 7);
+      rh = run_head(g, run);
+    }
+  }
   if (ending_any) flush_min<128>(sm_best, best);
 }
 
@@ -2893,6 +2912,7 @@ __device__ __forceinline__ void advance_body(SlotState* slots, const ReadDesc* q
   if (r == 0) {
     ctl->any_active = s_active;
     ctl->any_ending = s_ending;
+    ctl->run_next = 0;
     if (s_active) ctl->steps += 1;
   }
 }
