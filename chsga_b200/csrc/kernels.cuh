@@ -1146,24 +1146,28 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
                                           const uint32_t* DZ,
                                           const uint16_t* DH, uint32_t* TZ, uint16_t* TH, uint16_t* BV,
                                           const uint16_t* FL, const uint32_t* slot_word, uint32_t* warp_ring,
-                                          const uint2* lut, unsigned long long* sm_best, bool ending_any,
-                                          StepCtl* ctl) {
+                                          const uint2* lut, const uint2* dtl, unsigned long long* sm_best,
+                                          bool ending_any, StepCtl* ctl) {
   constexpr int R = 128, P = 2, W = kDeltaRing;
+  // a first score that no closure candidate F + (c - first) can beat: above
+  // every score (at most 65001) and, plus a vertex offset (at most 511), still
+  // below 2^16
+  constexpr uint32_t NO_CLOSURE = 0xFDFFFDFFu;
   constexpr uint32_t ONES = 0x00010001u;
   constexpr unsigned FULL = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const uint32_t s0 = run_index * 32;
   const size_t so = (size_t)lane * 4;
   uint32_t* ring = warp_ring + lane;  // word k of this lane at ring[k * 32]
-  uint32_t dtab[P], imask[P], fmask[P], amask[P];
+  // (the mismatch increments of every key come from the block's table dtl)
+  uint32_t imask[P], fmask[P], amask[P];
   bool any_fix = false, any_end = false;
 #pragma unroll
   for (int p = 0; p < P; ++p) {
-    dtab[p] = imask[p] = fmask[p] = amask[p] = 0;
+    imask[p] = fmask[p] = amask[p] = 0;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const uint32_t w = COH ? slot_word[so + 2 * p + h] : __ldg(slot_word + so + 2 * p + h);
-      dtab[p] |= ((w >> SW_MASK_SHIFT) & SW_MASK) << (16 * h);
       if (w & SW_INIT) imask[p] |= 0xFFFFu << (16 * h);
       if (w & SW_FIX) fmask[p] |= 0xFFFFu << (16 * h);
       if (w & SW_ACTIVE) amask[p] |= 0xFFFFu << (16 * h);
@@ -1276,16 +1280,19 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
     for (uint32_t i = 0; i < nv; ++i) {
       if (i + 1 < nv) prefetch(i + 1, nxt);
       const uint32_t f = cur.f, len = cur.len;
-      const U2<P> F = cur.F;
+      // slots without the deferred closure take NO_CLOSURE, so it never wins
+      U2<P> F;
+#pragma unroll
+      for (int p = 0; p < P; ++p) F.h[p] = sel(cur.F.h[p], NO_CLOSURE, fmask[p]);
       U2<P> t, draw = cur.H, dprev = cur.H;
       // first char: its byte of the group is unused
       {
         const uint32_t key = kw.next();
-        uint32_t delta[P];
+        const uint2 dl = dtl[key * 32];  // the char's mismatch increments, both pairs
+        const uint32_t delta[P] = {dl.x, dl.y};
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-          delta[p] = (dtab[p] >> key) & ONES;
-          if (FIX) dprev.h[p] = sel(__vminu2(dprev.h[p], F.h[p]), dprev.h[p], fmask[p]);
+          if (FIX) dprev.h[p] = __vminu2(dprev.h[p], F.h[p]);
           t.h[p] = dprev.h[p] + ONES;
         }
 #pragma unroll
@@ -1320,10 +1327,11 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
         U2<P> dq = draw;
         off2 += ONES;
         const U2<P> tp = t;
+        const uint2 dl = dtl[key * 32];
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-          const uint32_t delta = (dtab[p] >> key) & ONES;
-          if (FIX) dq.h[p] = sel(__viaddmin_u16x2(F.h[p], off2, dq.h[p]), dq.h[p], fmask[p]);
+          const uint32_t delta = p == 0 ? dl.x : dl.y;
+          if (FIX) dq.h[p] = __viaddmin_u16x2(F.h[p], off2, dq.h[p]);
           uint32_t x = __viaddmin_u16x2(t.h[p], ONES, dq.h[p] + ONES);
           x = __viaddmin_u16x2(dprev.h[p], delta, x);
           t.h[p] = INIT ? sel(delta, x, imask[p]) : x;
@@ -1439,6 +1447,20 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_DELTA_BLOCKS) k_row_d
     delta_expand((uint32_t)v, e0, e1);
     s_lut[v] = make_uint2(e0 - 0x00010001u, e1 - 0x00010001u);
   }
+  // label key -> mismatch increments of lane L's two slot pairs (slots 4L ..
+  // 4L + 3, 1 in a half where the slot's read base mismatches the key)
+  __shared__ uint2 s_dtab[16 * 32];
+  for (int i = threadIdx.x; i < 16 * 32; i += blockDim.x) {
+    const uint32_t key = (uint32_t)i >> 5, L = (uint32_t)i & 31u;
+    uint32_t v[2];
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const uint32_t m0 = (__ldg(slot_word + 4 * L + 2 * p) >> SW_MASK_SHIFT) & SW_MASK;
+      const uint32_t m1 = (__ldg(slot_word + 4 * L + 2 * p + 1) >> SW_MASK_SHIFT) & SW_MASK;
+      v[p] = ((m0 >> key) & 1u) | (((m1 >> key) & 1u) << 16);
+    }
+    s_dtab[i] = make_uint2(v[0], v[1]);
+  }
   __syncthreads();
   const size_t hoff = delta_h_offset(g.N);
   while (k < nruns) {
@@ -1446,8 +1468,8 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_DELTA_BLOCKS) k_row_d
                      reinterpret_cast<const uint16_t*>(reinterpret_cast<const unsigned char*>(D) + hoff),
                      reinterpret_cast<uint32_t*>(T),
                      reinterpret_cast<uint16_t*>(reinterpret_cast<unsigned char*>(T) + hoff), BV, FL, slot_word,
-                     dring_smem + (size_t)(threadIdx.x >> 5) * kDeltaRing * 32, s_lut, sm_best, ending_any,
-                     ctl);
+                     dring_smem + (size_t)(threadIdx.x >> 5) * kDeltaRing * 32, s_lut, s_dtab + (threadIdx.x & 31),
+                     sm_best, ending_any, ctl);
     uint32_t nk = 0;
     if ((threadIdx.x & 31) == 0) nk = nwarps + atomicAdd(&ctl->run_next, 1u);
     k = __shfl_sync(FULL, nk, 0);
