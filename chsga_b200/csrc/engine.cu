@@ -505,6 +505,7 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   if (ev) CK(cudaEventRecord(ev->e[0], s));
   ST* FL = reinterpret_cast<ST*>(b.FL.p);
   bool done = false;
+  bool delta_rows = false;  // the delta row kernel reads first scores from BV, so FL holds last scores only
   if constexpr (std::is_same_v<ST, uint16_t> && R == 1) {
     // one read: a warp per tile of whole vertices, a lane per 8 chars
     if (c.g->t1.ntiles && c.row_kernel == RowKernel::Auto) {
@@ -526,6 +527,7 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
       chain_launch(c, dev::k_row_delta, grid, tpb, dev::delta_smem_bytes(), s, c.g->gp, D, T, BVc, FL, b.word.p,
                    b.best.p, b.ctl.p, (const uint32_t*)c.g->gd.delta_order.p, runs);
       done = true;
+      delta_rows = true;
     }
   }
   if constexpr (std::is_same_v<ST, uint16_t> && R >= 2) {
@@ -587,10 +589,14 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
   }
   if (ev) CK(cudaEventRecord(ev->e[3], s));
   auto down = [&](uint32_t lo, uint32_t mid, uint32_t hi) {
-    if constexpr (std::is_same_v<ST, uint16_t> && DEFER && R >= 8)
-      chain_launch(c, dev::k_down16<R>, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, c.g->gp, BVc, FL, lo,
-                   mid, hi, b.word.p, b.best.p, b.ctl.p);
-    else
+    if constexpr (std::is_same_v<ST, uint16_t> && DEFER && R >= 8) {
+      auto k = dev::k_down16<R, true>;
+      if constexpr (R == 128) {
+        if (delta_rows) k = dev::k_down16<R, false>;
+      }
+      chain_launch(c, k, nblocks((uint64_t)(hi - lo) * (R / 8)), 256, 0, s, c.g->gp, BVc, FL, lo, mid, hi,
+                   b.word.p, b.best.p, b.ctl.p);
+    } else
       chain_launch(c, dev::k_down<R, !DEFER, ST>, nblocks((uint64_t)(hi - lo) * G), 256, 0, s, c.g->gp, BVc, T,
                    FL, lo, mid, hi, b.word.p, b.best.p, b.ctl.p);
   };

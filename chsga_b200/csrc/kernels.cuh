@@ -1224,7 +1224,9 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
 #pragma unroll
     for (int p = 0; p < P; ++p) v.F.h[p] = v.u[0].h[p] = v.u[1].h[p] = 0;
     v.H = ldp_src<P, COH>(DH + (size_t)(s0 + i) * R + so);
-    if (any_fix) v.F = ldp_src<P, COH>(FL + (size_t)(2 * (s0 + i)) * R + so);
+    // the vertex's final first score of the previous row: BV[2d], which this
+    // warp alone overwrites, later, with the new row's raw first score
+    if (any_fix) v.F = ldp_src<P, true>(BV + (size_t)(2 * v.d) * R + so);
 #pragma unroll
     for (int j = 0; j < 2; ++j)
       if (v.k0 + j < v.k1) v.u[j] = ldp_src<P, COH>(FL + (size_t)(2 * src_at(v.k0 + j) + 1) * R + so);
@@ -2513,7 +2515,7 @@ __global__ void __launch_bounds__(256) k_down(GraphPtrs g, ST* __restrict__ BV, 
 // final first and last scores into FL and the first scores of slots on
 // their last row into the per-slot minimum.
 // ---------------------------------------------------------------------------
-template <int R, bool COH>
+template <int R, bool COH, bool WF = true>
 __device__ __forceinline__ void down16_item(const GraphPtrs& g, uint16_t* BV, uint16_t* FL, uint32_t d,
                                             int lane, const DownHead& hd, const uint32_t* slot_word,
                                             unsigned long long* sm_best, bool ending_any) {
@@ -2559,7 +2561,9 @@ __device__ __forceinline__ void down16_item(const GraphPtrs& g, uint16_t* BV, ui
     lf.z = __vminu2(raw.z, __vaddus2(f.z, ww));
     lf.w = __vminu2(raw.w, __vaddus2(f.w, ww));
   }
-  *reinterpret_cast<uint4*>(FL + (size_t)(2 * sv) * R + so) = f;
+  // WF = false (the delta rows read a vertex's final first score from BV[2d],
+  // where it also is): only the last score goes to FL
+  if (WF) *reinterpret_cast<uint4*>(FL + (size_t)(2 * sv) * R + so) = f;
   *reinterpret_cast<uint4*>(FL + (size_t)(2 * sv + 1) * R + so) = lf;
   if (ending_any) {
     const uint32_t fw[4] = {f.x, f.y, f.z, f.w};
@@ -2572,7 +2576,7 @@ __device__ __forceinline__ void down16_item(const GraphPtrs& g, uint16_t* BV, ui
   }
 }
 
-template <int R>
+template <int R, bool WF = true>
 __global__ void __launch_bounds__(256) k_down16(GraphPtrs g, uint16_t* __restrict__ BV,
                                                 uint16_t* __restrict__ FL, uint32_t lo,
                                                 uint32_t mid, uint32_t hi,
@@ -2592,7 +2596,7 @@ __global__ void __launch_bounds__(256) k_down16(GraphPtrs g, uint16_t* __restric
     for (int r = threadIdx.x; r < R; r += blockDim.x) sm_best[r] = ~0ull;
     __syncthreads();
   }
-  if (d < hi) down16_item<R, false>(g, BV, FL, d, (int)(gt % G), hd, slot_word, sm_best, ending_any);
+  if (d < hi) down16_item<R, false, WF>(g, BV, FL, d, (int)(gt % G), hd, slot_word, sm_best, ending_any);
   if (ending_any) flush_min<R>(sm_best, best);
 }
 
