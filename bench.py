@@ -191,21 +191,22 @@ def algorithmic_delta_row_bytes(st, slots, multi):
             + 3 * N / 8 + 12 * S + 4 * e_first)
 
 
-def algorithmic_sweep_bytes(st, lay, slots, score_bytes):
+def algorithmic_sweep_bytes(st, lay, slots, score_bytes, fl_first=True):
     """Bytes per row-step of the grid-wide sweep kernels below the top
     region (16-byte pull-list heads and vertex words, w bytes per score):
     up (k_pull_lv, k_pull_lv16): per target its head, first score read and written, one
     gathered score per edge, 8 bytes per edge after the first;
     down (k_down, k_down16): per position its vertex words, first and raw last score
-    read, final first and last written to FL; per target below the top its
-    head, first score written, one gathered score per edge, 8 bytes per edge
-    after the first."""
+    read, final first (unless fl_first is false: with delta rows the row
+    kernel reads it from BV) and last written to FL; per target below the
+    top its head, first score written, one gathered score per edge, 8 bytes
+    per edge after the first."""
     S = st["num_strings"]
     wr = score_bytes * slots
     ut, ue = lay["sweep_up_targets"], lay["sweep_up_edges"]
     dt, de = lay["sweep_down_targets"], lay["sweep_down_edges"]
     up = ut * (16 + 2 * wr) + ue * wr + (ue - ut) * 8
-    down = S * (16 + 4 * wr) + dt * (16 + wr) + de * wr + (de - dt) * 8
+    down = S * (16 + (4 if fl_first else 3) * wr) + dt * (16 + wr) + de * wr + (de - dt) * 8
     return up, down
 
 
@@ -950,7 +951,7 @@ def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits):
                                                                  "other_ms")) / max(1, qs["row_launches"])}
     # sweep kernels below the top region (the top region the run used)
     lay = g.check_layout(R, pr["row_bits"], opts["top_vertices"] if R > 1 else 0)
-    up_b, down_b = algorithmic_sweep_bytes(st, lay, R, w)
+    up_b, down_b = algorithmic_sweep_bytes(st, lay, R, w, fl_first=kname != "k_row_delta")
     up_s = pr["sweep_up_ms"] / max(1, pr["row_launches"]) / 1e3
     down_s = pr["sweep_down_ms"] / max(1, pr["row_launches"]) / 1e3
     # 16-bit rows with R >= 8 run the packed forms of both sweeps
