@@ -196,17 +196,18 @@ def algorithmic_sweep_bytes(st, lay, slots, score_bytes, fl_first=True):
     region (16-byte pull-list heads and vertex words, w bytes per score):
     up (k_pull_lv, k_pull_lv16): per target its head, first score read and written, one
     gathered score per edge, 8 bytes per edge after the first;
-    down (k_down, k_down16): per position its vertex words, first and raw last score
-    read, final first (unless fl_first is false: with delta rows the row
-    kernel reads it from BV) and last written to FL; per target below the
-    top its head, first score written, one gathered score per edge, 8 bytes
-    per edge after the first."""
+    down (k_down, k_down16): per position its vertex words, first score read,
+    raw last score read (vertices of two or more chars), final first (unless
+    fl_first is false: with delta rows the row kernel reads it from BV) and
+    last written to FL; per target below the top its head, first score
+    written, one gathered score per edge, 8 bytes per edge after the first."""
     S = st["num_strings"]
     wr = score_bytes * slots
     ut, ue = lay["sweep_up_targets"], lay["sweep_up_edges"]
     dt, de = lay["sweep_down_targets"], lay["sweep_down_edges"]
     up = ut * (16 + 2 * wr) + ue * wr + (ue - ut) * 8
-    down = S * (16 + (4 if fl_first else 3) * wr) + dt * (16 + wr) + de * wr + (de - dt) * 8
+    down = (S * (16 + (4 if fl_first else 3) * wr) - st["single_char_strings"] * wr + dt * (16 + wr) + de * wr
+            + (de - dt) * 8)
     return up, down
 
 

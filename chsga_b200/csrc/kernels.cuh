@@ -2391,7 +2391,8 @@ __device__ __forceinline__ void down_item(const GraphPtrs& g, ST* BV, ST* T, ST*
     }
 #endif
     IV<V> f = ld<V>(p);
-    const IV<V> raw = ld<V>(BV + (size_t)(2 * d + 1) * R + so);
+    IV<V> raw{};
+    if (m.y > 1) raw = ld<V>(BV + (size_t)(2 * d + 1) * R + so);
     if (h.y > h.x) {
       bool changed = false;
       auto relax = [&](const IV<V>& x, int w) {
@@ -2528,7 +2529,9 @@ __device__ __forceinline__ void down16_item(const GraphPtrs& g, uint16_t* BV, ui
   h.z = CHSGA_CHK(h.z, 2 * (uint64_t)g.S, 14);
   m.z = CHSGA_CHK(m.z, g.S, 15);
   const uint4 f0 = *p;
-  const uint4 raw = *reinterpret_cast<const uint4*>(BV + (size_t)(2 * d + 1) * R + so);
+  // the raw last score only matters for a vertex of two or more chars
+  const uint4 raw = m.y > 1 ? *reinterpret_cast<const uint4*>(BV + (size_t)(2 * d + 1) * R + so)
+                            : make_uint4(0, 0, 0, 0);
   uint4 f = f0;
   auto relax = [&](const uint4& x, uint32_t w) {
     const uint32_t ww = min(w, 0xFFFFu) * 0x10001u;
