@@ -654,8 +654,9 @@ def run_launch_compare(args):
             runs.append(("graphs_pull_coop", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16,
                                                   ctx=ctx_coop)))
         if R == 128:
-            runs.append(("graphs_delta_rows", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16,
-                                                   row_kernel=cb.ROW_DELTA)))
+            # AUTO runs delta rows here; the 16-bit stream rows for comparison
+            runs.append(("graphs_stream_rows", dict(use_graphs=cb.LAUNCH_GRAPHS, steps_per_graph=16,
+                                                    row_kernel=cb.ROW_STREAM)))
         rec = {"slots": R, "reads": len(reads), "bases": sum(len(r) for r in reads)}
         ref = None
         for name, kw in runs:
