@@ -889,7 +889,7 @@ def ctypes_labels(g):
     return ctypes.string_at(v.labels, v.num_chars)
 
 
-def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits):
+def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits, clk_mhz=None):
     """A profiled pass (CUDA events around every kernel group of every
     row-step) with R slots; the row kernel's achieved bandwidth against the
     algorithmic bytes of one launch, and the sweep kernels' per row-step.
@@ -938,7 +938,21 @@ def profiled_roofline(cb, g, st, multi, device, R, opts, peak, src, row_bits):
     if kname == "k_row_delta":
         # delta rows move about a quarter of the 16-bit rows' bytes and are bound by
         # instruction issue; the 16-bit stream kernel on the same reads, for context
-        out["limiter"] = "instruction issue (2-bit rows: a quarter of the 16-bit rows' bytes)"
+        out["limiter"] = "instruction issue (2-bit rows: a third of the 16-bit rows' bytes)"
+        # the issue roofline: warp-instructions per char from the ncu capture
+        # (profiles/k_row_delta_traffic.json) x chars per launch / launch time,
+        # against one warp-instruction per cycle per scheduler (4 per SM) at
+        # the SM clock sampled during the timed steps
+        if tr and tr.get("warp_inst_per_char"):
+            import torch
+            sm_count = torch.cuda.get_device_properties(device).multi_processor_count
+            inst = tr["warp_inst_per_char"] * st["num_chars"]
+            mhz = clk_mhz or 1965.0
+            ipeak = 4 * sm_count * mhz * 1e6
+            out["issue"] = {"warp_inst_per_launch": inst, "warp_inst_per_char": tr["warp_inst_per_char"],
+                            "achieved_warp_inst_per_s": inst / row_avg_s, "peak_warp_inst_per_s": ipeak,
+                            "frac": inst / row_avg_s / ipeak,
+                            "peak_source": f"4 schedulers x {sm_count} SMs x {mhz:.0f} MHz"}
         q = cb.Context(device, flags=cb.FLAG_PROFILE)
         q.load(g)
         q.align_scores_batched(sample, **dict(opts, slots=R, row_kernel=cb.ROW_STREAM), row_bits=16)
@@ -1126,7 +1140,8 @@ def main():
     if rank == 0 and not args.no_profile and not args.kernels_only:
         peak, src = measured_peak()
         R = opts["slots"]
-        line["roofline"] = profiled_roofline(cb, g, st, multi, local, R, opts, peak, src, 0)
+        line["roofline"] = profiled_roofline(cb, g, st, multi, local, R, opts, peak, src, 0,
+                                             clk_mhz=(line.get("clocks") or {}).get("sm_mhz"))
         line["roofline_plain"] = profiled_roofline(cb, g, st, multi, local, 1, opts, peak, src, 0)
         line["roofline_int32_rows"] = profiled_roofline(cb, g, st, multi, local, R, opts, peak, src, 32)
         cb_info, picked, ref_scores = cpu_baseline(g, batches[0], args.cpu_sample_s)
