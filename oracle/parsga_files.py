@@ -35,11 +35,16 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PARSGA_BIN = os.path.join(HERE, "_ref", "ParSGA")
+PARSGA_TB_BIN = os.path.join(HERE, "_ref", "ParSGA_traceback")
 BASES = "TCGAN"  # src/config.hpp:8-9, ALPHABET_SIZE 5
 
 
 def available() -> bool:
     return os.path.exists(PARSGA_BIN)
+
+
+def traceback_available() -> bool:
+    return os.path.exists(PARSGA_TB_BIN)
 
 
 def _components(n: int, src: np.ndarray, dst: np.ndarray) -> np.ndarray:
@@ -151,3 +156,47 @@ def run(prefix: str, reads: Sequence[bytes], threads: int, workdir: str) -> np.n
             raise RuntimeError("ParSGA printed no score line:\n" + res.stdout[-2000:] + res.stderr[-2000:])
         out.extend(int(x) for x in m.group(1).split())
     return np.array(out, dtype=np.int32)
+
+
+_TB_READ = re.compile(r'^read\[(\d+)\] = "([^"]*)"\n'
+                      r'\s+CIGAR\s+: (\S*)\n'
+                      r'\s+path_score\s+: (-?\d+)\s+parallel_ref : (-?\d+)\s+score_ok : (\w+)\n'
+                      r'\s+last_row\s+: (-?\d+)\s+expected : (-?\d+)\s+row_ok : (\w+)', re.M)
+
+
+def run_traceback(prefix: str, reads: Sequence[bytes], threads: int, workdir: str, k: int = 500) -> List[dict]:
+    """Tracebacks from the reference's ParSGA traceback driver
+    (par_csr_align_reads_with_traceback, src/csr_traceback.hpp:825-1072,
+    checkpoints every k rows under workdir) with `threads` OpenMP threads,
+    five reads per run (src/load_reads.hpp:5). Per read: the CIGAR, the
+    path's score, the forward pass's score (parallel_align_CSR) and the
+    driver's own checks that the two agree and that the path ends on the
+    read's last row (src/ParSGA_traceback.cpp:172-209). The driver exits 1
+    when a check fails; its lines are returned either way."""
+    out = []
+    for k0 in range(0, len(reads), 5):
+        fa = os.path.join(workdir, f"parsga_tb_reads_{k0}.fa")
+        with open(fa, "wb") as f:
+            for i, r in enumerate(reads[k0:k0 + 5]):
+                f.write(b">r%d\n%s\n" % (i, r))
+        res = subprocess.run([PARSGA_TB_BIN, "-k", str(k), "-d", os.path.join(workdir, "parsga_tb_ckpt"),
+                              prefix, os.path.join(workdir, "parsga_tb_out"), fa, str(threads)],
+                             capture_output=True, text=True,
+                             env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+        if res.returncode not in (0, 1):
+            raise RuntimeError(f"ParSGA_traceback exited {res.returncode}:\n" + res.stdout[-2000:]
+                               + res.stderr[-2000:])
+        got = [{"read": m.group(2).encode(), "cigar": m.group(3), "path_score": int(m.group(4)),
+                "forward_score": int(m.group(5)), "score_ok": m.group(6) == "YES",
+                "last_row": int(m.group(7)), "row_ok": m.group(9) == "YES"}
+               for m in _TB_READ.finditer(res.stdout)]
+        if len(got) != len(reads[k0:k0 + 5]):
+            raise RuntimeError("ParSGA_traceback printed no traceback for some reads:\n" + res.stdout[-2000:])
+        out.extend(got)
+    return out
+
+
+def cigar_read_length(cigar: str) -> int:
+    """Read chars a CIGAR of the ParSGA traceback consumes: M and D ops take
+    one read row each, I ops none (src/ParSGA_traceback.cpp:178-191)."""
+    return sum(int(n) for n, op in re.findall(r"(\d+)([MDI])", cigar) if op in "MD")

@@ -1,7 +1,8 @@
 """ParSGA as a second comparison method (src/ParSGA.cpp, parallel_align_CSR
-in src/ParSGAoverrides/csr_align.hpp:527-618), on graphs of single-char
-vertices, where ConSGA's sweep quirk cannot arise and every method computes
-the exact DP.
+in src/ParSGAoverrides/csr_align.hpp:527-618, and src/ParSGA_traceback.cpp,
+par_csr_align_reads_with_traceback in src/csr_traceback.hpp:825-1072), on
+graphs of single-char vertices, where ConSGA's sweep quirk cannot arise and
+every method computes the exact DP.
 
 The reference's ParSGA driver is compiled unchanged in oracle/_ref; its
 per-base match-cut graphs, component orders and thread offsets are written
@@ -60,3 +61,58 @@ def test_parsga_equals_serial_exact_dp_and_oracle(tmp_path, seed):
     for T in (1, 2, 4):
         got = pf.run(prefix, reads, T, str(tmp_path))
         np.testing.assert_array_equal(got, want, err_msg=f"{T} threads")
+
+
+@pytest.mark.skipif(not pf.traceback_available(), reason="the reference's ParSGA traceback driver is not built")
+@pytest.mark.parametrize("seed,k", [(44, 500), (45, 16)])
+def test_parsga_traceback_paths_score_the_optimum(tmp_path, seed, k):
+    """The reference's ParSGA traceback (par_csr_align_reads_with_traceback,
+    src/csr_traceback.hpp:825-1072, checkpointed every k rows; k = 16 makes
+    every read of 40+ bases recompute several segments): every path's score
+    equals the ConSGA oracle's optimum, the driver's own checks pass (path
+    score = its forward pass, path ends on the read's last row), and the
+    CIGAR consumes every read base."""
+    g, files = gen_graph(tmp_path, f"t{seed}", backbone_len=1200, seed=seed, vlen_min=1, vlen_max=1,
+                         bubble_gap_mean=6.0, p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=2, alt_max=20)
+    labels = open(files[3], "rb").read().replace(b"\n", b"")
+    off, tgt = _char_csr(files)
+    prefix = str(tmp_path / f"tb{seed}")
+    pf.write_inputs(prefix, labels, off, tgt, threads=(2,))
+    reads = g.gen_reads(10, seed, 40, 120, sub_rate=0.05, indel_rate=0.04, n_rate=0.02).to_list()
+    want = orc.Oracle(files).scores(reads)
+    got = pf.run_traceback(prefix, reads, 2, str(tmp_path), k=k)
+    assert [r["read"] for r in got] == reads
+    np.testing.assert_array_equal([r["path_score"] for r in got], want)
+    np.testing.assert_array_equal([r["forward_score"] for r in got], want)
+    assert all(r["score_ok"] and r["row_ok"] for r in got)
+    assert [pf.cigar_read_length(r["cigar"]) for r in got] == [len(r) for r in reads]
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not pf.traceback_available(), reason="the reference's ParSGA traceback driver is not built")
+def test_gpu_traceback_matches_parsga_traceback_scores(tmp_path):
+    """The GPU traceback (one read, checkpointed every 16 rows, and batched)
+    on a single-char graph: every path scores what the reference's ParSGA
+    traceback's path scores, and ends on the read's last row. The two walks
+    break ties differently (ConSGA's and ParSGA's op orders), so the paths
+    themselves may differ."""
+    import chsga_b200 as cb
+    g, files = gen_graph(tmp_path, "tg", backbone_len=1200, seed=46, vlen_min=1, vlen_max=1,
+                         bubble_gap_mean=6.0, p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=2, alt_max=20)
+    labels_raw = open(files[3], "rb").read().replace(b"\n", b"")
+    off, tgt = _char_csr(files)
+    prefix = str(tmp_path / "tbg")
+    pf.write_inputs(prefix, labels_raw, off, tgt, threads=(2,))
+    reads = g.gen_reads(10, 46, 40, 120, sub_rate=0.05, indel_rate=0.04, n_rate=0.02).to_list()
+    par = pf.run_traceback(prefix, reads, 2, str(tmp_path), k=16)
+    want = [r["path_score"] for r in par]
+    labels = labels_raw
+    ctx = cb.Context(0).load(g)
+    try:
+        for rd, w in zip(reads, want):
+            ops, score, _ = ctx.align_traceback(rd, k=16)
+            assert score == w and orc.rescore(ops, rd, labels) == (w, len(rd) - 1)
+        for rd, w, (ops, score, _) in zip(reads, want, ctx.align_traceback_batched(reads, slots=8)):
+            assert score == w and orc.rescore(ops, rd, labels) == (w, len(rd) - 1)
+    finally:
+        ctx.close()
