@@ -1176,7 +1176,11 @@ __device__ __forceinline__ void delta_run(const GraphPtrs& g, uint32_t run_index
     any_fix |= fmask[p] != 0;
     // an idle slot computes a row-0 row of a read that matches everywhere
     // (its mismatch mask is empty): all 0, so every slot's scores stay in
-    // 0..65535 and the pair arithmetic below never carries between halves
+    // 0..65535 and the pair arithmetic below never carries between halves.
+    // The rows a slot on row 0 reads are the ones its previous read (or the
+    // row-0 path) left, also in range; only the first step of a call reads
+    // rows no step of the call wrote, and there every slot is on row 0 or
+    // idle, so both halves of every pair are replaced by their row-0 values
     imask[p] |= ~amask[p];
   }
   any_fix = __any_sync(FULL, any_fix);
