@@ -568,8 +568,9 @@ void row_step(chsga_ctx& c, SlotBufs& b, const ST* D, ST* T, cudaStream_t s,
     if (L.lvl_up_edges[l] == 0) continue;
     const uint32_t lo = L.lvl_off[l], hi = L.lvl_off[l + 1];
     if constexpr (std::is_same_v<ST, uint16_t> && R >= 8) {
-      // the two-edge form where no target of the level has more
-      auto k = c.pull_lean && L.lvl_up_maxdeg[l] <= 2 ? dev::k_pull_lv16<R, 2> : dev::k_pull_lv16<R, 0>;
+      // the two- or four-edge form where no target of the level has more
+      const uint32_t md = c.pull_lean ? L.lvl_up_maxdeg[l] : ~0u;
+      auto k = md <= 2 ? dev::k_pull_lv16<R, 2> : md <= 4 ? dev::k_pull_lv16<R, 4> : dev::k_pull_lv16<R, 0>;
       if constexpr (R >= 64) {
         if (c.pull_coop) k = dev::k_pull_lv16c<R>;
       }

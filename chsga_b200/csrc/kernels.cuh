@@ -2186,13 +2186,15 @@ __global__ void __launch_bounds__(256) k_pull_lv(ST* __restrict__ BV, uint32_t l
 // MAXE = 2: every target of the level has at most the head's two edges (the
 // host knows each level's largest list), so the form has no edge loop and
 // needs about half the registers (26 against 48 at 128 slots): eight blocks
-// per SM instead of five. MAXE = 0: any number of edges.
+// per SM instead of five. MAXE = 4: at most the head's two and the two
+// prefetched after them, every gather at once, no loop (38 registers, six
+// blocks per SM). MAXE = 0: any number of edges.
 template <int R, bool COH, int MAXE = 0, int NE = kPullHeadEdges>
 __device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lane, const PullHeadT<NE>& hd,
                                                const int2* __restrict__ edges) {
   static_assert(R >= 8 && R % 8 == 0, "8 slots per lane");
-  static_assert(MAXE == 0 || MAXE == 2, "edge bound");
-  static_assert(MAXE == 2 || NE == kPullHeadEdges, "the prefetched edges");
+  static_assert(MAXE == 0 || MAXE == 2 || MAXE == 4, "edge bound");
+  static_assert(MAXE == 2 || NE >= MAXE - 2, "the prefetched edges");
   constexpr int B = kPullHeadEdges;
   uint4 h = hd.h, h2 = hd.h2;
   if (h.x == h.y) return;
@@ -2217,6 +2219,19 @@ __device__ __forceinline__ void pull_lv16_item(uint16_t* BV, uint32_t d, int lan
   if constexpr (MAXE == 2) {
     relax(x0, h.w);
     if (two) relax(x1, h2.y);
+    if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
+    return;
+  }
+  if constexpr (MAXE == 4) {
+    // the head's two edges and the two prefetched after them, gathered at once
+    const bool three = h.y - h.x > 2, four = h.y - h.x > 3;
+    uint4 x2 = x0, x3 = x0;
+    if (three) x2 = src(CHSGA_CHK((uint32_t)hd.e[0].x, 2 * (uint64_t)d, 12));
+    if (four) x3 = src(CHSGA_CHK((uint32_t)hd.e[1].x, 2 * (uint64_t)d, 12));
+    relax(x0, h.w);
+    if (two) relax(x1, h2.y);
+    if (three) relax(x2, (uint32_t)hd.e[0].y);
+    if (four) relax(x3, (uint32_t)hd.e[1].y);
     if (f.x != f0.x || f.y != f0.y || f.z != f0.z || f.w != f0.w) *p = f;
     return;
   }
@@ -2249,7 +2264,7 @@ __global__ void __launch_bounds__(256) k_pull_lv16(uint16_t* __restrict__ BV, ui
                                                    const int2* __restrict__ edges, uint32_t n_edges,
                                                    const StepCtl* __restrict__ ctl) {
   constexpr int G = R / 8;
-  constexpr int NE = MAXE == 2 ? 0 : kPullHeadEdges;
+  constexpr int NE = MAXE == 2 ? 0 : MAXE == 4 ? 2 : kPullHeadEdges;
   const uint64_t gt = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t d = lo + (uint32_t)(gt / G);
   PullHeadT<NE> hd{};
@@ -2738,11 +2753,16 @@ __device__ __forceinline__ bool top_body(ST* BV, const TopPtrs& t, StepCtl* ctl,
       }
     } else if (ok && threadIdx.x < 32) {
       // warp chunk: a run of small levels in rounds of 32 edges, each level
-      // whole rounds, the rounds ordered by the warp barrier
-      for (int i = threadIdx.x; i < -n; i += 32) {
-        const int2 x = e[i];
+      // whole rounds, the rounds ordered by the warp barrier. The buffer is
+      // complete and unchanging while the chunk runs, so a round's edge is
+      // loaded before the barrier that ends the round before it
+      const int m = -n;  // a multiple of 32: every lane runs every round
+      int2 x = (int)threadIdx.x < m ? e[threadIdx.x] : make_int2(0, 0);
+      for (int i = threadIdx.x; i < m; i += 32) {
+        const int2 xn = i + 32 < m ? e[i + 32] : x;
         atomicMin(&sm[2 * CHSGA_CHK(x.x >> 16, t.K + 1, 17)], sm[CHSGA_CHK(x.x & 0xFFFF, 2 * t.K + 2, 18)] + x.y);
         __syncwarp();
+        x = xn;
       }
     }
     __syncthreads();
