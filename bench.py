@@ -1096,9 +1096,12 @@ def main():
         "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "row_storage": "uint16 rows with u16x2 DPX arithmetic: int32 results exactly, since every "
-                       "row-i value is at most i + 1 (reads of at most 65000 bases; longer reads "
-                       "run int32 rows)",
+        "row_storage": (("2-bit delta rows (per char and slot, T[c] - T[c-1] + 1 in 0..2 within a "
+                         "vertex) plus the raw first score of every vertex in 16 bits, u16x2 DPX "
+                         "arithmetic" if opts["slots"] == 128 and opts["row_kernel"] in (0, 5) else
+                         "uint16 rows with u16x2 DPX arithmetic")
+                        + ": int32 results exactly, since every row-i value is at most i + 1 (reads "
+                          "of at most 65000 bases; longer reads run int32 rows)"),
         "config": {"workload": WORKLOAD, "num_chars": N, "num_strings": st["num_strings"],
                    "hierarchy_levels": st["pch_levels"], "batch_reads": args.batch,
                    "engine": opts, "parallelism": f"replicas x{ws}",
