@@ -281,8 +281,10 @@ typedef struct {
  * DELTA (128 slots, score-only) = STREAM over rows stored
  * as the raw first score of every vertex (16 bits per slot) and, per char,
  * the difference to the char before in 2 bits per slot (consecutive chars of
- * a vertex differ by at most 1 in every row): 0.26 bytes per cell instead of
- * 2, bound by instruction issue rather than memory.
+ * a vertex differ by at most 1 in every row): about 0.4 bytes per cell (0.25
+ * for the differences, the rest for the first scores, 11.6 chars per vertex
+ * on the config-2 graph) instead of 2, bound by instruction issue rather than
+ * memory.
  * DIRECT = one thread group per string vertex, 16- or 32-bit rows;
  * TILED = shared-memory tiles of consecutive string vertices staged by TMA
  * bulk copies (slots >= 32); DPX = two 16-bit scores per register on the
