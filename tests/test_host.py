@@ -288,3 +288,17 @@ def test_packed_u16_relaxation_is_exact():
     raw, ln = x, rng.integers(1, 1 << 29, f.size)
     np.testing.assert_array_equal(np.minimum(raw, sat(f + np.minimum(ln - 1, 65535))),
                                   np.minimum(raw, f + ln - 1))
+
+
+def test_default_top_region_is_the_8000_vertex_region():
+    """top_vertices = 0 selects the 8000-vertex region (the levels from the
+    highest down while they fit), and larger caps take lower levels."""
+    g = cb.HostGraph.generate(**dict(cb.GRAPH_CONFIGS["cfg2"], backbone_len=200_000, seed=5))
+    g.build_pch()
+    d, k8 = g.check_layout(128, 16, 0), g.check_layout(128, 16, 8000)
+    assert (d["top_first_level"], d["top_vertices"]) == (k8["top_first_level"], k8["top_vertices"])
+    assert 0 < d["top_vertices"] <= 8000
+    big = g.check_layout(128, 16, 23000)
+    assert big["top_first_level"] <= d["top_first_level"] and big["top_vertices"] >= d["top_vertices"]
+    with pytest.raises(cb.ChsgaError):
+        g.check_layout(128, 16, 23001)
