@@ -1119,7 +1119,10 @@ __global__ void __launch_bounds__(kStreamWarps * 32, CHSGA_STREAM_BLOCKS) k_row_
 // call fails instead of returning a wrong score.
 // ---------------------------------------------------------------------------
 constexpr uint32_t ERR_ROW_DELTA = 8;
-constexpr int kDeltaRing = 16;  // Z words in flight per lane (64 chars)
+#ifndef CHSGA_DELTA_RING
+#define CHSGA_DELTA_RING 16  // Z words in flight per lane (4 chars each; build-time tuning)
+#endif
+constexpr int kDeltaRing = CHSGA_DELTA_RING;
 
 __host__ __device__ constexpr size_t delta_z_bytes(size_t N) { return ((N + 3) / 4 + 1) * 32 * 4; }
 __host__ __device__ constexpr size_t delta_h_offset(size_t N) { return (delta_z_bytes(N) + 255) / 256 * 256; }
