@@ -109,3 +109,17 @@ def pch_digest(a):
         h.update(k.encode())
         h.update(v.tobytes() if hasattr(v, "tobytes") else str(v).encode())
     return h.hexdigest()
+
+
+def edge_reads(g, seed):
+    """Reads at the edges of the input domain: one base, a lone N, all N,
+    longer than any path of the graph (insertions), a homopolymer, lower
+    case and bytes outside the alphabet (compared byte for byte, so they
+    mismatch every label), a NUL byte, and the empty read (scored as row 0
+    against '\\0', i.e. 1)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    n = g.stats()["num_chars"]
+    long_read = bytes(rng.choice(np.frombuffer(b"ACGT", np.uint8), 3 * n).astype(np.uint8))
+    return [b"A", b"N", b"ACGT", b"N" * 40, long_read, b"T" * 200, b"acgtXYZ-ACGT", b"\x00ACGT", b""]
+

@@ -18,7 +18,7 @@ import pytest
 
 import chsga_b200 as cb
 import oracle as orc
-from conftest import gen_graph
+from conftest import edge_reads, gen_graph
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 needs_ref = pytest.mark.skipif(not orc.ref_available(), reason="oracle/_ref not built")
@@ -188,3 +188,14 @@ def test_rows_change_by_at_most_one_within_a_vertex(tmp_path, seed, vmax, gap):
         diff = np.diff(rows, axis=1)
         chain = ~heads[1:]  # char c (c >= 1) continues the vertex of c - 1
         assert np.abs(diff[:, chain]).max() <= 1
+
+
+@needs_ref
+def test_edge_reads_match_reference_code(tmp_path):
+    g, files = gen_graph(tmp_path, "edge", backbone_len=600, seed=71, vlen_max=8, bubble_gap_mean=10.0,
+                         p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=3, alt_max=30)
+    reads = edge_reads(g, 71)
+    o, r = orc.Oracle(files), orc.RefHarness(files)
+    want = r.scores(reads)
+    np.testing.assert_array_equal(o.scores(reads), want)
+    assert want[-1] == 1 and want[3] == 40  # empty read, 40 N (every base costs one)
