@@ -199,3 +199,18 @@ def test_edge_reads_match_reference_code(tmp_path):
     want = r.scores(reads)
     np.testing.assert_array_equal(o.scores(reads), want)
     assert want[-1] == 1 and want[3] == 40  # empty read, 40 N (every base costs one)
+
+
+@needs_ref
+def test_edge_reads_match_reference_code_matchn(tmp_path):
+    """The edge-case reads under matchN scoring ('N' in a read or label
+    matches every base): the matchN restatement equals the reference's
+    ALPHABET_SIZE=4 build; a read of N costs nothing there."""
+    from conftest import sprinkle_n
+    g, files = gen_graph(tmp_path, "edgen", backbone_len=600, seed=72, vlen_max=8, bubble_gap_mean=10.0,
+                         p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=3, alt_max=30)
+    g = sprinkle_n(files, 0.03, 72)  # N in the labels too
+    reads = edge_reads(g, 72)
+    want = orc.RefHarness(files, match_n=True).scores(reads)
+    np.testing.assert_array_equal(orc.Oracle(files, match_n=True).scores(reads), want)
+    assert want[1] == 0 and want[3] == 0  # a lone N and 40 N match anywhere
