@@ -214,3 +214,23 @@ def test_edge_reads_match_reference_code_matchn(tmp_path):
     want = orc.RefHarness(files, match_n=True).scores(reads)
     np.testing.assert_array_equal(orc.Oracle(files, match_n=True).scores(reads), want)
     assert want[1] == 0 and want[3] == 0  # a lone N and 40 N match anywhere
+
+
+@needs_ref
+def test_checkpoint_rows_of_edge_reads_byte_identical_to_reference(tmp_path):
+    """Checkpoint files of edge-case reads (all N; longer than any path; odd
+    bytes) from the reference's checkpointed traceback and from the oracle's
+    are byte-identical, and both paths have the same score."""
+    g, files = gen_graph(tmp_path, "ke", backbone_len=600, seed=73, vlen_max=8, bubble_gap_mean=10.0,
+                         p_snp=0.5, p_indel=0.3, p_alt=0.2, alt_min=3, alt_max=30)
+    reads = [r for r in edge_reads(g, 73) if len(r) >= 12]
+    labels = open(files[3], "rb").read().replace(b"\n", b"")
+    for i, rd in enumerate(reads):
+        a, b = tmp_path / f"ref{i}", tmp_path / f"orc{i}"
+        ref_ops = orc.RefHarness(files, True).traceback(rd, k=11, ckpt_dir=str(a), cleanup=False)
+        _, so, ck = orc.Oracle(files).traceback(rd, k=11, fast_cap_bytes=0, ckpt_dir=str(b), cleanup=False)
+        assert ck and orc.rescore(ref_ops, rd, labels) == (so, len(rd) - 1)
+        names = sorted(os.listdir(a))
+        assert names == sorted(os.listdir(b)) and len(names) == (len(rd) - 1) // 11 + 1
+        for n in names:
+            assert (a / n).read_bytes() == (b / n).read_bytes(), (i, n)
