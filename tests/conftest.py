@@ -123,3 +123,23 @@ def edge_reads(g, seed):
     long_read = bytes(rng.choice(np.frombuffer(b"ACGT", np.uint8), 3 * n).astype(np.uint8))
     return [b"A", b"N", b"ACGT", b"N" * 40, long_read, b"T" * 200, b"acgtXYZ-ACGT", b"\x00ACGT", b""]
 
+
+
+TINY_GFA = {
+    "one_segment": "H\tVN:Z:1.0\nS\t1\tACGTTGCA\n",
+    "one_char": "H\tVN:Z:1.0\nS\t1\tA\n",
+    "bubble": ("H\tVN:Z:1.0\nS\t1\tACG\nS\t2\tT\nS\t3\tC\nS\t4\tGGA\n"
+               "L\t1\t+\t2\t+\t0M\nL\t1\t+\t3\t+\t0M\nL\t2\t+\t4\t+\t0M\nL\t3\t+\t4\t+\t0M\n"),
+}
+TINY_READS = [b"A", b"ACGT", b"TTTT", b"ACGTTGCAACGT", b"N" * 5, b""]
+
+
+def tiny_graph(tmpdir, name):
+    """A GFA graph of one segment, one base, or a four-segment bubble (both
+    orientations), its hierarchy and files."""
+    p = os.path.join(str(tmpdir), name + ".gfa")
+    with open(p, "w") as f:
+        f.write(TINY_GFA[name])
+    g = cb.HostGraph.from_gfa(p)
+    g.build_pch()
+    return g, g.write_files(os.path.join(str(tmpdir), name))

@@ -74,3 +74,28 @@ def test_gpu_checkpoints_of_edge_reads_equal_the_oracles(tmp_path):
                 assert (a / nm).read_bytes() == (b / nm).read_bytes(), (i, nm)
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("name", ["one_segment", "one_char", "bubble"])
+def test_gpu_paths_on_tiny_graphs(tmp_path, name):
+    """Graphs of two to eight string vertices (conftest.TINY_GFA): a single
+    run of vertices, a hierarchy of one or two levels all in the top region.
+    Plain, batched at 8 and 128 slots, and the traceback of every non-empty
+    read equal the oracle (which equals the reference's code on these graphs,
+    tests/test_oracle.py)."""
+    from conftest import TINY_READS, tiny_graph
+    g, files = tiny_graph(tmp_path, name)
+    want = orc.Oracle(files).scores(TINY_READS)
+    labels = open(files[3], "rb").read().replace(b"\n", b"")
+    ctx = cb.Context(0).load(g)
+    try:
+        np.testing.assert_array_equal(ctx.align_scores(TINY_READS), want)
+        for slots in (8, 128):
+            np.testing.assert_array_equal(ctx.align_scores_batched(TINY_READS, slots=slots), want,
+                                          err_msg=f"{slots} slots")
+        for rd, w in zip(TINY_READS, want):
+            if rd:
+                ops, score, _ = ctx.align_traceback(rd)
+                assert score == w and orc.rescore(ops, rd, labels) == (w, len(rd) - 1)
+    finally:
+        ctx.close()

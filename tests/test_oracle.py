@@ -234,3 +234,17 @@ def test_checkpoint_rows_of_edge_reads_byte_identical_to_reference(tmp_path):
         assert names == sorted(os.listdir(b)) and len(names) == (len(rd) - 1) // 11 + 1
         for n in names:
             assert (a / n).read_bytes() == (b / n).read_bytes(), (i, n)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["one_segment", "one_char", "bubble"])
+def test_tiny_graphs_match_reference_code(tmp_path, name):
+    """Graphs of two to eight string vertices (a single GFA segment, a single
+    base, a bubble; both orientations): the oracle equals the reference's
+    code on scores and every row."""
+    from conftest import TINY_READS, tiny_graph
+    g, files = tiny_graph(tmp_path, name)
+    o, r = orc.Oracle(files), orc.RefHarness(files)
+    np.testing.assert_array_equal(o.scores(TINY_READS), r.scores(TINY_READS))
+    for rd in TINY_READS[:4]:
+        np.testing.assert_array_equal(o.rows(rd), r.rows(rd, o.num_chars))
